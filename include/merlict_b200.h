@@ -1,0 +1,284 @@
+/*
+ * merlict_b200.h -- C ABI of the B200 photon-propagation engine.
+ *
+ * The engine replaces merlict's per-photon propagation loop and the
+ * arrival binning that follows it:
+ *
+ *   merlict::propagate_photons_in_frame_with_config(
+ *       std::vector<Photon>*, const Frame*, const PropagationConfig*,
+ *       random::Generator*)                    merlict/Photons.h:12-16
+ *   merlict::propagate_photons_in_frame_with_config_multi_thread(...)
+ *                                 merlict_multi_thread/merlict_multi_thread.h:12-16
+ *   merlict::sensor::Sensors::assign_photons(const std::vector<Photon>*)
+ *                                              merlict/sensor/Sensors.h:35
+ *
+ * The caller first flattens its frame tree (merlict/Frame.h) into an
+ * mlgpu_flat_scene: nodes in depth-first preorder with escape indices,
+ * leaf surfaces with their 3x4 frame-to-world transforms and primitive
+ * parameters, and the piecewise-linear property tables (merlict/function/
+ * Func1.h).  The scene is uploaded once; photons are then traced in batches.
+ *
+ * No C++ types cross this boundary: plain pointers and sizes only.  Every
+ * entry point returns an int status (MLGPU_OK == 0).  On failure a message
+ * is kept per thread and can be read with mlgpu_last_error().
+ */
+#ifndef MERLICT_B200_H_
+#define MERLICT_B200_H_
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define MLGPU_ABI_VERSION 1
+
+/* ---- status codes ------------------------------------------------------ */
+enum {
+    MLGPU_OK = 0,
+    MLGPU_ERR_INVALID_ARGUMENT = 1, /* std::invalid_argument in the reference */
+    MLGPU_ERR_OUT_OF_RANGE = 2,     /* std::out_of_range, e.g. a wavelength
+                                       outside a Func1 table, Limits.cpp:37-46 */
+    MLGPU_ERR_RUNTIME = 3,          /* std::runtime_error */
+    MLGPU_ERR_CUDA = 4,             /* a CUDA runtime call failed */
+    MLGPU_ERR_NO_DEVICE = 5
+};
+
+/* ---- interactions, same numbering as merlict/RayForPropagation.h:14-28 -- */
+enum {
+    MLGPU_PRODUCTION = 0,
+    MLGPU_ABSORPTION_IN_VOID = 1,
+    MLGPU_ABSORPTION_IN_MEDIUM = 2,
+    MLGPU_ABSORPTION_ON_SURFACE = 3,
+    MLGPU_FRESNEL_REFLECTION_ON_SURFACE = 4,
+    MLGPU_REFLECTION_ON_SURFACE = 5,
+    MLGPU_REFRACTION_TO_OUTSIDE = 6,
+    MLGPU_REFRACTION_TO_INSIDE = 7
+};
+
+/* ---- leaf primitives (merlict/scenery/primitive/primitive.h:5-19) -------
+ * Parameters per leaf (leaf_params, 8 doubles, unused slots are 0):      */
+enum {
+    MLGPU_PRIM_NONE = 0,             /* frame or surface without geometry   */
+    MLGPU_PRIM_SPHERE_CAP_HEX = 1,   /* R, hex inner radius                 */
+    MLGPU_PRIM_SPHERE_CAP_CYL = 2,   /* R, bound radius^2                   */
+    MLGPU_PRIM_SPHERE_CAP_RECT = 3,  /* R, half x width, half y width       */
+    MLGPU_PRIM_ELLIPTIC_CAP_HEX = 4, /* A, B, C, 1/A^2, 1/B^2, 1/C^2, hex inner */
+    MLGPU_PRIM_DISC = 5,             /* radius^2                            */
+    MLGPU_PRIM_HEX_PLANE = 6,        /* hex inner radius                    */
+    MLGPU_PRIM_PLANE = 7,            /* half x width, half y width          */
+    MLGPU_PRIM_ANNULUS = 8,          /* outer radius^2, inner radius^2      */
+    MLGPU_PRIM_PLANE_DUAL_SPHERE = 9,/* circ1 x, circ1 y, circ2 x, circ2 y, circle radius */
+    MLGPU_PRIM_TRIANGLE = 10,        /* Ax, Ay, Bx, By, Cx, Cy              */
+    MLGPU_PRIM_CYLINDER = 11,        /* radius, length                      */
+    MLGPU_PRIM_SPHERE = 12,          /* radius                              */
+    MLGPU_PRIM_COUNT = 13
+};
+
+#define MLGPU_LEAF_PARAMS 8
+
+/* leaf_surface columns: six property-table ids, the node a refraction into
+ * the medium restricts traversal to (or -1), and flag bits.                */
+enum {
+    MLGPU_SURF_OUTER_REFLECTION = 0,
+    MLGPU_SURF_INNER_REFLECTION = 1,
+    MLGPU_SURF_OUTER_REFRACTION = 2,
+    MLGPU_SURF_INNER_REFRACTION = 3,
+    MLGPU_SURF_OUTER_ABSORPTION = 4,
+    MLGPU_SURF_INNER_ABSORPTION = 5,
+    MLGPU_SURF_ALLOWED_NODE = 6,
+    MLGPU_SURF_FLAGS = 7,
+    MLGPU_SURF_COLUMNS = 8
+};
+
+enum {
+    MLGPU_FLAG_TRANSPARENT = 1,            /* SurfaceEntity.cpp:67-74        */
+    MLGPU_FLAG_INNER_REFRACTION_DEFAULT = 2, /* inner_refraction is the default table */
+    MLGPU_FLAG_OUTER_REFRACTION_DEFAULT = 4  /* outer_refraction is the default table */
+};
+
+/* Special leaf ids in results and histories. */
+#define MLGPU_LEAF_VOID (-1)           /* no surface hit: VOID_SURFACE_ENTITY   */
+#define MLGPU_LEAF_PHOTON_SOURCE (-2)  /* only the production entry exists     */
+
+/* Flattened frame tree.  All pointers are host pointers. */
+typedef struct mlgpu_flat_scene {
+    /* Nodes: the frames of the tree in depth-first preorder, children in
+     * their stored order (merlict/RayAndFrame.cpp:137-149).  Node 0 is the
+     * tree root.  The subtree of node i is the index range
+     * [i, node_skip[i]).                                                  */
+    int32_t num_nodes;
+    const double* node_sphere;   /* [num_nodes][4]: world x, y, z, bounding radius */
+    const int32_t* node_skip;    /* [num_nodes]                                    */
+    const int32_t* node_leaf;    /* [num_nodes]: leaf index, -1 if the frame has children */
+
+    /* Leaves: frames without children. */
+    int32_t num_leaves;
+    const int32_t* leaf_node;        /* [num_leaves]                         */
+    const double* leaf_frame2world;  /* [num_leaves][12]: rows of the 3x4 T  */
+    const int32_t* leaf_primitive;   /* [num_leaves]                         */
+    const double* leaf_params;       /* [num_leaves][MLGPU_LEAF_PARAMS]      */
+    const int32_t* leaf_surface;     /* [num_leaves][MLGPU_SURF_COLUMNS]     */
+    const int32_t* leaf_sensor;      /* [num_leaves]: sensor index or -1     */
+
+    /* Property tables Func1: points (x, y, slope) sorted by x. */
+    int32_t num_functions;
+    const int32_t* function_offset;  /* [num_functions + 1] into the points  */
+    const double* function_points;   /* [total points][3]                    */
+    int32_t default_refraction;      /* id of the default refraction table   */
+
+    /* Unit vectors of the hexagonal bound (HexagonalPrismZ.h:11-17), as the
+     * host computed them, so that host and device agree bit for bit.      */
+    double hex_unit_u[3];
+    double hex_unit_v[3];
+    double hex_unit_w[3];
+
+    int32_t num_sensors;             /* sensor indices are 0 .. num_sensors-1 */
+} mlgpu_flat_scene;
+
+/* Photon batch: seven planes of one element type plus optional ids.
+ * Pointers are device pointers for mlgpu_propagate and host pointers for
+ * mlgpu_propagate_host.                                                   */
+enum { MLGPU_F64 = 0, MLGPU_F32 = 1 };
+
+typedef struct mlgpu_photons {
+    int32_t dtype;                    /* MLGPU_F64 or MLGPU_F32            */
+    const void* support_x;
+    const void* support_y;
+    const void* support_z;
+    const void* direction_x;
+    const void* direction_y;
+    const void* direction_z;
+    const void* wavelength;           /* metres                            */
+    const int32_t* simulation_truth_id; /* may be NULL                     */
+} mlgpu_photons;
+
+/* One entry of a photon's history (Intersection + Interaction,
+ * merlict/RayForPropagation.h:32-64). */
+typedef struct mlgpu_history_entry {
+    double position[3];   /* in the object frame of the surface            */
+    double normal[3];     /* surface normal in the object frame            */
+    double distance;      /* from the ray support to the intersection      */
+    int32_t leaf;         /* leaf index, MLGPU_LEAF_VOID or _PHOTON_SOURCE */
+    uint8_t interaction;
+    uint8_t from_outside_to_inside;
+    uint8_t pad[2];
+} mlgpu_history_entry;
+
+/* Per-photon results.  Any pointer may be NULL to skip that output, except
+ * `sensor`.  x, y (and time) are written as `dtype` (x, y) and double (time).
+ * info = interaction | num_interactions << 8 | uniforms used << 16
+ *        | error << 24.                                                   */
+typedef struct mlgpu_results {
+    int32_t dtype;            /* element type of x, y, theta_x, theta_y     */
+    int32_t* sensor;          /* sensor index of the final surface or -1    */
+    void* x;                  /* final intersection, object frame (Sensor.cpp:14-30) */
+    void* y;
+    double* time;             /* time of flight, Photon.cpp:44-56           */
+    void* theta_x;            /* -incident direction in the sensor frame    */
+    void* theta_y;
+    int32_t* final_leaf;
+    uint32_t* info;
+    double* final_position;   /* [n][3] world position of the final intersection */
+    double* final_direction;  /* [n][3] direction of the photon at the end  */
+    mlgpu_history_entry* history; /* [n][max_num_interactions_per_photon + 1] */
+} mlgpu_results;
+
+/* Random numbers.  PHILOX: Philox4x32-10 keyed by `seed`, photon i draws
+ * from the counter stream (photon_offset + i); the k-th uniform of a photon
+ * is (bits >> 11) * 2^-53 of the k-th block.  REPLAY: photon i consumes
+ * uniforms[i * stride + k], k < stride (an exhausted stream is an error). */
+enum { MLGPU_RNG_PHILOX = 0, MLGPU_RNG_REPLAY = 1 };
+
+typedef struct mlgpu_rng {
+    int32_t mode;
+    uint32_t stride;
+    uint64_t seed;
+    uint64_t photon_offset;
+    const double* uniforms;   /* device pointer (host for _host calls)    */
+} mlgpu_rng;
+
+/* Tracer forms. */
+enum {
+    MLGPU_TRACER_FP64 = 0,        /* plain FP64, replicates the reference bit for bit */
+    MLGPU_TRACER_FP32 = 1,        /* FP32 bulk math, FP64 where stability needs it   */
+    MLGPU_TRACER_FP32_PURE = 2    /* FP32 everywhere (precision study only)          */
+};
+
+/* PropagationConfig (merlict/PropagationConfig.h:10-13) plus engine knobs. */
+typedef struct mlgpu_settings {
+    uint32_t max_num_interactions_per_photon;
+    int32_t start_node;     /* node of the `world` frame passed by the caller */
+    int32_t tracer;         /* MLGPU_TRACER_*                                 */
+    int32_t block_size;     /* 0 = default                                    */
+} mlgpu_settings;
+
+typedef struct mlgpu_scene mlgpu_scene;
+
+/* ---- library -------------------------------------------------------- */
+int mlgpu_abi_version(void);
+int mlgpu_last_error(char* buffer, size_t buffer_size);
+
+/* ---- scene ---------------------------------------------------------- *
+ * Replaces the per-call frame-tree walk of CausalIntersection
+ * (merlict/RayAndFrame.cpp:126-173) by a device copy of the tree.
+ * Validates the flat scene (index ranges, sorted tables) and uploads it to
+ * the current CUDA device.                                              */
+int mlgpu_scene_create(const mlgpu_flat_scene* flat, mlgpu_scene** scene);
+int mlgpu_scene_destroy(mlgpu_scene* scene);
+
+/* ---- propagation ------------------------------------------------------ *
+ * Replaces propagate_photons_in_frame_with_config (merlict/Photons.cpp:9-22)
+ * and its thread-pool twin (merlict_multi_thread.cpp:28-55).
+ * Device pointers, asynchronous on `cuda_stream` (a cudaStream_t, NULL =
+ * default stream).  Errors found on the device (a wavelength outside a
+ * property table, an exhausted replay stream) are reported by
+ * mlgpu_scene_sync_errors().                                             */
+int mlgpu_propagate(
+    mlgpu_scene* scene,
+    const mlgpu_photons* photons,
+    uint64_t num_photons,
+    const mlgpu_settings* settings,
+    const mlgpu_rng* rng,
+    mlgpu_results* results,
+    void* cuda_stream);
+
+/* Waits for `cuda_stream` and returns the first device-side error raised
+ * since the previous call (then clears it).                             */
+int mlgpu_scene_sync_errors(mlgpu_scene* scene, void* cuda_stream);
+
+/* Same as mlgpu_propagate but with host pointers: copies the photons in,
+ * traces, copies the results out and synchronises.  This is the call the
+ * reference-side C++ shim makes.                                         */
+int mlgpu_propagate_host(
+    mlgpu_scene* scene,
+    const mlgpu_photons* photons,
+    uint64_t num_photons,
+    const mlgpu_settings* settings,
+    const mlgpu_rng* rng,
+    mlgpu_results* results);
+
+/* ---- arrival binning ------------------------------------------------- *
+ * Replaces Sensors::assign_photons (merlict/sensor/Sensors.cpp:79-81) for
+ * callers that want per-sensor statistics rather than arrival lists:
+ * counts[s] = photons whose final surface is sensor s; time_hist[s][b] =
+ * those arrivals with time in bin b of [t_min, t_max) (num_time_bins, may
+ * be 0).  Device pointers.  `counts` and `time_hist` are overwritten.     */
+int mlgpu_bin_arrivals(
+    mlgpu_scene* scene,
+    const int32_t* sensor,
+    const double* time,
+    uint64_t num_photons,
+    uint32_t* counts,
+    uint32_t* time_hist,
+    uint32_t num_time_bins,
+    double t_min,
+    double t_max,
+    void* cuda_stream);
+
+#ifdef __cplusplus
+}  /* extern "C" */
+#endif
+
+#endif  /* MERLICT_B200_H_ */

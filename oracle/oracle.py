@@ -1,0 +1,213 @@
+"""TEST INFRASTRUCTURE -- Python access to the checkers under oracle/.
+
+* `Oracle` wraps _build/libmerlict_oracle.so, the C restatement of merlict's
+  propagation (merlict_oracle.c), run on a FlatScene.
+* `RefScene` wraps _ref/libmerlict_ref_harness.so: a scene built with the
+  reference library's own classes and factories, flattened by the product's
+  shim, and propagated by the reference's own Propagator.
+
+Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg use
+this module; the product never imports it.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+from merlict_development_kit_b200 import abi
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ORACLE_SO = os.path.join(HERE, "_build", "libmerlict_oracle.so")
+HARNESS_SO = os.path.join(HERE, "_ref", "libmerlict_ref_harness.so")
+REFERENCE_DIR = os.environ.get("MERLICT_REFERENCE_DIR", "/root/reference")
+
+
+class OracleCounters(C.Structure):
+    _fields_ = [(k, C.c_uint64) for k in (
+        "nodes", "leaves", "caps", "cap_bounds", "planes", "others",
+        "reflections", "fresnels", "segments", "funcs", "steps")]
+
+    def as_dict(self) -> dict:
+        return {k: int(getattr(self, k)) for k, _ in self._fields_}
+
+
+def build(reference: bool = True) -> None:
+    """Builds the oracle, and the reference harness when the reference
+    sources are present."""
+    targets = ["oracle"]
+    if reference and os.path.isdir(REFERENCE_DIR):
+        targets.append("ref")
+    subprocess.run(["make", "-s", "-C", HERE, f"-j{os.cpu_count() or 4}",
+                    f"REF={REFERENCE_DIR}"] + targets, check=True)
+
+
+def harness_available() -> bool:
+    return os.path.exists(HARNESS_SO)
+
+
+def _photon_struct(ph: dict) -> tuple[abi.mlgpu_photons, list]:
+    keep = []
+    s = abi.mlgpu_photons()
+    s.dtype = abi.F64
+    for name in ("support_x", "support_y", "support_z", "direction_x",
+                 "direction_y", "direction_z", "wavelength"):
+        a = np.ascontiguousarray(ph[name], dtype=np.float64)
+        keep.append(a)
+        setattr(s, name, a.ctypes.data)
+    if ph.get("id") is not None:
+        a = np.ascontiguousarray(ph["id"], dtype=np.int32)
+        keep.append(a)
+        s.simulation_truth_id = a.ctypes.data
+    return s, keep
+
+
+def alloc_results(n: int, max_interactions: int, history: bool):
+    out = {
+        "sensor": np.zeros(n, np.int32),
+        "x": np.zeros(n), "y": np.zeros(n), "time": np.zeros(n),
+        "theta_x": np.zeros(n), "theta_y": np.zeros(n),
+        "final_leaf": np.zeros(n, np.int32), "info": np.zeros(n, np.uint32),
+        "final_position": np.zeros((n, 3)), "final_direction": np.zeros((n, 3)),
+    }
+    if history:
+        out["history"] = np.zeros((n, max_interactions + 1), abi.HISTORY_DTYPE)
+    r = abi.mlgpu_results()
+    r.dtype = abi.F64
+    for k, a in out.items():
+        setattr(r, k, a.ctypes.data)
+    return r, out
+
+
+class Oracle:
+    def __init__(self, path: str = ORACLE_SO):
+        if not os.path.exists(path):
+            build(reference=False)
+        self.lib = C.CDLL(path)
+        self.lib.oracle_propagate.restype = C.c_int
+        self.lib.oracle_propagate.argtypes = [
+            C.POINTER(abi.mlgpu_flat_scene), C.POINTER(abi.mlgpu_photons), C.c_uint64,
+            C.POINTER(abi.mlgpu_settings), C.POINTER(abi.mlgpu_rng),
+            C.POINTER(abi.mlgpu_results), C.POINTER(OracleCounters)]
+        self.lib.oracle_bin_arrivals.restype = None
+        assert self.lib.oracle_sizeof_history_entry() == 64
+
+    def propagate(self, scene: abi.FlatScene, photons: dict, max_interactions: int = 5,
+                  seed: int = 0, uniforms: np.ndarray | None = None,
+                  start_node: int = 0, history: bool = False,
+                  photon_offset: int = 0):
+        """Returns (status, results dict, counters dict)."""
+        n = len(photons["wavelength"])
+        ps, keep = _photon_struct(photons)
+        st = abi.mlgpu_settings(max_interactions, start_node, abi.TRACER_FP64, 0)
+        rng = abi.mlgpu_rng()
+        if uniforms is not None:
+            u = np.ascontiguousarray(uniforms, dtype=np.float64)
+            keep.append(u)
+            rng.mode = abi.RNG_REPLAY
+            rng.stride = u.shape[1]
+            rng.uniforms = u.ctypes.data
+        else:
+            rng.mode = abi.RNG_PHILOX
+            rng.seed = seed
+            rng.photon_offset = photon_offset
+        rs, out = alloc_results(n, max_interactions, history)
+        cnt = OracleCounters()
+        fs = scene.as_struct()
+        status = self.lib.oracle_propagate(C.byref(fs), C.byref(ps), n, C.byref(st),
+                                           C.byref(rng), C.byref(rs), C.byref(cnt))
+        return status, out, cnt.as_dict()
+
+    def bin_arrivals(self, sensor, time, num_sensors, num_bins=0, t_min=0.0, t_max=1.0):
+        sensor = np.ascontiguousarray(sensor, np.int32)
+        time = np.ascontiguousarray(time, np.float64)
+        counts = np.zeros(num_sensors, np.uint32)
+        hist = np.zeros((num_sensors, max(num_bins, 1)), np.uint32)
+        self.lib.oracle_bin_arrivals(
+            sensor.ctypes.data_as(C.c_void_p), time.ctypes.data_as(C.c_void_p),
+            C.c_uint64(len(sensor)), C.c_int32(num_sensors),
+            counts.ctypes.data_as(C.c_void_p),
+            hist.ctypes.data_as(C.c_void_p) if num_bins else None,
+            C.c_uint32(num_bins), C.c_double(t_min), C.c_double(t_max))
+        return counts, (hist if num_bins else None)
+
+
+_harness = None
+
+
+def harness():
+    global _harness
+    if _harness is None:
+        if not os.path.exists(HARNESS_SO):
+            raise RuntimeError("reference harness not built (oracle/Makefile target ref)")
+        lib = C.CDLL(HARNESS_SO)
+        lib.ref_scene_build.restype = C.c_void_p
+        lib.ref_scene_build.argtypes = [C.c_char_p, C.POINTER(C.c_double), C.c_int]
+        lib.ref_scene_free.argtypes = [C.c_void_p]
+        lib.ref_scene_flat.argtypes = [C.c_void_p, C.POINTER(abi.mlgpu_flat_scene)]
+        lib.ref_scene_num_sensors.argtypes = [C.c_void_p]
+        lib.ref_last_error.restype = C.c_char_p
+        lib.ref_propagate.restype = C.c_int
+        lib.ref_propagate.argtypes = [
+            C.c_void_p, C.POINTER(abi.mlgpu_photons), C.c_uint64, C.c_uint32,
+            C.c_int, C.c_uint64, C.c_void_p, C.c_uint32, C.c_int,
+            C.POINTER(abi.mlgpu_results), C.POINTER(C.c_double)]
+        _harness = lib
+    return _harness
+
+
+# propagation modes of ref_propagate
+REPLAY_PHILOX = 0
+REPLAY_UNIFORMS = 1
+REFERENCE_SINGLE_THREAD = 2
+REFERENCE_MULTI_THREAD = 3
+
+
+class RefScene:
+    """A scene built and propagated by the reference library."""
+
+    def __init__(self, kind: str, params=()):
+        self.lib = harness()
+        p = (C.c_double * max(len(params), 1))(*params)
+        self.h = self.lib.ref_scene_build(kind.encode(), p, len(params))
+        if not self.h:
+            raise RuntimeError(self.lib.ref_last_error().decode())
+        self.kind = kind
+        self.params = tuple(params)
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            self.lib.ref_scene_free(self.h)
+            self.h = None
+
+    def flat(self) -> abi.FlatScene:
+        s = abi.mlgpu_flat_scene()
+        if self.lib.ref_scene_flat(self.h, C.byref(s)) != 0:
+            raise RuntimeError(self.lib.ref_last_error().decode())
+        return abi.FlatScene.from_struct(s)
+
+    def propagate(self, photons: dict, max_interactions: int = 5,
+                  mode: int = REPLAY_PHILOX, seed: int = 0,
+                  uniforms: np.ndarray | None = None, threads: int = 1,
+                  history: bool = False, results: bool = True):
+        """Returns (status, results dict or None, seconds)."""
+        n = len(photons["wavelength"])
+        ps, keep = _photon_struct(photons)
+        up, stride = None, 0
+        if uniforms is not None:
+            u = np.ascontiguousarray(uniforms, dtype=np.float64)
+            keep.append(u)
+            up, stride = u.ctypes.data, u.shape[1]
+        out = None
+        rs_ptr = None
+        if results:
+            rs, out = alloc_results(n, max_interactions, history)
+            rs_ptr = C.byref(rs)
+        sec = C.c_double(0.0)
+        status = self.lib.ref_propagate(self.h, C.byref(ps), n, max_interactions, mode,
+                                        seed, up, stride, threads, rs_ptr, C.byref(sec))
+        if status != 0 and out is None:
+            raise RuntimeError(self.lib.ref_last_error().decode())
+        return status, out, sec.value

@@ -1,0 +1,604 @@
+// ref_harness.cpp -- TEST INFRASTRUCTURE, not product code.
+//
+// C entry points around the unmodified reference library (compiled from the
+// reference sources by oracle/Makefile) for the parity tests, the golden
+// fixture generator and the CPU baseline of the bench:
+//
+//  * ref_scene_build  builds a scene with the reference's own classes and
+//    factories (segmented_imaging_reflector::Factory, light_field_sensor::
+//    Factory, the test benches of merlict/tests/PhotonTest.cpp and
+//    BiConvexLensTest.cpp) and runs Frame::init_tree_based_on_mother_child_
+//    relations;
+//  * ref_scene_flat   flattens it with merlict_b200::flatten (the product's
+//    drop-in shim) into the layout of include/merlict_b200.h;
+//  * ref_propagate    runs merlict's Propagator on given photons, either
+//    photon by photon with a random::Generator that replays the engine's
+//    Philox stream (or an explicit uniform stream), exactly as
+//    merlict_multi_thread.cpp:12-26 drives it, or through the reference's
+//    own propagate_photons_in_frame_with_config[_multi_thread] with its
+//    Mt19937; then Sensors::assign_photons.  Per-photon results and
+//    histories are read back through merlict's public accessors.
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstring>
+#include <memory>
+#include <sstream>
+#include <stdexcept>
+#include <string>
+#include <thread>
+#include <vector>
+
+#include "merlict/merlict.h"
+#include "merlict/scenery/segmented_imaging_reflector/segmented_imaging_reflector.h"
+#include "merlict_multi_thread/merlict_multi_thread.h"
+#include "merlict_portal_plenoscope/light_field_sensor/LightFieldSensor.h"
+#include "merlict_b200.h"
+#include "merlict_b200_philox.h"
+#include "merlict_b200_shim.h"
+
+namespace ml = merlict;
+
+namespace {
+
+thread_local std::string last_error;
+
+struct Handle {
+    ml::Scenery scenery;
+    std::vector<ml::sensor::Sensor*> owned_sensors;
+    ml::sensor::Sensors sensors;
+    merlict_b200::FlatScene flat;
+    bool flattened = false;
+    std::vector<std::unique_ptr<ml::function::Func1>> functions;
+    const ml::function::Func1* fn(std::vector<std::vector<double>> xy) {
+        functions.emplace_back(new ml::function::Func1(xy));
+        return functions.back().get();
+    }
+    ~Handle() {
+        for (ml::sensor::Sensor* s : owned_sensors) delete s;
+    }
+};
+
+double param(const double* p, int n, int k, double fallback) {
+    return k < n ? p[k] : fallback;
+}
+
+// ---- test benches of merlict/tests/PhotonTest.cpp ------------------------
+
+void build_two_mirrors(Handle* h) {  // PhotonTest.cpp:27-82
+    ml::Frame* table = h->scenery.root.add<ml::Plane>();
+    table->set_name_pos_rot("optical_table", ml::VEC3_ORIGIN, ml::ROT3_UNITY);
+    const ml::function::Func1* refl = h->fn({{200e-9, 1}, {1200e-9, 1}});
+    ml::Plane* m1 = table->add<ml::Plane>();
+    m1->set_name_pos_rot("mirror_1", ml::VEC3_ORIGIN, ml::ROT3_UNITY);
+    m1->outer_reflection = refl; m1->inner_reflection = refl;
+    m1->set_x_y_width(1.0, 1.0);
+    ml::Plane* m2 = table->add<ml::Plane>();
+    m2->set_name_pos_rot("mirror_2", ml::Vec3(0.0, 0.0, 1.0), ml::ROT3_UNITY);
+    m2->outer_reflection = refl; m2->inner_reflection = refl;
+    m2->set_x_y_width(1.0, 1.0);
+}
+
+void build_mirror_absorber(Handle* h) {  // PhotonTest.cpp:84-175
+    ml::Frame* table = h->scenery.root.add<ml::Plane>();
+    table->set_name_pos_rot("optical_table", ml::VEC3_ORIGIN, ml::ROT3_UNITY);
+    const ml::function::Func1* refl = h->fn({{200e-9, 0.42}, {1200e-9, 0.42}});
+    ml::Plane* mirror = table->add<ml::Plane>();
+    mirror->set_name_pos_rot("mirror", ml::VEC3_ORIGIN,
+                             ml::Rot3(0, ml::deg2rad(90), ml::deg2rad(45)));
+    mirror->outer_reflection = refl; mirror->inner_reflection = refl;
+    mirror->set_x_y_width(1.0, 1.0);
+    ml::Plane* absorber = table->add<ml::Plane>();
+    absorber->set_name_pos_rot("absorber", ml::Vec3(0, 2, 0), ml::Rot3(ml::deg2rad(90), 0, 0));
+    absorber->set_x_y_width(1.0, 1.0);
+    h->owned_sensors.push_back(new ml::sensor::Sensor(0, absorber));
+}
+
+void build_water_box(Handle* h, bool absorbing) {  // PhotonTest.cpp:177-302
+    const ml::function::Func1* water = h->fn({{200e-9, 1.33}, {1200e-9, 1.33}});
+    ml::RectangularBox* box = h->scenery.root.add<ml::RectangularBox>();
+    box->set_name_pos_rot("box", ml::Vec3(0.0, 0.0, 1.0), ml::Rot3(0.0, 0.0, 0.0));
+    if (absorbing) box->inner_absorption = h->fn({{200e-9, 1.0}, {1200e-9, 1.0}});
+    box->inner_refraction = water;
+    box->set_xyz_width(1.0, 1.0, 1.0);
+    ml::Plane* absorber = h->scenery.root.add<ml::Plane>();
+    absorber->set_name_pos_rot("absorber", ml::Vec3(0.0, 0.0, 3.0), ml::ROT3_UNITY);
+    absorber->set_x_y_width(1.0, 1.0);
+    h->owned_sensors.push_back(new ml::sensor::Sensor(0, absorber));
+}
+
+void build_biconvex_lens(Handle* h) {  // BiConvexLensTest.cpp:8-82
+    ml::Frame* bench = h->scenery.root.add<ml::Frame>();
+    bench->set_name_pos_rot("BiConvexLens_test_world", ml::VEC3_ORIGIN, ml::ROT3_UNITY);
+    ml::lens_maker::Config cfg;
+    cfg.focal_length = 1.0;
+    cfg.aperture_radius = 0.125;
+    cfg.refractive_index = 1.49;
+    ml::BiConvexLens* lens = bench->add<ml::BiConvexLens>();
+    lens->set_name_pos_rot("little_lens", ml::VEC3_ORIGIN, ml::ROT3_UNITY);
+    lens->inner_refraction = h->fn({{200e-9, 1.49}, {1200e-9, 1.49}});
+    lens->set_curvature_radius_and_aperture_radius(
+        ml::lens_maker::get_curvature_radius(cfg), cfg.aperture_radius);
+    ml::Disc* sensor = bench->add<ml::Disc>();
+    sensor->set_name_pos_rot("sensor_disc", ml::Vec3(0.0, 0.0, -1.0), ml::ROT3_UNITY);
+    sensor->set_radius(cfg.aperture_radius);
+    h->owned_sensors.push_back(new ml::sensor::Sensor(0, sensor));
+}
+
+void build_sphere(Handle* h) {  // SphereIntersectionTest.cpp:6-33
+    ml::Sphere* s = h->scenery.root.add<ml::Sphere>();
+    s->set_name_pos_rot("my_sphere", ml::Vec3(0, 0, 0), ml::Rot3(0, 0, 0));
+    s->set_radius(1.0);
+}
+
+// One leaf of every primitive kind, in several poses, with mirrors, glass,
+// absorbers, an absorbing medium and sensors; more than 16 children at the
+// root so that octant clustering (Frame.cpp:190-255) is exercised.
+void build_primitive_zoo(Handle* h) {
+    const ml::function::Func1* mirror = h->fn({{200e-9, 0.8}, {400e-9, 0.9}, {1200e-9, 0.7}});
+    const ml::function::Func1* half = h->fn({{200e-9, 0.5}, {1200e-9, 0.5}});
+    const ml::function::Func1* glass = h->fn({{200e-9, 1.52}, {500e-9, 1.49}, {1200e-9, 1.46}});
+    const ml::function::Func1* water = h->fn({{200e-9, 1.33}, {1200e-9, 1.33}});
+    const ml::function::Func1* murky = h->fn({{200e-9, 0.7}, {1200e-9, 2.0}});
+    ml::Frame& root = h->scenery.root;
+    unsigned sensor_id = 0;
+    auto sense = [&](const ml::Frame* f) {
+        h->owned_sensors.push_back(new ml::sensor::Sensor(sensor_id++, f));
+    };
+    const double deg = M_PI/180.0;
+
+    ml::Annulus* annulus = root.add<ml::Annulus>();
+    annulus->set_name_pos_rot("annulus", ml::Vec3(1.5, 0.2, -0.3), ml::Rot3(0.3, -0.2, 0.1));
+    annulus->set_outer_inner_radius(0.6, 0.25);
+    annulus->outer_reflection = mirror;
+    sense(annulus);
+
+    ml::BiConvexLensHexBound* lens = root.add<ml::BiConvexLensHexBound>();
+    lens->set_name_pos_rot("hexlens", ml::Vec3(-1.2, 0.8, 0.4), ml::Rot3(10*deg, 5*deg, 0.0));
+    lens->inner_refraction = glass;
+    lens->set_curvature_radius_and_outer_hex_radius(1.2, 0.45);
+
+    ml::BiConvexLens* lens2 = root.add<ml::BiConvexLens>();
+    lens2->set_name_pos_rot("roundlens", ml::Vec3(0.2, -1.5, 0.9), ml::Rot3(-20*deg, 0.0, 30*deg));
+    lens2->inner_refraction = glass;
+    lens2->set_curvature_radius_and_aperture_radius(0.9, 0.35);
+
+    ml::Cylinder* cyl = root.add<ml::Cylinder>();
+    cyl->set_name_pos_rot("cylinder", ml::VEC3_ORIGIN, ml::ROT3_UNITY);
+    cyl->set_cylinder(0.3, ml::Vec3(-0.5, -0.4, -1.2), ml::Vec3(0.6, 0.2, -0.6));
+    cyl->inner_reflection = half;
+    cyl->outer_reflection = mirror;
+
+    ml::Disc* disc = root.add<ml::Disc>();
+    disc->set_name_pos_rot("disc", ml::Vec3(0.0, 0.0, 2.2), ml::Rot3(0.0, 15*deg, 0.0));
+    disc->set_radius(0.7);
+    sense(disc);
+
+    ml::EllipticalCapWithHexagonalBound* ell = root.add<ml::EllipticalCapWithHexagonalBound>();
+    ell->set_name_pos_rot("ellipse", ml::Vec3(0.9, 1.3, -1.4), ml::Rot3(0.1, 0.2, 0.3));
+    ell->set_focalLength_radiiRatio_hexAngel_hexRadius(3.0, 1.2, 0.0, 0.5);
+    ell->outer_reflection = mirror;
+
+    ml::HexPlane* hex = root.add<ml::HexPlane>();
+    hex->set_name_pos_rot("hexplane", ml::Vec3(-1.6, -1.0, -0.8), ml::Rot3(0.0, 0.0, 30*deg));
+    hex->set_outer_hex_radius(0.5);
+    sense(hex);
+
+    ml::Plane* plane = root.add<ml::Plane>();
+    plane->set_name_pos_rot("plane", ml::Vec3(0.5, 0.5, 3.0), ml::Rot3(5*deg, -7*deg, 0.0));
+    plane->set_x_y_width(2.5, 1.5);
+    plane->inner_reflection = half;
+    sense(plane);
+
+    ml::PlaneDualSphericalBound* dual = root.add<ml::PlaneDualSphericalBound>();
+    dual->set_name_pos_rot("dualsphere", ml::Vec3(1.8, -1.2, 0.5), ml::Rot3(M_PI*0.5, M_PI*0.5, 0.4));
+    dual->set_x_hight_and_y_width(0.3, 0.6);
+    dual->outer_reflection = half;
+
+    ml::RectangularBox* box = root.add<ml::RectangularBox>();
+    box->set_name_pos_rot("waterbox", ml::Vec3(-0.4, 1.8, -0.2), ml::Rot3(0.2, 0.1, -0.3));
+    box->inner_refraction = water;
+    box->inner_absorption = murky;
+    box->set_xyz_width(0.6, 0.5, 0.4);
+
+    ml::Sphere* sphere = root.add<ml::Sphere>();
+    sphere->set_name_pos_rot("sphere", ml::Vec3(0.0, 0.0, 0.0), ml::ROT3_UNITY);
+    sphere->set_radius(0.35);
+    sphere->inner_refraction = glass;
+
+    ml::SphereCapWithCylinderBound* capc = root.add<ml::SphereCapWithCylinderBound>();
+    capc->set_name_pos_rot("cap_cyl", ml::Vec3(-0.3, -0.2, -2.2), ml::Rot3(0.05, -0.04, 0.0));
+    capc->set_curvature_radius_and_outer_radius(3.0, 0.8);
+    capc->outer_reflection = mirror;
+
+    ml::SphereCapWithHexagonalBound* caph = root.add<ml::SphereCapWithHexagonalBound>();
+    caph->set_name_pos_rot("cap_hex", ml::Vec3(1.4, -0.6, -2.0), ml::Rot3(0.0, 0.1, 0.2));
+    caph->set_curvature_radius_and_outer_hex_radius(4.0, 0.6);
+    caph->outer_reflection = mirror;
+    caph->inner_reflection = half;
+
+    ml::SphereCapWithRectangularBound* capr = root.add<ml::SphereCapWithRectangularBound>();
+    capr->set_name_pos_rot("cap_rect", ml::Vec3(-1.5, 0.3, -1.9), ml::Rot3(-0.1, 0.0, 0.0));
+    capr->set_curvature_radius_and_x_y_width(2.5, 0.9, 0.6);
+    capr->outer_reflection = mirror;
+
+    ml::Triangle* tri = root.add<ml::Triangle>();
+    tri->set_name_pos_rot("triangle", ml::Vec3(0.0, -1.0, 1.6), ml::Rot3(0.4, 0.0, 0.0));
+    tri->set_corners_in_xy_plane(-0.5, -0.3, 0.6, -0.2, 0.1, 0.7);
+    sense(tri);
+
+    ml::Triangle* tri2 = root.add<ml::Triangle>();
+    tri2->set_name_pos_rot("triangle_n", ml::VEC3_ORIGIN, ml::ROT3_UNITY);
+    tri2->set_normal_and_3_vertecies(
+        ml::Vec3(0.3, 0.2, 1.0),
+        ml::Vec3(1.2, 1.1, 1.4), ml::Vec3(1.9, 1.0, 1.3), ml::Vec3(1.5, 1.7, 1.2));
+    tri2->outer_reflection = half;
+
+    ml::Frame* empty = root.add<ml::Frame>();
+    empty->set_name_pos_rot("empty_frame", ml::Vec3(0.3, 0.3, 0.3), ml::ROT3_UNITY);
+
+    // a small grid of hexagonal pixels as a nested frame
+    ml::Frame* cam = root.add<ml::Frame>();
+    cam->set_name_pos_rot("camera", ml::Vec3(0.0, 0.0, -2.9), ml::Rot3(0.0, 0.0, 0.1));
+    ml::HexGridAnnulus grid(0.9, 0.25);
+    const std::vector<ml::Vec3> cells = grid.get_grid();
+    for (size_t i = 0; i < cells.size(); i++) {
+        ml::HexPlane* pix = cam->add<ml::HexPlane>();
+        pix->set_name_pos_rot("pixel_" + std::to_string(i), cells[i],
+                              ml::Rot3(0.0, 0.0, 30*deg));
+        pix->set_outer_hex_radius(0.25/std::sqrt(3.0));
+        sense(pix);
+    }
+}
+
+// ---- optical systems of the benchmark configurations ---------------------
+
+// Segmented imaging reflector (segmented_imaging_reflector::Factory) and a
+// flat camera of hexagonal pixels at the focal plane, plus an optional
+// shield disc just above the camera.
+// p: f, DC mixing, max aperture radius, min aperture radius, facet inner
+//    hex radius, gap, reflectivity, number of pixels, pixel flat-to-flat,
+//    shield radius (0: none)
+void build_reflector_camera(Handle* h, const double* p, int n) {
+    const double f = param(p, n, 0, 4.9);
+    ml::segmented_imaging_reflector::Config c;
+    c.focal_length = f;
+    c.DaviesCotton_over_parabolic_mixing_factor = param(p, n, 1, 1.0);
+    c.max_outer_aperture_radius = param(p, n, 2, 2.1);
+    c.min_inner_aperture_radius = param(p, n, 3, 0.0);
+    c.facet_inner_hex_radius = param(p, n, 4, 0.3);
+    c.gap_between_facets = param(p, n, 5, 0.01);
+    const double reflectivity = param(p, n, 6, 0.9);
+    const unsigned num_pixels = static_cast<unsigned>(param(p, n, 7, 1440));
+    const double pixel_f2f = param(p, n, 8, 0.0095);
+    const double shield = param(p, n, 9, 0.0);
+
+    ml::SurfaceEntity* reflector = h->scenery.root.add<ml::SurfaceEntity>();
+    reflector->set_name_pos_rot("reflector", ml::VEC3_ORIGIN, ml::ROT3_UNITY);
+    reflector->outer_reflection = h->fn({{200e-9, reflectivity}, {1200e-9, reflectivity}});
+    ml::segmented_imaging_reflector::Factory fab(c);
+    fab.add_to_SurfaceEntity(reflector);
+
+    ml::Frame* cam = h->scenery.root.add<ml::Frame>();
+    cam->set_name_pos_rot("camera", ml::Vec3(0.0, 0.0, f), ml::ROT3_UNITY);
+    // pixel centres: the hexagonal grid closest to the optical axis
+    const double grid_radius = pixel_f2f*(std::sqrt(static_cast<double>(num_pixels)) + 2.0);
+    ml::HexGridAnnulus grid(grid_radius, pixel_f2f);
+    std::vector<ml::Vec3> cells = grid.get_grid();
+    std::vector<size_t> order(cells.size());
+    for (size_t i = 0; i < order.size(); i++) order[i] = i;
+    std::stable_sort(order.begin(), order.end(), [&](size_t a, size_t b) {
+        return cells[a].norm() < cells[b].norm();
+    });
+    if (order.size() < num_pixels) throw std::runtime_error("pixel grid too small");
+    for (unsigned i = 0; i < num_pixels; i++) {
+        ml::HexPlane* pix = cam->add<ml::HexPlane>();
+        pix->set_name_pos_rot("pixel_" + std::to_string(i), cells[order[i]],
+                              ml::Rot3(0.0, 0.0, ml::deg2rad(30.0)));
+        pix->set_outer_hex_radius(pixel_f2f/std::sqrt(3.0));
+        h->owned_sensors.push_back(new ml::sensor::Sensor(i, pix));
+    }
+    if (shield > 0.0) {
+        ml::Disc* disc = h->scenery.root.add<ml::Disc>();
+        disc->set_name_pos_rot("shield", ml::Vec3(0.0, 0.0, f + 1e-3), ml::ROT3_UNITY);
+        disc->set_radius(shield);
+    }
+}
+
+// Segmented reflector plus the light-field sensor of
+// merlict_portal_plenoscope/light_field_sensor/Factory.cpp:235-249 at the
+// focal plane.
+// p: f, max aperture radius, FoV diameter [deg], pixel FoV [deg], paxels on
+//    the pixel diagonal, housing overhead, reflectivity, DC mixing, facet
+//    inner hex radius, gap
+void build_light_field_sensor(Handle* h, const double* p, int n) {
+    const double f = param(p, n, 0, 10.7);
+    const double R = param(p, n, 1, 5.35);
+    ml::segmented_imaging_reflector::Config c;
+    c.focal_length = f;
+    c.DaviesCotton_over_parabolic_mixing_factor = param(p, n, 7, 1.0);
+    c.max_outer_aperture_radius = R;
+    c.min_inner_aperture_radius = 0.0;
+    c.facet_inner_hex_radius = param(p, n, 8, 0.3);
+    c.gap_between_facets = param(p, n, 9, 0.01);
+    const double reflectivity = param(p, n, 6, 0.9);
+    const ml::function::Func1* refl = h->fn({{200e-9, reflectivity}, {1200e-9, reflectivity}});
+    const ml::function::Func1* n_lens =
+        h->fn({{200e-9, 1.52}, {300e-9, 1.50}, {700e-9, 1.47}, {1200e-9, 1.46}});
+
+    ml::SurfaceEntity* reflector = h->scenery.root.add<ml::SurfaceEntity>();
+    reflector->set_name_pos_rot("reflector", ml::VEC3_ORIGIN, ml::ROT3_UNITY);
+    reflector->outer_reflection = refl;
+    ml::segmented_imaging_reflector::Factory fab(c);
+    fab.add_to_SurfaceEntity(reflector);
+
+    plenoscope::light_field_sensor::Config lc;
+    lc.expected_imaging_system_focal_length = f;
+    lc.expected_imaging_system_max_aperture_radius = R;
+    lc.max_FoV_diameter = ml::deg2rad(param(p, n, 2, 6.5));
+    lc.pixel_FoV_hex_flat2flat = ml::deg2rad(param(p, n, 3, 0.186));
+    lc.num_paxel_on_pixel_diagonal = static_cast<unsigned>(param(p, n, 4, 9));
+    lc.housing_overhead = param(p, n, 5, 1.1);
+    lc.lens_refraction = n_lens;
+    lc.bin_reflection = refl;
+    auto* geometry = new plenoscope::light_field_sensor::Geometry(lc);
+    ml::Frame* lfs = h->scenery.root.add<ml::Frame>();
+    lfs->set_name_pos_rot("light_field_sensor", ml::Vec3(0, 0, f), ml::ROT3_UNITY);
+    plenoscope::light_field_sensor::Factory factory(geometry);
+    factory.add_light_field_sensor_to_frame_in_scenery(lfs, &h->scenery);
+    ml::sensor::Sensors* lixels = factory.get_sub_pixels();
+    for (ml::sensor::Sensor* s : lixels->by_occurence) h->owned_sensors.push_back(s);
+    delete lixels;   // the Sensor objects are kept in owned_sensors
+}
+
+// ---- a random::Generator that replays a given stream ---------------------
+
+class ReplayGenerator : public ml::random::Generator {
+ public:
+    int mode = 0;               // 0: Philox stream, 1: explicit uniforms
+    uint64_t philox_seed = 0;
+    uint64_t stream = 0;
+    const double* uniforms = nullptr;
+    uint32_t stride = 0;
+    uint32_t used = 0;
+    bool exhausted = false;
+    double uniform() override {
+        const uint32_t k = used++;
+        if (mode == 0) return mlgpu_philox_uniform(philox_seed, stream, k);
+        if (k >= stride) { exhausted = true; return 0.5; }
+        return uniforms[static_cast<size_t>(stream)*stride + k];
+    }
+    uint64_t create_seed() override { return 0; }
+    double normal(const double mean, const double std_dev) override {
+        (void)std_dev; return mean;
+    }
+};
+
+template <typename Tag, typename Tag::type Member>
+struct Accessor { friend typename Tag::type member_of(Tag) { return Member; } };
+struct InteractionHistory {
+    typedef std::vector<ml::Interaction> ml::RayForPropagation::*type;
+    friend type member_of(InteractionHistory);
+};
+template struct Accessor<InteractionHistory, &ml::RayForPropagation::interaction_history>;
+
+}  // namespace
+
+extern "C" {
+
+const char* ref_last_error(void) { return last_error.c_str(); }
+
+void* ref_scene_build(const char* kind, const double* params, int num_params) {
+    try {
+        std::unique_ptr<Handle> h(new Handle);
+        const std::string k(kind);
+        if (k == "two_mirrors") build_two_mirrors(h.get());
+        else if (k == "mirror_absorber") build_mirror_absorber(h.get());
+        else if (k == "water_box") build_water_box(h.get(), false);
+        else if (k == "absorbing_box") build_water_box(h.get(), true);
+        else if (k == "biconvex_lens") build_biconvex_lens(h.get());
+        else if (k == "sphere") build_sphere(h.get());
+        else if (k == "primitive_zoo") build_primitive_zoo(h.get());
+        else if (k == "reflector_camera") build_reflector_camera(h.get(), params, num_params);
+        else if (k == "light_field_sensor") build_light_field_sensor(h.get(), params, num_params);
+        else throw std::invalid_argument("unknown scene kind '" + k + "'");
+        h->sensors.init(h->owned_sensors);
+        h->scenery.root.init_tree_based_on_mother_child_relations();
+        return h.release();
+    } catch (const std::exception& e) {
+        last_error = e.what();
+        return nullptr;
+    }
+}
+
+void ref_scene_free(void* handle) { delete static_cast<Handle*>(handle); }
+
+int ref_scene_flat(void* handle, mlgpu_flat_scene* out) {
+    Handle* h = static_cast<Handle*>(handle);
+    try {
+        if (!h->flattened) {
+            h->flat = merlict_b200::flatten(&h->scenery.root, &h->sensors);
+            h->flattened = true;
+        }
+        *out = h->flat.view();
+        return 0;
+    } catch (const std::exception& e) {
+        last_error = e.what();
+        return 1;
+    }
+}
+
+int ref_scene_num_sensors(void* handle) {
+    return static_cast<int>(static_cast<Handle*>(handle)->sensors.size());
+}
+
+// mode 0: per-photon Propagator on the Philox stream (seed) -- "replay"
+// mode 1: per-photon Propagator on explicit uniforms[n][stride]
+// mode 2: reference propagate_photons_in_frame_with_config, Mt19937(seed)
+// mode 3: reference ..._multi_thread, Mt19937(seed) seeding per photon
+// Results are written to `out` (host pointers, double precision); the time
+// of propagate + Sensors::assign_photons goes to *seconds.
+int ref_propagate(void* handle, const mlgpu_photons* ph, uint64_t n,
+                  uint32_t max_interactions, int mode, uint64_t seed,
+                  const double* uniforms, uint32_t stride, int num_threads,
+                  mlgpu_results* out, double* seconds) {
+    Handle* h = static_cast<Handle*>(handle);
+    try {
+        std::vector<ml::Photon> photons;
+        photons.reserve(n);
+        for (uint64_t i = 0; i < n; i++) {
+            const ml::Vec3 s(((const double*)ph->support_x)[i], ((const double*)ph->support_y)[i],
+                             ((const double*)ph->support_z)[i]);
+            const ml::Vec3 d(((const double*)ph->direction_x)[i], ((const double*)ph->direction_y)[i],
+                             ((const double*)ph->direction_z)[i]);
+            ml::Photon p(s, d, ((const double*)ph->wavelength)[i]);
+            p.simulation_truth_id = static_cast<int32_t>(i);
+            photons.push_back(p);
+        }
+        ml::PropagationConfig cfg;
+        cfg.max_num_interactions_per_photon = max_interactions;
+        std::vector<uint32_t> used(n, 0);
+        h->sensors.clear_history();
+
+        const auto t0 = std::chrono::steady_clock::now();
+        if (mode == 0 || mode == 1) {
+            auto work = [&](uint64_t begin, uint64_t end) {
+                for (uint64_t i = begin; i < end; i++) {
+                    ReplayGenerator g;
+                    g.mode = mode; g.philox_seed = seed; g.stream = i;
+                    g.uniforms = uniforms; g.stride = stride;
+                    ml::PropagationEnvironment env;
+                    env.root_frame = &h->scenery.root;
+                    env.config = &cfg;
+                    env.prng = &g;
+                    ml::Propagator(&photons[i], env);
+                    used[i] = g.used;
+                }
+            };
+            const int nt = num_threads > 1 ? num_threads : 1;
+            std::vector<std::thread> pool;
+            for (int t = 0; t < nt; t++)
+                pool.emplace_back(work, n*t/nt, n*(t + 1)/nt);
+            for (std::thread& t : pool) t.join();
+        } else if (mode == 2) {
+            ml::random::Mt19937 prng(seed);
+            ml::propagate_photons_in_frame_with_config(&photons, &h->scenery.root, &cfg, &prng);
+        } else if (mode == 3) {
+            ml::random::Mt19937 prng(seed);
+            ml::propagate_photons_in_frame_with_config_multi_thread(
+                &photons, &h->scenery.root, &cfg, &prng);
+        } else {
+            throw std::invalid_argument("unknown mode");
+        }
+        h->sensors.assign_photons(&photons);
+        const auto t1 = std::chrono::steady_clock::now();
+        if (seconds) *seconds = std::chrono::duration<double>(t1 - t0).count();
+
+        if (!out) return 0;
+        const merlict_b200::FlatScene* flat = nullptr;
+        if (!h->flattened) {
+            h->flat = merlict_b200::flatten(&h->scenery.root, &h->sensors);
+            h->flattened = true;
+        }
+        flat = &h->flat;
+        std::map<const ml::Frame*, int32_t> leaf_of;
+        for (size_t l = 0; l < flat->leaf_node.size(); l++)
+            leaf_of[flat->node_frame[flat->leaf_node[l]]] = static_cast<int32_t>(l);
+        auto leaf_id = [&](const ml::SurfaceEntity* o) -> int32_t {
+            if (o == &ml::VOID_SURFACE_ENTITY) return MLGPU_LEAF_VOID;
+            auto it = leaf_of.find(o);
+            return it == leaf_of.end() ? MLGPU_LEAF_PHOTON_SOURCE : it->second;
+        };
+        // arrivals by photon id (simulation_truth_id == photon index)
+        std::vector<int32_t> sensor_of(n, -1);
+        std::vector<const ml::sensor::PhotonArrival*> arrival_of(n, nullptr);
+        for (size_t s = 0; s < h->sensors.by_occurence.size(); s++)
+            for (const ml::sensor::PhotonArrival& a : h->sensors.by_occurence[s]->photon_arrival_history) {
+                sensor_of[a.simulation_truth_id] = static_cast<int32_t>(s);
+                arrival_of[a.simulation_truth_id] = &a;
+            }
+        const uint32_t len = max_interactions + 1;
+        for (uint64_t i = 0; i < n; i++) {
+            const ml::Photon& p = photons[i];
+            const ml::Intersection& fin = p.final_intersection();
+            const int32_t leaf = p.num_interactions() > 1 ? leaf_id(fin.object())
+                                                          : MLGPU_LEAF_PHOTON_SOURCE;
+            out->sensor[i] = sensor_of[i];
+            double x = fin.position_in_object_frame().x;
+            double y = fin.position_in_object_frame().y;
+            double t, tx, ty;
+            if (arrival_of[i]) {
+                t = arrival_of[i]->arrival_time;
+                tx = arrival_of[i]->theta_x;
+                ty = arrival_of[i]->theta_y;
+                x = arrival_of[i]->x_intersect;
+                y = arrival_of[i]->y_intersect;
+            } else {
+                // merlict evaluates the time of flight only for photons given
+                // to a sensor (Sensor.cpp:14-30).  For a photon that ended in
+                // the void it would dereference the refraction table of
+                // VOID_SURFACE_ENTITY, which is built before the default
+                // tables in SurfaceEntity.cpp:9-27 and holds null pointers.
+                t = NAN;
+                const ml::Vec3 inc = p.final_intersection_incident_direction_wrt_frame();
+                tx = -1.0*inc.x; ty = -1.0*inc.y;
+            }
+            if (out->x) ((double*)out->x)[i] = x;
+            if (out->y) ((double*)out->y)[i] = y;
+            if (out->time) out->time[i] = t;
+            if (out->theta_x) ((double*)out->theta_x)[i] = tx;
+            if (out->theta_y) ((double*)out->theta_y)[i] = ty;
+            if (out->final_leaf) out->final_leaf[i] = leaf;
+            if (out->info) {
+                const uint32_t u = used[i] > 255 ? 255 : used[i];
+                out->info[i] = static_cast<uint32_t>(p.final_interaction()) |
+                    (p.num_interactions() << 8) | (u << 16);
+            }
+            if (out->final_position) {
+                const ml::Vec3 w = fin.position_in_root_frame();
+                out->final_position[3*i] = w.x;
+                out->final_position[3*i + 1] = w.y;
+                out->final_position[3*i + 2] = w.z;
+            }
+            if (out->final_direction) {
+                out->final_direction[3*i] = p.direction().x;
+                out->final_direction[3*i + 1] = p.direction().y;
+                out->final_direction[3*i + 2] = p.direction().z;
+            }
+            if (out->history) {
+                const std::vector<ml::Interaction>& kinds = p.*member_of(InteractionHistory());
+                for (uint32_t k = 0; k < len; k++) {
+                    mlgpu_history_entry* e = &out->history[i*len + k];
+                    std::memset(e, 0, sizeof(*e));
+                    e->leaf = MLGPU_LEAF_PHOTON_SOURCE;
+                    if (k >= p.num_interactions()) continue;
+                    const ml::Intersection& is = p.intersection_at(k);
+                    const ml::Vec3 pos = is.position_in_object_frame();
+                    const ml::Vec3 nrm = is.surface_normal_in_object_frame();
+                    e->position[0] = pos.x; e->position[1] = pos.y; e->position[2] = pos.z;
+                    e->normal[0] = nrm.x; e->normal[1] = nrm.y; e->normal[2] = nrm.z;
+                    e->distance = is.distance_to_ray_support();
+                    e->leaf = k == 0 ? MLGPU_LEAF_PHOTON_SOURCE : leaf_id(is.object());
+                    e->interaction = static_cast<uint8_t>(kinds[k]);
+                    e->from_outside_to_inside = is.from_outside_to_inside() ? 1 : 0;
+                }
+            }
+        }
+        return 0;
+    } catch (const std::out_of_range& e) {
+        last_error = e.what();
+        return MLGPU_ERR_OUT_OF_RANGE;
+    } catch (const std::invalid_argument& e) {
+        last_error = e.what();
+        return MLGPU_ERR_INVALID_ARGUMENT;
+    } catch (const std::exception& e) {
+        last_error = e.what();
+        return MLGPU_ERR_RUNTIME;
+    }
+}
+
+int ref_hardware_concurrency(void) {
+    return static_cast<int>(std::thread::hardware_concurrency());
+}
+
+}  // extern "C"
