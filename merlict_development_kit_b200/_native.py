@@ -1,0 +1,86 @@
+"""Loads libmerlict_b200.so (the CUDA engine) and declares its C ABI.
+
+There is no CPU fallback: if the library is missing or was built for another
+GPU, importing the engine raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+from . import abi
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "_build", "libmerlict_b200.so")
+
+_lib = None
+
+
+class EngineError(RuntimeError):
+    """An engine status other than MLGPU_OK."""
+
+    def __init__(self, status: int, message: str):
+        super().__init__(message)
+        self.status = status
+
+
+def _exception_for(status: int, message: str) -> Exception:
+    # the std:: exceptions merlict throws for the same conditions
+    if status == abi.ERR_INVALID_ARGUMENT:
+        return ValueError(message)
+    if status == abi.ERR_OUT_OF_RANGE:
+        return IndexError(message)
+    return EngineError(status, message)
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise ImportError(
+                f"{LIB_PATH} is missing: build it with "
+                "`python -m merlict_development_kit_b200.build` (needs nvcc)")
+        L = C.CDLL(LIB_PATH)
+        L.mlgpu_abi_version.restype = C.c_int
+        L.mlgpu_last_error.argtypes = [C.c_char_p, C.c_size_t]
+        L.mlgpu_last_error.restype = C.c_int
+        L.mlgpu_scene_create.argtypes = [C.POINTER(abi.mlgpu_flat_scene), C.POINTER(C.c_void_p)]
+        L.mlgpu_scene_destroy.argtypes = [C.c_void_p]
+        L.mlgpu_propagate.argtypes = [
+            C.c_void_p, C.POINTER(abi.mlgpu_photons), C.c_uint64,
+            C.POINTER(abi.mlgpu_settings), C.POINTER(abi.mlgpu_rng),
+            C.POINTER(abi.mlgpu_results), C.c_void_p]
+        L.mlgpu_propagate_host.argtypes = [
+            C.c_void_p, C.POINTER(abi.mlgpu_photons), C.c_uint64,
+            C.POINTER(abi.mlgpu_settings), C.POINTER(abi.mlgpu_rng),
+            C.POINTER(abi.mlgpu_results)]
+        L.mlgpu_scene_sync_errors.argtypes = [C.c_void_p, C.c_void_p]
+        L.mlgpu_bin_arrivals.argtypes = [
+            C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint64, C.c_void_p, C.c_void_p,
+            C.c_uint32, C.c_double, C.c_double, C.c_void_p]
+        for name in ("mlgpu_scene_create", "mlgpu_scene_destroy", "mlgpu_propagate",
+                     "mlgpu_propagate_host", "mlgpu_scene_sync_errors", "mlgpu_bin_arrivals"):
+            getattr(L, name).restype = C.c_int
+        if L.mlgpu_abi_version() != abi.ABI_VERSION:
+            raise ImportError("libmerlict_b200.so ABI version mismatch")
+        _lib = L
+    return _lib
+
+
+def last_error() -> str:
+    buf = C.create_string_buffer(2048)
+    lib().mlgpu_last_error(buf, len(buf))
+    return buf.value.decode(errors="replace")
+
+
+def check(status: int) -> None:
+    if status != abi.OK:
+        raise _exception_for(status, last_error())
+
+
+# every symbol include/merlict_b200.h declares
+EXPORTED = (
+    "mlgpu_abi_version", "mlgpu_last_error", "mlgpu_scene_create", "mlgpu_scene_destroy",
+    "mlgpu_propagate", "mlgpu_scene_sync_errors", "mlgpu_propagate_host",
+    "mlgpu_bin_arrivals",
+)

@@ -1,0 +1,473 @@
+// capi.cu -- the extern "C" entry points of include/merlict_b200.h.
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "mlgpu_internal.h"
+
+using namespace mlgpu;
+
+namespace {
+
+thread_local std::string g_last_error;
+
+int fail(int code, const char* fmt, ...) {
+    char buf[1024];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof(buf), fmt, ap);
+    va_end(ap);
+    g_last_error = buf;
+    return code;
+}
+
+int cuda_fail(cudaError_t e, const char* what) {
+    return fail(MLGPU_ERR_CUDA, "%s: %s", what, cudaGetErrorString(e));
+}
+
+#define MLGPU_CUDA(call)                                   \
+    do {                                                   \
+        cudaError_t e_ = (call);                           \
+        if (e_ != cudaSuccess) return cuda_fail(e_, #call); \
+    } while (0)
+
+// A device buffer that grows on demand.
+struct DeviceBuffer {
+    void* ptr = nullptr;
+    size_t bytes = 0;
+    cudaError_t reserve(size_t n) {
+        if (n <= bytes) return cudaSuccess;
+        if (ptr) cudaFree(ptr);
+        ptr = nullptr;
+        bytes = 0;
+        cudaError_t e = cudaMalloc(&ptr, n);
+        if (e == cudaSuccess) bytes = n;
+        return e;
+    }
+    void release() {
+        if (ptr) cudaFree(ptr);
+        ptr = nullptr;
+        bytes = 0;
+    }
+};
+
+}  // namespace
+
+struct mlgpu_scene {
+    int device = 0;
+    DevScene dev;
+    std::vector<void*> owned;        // device allocations of the scene
+    unsigned int* error_word = nullptr;
+    // staging for mlgpu_propagate_host and scratch for binning
+    DeviceBuffer staging_in, staging_out, staging_hist, staging_rng, bin_scratch;
+};
+
+namespace {
+
+template <typename T>
+int upload(mlgpu_scene* s, const T* host, size_t count, const T** out) {
+    if (count == 0) count = 1;
+    void* p = nullptr;
+    MLGPU_CUDA(cudaMalloc(&p, count*sizeof(T)));
+    s->owned.push_back(p);
+    if (host) MLGPU_CUDA(cudaMemcpy(p, host, count*sizeof(T), cudaMemcpyHostToDevice));
+    *out = static_cast<const T*>(p);
+    return MLGPU_OK;
+}
+
+// Host-side bounds checks of every index the kernels follow.
+int validate(const mlgpu_flat_scene* f) {
+    if (!f) return fail(MLGPU_ERR_INVALID_ARGUMENT, "flat scene is NULL");
+    const int32_t nn = f->num_nodes, nl = f->num_leaves, nf = f->num_functions;
+    if (nn < 1) return fail(MLGPU_ERR_INVALID_ARGUMENT, "scene has no nodes");
+    if (nl < 0 || nf < 1) return fail(MLGPU_ERR_INVALID_ARGUMENT, "bad leaf or function count");
+    if (!f->node_sphere || !f->node_skip || !f->node_leaf || !f->function_offset ||
+        !f->function_points)
+        return fail(MLGPU_ERR_INVALID_ARGUMENT, "missing scene array");
+    if (nl > 0 && (!f->leaf_node || !f->leaf_frame2world || !f->leaf_primitive ||
+                   !f->leaf_params || !f->leaf_surface || !f->leaf_sensor))
+        return fail(MLGPU_ERR_INVALID_ARGUMENT, "missing leaf array");
+    if (f->node_skip[0] != nn)
+        return fail(MLGPU_ERR_INVALID_ARGUMENT, "node 0 must be the root of the whole tree");
+    for (int32_t i = 0; i < nn; i++) {
+        const int32_t k = f->node_skip[i];
+        const int32_t leaf = f->node_leaf[i];
+        if (k <= i || k > nn)
+            return fail(MLGPU_ERR_INVALID_ARGUMENT, "node %d: skip %d out of range", i, k);
+        if (leaf < -1 || leaf >= nl)
+            return fail(MLGPU_ERR_INVALID_ARGUMENT, "node %d: leaf %d out of range", i, leaf);
+        if ((leaf >= 0) != (k == i + 1))
+            return fail(MLGPU_ERR_INVALID_ARGUMENT, "node %d: leaf/subtree mismatch", i);
+        if (leaf >= 0 && f->leaf_node[leaf] != i)
+            return fail(MLGPU_ERR_INVALID_ARGUMENT, "node %d: leaf_node disagrees", i);
+        if (!(f->node_sphere[4*i + 3] >= 0.0))
+            return fail(MLGPU_ERR_INVALID_ARGUMENT, "node %d: negative bounding radius", i);
+    }
+    for (int32_t l = 0; l < nl; l++) {
+        const int32_t prim = f->leaf_primitive[l];
+        if (prim < 0 || prim >= MLGPU_PRIM_COUNT)
+            return fail(MLGPU_ERR_INVALID_ARGUMENT, "leaf %d: unknown primitive %d", l, prim);
+        const int32_t* su = f->leaf_surface + (size_t)l*MLGPU_SURF_COLUMNS;
+        for (int c = 0; c < 6; c++)
+            if (su[c] < 0 || su[c] >= nf)
+                return fail(MLGPU_ERR_INVALID_ARGUMENT, "leaf %d: table id %d out of range", l, su[c]);
+        if (su[MLGPU_SURF_ALLOWED_NODE] < -1 || su[MLGPU_SURF_ALLOWED_NODE] >= nn)
+            return fail(MLGPU_ERR_INVALID_ARGUMENT, "leaf %d: allowed node out of range", l);
+        if (f->leaf_sensor[l] < -1 || f->leaf_sensor[l] >= f->num_sensors)
+            return fail(MLGPU_ERR_INVALID_ARGUMENT, "leaf %d: sensor out of range", l);
+    }
+    if (f->function_offset[0] != 0)
+        return fail(MLGPU_ERR_INVALID_ARGUMENT, "function offsets must start at 0");
+    for (int32_t k = 0; k < nf; k++) {
+        const int32_t b = f->function_offset[k], e = f->function_offset[k + 1];
+        if (e - b < 1) return fail(MLGPU_ERR_INVALID_ARGUMENT, "function %d is empty", k);
+        for (int32_t j = b + 1; j < e; j++)
+            if (!(f->function_points[3*j] > f->function_points[3*(j - 1)]))
+                return fail(MLGPU_ERR_INVALID_ARGUMENT,
+                            "function %d: arguments not strictly increasing", k);
+    }
+    if (f->default_refraction < 0 || f->default_refraction >= nf)
+        return fail(MLGPU_ERR_INVALID_ARGUMENT, "default refraction id out of range");
+    return MLGPU_OK;
+}
+
+int build_device_scene(mlgpu_scene* s, const mlgpu_flat_scene* f) {
+    const int32_t nn = f->num_nodes, nl = f->num_leaves, nf = f->num_functions;
+    std::vector<double4> node(nn);
+    std::vector<int2> meta(nn);
+    std::vector<float4> node_f(nn);
+    for (int32_t i = 0; i < nn; i++) {
+        const double* c = f->node_sphere + 4*(size_t)i;
+        node[i] = make_double4(c[0], c[1], c[2], c[3]*c[3]);
+        meta[i] = make_int2(f->node_skip[i], f->node_leaf[i]);
+        // FP32 cull sphere: centre rounded, radius widened by the rounding
+        // of the centre and of the ray so the cull stays conservative.
+        const float fx = (float)c[0], fy = (float)c[1], fz = (float)c[2];
+        const double dc = std::sqrt((fx - c[0])*(fx - c[0]) + (fy - c[1])*(fy - c[1]) +
+                                    (fz - c[2])*(fz - c[2]));
+        const double mag = std::fabs(c[0]) + std::fabs(c[1]) + std::fabs(c[2]);
+        const double r = c[3]*(1.0 + 1e-5) + dc + 4e-7*mag + 1e-6;
+        node_f[i] = make_float4(fx, fy, fz, (float)(r*r));
+    }
+    std::vector<LeafRec> leaf(nl > 0 ? nl : 1);
+    std::vector<LeafRecF> leaf_f(nl > 0 ? nl : 1);
+    std::vector<double> origin(3*(size_t)(nl > 0 ? nl : 1), 0.0);
+    std::memset(leaf.data(), 0, leaf.size()*sizeof(LeafRec));
+    std::memset(leaf_f.data(), 0, leaf_f.size()*sizeof(LeafRecF));
+    for (int32_t l = 0; l < nl; l++) {
+        LeafRec& L = leaf[l];
+        const double* t = f->leaf_frame2world + 12*(size_t)l;
+        for (int k = 0; k < 12; k++) L.T[k] = t[k];
+        // translation part of HomTra3::position_inverse, HomTra3.cpp:200-216
+        L.tinv[0] = t[0]*t[3] + t[4]*t[7] + t[8]*t[11];
+        L.tinv[1] = t[1]*t[3] + t[5]*t[7] + t[9]*t[11];
+        L.tinv[2] = t[2]*t[3] + t[6]*t[7] + t[10]*t[11];
+        for (int k = 0; k < MLGPU_LEAF_PARAMS; k++) L.params[k] = f->leaf_params[MLGPU_LEAF_PARAMS*(size_t)l + k];
+        const double r = f->node_sphere[4*(size_t)f->leaf_node[l] + 3];
+        L.r2 = r*r;
+        L.primitive = f->leaf_primitive[l];
+        L.sensor = f->leaf_sensor[l];
+        const int32_t* su = f->leaf_surface + (size_t)l*MLGPU_SURF_COLUMNS;
+        L.allowed_node = su[MLGPU_SURF_ALLOWED_NODE];
+        L.flags = su[MLGPU_SURF_FLAGS];
+        for (int k = 0; k < 6; k++) L.fn[k] = su[k];
+
+        LeafRecF& F = leaf_f[l];
+        for (int rr = 0; rr < 3; rr++)
+            for (int cc = 0; cc < 3; cc++) F.R[3*rr + cc] = (float)t[4*rr + cc];
+        for (int k = 0; k < MLGPU_LEAF_PARAMS; k++) F.params[k] = (float)L.params[k];
+        F.r2 = (float)L.r2;
+        F.primitive = L.primitive;
+        F.sensor = L.sensor;
+        F.allowed_node = L.allowed_node;
+        F.flags = L.flags;
+        for (int k = 0; k < 6; k++) F.fn[k] = L.fn[k];
+        origin[3*(size_t)l] = t[3];
+        origin[3*(size_t)l + 1] = t[7];
+        origin[3*(size_t)l + 2] = t[11];
+    }
+    const int32_t npts = f->function_offset[nf];
+    std::vector<float> pts_f(3*(size_t)npts);
+    for (int32_t k = 0; k < 3*npts; k++) pts_f[k] = (float)f->function_points[k];
+
+    int st;
+    if ((st = upload(s, node.data(), nn, &s->dev.node))) return st;
+    if ((st = upload(s, meta.data(), nn, &s->dev.node_meta))) return st;
+    if ((st = upload(s, leaf.data(), leaf.size(), &s->dev.leaf))) return st;
+    if ((st = upload(s, f->function_points, 3*(size_t)npts, &s->dev.fn_points))) return st;
+    if ((st = upload(s, f->function_offset, (size_t)nf + 1, &s->dev.fn_offset))) return st;
+    if ((st = upload(s, node_f.data(), nn, &s->dev.node_f))) return st;
+    if ((st = upload(s, leaf_f.data(), leaf_f.size(), &s->dev.leaf_f))) return st;
+    if ((st = upload(s, origin.data(), origin.size(), &s->dev.leaf_origin))) return st;
+    if ((st = upload(s, pts_f.data(), pts_f.size(), &s->dev.fn_points_f))) return st;
+    const unsigned int* ew = nullptr;
+    if ((st = upload<unsigned int>(s, nullptr, 1, &ew))) return st;
+    s->error_word = const_cast<unsigned int*>(ew);
+    MLGPU_CUDA(cudaMemset(s->error_word, 0, sizeof(unsigned int)));
+    s->dev.error_word = s->error_word;
+    s->dev.num_nodes = nn;
+    s->dev.num_leaves = nl;
+    s->dev.num_functions = nf;
+    s->dev.default_refraction = f->default_refraction;
+    s->dev.num_sensors = f->num_sensors;
+    for (int k = 0; k < 3; k++) {
+        s->dev.hex_u[k] = f->hex_unit_u[k];
+        s->dev.hex_v[k] = f->hex_unit_v[k];
+        s->dev.hex_w[k] = f->hex_unit_w[k];
+    }
+    return MLGPU_OK;
+}
+
+int check_propagate_args(const mlgpu_scene* scene, const mlgpu_photons* ph,
+                         const mlgpu_settings* st, const mlgpu_rng* rng,
+                         const mlgpu_results* res) {
+    if (!scene || !ph || !st || !rng || !res)
+        return fail(MLGPU_ERR_INVALID_ARGUMENT, "NULL argument");
+    if (ph->dtype != MLGPU_F64 && ph->dtype != MLGPU_F32)
+        return fail(MLGPU_ERR_INVALID_ARGUMENT, "photon dtype must be MLGPU_F64 or MLGPU_F32");
+    if (res->dtype != MLGPU_F64 && res->dtype != MLGPU_F32)
+        return fail(MLGPU_ERR_INVALID_ARGUMENT, "result dtype must be MLGPU_F64 or MLGPU_F32");
+    if (!ph->support_x || !ph->support_y || !ph->support_z || !ph->direction_x ||
+        !ph->direction_y || !ph->direction_z || !ph->wavelength)
+        return fail(MLGPU_ERR_INVALID_ARGUMENT, "photon plane is NULL");
+    if (!res->sensor) return fail(MLGPU_ERR_INVALID_ARGUMENT, "results.sensor is NULL");
+    if (st->start_node < 0 || st->start_node >= scene->dev.num_nodes)
+        return fail(MLGPU_ERR_INVALID_ARGUMENT, "start node %d out of range", st->start_node);
+    if (st->max_num_interactions_per_photon > 254)
+        return fail(MLGPU_ERR_INVALID_ARGUMENT, "max_num_interactions_per_photon must be <= 254");
+    if (rng->mode != MLGPU_RNG_PHILOX && rng->mode != MLGPU_RNG_REPLAY)
+        return fail(MLGPU_ERR_INVALID_ARGUMENT, "unknown rng mode");
+    if (rng->mode == MLGPU_RNG_REPLAY && !rng->uniforms)
+        return fail(MLGPU_ERR_INVALID_ARGUMENT, "replay rng without uniforms");
+    if (st->tracer != MLGPU_TRACER_FP64 && st->tracer != MLGPU_TRACER_FP32 &&
+        st->tracer != MLGPU_TRACER_FP32_PURE)
+        return fail(MLGPU_ERR_INVALID_ARGUMENT, "unknown tracer %d", st->tracer);
+    if (st->tracer != MLGPU_TRACER_FP64 && res->history)
+        return fail(MLGPU_ERR_INVALID_ARGUMENT, "histories are recorded by the FP64 tracer only");
+    return MLGPU_OK;
+}
+
+TraceArgs make_args(const mlgpu_scene* scene, const mlgpu_photons* ph, uint64_t n,
+                    const mlgpu_settings* st, const mlgpu_rng* rng, const mlgpu_results* res) {
+    TraceArgs a;
+    std::memset(&a, 0, sizeof(a));
+    a.scene = scene->dev;
+    a.photons.sx = ph->support_x; a.photons.sy = ph->support_y; a.photons.sz = ph->support_z;
+    a.photons.dx = ph->direction_x; a.photons.dy = ph->direction_y; a.photons.dz = ph->direction_z;
+    a.photons.wavelength = ph->wavelength;
+    a.in_dtype = ph->dtype;
+    a.results.sensor = res->sensor;
+    a.results.x = res->x; a.results.y = res->y; a.results.time = res->time;
+    a.results.theta_x = res->theta_x; a.results.theta_y = res->theta_y;
+    a.results.final_leaf = res->final_leaf; a.results.info = res->info;
+    a.results.final_position = res->final_position;
+    a.results.final_direction = res->final_direction;
+    a.results.history = res->history;
+    a.out_dtype = res->dtype;
+    a.rng.mode = rng->mode; a.rng.stride = rng->stride; a.rng.seed = rng->seed;
+    a.rng.photon_offset = rng->photon_offset; a.rng.uniforms = rng->uniforms;
+    a.num_photons = n;
+    a.max_interactions = st->max_num_interactions_per_photon;
+    a.start_node = st->start_node;
+    return a;
+}
+
+int launch(const mlgpu_scene* scene, const TraceArgs& a, const mlgpu_settings* st,
+           cudaStream_t stream) {
+    cudaError_t e;
+    switch (st->tracer) {
+    case MLGPU_TRACER_FP64: e = launch_trace_fp64(a, st->block_size, stream); break;
+    case MLGPU_TRACER_FP32: e = launch_trace_fp32(a, st->block_size, false, stream); break;
+    default: e = launch_trace_fp32(a, st->block_size, true, stream); break;
+    }
+    (void)scene;
+    if (e != cudaSuccess) return cuda_fail(e, "trace kernel launch");
+    return MLGPU_OK;
+}
+
+const char* device_error_text(unsigned int code) {
+    switch (code) {
+    case MLGPU_ERR_OUT_OF_RANGE:
+        return "a photon's wavelength is outside the argument range of a surface "
+               "property table (Func1 limits [x_first, x_last))";
+    case MLGPU_ERR_RUNTIME:
+        return "a photon consumed more uniforms than its replay stream holds";
+    default:
+        return "device-side error";
+    }
+}
+
+}  // namespace
+
+extern "C" {
+
+int mlgpu_abi_version(void) { return MLGPU_ABI_VERSION; }
+
+int mlgpu_last_error(char* buffer, size_t buffer_size) {
+    if (!buffer || buffer_size == 0) return (int)g_last_error.size();
+    std::snprintf(buffer, buffer_size, "%s", g_last_error.c_str());
+    return (int)g_last_error.size();
+}
+
+int mlgpu_scene_create(const mlgpu_flat_scene* flat, mlgpu_scene** scene) {
+    if (!scene) return fail(MLGPU_ERR_INVALID_ARGUMENT, "scene out-pointer is NULL");
+    *scene = nullptr;
+    int st = validate(flat);
+    if (st) return st;
+    int count = 0;
+    if (cudaGetDeviceCount(&count) != cudaSuccess || count == 0)
+        return fail(MLGPU_ERR_NO_DEVICE, "no CUDA device is visible");
+    mlgpu_scene* s = new mlgpu_scene;
+    std::memset(&s->dev, 0, sizeof(s->dev));
+    cudaGetDevice(&s->device);
+    st = build_device_scene(s, flat);
+    if (st) {
+        mlgpu_scene_destroy(s);
+        return st;
+    }
+    *scene = s;
+    return MLGPU_OK;
+}
+
+int mlgpu_scene_destroy(mlgpu_scene* scene) {
+    if (!scene) return MLGPU_OK;
+    for (void* p : scene->owned) cudaFree(p);
+    scene->staging_in.release();
+    scene->staging_out.release();
+    scene->staging_hist.release();
+    scene->staging_rng.release();
+    scene->bin_scratch.release();
+    delete scene;
+    return MLGPU_OK;
+}
+
+int mlgpu_propagate(mlgpu_scene* scene, const mlgpu_photons* photons, uint64_t num_photons,
+                    const mlgpu_settings* settings, const mlgpu_rng* rng,
+                    mlgpu_results* results, void* cuda_stream) {
+    int st = check_propagate_args(scene, photons, settings, rng, results);
+    if (st) return st;
+    if (num_photons == 0) return MLGPU_OK;
+    const TraceArgs a = make_args(scene, photons, num_photons, settings, rng, results);
+    return launch(scene, a, settings, static_cast<cudaStream_t>(cuda_stream));
+}
+
+int mlgpu_scene_sync_errors(mlgpu_scene* scene, void* cuda_stream) {
+    if (!scene) return fail(MLGPU_ERR_INVALID_ARGUMENT, "scene is NULL");
+    cudaStream_t s = static_cast<cudaStream_t>(cuda_stream);
+    MLGPU_CUDA(cudaStreamSynchronize(s));
+    unsigned int code = 0;
+    MLGPU_CUDA(cudaMemcpy(&code, scene->error_word, sizeof(code), cudaMemcpyDeviceToHost));
+    if (code) {
+        MLGPU_CUDA(cudaMemset(scene->error_word, 0, sizeof(unsigned int)));
+        return fail((int)code, "%s", device_error_text(code));
+    }
+    return MLGPU_OK;
+}
+
+int mlgpu_propagate_host(mlgpu_scene* scene, const mlgpu_photons* photons, uint64_t n,
+                         const mlgpu_settings* settings, const mlgpu_rng* rng,
+                         mlgpu_results* results) {
+    int st = check_propagate_args(scene, photons, settings, rng, results);
+    if (st) return st;
+    if (n == 0) return MLGPU_OK;
+    const size_t ein = photons->dtype == MLGPU_F64 ? 8 : 4;
+    const size_t eout = results->dtype == MLGPU_F64 ? 8 : 4;
+    const size_t hist_len = settings->max_num_interactions_per_photon + 1;
+    // input planes, then output planes laid out one after another
+    MLGPU_CUDA(scene->staging_in.reserve(7*ein*n));
+    const size_t out_bytes = n*(4 + 2*eout + 8 + 2*eout + 4 + 4 + 3*8 + 3*8);
+    MLGPU_CUDA(scene->staging_out.reserve(out_bytes));
+    if (results->history)
+        MLGPU_CUDA(scene->staging_hist.reserve(n*hist_len*sizeof(mlgpu_history_entry)));
+    char* din = static_cast<char*>(scene->staging_in.ptr);
+    const void* planes[7] = {photons->support_x, photons->support_y, photons->support_z,
+                             photons->direction_x, photons->direction_y, photons->direction_z,
+                             photons->wavelength};
+    mlgpu_photons dph = *photons;
+    const void** dplanes[7] = {&dph.support_x, &dph.support_y, &dph.support_z,
+                               &dph.direction_x, &dph.direction_y, &dph.direction_z,
+                               &dph.wavelength};
+    cudaStream_t stream = 0;
+    for (int k = 0; k < 7; k++) {
+        MLGPU_CUDA(cudaMemcpyAsync(din + k*ein*n, planes[k], ein*n, cudaMemcpyHostToDevice, stream));
+        *dplanes[k] = din + k*ein*n;
+    }
+    dph.simulation_truth_id = nullptr;
+    mlgpu_rng drng = *rng;
+    if (rng->mode == MLGPU_RNG_REPLAY) {
+        const size_t ub = n*(size_t)rng->stride*sizeof(double);
+        MLGPU_CUDA(scene->staging_rng.reserve(ub));
+        MLGPU_CUDA(cudaMemcpyAsync(scene->staging_rng.ptr, rng->uniforms, ub,
+                                   cudaMemcpyHostToDevice, stream));
+        drng.uniforms = static_cast<const double*>(scene->staging_rng.ptr);
+    }
+    char* dout = static_cast<char*>(scene->staging_out.ptr);
+    mlgpu_results dres;
+    std::memset(&dres, 0, sizeof(dres));
+    dres.dtype = results->dtype;
+    size_t off = 0;
+    auto take = [&](const void* host, size_t bytes) -> void* {
+        if (!host) return nullptr;
+        void* p = dout + off;
+        off += (bytes + 255) & ~size_t(255);
+        return p;
+    };
+    // (re-laid out with 256-byte alignment; reserve enough)
+    MLGPU_CUDA(scene->staging_out.reserve(out_bytes + 16*256));
+    dout = static_cast<char*>(scene->staging_out.ptr);
+    dres.sensor = static_cast<int32_t*>(take(results->sensor, 4*n));
+    dres.x = take(results->x, eout*n);
+    dres.y = take(results->y, eout*n);
+    dres.time = static_cast<double*>(take(results->time, 8*n));
+    dres.theta_x = take(results->theta_x, eout*n);
+    dres.theta_y = take(results->theta_y, eout*n);
+    dres.final_leaf = static_cast<int32_t*>(take(results->final_leaf, 4*n));
+    dres.info = static_cast<uint32_t*>(take(results->info, 4*n));
+    dres.final_position = static_cast<double*>(take(results->final_position, 24*n));
+    dres.final_direction = static_cast<double*>(take(results->final_direction, 24*n));
+    dres.history = results->history
+        ? static_cast<mlgpu_history_entry*>(scene->staging_hist.ptr) : nullptr;
+    const TraceArgs a = make_args(scene, &dph, n, settings, &drng, &dres);
+    st = launch(scene, a, settings, stream);
+    if (st) return st;
+    struct Back { void* host; const void* dev; size_t bytes; };
+    const Back back[] = {
+        {results->sensor, dres.sensor, 4*n}, {results->x, dres.x, eout*n},
+        {results->y, dres.y, eout*n}, {results->time, dres.time, 8*n},
+        {results->theta_x, dres.theta_x, eout*n}, {results->theta_y, dres.theta_y, eout*n},
+        {results->final_leaf, dres.final_leaf, 4*n}, {results->info, dres.info, 4*n},
+        {results->final_position, dres.final_position, 24*n},
+        {results->final_direction, dres.final_direction, 24*n},
+        {results->history, dres.history, n*hist_len*sizeof(mlgpu_history_entry)},
+    };
+    for (const Back& b : back)
+        if (b.host) MLGPU_CUDA(cudaMemcpyAsync(b.host, b.dev, b.bytes, cudaMemcpyDeviceToHost, stream));
+    return mlgpu_scene_sync_errors(scene, stream);
+}
+
+int mlgpu_bin_arrivals(mlgpu_scene* scene, const int32_t* sensor, const double* time,
+                       uint64_t n, uint32_t* counts, uint32_t* time_hist,
+                       uint32_t num_time_bins, double t_min, double t_max,
+                       void* cuda_stream) {
+    if (!scene || !sensor || !counts)
+        return fail(MLGPU_ERR_INVALID_ARGUMENT, "NULL argument");
+    if (num_time_bins > 0 && (!time || !time_hist || !(t_max > t_min)))
+        return fail(MLGPU_ERR_INVALID_ARGUMENT, "time histogram needs times, output and t_max > t_min");
+    const uint64_t keys = (uint64_t)scene->dev.num_sensors * (num_time_bins + 1ull);
+    if (keys >= (1ull << 31))
+        return fail(MLGPU_ERR_INVALID_ARGUMENT, "too many sensor x time bins");
+    // partial histograms: one slice of `keys` words per photon slice
+    const size_t slices = 32;
+    MLGPU_CUDA(scene->bin_scratch.reserve(slices*keys*sizeof(uint32_t) + 256));
+    const cudaError_t e = launch_bin_arrivals(
+        scene->dev, sensor, time, n, counts, num_time_bins ? time_hist : nullptr,
+        num_time_bins, t_min, t_max, static_cast<uint32_t*>(scene->bin_scratch.ptr),
+        scene->bin_scratch.bytes / sizeof(uint32_t), static_cast<cudaStream_t>(cuda_stream));
+    if (e != cudaSuccess) return cuda_fail(e, "binning kernels");
+    return MLGPU_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,113 @@
+// mlgpu_internal.h -- device-side scene layout and launch interfaces shared
+// by the kernels and the C ABI implementation.
+#ifndef MLGPU_INTERNAL_H_
+#define MLGPU_INTERNAL_H_
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "merlict_b200.h"
+
+namespace mlgpu {
+
+// One leaf surface in 256 bytes (two 128-byte lines): the 3x4 frame-to-world
+// transform, the translation part of its inverse, primitive parameters, the
+// squared bounding radius and the surface's property-table ids.
+struct __align__(256) LeafRec {
+    double T[12];          // rows of the 3x4 homogeneous transform
+    double tinv[3];        // T00*T03 + T10*T13 + T20*T23, ... (HomTra3.cpp:200-216)
+    double params[MLGPU_LEAF_PARAMS];
+    double r2;             // bounding sphere radius squared
+    int32_t primitive;
+    int32_t sensor;
+    int32_t allowed_node;
+    int32_t flags;
+    int32_t fn[6];         // outer/inner reflection, refraction, absorption
+    int32_t pad[2];
+};
+static_assert(sizeof(LeafRec) == 256, "LeafRec must be 256 bytes");
+
+// FP32 image of a leaf for the batched tracer: transform relative to the
+// leaf's own origin, parameters in float, 128 bytes.
+struct __align__(128) LeafRecF {
+    float R[9];            // rotation rows
+    float params[MLGPU_LEAF_PARAMS];
+    float r2;
+    int32_t primitive;
+    int32_t sensor;
+    int32_t allowed_node;
+    int32_t flags;
+    int32_t fn[6];
+    int32_t pad[2];
+};
+static_assert(sizeof(LeafRecF) == 128, "LeafRecF must be 128 bytes");
+
+struct DevScene {
+    const double4* node;        // x, y, z, radius^2
+    const int2* node_meta;      // skip, leaf
+    const LeafRec* leaf;
+    const double* fn_points;    // (x, y, slope) triplets
+    const int32_t* fn_offset;
+    // FP32 copies for the batched tracer
+    const float4* node_f;       // x, y, z (relative to the scene origin), radius^2 (rounded up)
+    const LeafRecF* leaf_f;
+    const double* leaf_origin;  // [num_leaves][3] translation of each leaf, FP64
+    const float* fn_points_f;
+    int32_t num_nodes;
+    int32_t num_leaves;
+    int32_t num_functions;
+    int32_t default_refraction;
+    int32_t num_sensors;
+    double hex_u[3], hex_v[3], hex_w[3];
+    unsigned int* error_word;   // first device-side error code
+};
+
+struct DevPhotons {
+    const void* sx; const void* sy; const void* sz;
+    const void* dx; const void* dy; const void* dz;
+    const void* wavelength;
+};
+
+struct DevResults {
+    int32_t* sensor;
+    void* x; void* y;
+    double* time;
+    void* theta_x; void* theta_y;
+    int32_t* final_leaf;
+    uint32_t* info;
+    double* final_position;
+    double* final_direction;
+    mlgpu_history_entry* history;
+};
+
+struct DevRng {
+    int32_t mode;
+    uint32_t stride;
+    uint64_t seed;
+    uint64_t photon_offset;
+    const double* uniforms;
+};
+
+struct TraceArgs {
+    DevScene scene;
+    DevPhotons photons;
+    int32_t in_dtype;
+    DevResults results;
+    int32_t out_dtype;
+    DevRng rng;
+    uint64_t num_photons;
+    uint32_t max_interactions;
+    int32_t start_node;
+};
+
+cudaError_t launch_trace_fp64(const TraceArgs& a, int block, cudaStream_t s);
+cudaError_t launch_trace_fp32(const TraceArgs& a, int block, bool pure, cudaStream_t s);
+cudaError_t launch_bin_arrivals(const DevScene& sc, const int32_t* sensor,
+                                const double* time, uint64_t n, uint32_t* counts,
+                                uint32_t* time_hist, uint32_t num_bins,
+                                double t_min, double t_max, uint32_t* scratch,
+                                size_t scratch_words, cudaStream_t s);
+
+}  // namespace mlgpu
+
+#endif  // MLGPU_INTERNAL_H_

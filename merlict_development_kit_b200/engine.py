@@ -1,0 +1,201 @@
+"""Device scene and propagation calls over the engine's C ABI.
+
+PyTorch provides device memory and streams; the work is done by the CUDA
+kernels in libmerlict_b200.so.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass
+
+import numpy as np
+import torch
+
+from . import abi
+from ._native import check, lib
+from .photons import PLANES
+
+TRACERS = {"fp64": abi.TRACER_FP64, "fp32": abi.TRACER_FP32, "fp32_pure": abi.TRACER_FP32_PURE}
+
+
+@dataclass
+class PropagationConfig:
+    """merlict::PropagationConfig (merlict/PropagationConfig.h:10-13)."""
+    max_num_interactions_per_photon: int = 5
+
+
+class Philox:
+    """Counter-based generator: photon i of a call draws from stream
+    (photon_offset + i) of key `seed`.  Stands in for merlict's
+    random::Generator on the device."""
+
+    def __init__(self, seed: int = 0, photon_offset: int = 0):
+        self.seed = int(seed) & 0xFFFFFFFFFFFFFFFF
+        self.photon_offset = int(photon_offset)
+
+    def _struct(self, n: int):
+        r = abi.mlgpu_rng()
+        r.mode = abi.RNG_PHILOX
+        r.seed = self.seed
+        r.photon_offset = self.photon_offset
+        return r, None
+
+    def advance(self, n: int) -> None:
+        self.photon_offset += int(n)
+
+
+class Replay:
+    """Replays recorded uniforms: photon i consumes uniforms[i, k], k = 0, 1,
+    ... (an exhausted row is an error)."""
+
+    def __init__(self, uniforms):
+        self.uniforms = uniforms
+
+    def _struct(self, n: int):
+        u = self.uniforms
+        if not isinstance(u, torch.Tensor):
+            u = torch.as_tensor(np.ascontiguousarray(u, dtype=np.float64))
+        u = u.to(device="cuda", dtype=torch.float64).contiguous()
+        if u.dim() != 2 or u.shape[0] < n:
+            raise ValueError("replay uniforms must have shape [num_photons, stride]")
+        r = abi.mlgpu_rng()
+        r.mode = abi.RNG_REPLAY
+        r.stride = int(u.shape[1])
+        r.uniforms = u.data_ptr()
+        return r, u
+
+    def advance(self, n: int) -> None:
+        pass
+
+
+def _stream_handle(stream) -> int:
+    s = stream if stream is not None else torch.cuda.current_stream()
+    return int(s.cuda_stream)
+
+
+def photons_to_device(batch: dict, dtype=torch.float64) -> dict:
+    """Copies a photon batch (numpy or torch) to the current CUDA device."""
+    out = {}
+    for k in PLANES:
+        v = batch[k]
+        t = v if isinstance(v, torch.Tensor) else torch.from_numpy(np.ascontiguousarray(v))
+        out[k] = t.to(device="cuda", dtype=dtype, non_blocking=True).contiguous()
+    if batch.get("id") is not None:
+        v = batch["id"]
+        t = v if isinstance(v, torch.Tensor) else torch.from_numpy(np.ascontiguousarray(v))
+        out["id"] = t.to(device="cuda", dtype=torch.int32).contiguous()
+    return out
+
+
+class Scene:
+    """A flattened frame tree resident on the current CUDA device."""
+
+    def __init__(self, flat: abi.FlatScene):
+        if not torch.cuda.is_available():
+            raise RuntimeError("merlict_development_kit_b200 needs a CUDA device")
+        torch.cuda.init()
+        flat.validate()
+        self.flat = flat
+        self._struct = flat.as_struct()
+        h = C.c_void_p()
+        check(lib().mlgpu_scene_create(C.byref(self._struct), C.byref(h)))
+        self._h = h
+        self.num_sensors = flat.num_sensors
+
+    def close(self) -> None:
+        if getattr(self, "_h", None) is not None and self._h.value:
+            lib().mlgpu_scene_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def handle(self):
+        return self._h
+
+    def propagate(self, photons: dict, config: PropagationConfig | None = None,
+                  rng=None, tracer: str = "fp64", start_node: int = 0,
+                  outputs=("sensor", "x", "y", "time"), history: bool = False,
+                  out_dtype=torch.float64, stream=None, sync: bool = True,
+                  results: dict | None = None) -> dict:
+        """Traces a batch of device-resident photons.
+
+        `photons` is a dict of CUDA tensors (see photons.PLANES).  Returns a
+        dict of CUDA tensors with the requested outputs.  With sync=True the
+        call waits and raises on device-side errors (a wavelength outside a
+        property table raises IndexError, like merlict's std::out_of_range).
+        """
+        config = config or PropagationConfig()
+        rng = rng if rng is not None else Philox(0)
+        n = int(photons["wavelength"].shape[0])
+        in_dtype = photons["wavelength"].dtype
+        ph = abi.mlgpu_photons()
+        ph.dtype = abi.F64 if in_dtype == torch.float64 else abi.F32
+        for k in PLANES:
+            t = photons[k]
+            if t.dtype != in_dtype or not t.is_cuda or not t.is_contiguous() or t.shape[0] != n:
+                raise ValueError(f"photon plane {k} must be a contiguous CUDA tensor of {in_dtype}")
+            setattr(ph, k, t.data_ptr())
+        dev = photons["wavelength"].device
+        res = abi.mlgpu_results()
+        res.dtype = abi.F64 if out_dtype == torch.float64 else abi.F32
+        out = {} if results is None else results
+        spec = {
+            "sensor": ((n,), torch.int32), "x": ((n,), out_dtype), "y": ((n,), out_dtype),
+            "time": ((n,), torch.float64), "theta_x": ((n,), out_dtype),
+            "theta_y": ((n,), out_dtype), "final_leaf": ((n,), torch.int32),
+            "info": ((n,), torch.int32), "final_position": ((n, 3), torch.float64),
+            "final_direction": ((n, 3), torch.float64),
+        }
+        wanted = set(outputs) | {"sensor"}
+        for k, (shape, dt) in spec.items():
+            if k in wanted:
+                if k not in out or out[k].shape[0] < n:
+                    out[k] = torch.empty(shape, dtype=dt, device=dev)
+                setattr(res, k, out[k].data_ptr())
+        if history:
+            m = config.max_num_interactions_per_photon + 1
+            out["history"] = torch.empty((n, m, abi.HISTORY_DTYPE.itemsize), dtype=torch.uint8, device=dev)
+            res.history = out["history"].data_ptr()
+        st = abi.mlgpu_settings(int(config.max_num_interactions_per_photon), int(start_node),
+                                TRACERS[tracer], 0)
+        r, keep = rng._struct(n)
+        sh = _stream_handle(stream)
+        check(lib().mlgpu_propagate(self._h, C.byref(ph), n, C.byref(st), C.byref(r),
+                                    C.byref(res), C.c_void_p(sh)))
+        rng.advance(n)
+        if sync:
+            check(lib().mlgpu_scene_sync_errors(self._h, C.c_void_p(sh)))
+        del keep
+        return out
+
+    def sync_errors(self, stream=None) -> None:
+        check(lib().mlgpu_scene_sync_errors(self._h, C.c_void_p(_stream_handle(stream))))
+
+    def bin_arrivals(self, sensor: torch.Tensor, time: torch.Tensor | None = None,
+                     num_time_bins: int = 0, t_min: float = 0.0, t_max: float = 1.0,
+                     stream=None):
+        """Per-sensor counts (and time histograms) of device results."""
+        n = int(sensor.shape[0])
+        counts = torch.empty(self.num_sensors, dtype=torch.int32, device=sensor.device)
+        hist = None
+        tp = None
+        if num_time_bins:
+            hist = torch.empty((self.num_sensors, num_time_bins), dtype=torch.int32,
+                               device=sensor.device)
+            tp = time.data_ptr()
+        check(lib().mlgpu_bin_arrivals(
+            self._h, C.c_void_p(sensor.data_ptr()), C.c_void_p(tp), n,
+            C.c_void_p(counts.data_ptr()), C.c_void_p(hist.data_ptr() if hist is not None else None),
+            int(num_time_bins), float(t_min), float(t_max), C.c_void_p(_stream_handle(stream))))
+        return counts, hist
+
+
+def history_to_numpy(h: torch.Tensor) -> np.ndarray:
+    """Device history bytes -> structured numpy array of mlgpu_history_entry."""
+    a = h.cpu().numpy()
+    return a.view(abi.HISTORY_DTYPE).reshape(a.shape[0], a.shape[1])

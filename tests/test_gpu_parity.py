@@ -1,0 +1,141 @@
+"""GPU parity: the CUDA FP64 tracer against the reference's own outputs
+(golden fixtures) and against the CPU oracle, through the C ABI."""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+from conftest import golden_names, load_golden
+from parity import history_mismatches, mismatches
+
+pytestmark = pytest.mark.gpu
+
+ALL_OUTPUTS = ("sensor", "x", "y", "time", "theta_x", "theta_y", "final_leaf", "info",
+               "final_position", "final_direction")
+
+
+@pytest.fixture(scope="module")
+def eng():
+    import torch
+    assert torch.cuda.is_available(), "GPU tests need a CUDA device"
+    from merlict_development_kit_b200 import engine
+    return engine
+
+
+def run_gpu(eng, flat, photons, max_int, seed=0, uniforms=None, history=False,
+            tracer="fp64", outputs=ALL_OUTPUTS):
+    scene = eng.Scene(flat)
+    dev = eng.photons_to_device(photons)
+    rng = eng.Replay(uniforms) if uniforms is not None else eng.Philox(seed)
+    out = scene.propagate(dev, eng.PropagationConfig(max_int), rng, tracer=tracer,
+                          outputs=outputs, history=history)
+    got = {k: v.cpu().numpy() for k, v in out.items() if k != "history"}
+    if "info" in got:
+        got["info"] = got["info"].view(np.uint32)
+    if history:
+        got["history"] = eng.history_to_numpy(out["history"])
+    scene.close()
+    return got
+
+
+@pytest.mark.parametrize("name", golden_names())
+def test_fp64_tracer_matches_reference_bit_for_bit(eng, name):
+    flat, photons, ref, meta = load_golden(name)
+    got = run_gpu(eng, flat, photons, meta["max_interactions"], seed=meta["seed"],
+                  uniforms=meta["uniforms"], history=True)
+    assert mismatches(ref, got) == {}
+    assert history_mismatches(ref["history"], got["history"]) == {}
+
+
+@pytest.mark.parametrize("name,n", [("reflector_camera", 200_000),
+                                    ("light_field_small", 100_000),
+                                    ("primitive_zoo", 200_000)])
+def test_fp64_tracer_matches_oracle_on_larger_batches(eng, oracle, name, n):
+    from merlict_development_kit_b200 import photons as P
+    flat, _, _, meta = load_golden(name)
+    if name == "primitive_zoo":
+        ph = P.isotropic_shell_source(n, 123, 4.0, 2.5)
+    elif name == "light_field_small":
+        ph = P.downward_disc_source(n, 123, 5.55, 21.4, 0.5)
+    else:
+        ph = P.downward_disc_source(n, 123, 2.0, 10.0, 1.5)
+    status, ref, _ = oracle.propagate(flat, ph, meta["max_interactions"], seed=77)
+    assert status == 0
+    got = run_gpu(eng, flat, ph, meta["max_interactions"], seed=77)
+    assert mismatches(ref, got) == {}
+
+
+def test_propagate_host_entry_point(eng):
+    """mlgpu_propagate_host: host buffers in and out, as the C++ shim calls it."""
+    from merlict_development_kit_b200 import _native, abi
+    from oracle.oracle import _photon_struct, alloc_results
+    flat, photons, ref, meta = load_golden("reflector_camera")
+    scene = eng.Scene(flat)
+    ps, keep = _photon_struct(photons)
+    n = len(photons["wavelength"])
+    rs, out = alloc_results(n, meta["max_interactions"], history=True)
+    st = abi.mlgpu_settings(meta["max_interactions"], 0, abi.TRACER_FP64, 0)
+    rng = abi.mlgpu_rng()
+    rng.mode = abi.RNG_PHILOX
+    rng.seed = meta["seed"]
+    _native.check(_native.lib().mlgpu_propagate_host(scene.handle, C.byref(ps), n, C.byref(st),
+                                                     C.byref(rng), C.byref(rs)))
+    assert mismatches(ref, out) == {}
+    assert history_mismatches(ref["history"], out["history"]) == {}
+
+
+def test_wavelength_outside_property_table_raises(eng):
+    flat, photons, ref, meta = load_golden("mirror_absorber")
+    ph = {k: v.copy() for k, v in photons.items()}
+    ph["wavelength"][:] = 1500e-9
+    with pytest.raises(IndexError):
+        run_gpu(eng, flat, ph, 5, seed=1)
+    # the scene stays usable afterwards
+    got = run_gpu(eng, flat, photons, 5, seed=meta["seed"])
+    assert mismatches(ref, got) == {}
+
+
+def test_exhausted_replay_stream_raises(eng):
+    flat, photons, ref, meta = load_golden("reflector_camera_replay")
+    with pytest.raises(Exception):
+        run_gpu(eng, flat, photons, 5, uniforms=meta["uniforms"][:, :1])
+
+
+def test_known_answer_statistics(eng):
+    """PhotonTest.cpp:84-302 on 1e5 photons each."""
+    from merlict_development_kit_b200 import photons as P
+    n = 100_000
+    flat, *_ = load_golden("mirror_absorber")
+    ph = P.make_batch(np.tile([-2.0, 0, 0], (n, 1)), np.tile([1.0, 0, 0], (n, 1)),
+                      np.arange(1, n + 1) / n * 100e-9 + 250e-9)
+    got = run_gpu(eng, flat, ph, 5, seed=5, outputs=("sensor",))
+    assert abs((got["sensor"] >= 0).mean() - 0.42) < 0.02
+    flat, *_ = load_golden("water_box")
+    ph = P.make_batch(np.zeros((n, 3)), np.tile([0, 0, 1.0], (n, 1)), np.full(n, 433e-9))
+    got = run_gpu(eng, flat, ph, 5, seed=6, outputs=("sensor", "time"))
+    hit = got["sensor"] >= 0
+    assert abs(hit.mean() - 0.95) < 0.02
+    assert abs(got["time"][hit].mean() - (2.0 + 1.33) / 299792458.0) < 1e-10
+    flat, *_ = load_golden("absorbing_box")
+    got = run_gpu(eng, flat, ph, 5, seed=7, outputs=("sensor",))
+    assert abs((got["sensor"] >= 0).mean() - 0.367) < 0.02
+
+
+def test_bin_arrivals_matches_oracle(eng, oracle):
+    import torch
+    from merlict_development_kit_b200 import photons as P
+    flat, _, _, meta = load_golden("light_field_small")
+    ph = P.downward_disc_source(300_000, 9, 5.55, 21.4, 0.5)
+    scene = eng.Scene(flat)
+    out = scene.propagate(eng.photons_to_device(ph), eng.PropagationConfig(10), eng.Philox(3),
+                          outputs=("sensor", "time"))
+    t = out["time"][out["sensor"] >= 0]
+    t0, t1 = float(t.min()) - 1e-12, float(t.max()) + 1e-12
+    counts, hist = scene.bin_arrivals(out["sensor"], out["time"], 16, t0, t1)
+    ref_counts, ref_hist = oracle.bin_arrivals(out["sensor"].cpu().numpy(), out["time"].cpu().numpy(),
+                                               flat.num_sensors, 16, t0, t1)
+    assert np.array_equal(counts.cpu().numpy().astype(np.uint32), ref_counts)
+    assert np.array_equal(hist.cpu().numpy().astype(np.uint32), ref_hist)
+    counts2, _ = scene.bin_arrivals(out["sensor"])
+    assert np.array_equal(counts2.cpu().numpy().astype(np.uint32), ref_counts)
+    torch.cuda.synchronize()
