@@ -1,0 +1,390 @@
+"""Benchmark: photons/s of the propagation hot path on the light-field
+telescope scene (the refraction-heavy configuration: a 252-facet f=10.7 m
+Davies-Cotton reflector with a light-field sensor of 1039 bi-convex lenses
+and 63,379 hexagonal lixels in its focal plane).
+
+One step = propagate one batch of photons (supports uniform on a 5.55 m
+disc 21.4 m above the dish, directions within 1.5 degrees of -z, wavelength
+300-700 nm, max. 10 interactions) and bin the arrivals per lixel.
+
+    python bench.py [--gpus N --steps K --warmup W] [--impl reference]
+                    [--tracer fp64|fp32] [--photons P]
+
+For N > 1 it runs under torch.distributed.run, one process per GPU; every
+rank traces its own batch (weak scaling) and the step time is the maximum
+over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+REPO = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, REPO)
+
+SCENE = dict(focal_length=10.7, aperture_radius=5.35, fov_deg=6.5, pixel_fov_deg=0.186,
+             paxels_on_diagonal=9, housing_overhead=1.1, reflectivity=0.9)
+SOURCE = dict(disc_radius=5.55, height=21.4, max_zenith_deg=1.5)
+MAX_INTERACTIONS = 10
+# algorithmic HBM bytes per photon: in 7 x f64 + id (60 B), out sensor id,
+# x, y, time (28 B); FP32 form: in 7 x f32 + id (32 B), out id + x, y f32 +
+# time f64 (20 B)
+BYTES_PER_PHOTON = {"fp64": 88, "fp32": 52}
+# FLOP weights of the operation counts (nodes tested, leaves transformed,
+# cap quadratics, cap bounds, plane tests, other quadrics, reflections,
+# Fresnel steps, time-of-flight segments, table look-ups)
+FLOP_WEIGHTS = {"nodes": 26, "leaves": 48, "caps": 29, "cap_bounds": 85, "planes": 36,
+                "others": 29, "reflections": 91, "fresnels": 110, "segments": 3, "funcs": 4}
+FP64_PEAK_TFLOPS_NOMINAL = 37.0   # B200 vector FP64, nominal (no measured figure)
+FP32_PEAK_TFLOPS_NOMINAL = 75.0   # B200 vector FP32 (non-tensor), nominal
+WORKLOAD = "light-field telescope, 1039 lenses x 61 lixels (config 1)"
+
+
+def scene_config_name():
+    return (f"f{SCENE['focal_length']}m_R{SCENE['aperture_radius']}m_fov{SCENE['fov_deg']}deg_"
+            f"pix{SCENE['pixel_fov_deg']}deg")
+
+
+def make_photons(n: int, seed: int):
+    from merlict_development_kit_b200 import photons as P
+    return P.downward_disc_source(n, seed, SOURCE["disc_radius"], SOURCE["height"],
+                                  SOURCE["max_zenith_deg"])
+
+
+def load_peaks():
+    p = os.path.join(REPO, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return d.get("hbm_gbs", 6650.0), "measured"
+    return 6650.0, "fallback"
+
+
+def flop_counts():
+    p = os.path.join(REPO, "tests", "golden", "flop_counts.json")
+    if not os.path.exists(p):
+        return None
+    with open(p) as f:
+        return json.load(f)
+
+
+class ClockSampler:
+    """nvidia-smi samples of SM clock and throttle reasons while running."""
+
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.QUERY}",
+                 "--format=csv,noheader,nounits", "-lms", "100"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except (OSError, FileNotFoundError):
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        time.sleep(0.15)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.lines:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax.append(float(parts[2]))
+            except ValueError:
+                continue
+            for name, flag in zip(names, parts[5:9]):
+                if flag.lower() == "active":
+                    reasons.add(name)
+        return {"sm_mhz": float(np.median(sm)) if sm else None,
+                "sm_max_mhz": max(smax) if smax else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def init_dist():
+    import torch
+    import torch.distributed as dist
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1 and not dist.is_initialized():
+        backend = "nccl" if torch.cuda.is_available() else "gloo"
+        from datetime import timedelta
+        dist.init_process_group(backend=backend, timeout=timedelta(seconds=120))
+    return world, rank, local
+
+
+def max_over_ranks(x: float, world: int) -> float:
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    dev = "cuda" if torch.cuda.is_available() and dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([x], dtype=torch.float64, device=dev)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(world: int):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+# ---- reference arm ------------------------------------------------------------
+
+def cpu_reference_run(photons_per_step: int, steps: int, warmup: int, threads_mode: str = "multi"):
+    """The reference's own multi-threaded CPU path (merlict_multi_thread) plus
+    Sensors::assign_photons, on the same scene built by the reference's own
+    factories; returns (photons/s, seconds, cores, kind, sample)."""
+    from oracle import oracle as O
+    if O.harness_available():
+        scene = O.RefScene("light_field_sensor",
+                           (SCENE["focal_length"], SCENE["aperture_radius"], SCENE["fov_deg"],
+                            SCENE["pixel_fov_deg"], SCENE["paxels_on_diagonal"],
+                            SCENE["housing_overhead"], SCENE["reflectivity"]))
+        mode = O.REFERENCE_MULTI_THREAD if threads_mode == "multi" else O.REFERENCE_SINGLE_THREAD
+        cores = scene.lib.ref_hardware_concurrency() if threads_mode == "multi" else 1
+        secs = []
+        for k in range(warmup + steps):
+            ph = make_photons(photons_per_step, 1000 + k)
+            _, _, sec = scene.propagate(ph, MAX_INTERACTIONS, mode, seed=1 + k, results=False)
+            if k >= warmup:
+                secs.append(sec)
+        total = float(sum(secs))
+        return photons_per_step * steps / total, total, cores, "reference", \
+            f"{steps} x {photons_per_step} photons, reference merlict_multi_thread + assign_photons"
+    # the C restatement when the reference library is not built here
+    from merlict_development_kit_b200 import factories as F
+    flat = F.light_field_telescope(**SCENE).flatten()
+    o = O.Oracle()
+    secs = []
+    for k in range(warmup + steps):
+        ph = make_photons(photons_per_step, 1000 + k)
+        t0 = time.perf_counter()
+        o.propagate(flat, ph, MAX_INTERACTIONS, seed=1 + k)
+        if k >= warmup:
+            secs.append(time.perf_counter() - t0)
+    total = float(sum(secs))
+    return photons_per_step * steps / total, total, 1, "port", \
+        f"{steps} x {photons_per_step} photons, C restatement, 1 thread"
+
+
+def run_reference_arm(args, world, rank):
+    if rank != 0:
+        return
+    per_step = args.ref_photons
+    value, secs, cores, kind, sample = cpu_reference_run(per_step, args.steps, args.warmup)
+    line = {
+        "metric": "photons/s", "value": value, "unit": "photons/s", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": 1e3 * secs / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "impl": "reference",
+        "config": {"workload": WORKLOAD, "scene": scene_config_name(),
+                   "photons_per_step": per_step, "max_interactions": MAX_INTERACTIONS},
+        "cpu_baseline": {"value": value, "unit": "photons/s", "cores": cores, "kind": kind,
+                         "sample": sample},
+        "e2e": {"value": value, "unit": "photons/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+# ---- our arm ------------------------------------------------------------------
+
+def run_ours(args, world, rank, local):
+    import torch
+    from merlict_development_kit_b200 import engine, factories as F, _native
+    import ctypes as C
+    from merlict_development_kit_b200 import abi
+
+    torch.cuda.set_device(local)
+    flat = F.light_field_telescope(**SCENE).flatten()
+    scene = engine.Scene(flat)
+    n = args.photons
+    tracer = args.tracer
+    in_dtype = torch.float64 if tracer == "fp64" else torch.float32
+    host = make_photons(n, 12345 + rank)
+    dev = engine.photons_to_device(host, dtype=in_dtype)
+    out_dtype = torch.float64 if tracer == "fp64" else torch.float32
+    cfg = engine.PropagationConfig(MAX_INTERACTIONS)
+    rng = engine.Philox(seed=7 + rank)
+    stream = torch.cuda.current_stream()
+    results = {}
+    launches_per_step = 3   # trace + 2 binning kernels
+
+    def step(ev=None):
+        if ev is not None:
+            ev[0].record(stream)
+        out = scene.propagate(dev, cfg, rng, tracer=tracer, outputs=("sensor", "x", "y", "time"),
+                              out_dtype=out_dtype, sync=False, results=results)
+        if ev is not None:
+            ev[1].record(stream)
+        scene.bin_arrivals(out["sensor"])
+        return out
+
+    for _ in range(args.warmup):
+        step()
+    scene.sync_errors()
+    torch.cuda.synchronize()
+
+    kernel_events = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+                     for _ in range(args.steps)]
+    clocks = ClockSampler(local)
+    clocks.start()
+    barrier(world)
+    torch.cuda.synchronize()
+    t_start = torch.cuda.Event(enable_timing=True)
+    t_stop = torch.cuda.Event(enable_timing=True)
+    t_start.record(stream)
+    for k in range(args.steps):
+        step(kernel_events[k])
+    t_stop.record(stream)
+    torch.cuda.synchronize()
+    barrier(world)
+    clk = clocks.stop()
+    scene.sync_errors()
+    elapsed_ms = t_start.elapsed_time(t_stop)
+    kernel_ms = float(np.mean([a.elapsed_time(b) for a, b in kernel_events]))
+    elapsed_ms = max_over_ranks(elapsed_ms, world)
+    value = n * world * args.steps / (elapsed_ms * 1e-3)
+
+    # e2e: the C-ABI host-buffer call (H2D of the batch, trace, D2H of the
+    # results, synchronise), pinned host memory, same batch size
+    pin = {k: torch.from_numpy(np.ascontiguousarray(host[k])).to(in_dtype).pin_memory()
+           for k in ("support_x", "support_y", "support_z", "direction_x", "direction_y",
+                     "direction_z", "wavelength")}
+    ph = abi.mlgpu_photons()
+    ph.dtype = abi.F64 if in_dtype == torch.float64 else abi.F32
+    for k, t in pin.items():
+        setattr(ph, k, t.data_ptr())
+    h_sensor = torch.empty(n, dtype=torch.int32).pin_memory()
+    h_x = torch.empty(n, dtype=out_dtype).pin_memory()
+    h_y = torch.empty(n, dtype=out_dtype).pin_memory()
+    h_t = torch.empty(n, dtype=torch.float64).pin_memory()
+    res = abi.mlgpu_results()
+    res.dtype = abi.F64 if out_dtype == torch.float64 else abi.F32
+    res.sensor, res.x, res.y, res.time = (h_sensor.data_ptr(), h_x.data_ptr(), h_y.data_ptr(),
+                                          h_t.data_ptr())
+    st = abi.mlgpu_settings(MAX_INTERACTIONS, 0, engine.TRACERS[tracer], 0)
+    r = abi.mlgpu_rng()
+    r.mode = abi.RNG_PHILOX
+    r.seed = 99 + rank
+    L = _native.lib()
+    e2e_steps = max(1, min(args.steps, 5))
+    for _ in range(1):
+        _native.check(L.mlgpu_propagate_host(scene.handle, C.byref(ph), n, C.byref(st),
+                                             C.byref(r), C.byref(res)))
+    barrier(world)
+    t0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        _native.check(L.mlgpu_propagate_host(scene.handle, C.byref(ph), n, C.byref(st),
+                                             C.byref(r), C.byref(res)))
+    e2e_s = max_over_ranks(time.perf_counter() - t0, world)
+    e2e_value = n * world * e2e_steps / e2e_s
+    elt = 8 if in_dtype == torch.float64 else 4
+    eout = 8 if out_dtype == torch.float64 else 4
+    h2d = 7 * elt * n
+    d2h = (4 + 2 * eout + 8) * n
+
+    if rank != 0:
+        return
+    hbm_peak, peak_kind = load_peaks()
+    bpp = BYTES_PER_PHOTON[tracer]
+    achieved_gbs = bpp * n / (kernel_ms * 1e-3) / 1e9
+    roofline = {"bound": "hbm", "achieved": achieved_gbs, "peak": hbm_peak, "unit": "GB/s",
+                "frac": achieved_gbs / hbm_peak, "traffic": None,
+                "peak_source": f"{peak_kind} MEASURED_PEAKS.json hbm_gbs",
+                "bytes_per_photon": bpp}
+    counts = flop_counts()
+    compute = None
+    if counts:
+        per = counts["per_photon"]
+        flops = sum(FLOP_WEIGHTS[k] * per.get(k, 0.0) for k in FLOP_WEIGHTS)
+        peak = FP64_PEAK_TFLOPS_NOMINAL if tracer == "fp64" else FP32_PEAK_TFLOPS_NOMINAL
+        achieved = flops * n / (kernel_ms * 1e-3) / 1e12
+        compute = {"bound": "fp64" if tracer == "fp64" else "fp32", "flops_per_photon": flops,
+                   "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+                   "frac": achieved / peak, "peak_source": "nominal B200 vector peak"}
+    cpu = None
+    if world == 1 and not args.no_cpu_baseline:
+        v, secs, cores, kind, sample = cpu_reference_run(args.ref_photons, 2, 1)
+        cpu = {"value": v, "unit": "photons/s", "cores": cores, "kind": kind, "sample": sample}
+    line = {
+        "metric": "photons/s", "value": value, "unit": "photons/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": elapsed_ms / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64" if tracer == "fp64" else "f32",
+        "data": "synthetic",
+        "config": {"workload": WORKLOAD, "scene": scene_config_name(), "tracer": tracer,
+                   "photons_per_step_per_gpu": n, "max_interactions": MAX_INTERACTIONS,
+                   "l2": "inputs larger than L2 (photon planes %.0f MB)" % (7 * elt * n / 1e6)},
+        "kernel_ms": kernel_ms,
+        "roofline": roofline,
+        "compute_roofline": compute,
+        "cpu_baseline": cpu,
+        "e2e": {"value": e2e_value, "unit": "photons/s", "h2d_bytes_per_step": h2d,
+                "d2h_bytes_per_step": d2h},
+        "gpu_launches": launches_per_step * args.steps,
+        "clocks": clk,
+    }
+    print(json.dumps(line), flush=True)
+    scene.close()
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--tracer", choices=["fp64", "fp32"], default="fp64")
+    ap.add_argument("--photons", type=int, default=10_000_000)
+    ap.add_argument("--ref-photons", type=int, default=100_000)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    world, rank, local = init_dist()
+    try:
+        if args.impl == "reference":
+            run_reference_arm(args, world, rank)
+        else:
+            run_ours(args, world, rank, local)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+            if dist.is_initialized():
+                dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()
