@@ -166,6 +166,12 @@ def t_orientation(T, v):
 
 # ---- property tables, merlict/function/Func1.cpp ----------------------------
 
+def _ieee_div(a: float, b: float) -> float:
+    """a / b with IEEE semantics for b == 0 (inf or nan, as in C++)."""
+    with np.errstate(all="ignore"):
+        return float(np.float64(a) / np.float64(b))
+
+
 class Func1:
     """Piecewise-linear table over [x_first, x_last)."""
 
@@ -176,7 +182,8 @@ class Func1:
         pts = []
         for i, (x, y) in enumerate(rows):
             # slope from the table as given, before sorting (Func1.cpp:42-48)
-            slope = (y - rows[i + 1][1]) / (x - rows[i + 1][0]) if i != len(rows) - 1 else 0.0
+            slope = (_ieee_div(y - rows[i + 1][1], x - rows[i + 1][0])
+                     if i != len(rows) - 1 else 0.0)
             pts.append((x, y, slope))
         pts.sort(key=lambda p: p[0])
         for a, b in zip(pts, pts[1:]):
