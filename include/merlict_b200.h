@@ -277,6 +277,46 @@ int mlgpu_bin_arrivals(
     double t_max,
     void* cuda_stream);
 
+/* ---- allocation-free arrival binning ------------------------------------ *
+ * No counterpart in the reference (merlict bins arrivals on the host).
+ *
+ * The same counts and time histograms as mlgpu_bin_arrivals, for callers
+ * that must not allocate device memory once they are running: a host
+ * application whose GPU memory is handed out by its own pool or caching
+ * allocator (a cudaMalloc behind its back can exceed its fixed budget or
+ * fragment the pool), or an event loop with real-time deadlines, where
+ * cudaMalloc and cudaFree may synchronise the device and stall the other
+ * streams.  mlgpu_bin_arrivals grows a scratch buffer with cudaMalloc on
+ * demand; this entry point instead uses one fixed scratch array compiled
+ * into the library: MLGPU_NOALLOC_BIN_SCRATCH_WORDS 32-bit words (16 MiB)
+ * on every GPU that loads the library, held until the process exits.
+ *
+ * Limit: num_sensors x (num_time_bins + 1) must not exceed
+ * MLGPU_NOALLOC_BIN_SCRATCH_WORDS; larger requests return
+ * MLGPU_ERR_INVALID_ARGUMENT and do nothing.  The inputs and outputs are
+ * the caller's device buffers, as for mlgpu_bin_arrivals.
+ *
+ * The first call on a device looks up the array's device address (this
+ * may load the library's device code into the context); make that first
+ * call before any stream capture.  Every call overwrites all the scratch
+ * words it reads, so nothing carries over from one call to the next; but
+ * all calls on a device share the one array, so calls that overlap on the
+ * GPU (issued to different streams, or from threads without ordering
+ * between them) race and give wrong results.  Calls allocate nothing.   */
+#define MLGPU_NOALLOC_BIN_SCRATCH_WORDS (4u * 1024u * 1024u)
+
+int mlgpu_bin_arrivals_noalloc(
+    mlgpu_scene* scene,
+    const int32_t* sensor,
+    const double* time,
+    uint64_t num_photons,
+    uint32_t* counts,
+    uint32_t* time_hist,
+    uint32_t num_time_bins,
+    double t_min,
+    double t_max,
+    void* cuda_stream);
+
 #ifdef __cplusplus
 }  /* extern "C" */
 #endif

@@ -302,6 +302,14 @@ const char* device_error_text(unsigned int code) {
 
 }  // namespace
 
+namespace mlgpu {
+
+int report_error(int code, const char* message) { return fail(code, "%s", message); }
+
+const DevScene* device_scene(const mlgpu_scene* scene) { return &scene->dev; }
+
+}  // namespace mlgpu
+
 extern "C" {
 
 int mlgpu_abi_version(void) { return MLGPU_ABI_VERSION; }

@@ -108,6 +108,11 @@ cudaError_t launch_bin_arrivals(const DevScene& sc, const int32_t* sensor,
                                 double t_min, double t_max, uint32_t* scratch,
                                 size_t scratch_words, cudaStream_t s);
 
+// Records a message for mlgpu_last_error and returns `code` (capi.cu).
+int report_error(int code, const char* message);
+// The device scene of a handle (capi.cu).
+const DevScene* device_scene(const mlgpu_scene* scene);
+
 }  // namespace mlgpu
 
 #endif  // MLGPU_INTERNAL_H_

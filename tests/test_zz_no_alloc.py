@@ -1,0 +1,86 @@
+"""Allocation-free arrival binning, mlgpu_bin_arrivals_noalloc.
+
+Some callers of this library cannot allocate device memory once they are
+running: an application whose GPU memory is handed out by its own pool or
+caching allocator, or an event loop with real-time deadlines, where
+cudaMalloc/cudaFree may synchronise the device.  mlgpu_bin_arrivals grows its
+scratch with cudaMalloc; mlgpu_bin_arrivals_noalloc uses a fixed scratch
+array compiled into the library instead.  This file checks, through the C
+ABI, that it gives exactly the counts and time histograms of
+mlgpu_bin_arrivals on two calls in a row (integer counts: the tolerance is
+zero), and that a request beyond the fixed scratch is refused.
+
+The file is named so that pytest collects it last.
+"""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+from conftest import load_golden
+
+pytestmark = pytest.mark.gpu
+
+
+def call_noalloc(scene, sensor, time, counts, hist, bins, t0, t1):
+    import torch
+    from merlict_development_kit_b200 import _native
+    stream = torch.cuda.current_stream().cuda_stream
+    status = _native.lib().mlgpu_bin_arrivals_noalloc(
+        scene.handle, C.c_void_p(sensor.data_ptr()),
+        C.c_void_p(time.data_ptr() if time is not None else None), int(sensor.shape[0]),
+        C.c_void_p(counts.data_ptr()), C.c_void_p(hist.data_ptr() if hist is not None else None),
+        int(bins), float(t0), float(t1), C.c_void_p(stream))
+    return status
+
+
+def test_noalloc_binning_matches_the_allocating_entry_point_on_two_calls():
+    import torch
+    from merlict_development_kit_b200 import _native, engine, photons as P
+    flat, _, _, _ = load_golden("light_field_small")
+    scene = engine.Scene(flat)
+    ph = P.downward_disc_source(200_000, 21, 5.55, 21.4, 0.5)
+    out = scene.propagate(engine.photons_to_device(ph), engine.PropagationConfig(10),
+                          engine.Philox(8), outputs=("sensor", "time"))
+    sensor, time = out["sensor"], out["time"]
+    t = time[sensor >= 0]
+    t0, t1 = float(t.min()) - 1e-12, float(t.max()) + 1e-12
+    n_s = flat.num_sensors
+
+    # first call: counts and a 16-bin time histogram of all photons
+    ref_counts, ref_hist = scene.bin_arrivals(sensor, time, 16, t0, t1)
+    counts = torch.full((n_s,), -1, dtype=torch.int32, device="cuda")
+    hist = torch.full((n_s, 16), -1, dtype=torch.int32, device="cuda")
+    _native.check(call_noalloc(scene, sensor, time, counts, hist, 16, t0, t1))
+    torch.cuda.synchronize()
+    assert torch.equal(counts, ref_counts)
+    assert torch.equal(hist, ref_hist)
+
+    # second call, right after: counts only, of a different (half) batch, so
+    # anything left over in the shared scratch from the first call would show
+    half = sensor[: sensor.shape[0] // 2].contiguous()
+    ref_counts2, _ = scene.bin_arrivals(half)
+    counts2 = torch.full((n_s,), -1, dtype=torch.int32, device="cuda")
+    _native.check(call_noalloc(scene, half, None, counts2, None, 0, 0.0, 1.0))
+    torch.cuda.synchronize()
+    assert torch.equal(counts2, ref_counts2)
+    assert int(counts2.sum()) == int((half >= 0).sum())
+    assert not torch.equal(counts2, counts)
+    scene.close()
+
+
+def test_noalloc_binning_refuses_requests_beyond_its_fixed_scratch():
+    import torch
+    from merlict_development_kit_b200 import _native, abi, engine
+    flat, _, _, _ = load_golden("light_field_small")
+    scene = engine.Scene(flat)
+    limit = 4 * 1024 * 1024
+    bins = limit // flat.num_sensors + 1          # sensors x (bins + 1) > limit
+    sensor = torch.zeros(16, dtype=torch.int32, device="cuda")
+    time = torch.zeros(16, dtype=torch.float64, device="cuda")
+    counts = torch.zeros(flat.num_sensors, dtype=torch.int32, device="cuda")
+    hist = torch.zeros(1, dtype=torch.int32, device="cuda")
+    status = call_noalloc(scene, sensor, time, counts, hist, bins, 0.0, 1.0)
+    assert status == abi.ERR_INVALID_ARGUMENT
+    assert "fixed scratch" in _native.last_error()
+    scene.close()
