@@ -32,7 +32,7 @@
 extern "C" {
 #endif
 
-#define MLGPU_ABI_VERSION 1
+#define MLGPU_ABI_VERSION 2
 
 /* ---- status codes ------------------------------------------------------ */
 enum {
@@ -199,12 +199,24 @@ typedef struct mlgpu_rng {
     const double* uniforms;   /* device pointer (host for _host calls)    */
 } mlgpu_rng;
 
-/* Tracer forms. */
+/* Tracer forms.  Both FP64 forms reproduce merlict bit for bit; the
+ * wavefront forms run per-step kernels over a pool of ray slots and wait
+ * on the stream a few times per call to learn when the pool has drained. */
 enum {
-    MLGPU_TRACER_FP64 = 0,        /* plain FP64, replicates the reference bit for bit */
-    MLGPU_TRACER_FP32 = 1,        /* FP32 bulk math, FP64 where stability needs it   */
-    MLGPU_TRACER_FP32_PURE = 2    /* FP32 everywhere (precision study only)          */
+    MLGPU_TRACER_FP64 = 0,        /* wavefront, FP64                                  */
+    MLGPU_TRACER_FP32 = 1,        /* wavefront, FP32 bulk math, FP64 where needed     */
+    MLGPU_TRACER_FP32_PURE = 2,   /* FP32 everywhere (precision study only)           */
+    MLGPU_TRACER_FP64_PLAIN = 3   /* one thread per photon, FP64                      */
 };
+
+/* How candidate surfaces are found for a ray in the whole tree.
+ * BVH: a 4-wide bounding-volume hierarchy built at scene creation proposes
+ * candidates; each still passes merlict's own bounding-sphere test of the
+ * leaf and merlict's intersection, ties broken in merlict's visiting order.
+ * FRAME_TREE: merlict's own walk over the frame tree's bounding spheres
+ * (RayAndFrame.cpp:137-149).  Traversal restricted to a lens (an allowed
+ * frame) always walks the frame tree.                                     */
+enum { MLGPU_TRAVERSAL_BVH = 0, MLGPU_TRAVERSAL_FRAME_TREE = 1 };
 
 /* PropagationConfig (merlict/PropagationConfig.h:10-13) plus engine knobs. */
 typedef struct mlgpu_settings {
@@ -212,6 +224,7 @@ typedef struct mlgpu_settings {
     int32_t start_node;     /* node of the `world` frame passed by the caller */
     int32_t tracer;         /* MLGPU_TRACER_*                                 */
     int32_t block_size;     /* 0 = default                                    */
+    int32_t traversal;      /* MLGPU_TRAVERSAL_*                              */
 } mlgpu_settings;
 
 typedef struct mlgpu_scene mlgpu_scene;

@@ -11,7 +11,7 @@ from dataclasses import dataclass, field
 
 import numpy as np
 
-ABI_VERSION = 1
+ABI_VERSION = 2
 
 # status codes
 OK = 0
@@ -85,6 +85,7 @@ RNG_REPLAY = 1
 TRACER_FP64 = 0
 TRACER_FP32 = 1
 TRACER_FP32_PURE = 2
+TRACER_FP64_PLAIN = 3
 
 _dp = C.POINTER(C.c_double)
 _ip = C.POINTER(C.c_int32)
@@ -179,12 +180,17 @@ class mlgpu_rng(C.Structure):
     ]
 
 
+TRAVERSAL_BVH = 0
+TRAVERSAL_FRAME_TREE = 1
+
+
 class mlgpu_settings(C.Structure):
     _fields_ = [
         ("max_num_interactions_per_photon", C.c_uint32),
         ("start_node", C.c_int32),
         ("tracer", C.c_int32),
         ("block_size", C.c_int32),
+        ("traversal", C.c_int32),
     ]
 
 

@@ -26,6 +26,7 @@ COMMON = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC,-ffp-contract=o
 EXTRA = {
     "trace_fp64.cu": ["--fmad=false"],
     "bin.cu": ["--fmad=false"],
+    "wavefront_fp64.cu": ["--fmad=false"],
 }
 
 

@@ -2,6 +2,7 @@
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
+#include <algorithm>
 #include <cstring>
 #include <string>
 #include <vector>
@@ -63,6 +64,10 @@ struct mlgpu_scene {
     unsigned int* error_word = nullptr;
     // staging for mlgpu_propagate_host and scratch for binning
     DeviceBuffer staging_in, staging_out, staging_hist, staging_rng, bin_scratch;
+    // ray pools of the wavefront tracers
+    DeviceBuffer wave;
+    WaveCounters* wave_host = nullptr;   // pinned copy of the counters
+    int wave_walk_blocks = 0;
 };
 
 namespace {
@@ -203,6 +208,20 @@ int build_device_scene(mlgpu_scene* s, const mlgpu_flat_scene* f) {
     if ((st = upload(s, leaf_f.data(), leaf_f.size(), &s->dev.leaf_f))) return st;
     if ((st = upload(s, origin.data(), origin.size(), &s->dev.leaf_origin))) return st;
     if ((st = upload(s, pts_f.data(), pts_f.size(), &s->dev.fn_points_f))) return st;
+    {
+        // BVH over the leaves; boxes widened for single-precision slab tests
+        const double* root = f->node_sphere;
+        const double extent = std::fabs(root[0]) + std::fabs(root[1]) + std::fabs(root[2]) +
+            2.0*root[3];
+        BvhHost bvh;
+        build_bvh4(f, 0.0, &bvh);
+        if (!bvh.nodes.empty()) {
+            if ((st = upload(s, bvh.nodes.data(), bvh.nodes.size(), &s->dev.bvh))) return st;
+            if ((st = upload(s, bvh.leaf_ids.data(), bvh.leaf_ids.size(), &s->dev.bvh_leaf))) return st;
+            s->dev.bvh_nodes = (int32_t)bvh.nodes.size();
+        }
+        s->dev.bvh_eps = (float)(1e-6 + 4e-7*extent);
+    }
     const unsigned int* ew = nullptr;
     if ((st = upload<unsigned int>(s, nullptr, 1, &ew))) return st;
     s->error_word = const_cast<unsigned int*>(ew);
@@ -243,9 +262,11 @@ int check_propagate_args(const mlgpu_scene* scene, const mlgpu_photons* ph,
     if (rng->mode == MLGPU_RNG_REPLAY && !rng->uniforms)
         return fail(MLGPU_ERR_INVALID_ARGUMENT, "replay rng without uniforms");
     if (st->tracer != MLGPU_TRACER_FP64 && st->tracer != MLGPU_TRACER_FP32 &&
-        st->tracer != MLGPU_TRACER_FP32_PURE)
+        st->tracer != MLGPU_TRACER_FP32_PURE && st->tracer != MLGPU_TRACER_FP64_PLAIN)
         return fail(MLGPU_ERR_INVALID_ARGUMENT, "unknown tracer %d", st->tracer);
-    if (st->tracer != MLGPU_TRACER_FP64 && res->history)
+    if (st->traversal != MLGPU_TRAVERSAL_BVH && st->traversal != MLGPU_TRAVERSAL_FRAME_TREE)
+        return fail(MLGPU_ERR_INVALID_ARGUMENT, "unknown traversal %d", st->traversal);
+    if (st->tracer != MLGPU_TRACER_FP64 && st->tracer != MLGPU_TRACER_FP64_PLAIN && res->history)
         return fail(MLGPU_ERR_INVALID_ARGUMENT, "histories are recorded by the FP64 tracer only");
     return MLGPU_OK;
 }
@@ -272,18 +293,76 @@ TraceArgs make_args(const mlgpu_scene* scene, const mlgpu_photons* ph, uint64_t 
     a.num_photons = n;
     a.max_interactions = st->max_num_interactions_per_photon;
     a.start_node = st->start_node;
+    a.traversal = st->traversal;
     return a;
 }
 
-int launch(const mlgpu_scene* scene, const TraceArgs& a, const mlgpu_settings* st,
+constexpr uint32_t kWavePool = 1u << 21;   // ray slots of the wavefront tracers
+
+// Carves the two ray pools, the candidate lists and the counters out of
+// one device buffer.
+int wave_buffers(mlgpu_scene* scene, uint32_t pool, WaveBuffers* w, RayPool* p0, RayPool* p1) {
+    const size_t per_pool = (size_t)pool*(8*8 + 5*4);
+    const size_t bytes = 2*per_pool + (size_t)pool*(4*32 + 4) + 4096;
+    MLGPU_CUDA(scene->wave.reserve(bytes));
+    if (!scene->wave_host) MLGPU_CUDA(cudaMallocHost(&scene->wave_host, sizeof(WaveCounters)));
+    if (!scene->wave_walk_blocks) scene->wave_walk_blocks = wave_fp64_walk_blocks();
+    char* b = static_cast<char*>(scene->wave.ptr);
+    w->counters = reinterpret_cast<WaveCounters*>(b);
+    b += 256;
+    RayPool* pools[2] = {p0, p1};
+    for (RayPool* p : pools) {
+        double** d[8] = {&p->sx, &p->sy, &p->sz, &p->dx, &p->dy, &p->dz, &p->lambda, &p->tof};
+        for (double** q : d) { *q = reinterpret_cast<double*>(b); b += (size_t)pool*8; }
+        int32_t** i[5] = {&p->photon, &p->root, &p->n_int, &p->k_draw, &p->err};
+        for (int32_t** q : i) { *q = reinterpret_cast<int32_t*>(b); b += ((size_t)pool*4 + 255) & ~size_t(255); }
+    }
+    w->cand = reinterpret_cast<int32_t*>(b);
+    b += (size_t)pool*32*4;
+    w->cand_count = reinterpret_cast<int32_t*>(b);
+    w->pool = pool;
+    return MLGPU_OK;
+}
+
+// Runs iterations of the wavefront tracer until every photon has finished,
+// checking the counters after every few iterations.
+int run_wavefront(mlgpu_scene* scene, const TraceArgs& a, cudaStream_t stream) {
+    const uint32_t pool = (uint32_t)std::min<uint64_t>(a.num_photons, kWavePool);
+    WaveBuffers w;
+    RayPool pools[2];
+    int st = wave_buffers(scene, pool, &w, &pools[0], &pools[1]);
+    if (st) return st;
+    MLGPU_CUDA(cudaMemsetAsync(w.counters, 0, sizeof(WaveCounters), stream));
+    // every iteration advances each live photon by one step
+    const uint64_t bound = (a.num_photons*(uint64_t)(a.max_interactions + 1))/pool +
+        a.max_interactions + 16;
+    uint64_t iteration = 0;
+    const int group = 4;
+    while (true) {
+        for (int g = 0; g < group; g++, iteration++) {
+            const cudaError_t e = launch_wave_fp64_iteration(
+                a, w, pools[iteration & 1], pools[(iteration + 1) & 1], scene->wave_walk_blocks, stream);
+            if (e != cudaSuccess) return cuda_fail(e, "wavefront kernels");
+        }
+        MLGPU_CUDA(cudaMemcpyAsync(scene->wave_host, w.counters, sizeof(WaveCounters),
+                                   cudaMemcpyDeviceToHost, stream));
+        MLGPU_CUDA(cudaStreamSynchronize(stream));
+        if (scene->wave_host->active == 0 && scene->wave_host->next_input >= a.num_photons) break;
+        if (iteration > bound)
+            return fail(MLGPU_ERR_RUNTIME, "wavefront tracer did not drain its pool");
+    }
+    return MLGPU_OK;
+}
+
+int launch(mlgpu_scene* scene, const TraceArgs& a, const mlgpu_settings* st,
            cudaStream_t stream) {
     cudaError_t e;
     switch (st->tracer) {
-    case MLGPU_TRACER_FP64: e = launch_trace_fp64(a, st->block_size, stream); break;
+    case MLGPU_TRACER_FP64: return run_wavefront(scene, a, stream);
+    case MLGPU_TRACER_FP64_PLAIN: e = launch_trace_fp64(a, st->block_size, stream); break;
     case MLGPU_TRACER_FP32: e = launch_trace_fp32(a, st->block_size, false, stream); break;
     default: e = launch_trace_fp32(a, st->block_size, true, stream); break;
     }
-    (void)scene;
     if (e != cudaSuccess) return cuda_fail(e, "trace kernel launch");
     return MLGPU_OK;
 }
@@ -348,6 +427,8 @@ int mlgpu_scene_destroy(mlgpu_scene* scene) {
     scene->staging_hist.release();
     scene->staging_rng.release();
     scene->bin_scratch.release();
+    scene->wave.release();
+    if (scene->wave_host) cudaFreeHost(scene->wave_host);
     delete scene;
     return MLGPU_OK;
 }

@@ -4,6 +4,7 @@
 #define MLGPU_INTERNAL_H_
 
 #include <cstdint>
+#include <vector>
 #include <cuda_runtime.h>
 
 #include "merlict_b200.h"
@@ -42,6 +43,20 @@ struct __align__(128) LeafRecF {
 };
 static_assert(sizeof(LeafRecF) == 128, "LeafRecF must be 128 bytes");
 
+// 4-wide BVH node: child boxes as [axis][child] (float, rounded outwards)
+// and child references: a node index, a leaf range (kBvhLeafFlag | start << 3
+// | count - 1, into DevScene::bvh_leaf) or kBvhEmpty.
+struct __align__(128) BvhNode4 {
+    float lo[3][4];
+    float hi[3][4];
+    int32_t child[4];
+    int32_t pad[4];
+};
+static_assert(sizeof(BvhNode4) == 128, "BvhNode4 must be 128 bytes");
+constexpr int32_t kBvhLeafFlag = (int32_t)0x80000000u;
+constexpr int32_t kBvhEmpty = 0x7fffffff;
+constexpr int kBvhStack = 48;
+
 struct DevScene {
     const double4* node;        // x, y, z, radius^2
     const int2* node_meta;      // skip, leaf
@@ -60,6 +75,11 @@ struct DevScene {
     int32_t num_sensors;
     double hex_u[3], hex_v[3], hex_w[3];
     unsigned int* error_word;   // first device-side error code
+    // BVH over the leaves with geometry (empty: walk the frame tree)
+    const BvhNode4* bvh;
+    const int32_t* bvh_leaf;
+    int32_t bvh_nodes;
+    float bvh_eps;              // box inflation per ray: bvh_eps + 4e-7 |origin|_1
 };
 
 struct DevPhotons {
@@ -98,9 +118,48 @@ struct TraceArgs {
     uint64_t num_photons;
     uint32_t max_interactions;
     int32_t start_node;
+    int32_t traversal;          // MLGPU_TRAVERSAL_*
+};
+
+struct BvhHost {
+    std::vector<BvhNode4> nodes;
+    std::vector<int32_t> leaf_ids;
+};
+void build_bvh4(const mlgpu_flat_scene* f, double inflate, BvhHost* out);
+
+// wavefront tracers: a pool of ray slots, two of them (current, next)
+struct WaveCounters {
+    unsigned long long next_input;   // photons taken into the pool so far
+    unsigned int active;             // rays carried over into the current pool
+    unsigned int total;              // active + new photons of this iteration
+    unsigned int next;               // survivors written to the next pool
+    unsigned int walk_fetch;         // slots handed out by the walk kernel
+};
+
+struct RayPool {
+    int32_t* photon;
+    double* sx; double* sy; double* sz;
+    double* dx; double* dy; double* dz;
+    double* lambda;
+    double* tof;
+    int32_t* root;
+    int32_t* n_int;
+    int32_t* k_draw;
+    int32_t* err;            // error | time-of-flight error << 8
+};
+
+struct WaveBuffers {
+    WaveCounters* counters;
+    int32_t* cand;           // [pool][32] candidate leaves of the current step
+    int32_t* cand_count;     // [pool]
+    uint32_t pool;
 };
 
 cudaError_t launch_trace_fp64(const TraceArgs& a, int block, cudaStream_t s);
+cudaError_t launch_wave_fp64_iteration(const TraceArgs& a, const WaveBuffers& w,
+                                       const RayPool& cur, const RayPool& nxt,
+                                       int walk_blocks, cudaStream_t s);
+int wave_fp64_walk_blocks();
 cudaError_t launch_trace_fp32(const TraceArgs& a, int block, bool pure, cudaStream_t s);
 cudaError_t launch_bin_arrivals(const DevScene& sc, const int32_t* sensor,
                                 const double* time, uint64_t n, uint32_t* counts,

@@ -15,7 +15,9 @@ from . import abi
 from ._native import check, lib
 from .photons import PLANES
 
-TRACERS = {"fp64": abi.TRACER_FP64, "fp32": abi.TRACER_FP32, "fp32_pure": abi.TRACER_FP32_PURE}
+TRACERS = {"fp64": abi.TRACER_FP64, "fp32": abi.TRACER_FP32, "fp32_pure": abi.TRACER_FP32_PURE,
+           "fp64_plain": abi.TRACER_FP64_PLAIN}
+TRAVERSALS = {"bvh": abi.TRAVERSAL_BVH, "frame_tree": abi.TRAVERSAL_FRAME_TREE}
 
 
 @dataclass
@@ -121,7 +123,7 @@ class Scene:
                   rng=None, tracer: str = "fp64", start_node: int = 0,
                   outputs=("sensor", "x", "y", "time"), history: bool = False,
                   out_dtype=torch.float64, stream=None, sync: bool = True,
-                  results: dict | None = None) -> dict:
+                  results: dict | None = None, traversal: str = "bvh") -> dict:
         """Traces a batch of device-resident photons.
 
         `photons` is a dict of CUDA tensors (see photons.PLANES).  Returns a
@@ -162,7 +164,7 @@ class Scene:
             out["history"] = torch.empty((n, m, abi.HISTORY_DTYPE.itemsize), dtype=torch.uint8, device=dev)
             res.history = out["history"].data_ptr()
         st = abi.mlgpu_settings(int(config.max_num_interactions_per_photon), int(start_node),
-                                TRACERS[tracer], 0)
+                                TRACERS[tracer], 0, TRAVERSALS[traversal])
         r, keep = rng._struct(n)
         sh = _stream_handle(stream)
         check(lib().mlgpu_propagate(self._h, C.byref(ph), n, C.byref(st), C.byref(r),

@@ -38,19 +38,24 @@ def run_gpu(eng, flat, photons, max_int, seed=0, uniforms=None, history=False,
     return got
 
 
+FP64_TRACERS = ("fp64", "fp64_plain")
+
+
+@pytest.mark.parametrize("tracer", FP64_TRACERS)
 @pytest.mark.parametrize("name", golden_names())
-def test_fp64_tracer_matches_reference_bit_for_bit(eng, name):
+def test_fp64_tracer_matches_reference_bit_for_bit(eng, name, tracer):
     flat, photons, ref, meta = load_golden(name)
     got = run_gpu(eng, flat, photons, meta["max_interactions"], seed=meta["seed"],
-                  uniforms=meta["uniforms"], history=True)
+                  uniforms=meta["uniforms"], history=True, tracer=tracer)
     assert mismatches(ref, got) == {}
     assert history_mismatches(ref["history"], got["history"]) == {}
 
 
+@pytest.mark.parametrize("tracer", FP64_TRACERS)
 @pytest.mark.parametrize("name,n", [("reflector_camera", 200_000),
                                     ("light_field_small", 100_000),
                                     ("primitive_zoo", 200_000)])
-def test_fp64_tracer_matches_oracle_on_larger_batches(eng, oracle, name, n):
+def test_fp64_tracer_matches_oracle_on_larger_batches(eng, oracle, name, n, tracer):
     from merlict_development_kit_b200 import photons as P
     flat, _, _, meta = load_golden(name)
     if name == "primitive_zoo":
@@ -61,8 +66,19 @@ def test_fp64_tracer_matches_oracle_on_larger_batches(eng, oracle, name, n):
         ph = P.downward_disc_source(n, 123, 2.0, 10.0, 1.5)
     status, ref, _ = oracle.propagate(flat, ph, meta["max_interactions"], seed=77)
     assert status == 0
-    got = run_gpu(eng, flat, ph, meta["max_interactions"], seed=77)
+    got = run_gpu(eng, flat, ph, meta["max_interactions"], seed=77, tracer=tracer)
     assert mismatches(ref, got) == {}
+
+
+@pytest.mark.parametrize("max_int", [0, 1, 2, 3])
+def test_interaction_limit_and_zero_limit(eng, oracle, max_int):
+    """PhotonAndFrame.cpp:18-21: the limit counts the production entry."""
+    flat, photons, ref, meta = load_golden("light_field_small")
+    status, ref, _ = oracle.propagate(flat, photons, max_int, seed=3, history=True)
+    for tracer in FP64_TRACERS:
+        got = run_gpu(eng, flat, photons, max_int, seed=3, history=True, tracer=tracer)
+        assert mismatches(ref, got) == {}, tracer
+        assert history_mismatches(ref["history"], got["history"]) == {}, tracer
 
 
 def test_propagate_host_entry_point(eng):
@@ -74,7 +90,7 @@ def test_propagate_host_entry_point(eng):
     ps, keep = _photon_struct(photons)
     n = len(photons["wavelength"])
     rs, out = alloc_results(n, meta["max_interactions"], history=True)
-    st = abi.mlgpu_settings(meta["max_interactions"], 0, abi.TRACER_FP64, 0)
+    st = abi.mlgpu_settings(meta["max_interactions"], 0, abi.TRACER_FP64, 0, abi.TRAVERSAL_BVH)
     rng = abi.mlgpu_rng()
     rng.mode = abi.RNG_PHILOX
     rng.seed = meta["seed"]
