@@ -36,7 +36,7 @@ MAX_INTERACTIONS = 10
 # algorithmic HBM bytes per photon: in 7 x f64 + id (60 B), out sensor id,
 # x, y, time (28 B); FP32 form: in 7 x f32 + id (32 B), out id + x, y f32 +
 # time f64 (20 B)
-BYTES_PER_PHOTON = {"fp64": 88, "fp32": 52}
+BYTES_PER_PHOTON = {"fp64": 88, "fp64_plain": 88, "fp32": 52}
 # FLOP weights of the operation counts (nodes tested, leaves transformed,
 # cap quadratics, cap bounds, plane tests, other quadrics, reflections,
 # Fresnel steps, time-of-flight segments, table look-ups)
@@ -233,21 +233,21 @@ def run_ours(args, world, rank, local):
     scene = engine.Scene(flat)
     n = args.photons
     tracer = args.tracer
-    in_dtype = torch.float64 if tracer == "fp64" else torch.float32
+    in_dtype = torch.float32 if tracer == "fp32" else torch.float64
     host = make_photons(n, 12345 + rank)
     dev = engine.photons_to_device(host, dtype=in_dtype)
-    out_dtype = torch.float64 if tracer == "fp64" else torch.float32
+    out_dtype = torch.float32 if tracer == "fp32" else torch.float64
     cfg = engine.PropagationConfig(MAX_INTERACTIONS)
     rng = engine.Philox(seed=7 + rank)
     stream = torch.cuda.current_stream()
     results = {}
-    launches_per_step = 3   # trace + 2 binning kernels
 
     def step(ev=None):
         if ev is not None:
             ev[0].record(stream)
         out = scene.propagate(dev, cfg, rng, tracer=tracer, outputs=("sensor", "x", "y", "time"),
-                              out_dtype=out_dtype, sync=False, results=results)
+                              out_dtype=out_dtype, sync=False, results=results,
+                              traversal="frame_tree")
         if ev is not None:
             ev[1].record(stream)
         scene.bin_arrivals(out["sensor"])
@@ -266,10 +266,12 @@ def run_ours(args, world, rank, local):
     torch.cuda.synchronize()
     t_start = torch.cuda.Event(enable_timing=True)
     t_stop = torch.cuda.Event(enable_timing=True)
+    launches0 = scene.kernel_launches()
     t_start.record(stream)
     for k in range(args.steps):
         step(kernel_events[k])
     t_stop.record(stream)
+    launches = scene.kernel_launches() - launches0
     torch.cuda.synchronize()
     barrier(world)
     clk = clocks.stop()
@@ -296,7 +298,7 @@ def run_ours(args, world, rank, local):
     res.dtype = abi.F64 if out_dtype == torch.float64 else abi.F32
     res.sensor, res.x, res.y, res.time = (h_sensor.data_ptr(), h_x.data_ptr(), h_y.data_ptr(),
                                           h_t.data_ptr())
-    st = abi.mlgpu_settings(MAX_INTERACTIONS, 0, engine.TRACERS[tracer], 0)
+    st = abi.mlgpu_settings(MAX_INTERACTIONS, 0, engine.TRACERS[tracer], 0, abi.TRAVERSAL_FRAME_TREE)
     r = abi.mlgpu_rng()
     r.mode = abi.RNG_PHILOX
     r.seed = 99 + rank
@@ -331,9 +333,9 @@ def run_ours(args, world, rank, local):
     if counts:
         per = counts["per_photon"]
         flops = sum(FLOP_WEIGHTS[k] * per.get(k, 0.0) for k in FLOP_WEIGHTS)
-        peak = FP64_PEAK_TFLOPS_NOMINAL if tracer == "fp64" else FP32_PEAK_TFLOPS_NOMINAL
+        peak = FP32_PEAK_TFLOPS_NOMINAL if tracer == "fp32" else FP64_PEAK_TFLOPS_NOMINAL
         achieved = flops * n / (kernel_ms * 1e-3) / 1e12
-        compute = {"bound": "fp64" if tracer == "fp64" else "fp32", "flops_per_photon": flops,
+        compute = {"bound": "fp32" if tracer == "fp32" else "fp64", "flops_per_photon": flops,
                    "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
                    "frac": achieved / peak, "peak_source": "nominal B200 vector peak"}
     cpu = None
@@ -344,7 +346,7 @@ def run_ours(args, world, rank, local):
         "metric": "photons/s", "value": value, "unit": "photons/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": elapsed_ms / args.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-        "dtype": "f64" if tracer == "fp64" else "f32",
+        "dtype": "f32" if tracer == "fp32" else "f64",
         "data": "synthetic",
         "config": {"workload": WORKLOAD, "scene": scene_config_name(), "tracer": tracer,
                    "photons_per_step_per_gpu": n, "max_interactions": MAX_INTERACTIONS,
@@ -355,7 +357,7 @@ def run_ours(args, world, rank, local):
         "cpu_baseline": cpu,
         "e2e": {"value": e2e_value, "unit": "photons/s", "h2d_bytes_per_step": h2d,
                 "d2h_bytes_per_step": d2h},
-        "gpu_launches": launches_per_step * args.steps,
+        "gpu_launches": launches,
         "clocks": clk,
     }
     print(json.dumps(line), flush=True)
@@ -368,7 +370,7 @@ def main():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--tracer", choices=["fp64", "fp32"], default="fp64")
+    ap.add_argument("--tracer", choices=["fp64", "fp64_plain", "fp32"], default="fp64")
     ap.add_argument("--photons", type=int, default=10_000_000)
     ap.add_argument("--ref-photons", type=int, default=100_000)
     ap.add_argument("--no-cpu-baseline", action="store_true")

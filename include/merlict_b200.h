@@ -241,6 +241,10 @@ int mlgpu_last_error(char* buffer, size_t buffer_size);
 int mlgpu_scene_create(const mlgpu_flat_scene* flat, mlgpu_scene** scene);
 int mlgpu_scene_destroy(mlgpu_scene* scene);
 
+/* Kernel launches this scene has made so far (all entry points), for
+ * callers that account for GPU work.                                      */
+int mlgpu_scene_kernel_launches(const mlgpu_scene* scene, uint64_t* launches);
+
 /* ---- propagation ------------------------------------------------------ *
  * Replaces propagate_photons_in_frame_with_config (merlict/Photons.cpp:9-22)
  * and its thread-pool twin (merlict_multi_thread.cpp:28-55).

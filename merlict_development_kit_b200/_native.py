@@ -58,12 +58,13 @@ def lib():
         L.mlgpu_bin_arrivals.argtypes = [
             C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint64, C.c_void_p, C.c_void_p,
             C.c_uint32, C.c_double, C.c_double, C.c_void_p]
+        L.mlgpu_scene_kernel_launches.argtypes = [C.c_void_p, C.POINTER(C.c_uint64)]
         L.mlgpu_bin_arrivals_noalloc.argtypes = [
             C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint64, C.c_void_p, C.c_void_p,
             C.c_uint32, C.c_double, C.c_double, C.c_void_p]
         for name in ("mlgpu_scene_create", "mlgpu_scene_destroy", "mlgpu_propagate",
                      "mlgpu_propagate_host", "mlgpu_scene_sync_errors", "mlgpu_bin_arrivals",
-                     "mlgpu_bin_arrivals_noalloc"):
+                     "mlgpu_bin_arrivals_noalloc", "mlgpu_scene_kernel_launches"):
             getattr(L, name).restype = C.c_int
         if L.mlgpu_abi_version() != abi.ABI_VERSION:
             raise ImportError("libmerlict_b200.so ABI version mismatch")
@@ -86,5 +87,5 @@ def check(status: int) -> None:
 EXPORTED = (
     "mlgpu_abi_version", "mlgpu_last_error", "mlgpu_scene_create", "mlgpu_scene_destroy",
     "mlgpu_propagate", "mlgpu_scene_sync_errors", "mlgpu_propagate_host",
-    "mlgpu_bin_arrivals", "mlgpu_bin_arrivals_noalloc",
+    "mlgpu_bin_arrivals", "mlgpu_bin_arrivals_noalloc", "mlgpu_scene_kernel_launches",
 )

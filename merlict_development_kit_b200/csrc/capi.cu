@@ -68,6 +68,7 @@ struct mlgpu_scene {
     DeviceBuffer wave;
     WaveCounters* wave_host = nullptr;   // pinned copy of the counters
     int wave_walk_blocks = 0;
+    uint64_t launches = 0;               // kernels launched for this scene
 };
 
 namespace {
@@ -218,6 +219,10 @@ int build_device_scene(mlgpu_scene* s, const mlgpu_flat_scene* f) {
         if (!bvh.nodes.empty()) {
             if ((st = upload(s, bvh.nodes.data(), bvh.nodes.size(), &s->dev.bvh))) return st;
             if ((st = upload(s, bvh.leaf_ids.data(), bvh.leaf_ids.size(), &s->dev.bvh_leaf))) return st;
+            // merlict's own bounding sphere of each leaf, in BVH order
+            std::vector<double4> sph(bvh.leaf_ids.size());
+            for (size_t j = 0; j < sph.size(); j++) sph[j] = node[f->leaf_node[bvh.leaf_ids[j]]];
+            if ((st = upload(s, sph.data(), sph.size(), &s->dev.bvh_sphere))) return st;
             s->dev.bvh_nodes = (int32_t)bvh.nodes.size();
         }
         s->dev.bvh_eps = (float)(1e-6 + 4e-7*extent);
@@ -343,6 +348,7 @@ int run_wavefront(mlgpu_scene* scene, const TraceArgs& a, cudaStream_t stream) {
             const cudaError_t e = launch_wave_fp64_iteration(
                 a, w, pools[iteration & 1], pools[(iteration + 1) & 1], scene->wave_walk_blocks, stream);
             if (e != cudaSuccess) return cuda_fail(e, "wavefront kernels");
+            scene->launches += 4;
         }
         MLGPU_CUDA(cudaMemcpyAsync(scene->wave_host, w.counters, sizeof(WaveCounters),
                                    cudaMemcpyDeviceToHost, stream));
@@ -359,7 +365,7 @@ int launch(mlgpu_scene* scene, const TraceArgs& a, const mlgpu_settings* st,
     cudaError_t e;
     switch (st->tracer) {
     case MLGPU_TRACER_FP64: return run_wavefront(scene, a, stream);
-    case MLGPU_TRACER_FP64_PLAIN: e = launch_trace_fp64(a, st->block_size, stream); break;
+    case MLGPU_TRACER_FP64_PLAIN: e = launch_trace_fp64(a, st->block_size, stream); scene->launches++; break;
     case MLGPU_TRACER_FP32: e = launch_trace_fp32(a, st->block_size, false, stream); break;
     default: e = launch_trace_fp32(a, st->block_size, true, stream); break;
     }
@@ -556,6 +562,13 @@ int mlgpu_bin_arrivals(mlgpu_scene* scene, const int32_t* sensor, const double* 
         num_time_bins, t_min, t_max, static_cast<uint32_t*>(scene->bin_scratch.ptr),
         scene->bin_scratch.bytes / sizeof(uint32_t), static_cast<cudaStream_t>(cuda_stream));
     if (e != cudaSuccess) return cuda_fail(e, "binning kernels");
+    scene->launches += 2;
+    return MLGPU_OK;
+}
+
+int mlgpu_scene_kernel_launches(const mlgpu_scene* scene, uint64_t* launches) {
+    if (!scene || !launches) return fail(MLGPU_ERR_INVALID_ARGUMENT, "NULL argument");
+    *launches = scene->launches;
     return MLGPU_OK;
 }
 

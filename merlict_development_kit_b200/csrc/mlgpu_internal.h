@@ -78,6 +78,7 @@ struct DevScene {
     // BVH over the leaves with geometry (empty: walk the frame tree)
     const BvhNode4* bvh;
     const int32_t* bvh_leaf;
+    const double4* bvh_sphere;  // per BVH leaf slot: world centre and radius^2 of that leaf
     int32_t bvh_nodes;
     float bvh_eps;              // box inflation per ray: bvh_eps + 4e-7 |origin|_1
 };

@@ -5,10 +5,13 @@
 // One iteration over the pool:
 //   walk     persistent kernel; every warp refills its idle lanes from a
 //            per-warp chunk of slots (one atomic per 64 slots), takes new
-//            photons into free slots, and walks merlict's frame tree
-//            (RayAndFrame.cpp:137-149), recording the candidate leaves;
+//            photons into free slots, and walks the BVH of the scene,
+//            recording the leaves that pass merlict's own bounding-sphere
+//            test (RayAndFrame.cpp:16-107) as candidates;
 //   resolve  one thread per slot: merlict's intersection of the candidates
-//            in visiting order (closest hit, RayAndFrame.cpp:151-173), the
+//            (closest hit, ties in merlict's visiting order,
+//            RayAndFrame.cpp:151-173) -- or, for a ray inside a lens,
+//            merlict's walk of that lens's subtree -- the
 //            interaction (absorption, reflection, Fresnel), the history
 //            entry and the time-of-flight term; survivors are compacted
 //            into the next pool with a warp ballot and one atomic per warp,
@@ -32,6 +35,7 @@ constexpr int kWaveCandidates = 32;     // candidate leaves recorded per ray ste
 constexpr int kWalkChunk = 64;          // slots a warp takes at a time
 constexpr int kWalkBurst = 16;          // tree nodes a lane visits between refills
 constexpr int kNoStep = -2;             // candidate count: photon takes no step
+constexpr int kWalkInline = -3;         // candidate count: resolve walks the frame tree itself
 
 template <typename T>
 __device__ __forceinline__ double load_in(const void* p, uint64_t i) {
@@ -69,8 +73,12 @@ wave_walk_kernel(const TraceArgs a, const WaveBuffers w, const RayPool cur) {
     int64_t item = -1;
     v3 s = mk(0, 0, 0), d = mk(0, 0, 0);
     double sd = 0.0;
-    int32_t i = 0, end = 0;
     int nc = 0;
+    bool overflow = false;
+    // BVH traversal state (single precision slab tests)
+    float ox = 0.f, oy = 0.f, oz = 0.f, idx = 0.f, idy = 0.f, idz = 0.f, eps = 0.f;
+    int32_t stack[kBvhStack];
+    int sp = 0;
     while (true) {
         // hand idle lanes new slots from the warp's chunk
         unsigned idle = __ballot_sync(kFull, item < 0);
@@ -121,11 +129,30 @@ wave_walk_kernel(const TraceArgs a, const WaveBuffers w, const RayPool cur) {
                 if (n_int > max_int) {
                     w.cand_count[slot] = kNoStep;
                     item = -1;
+                } else if (root != 0 || sc.bvh_nodes == 0 ||
+                           a.traversal == MLGPU_TRAVERSAL_FRAME_TREE) {
+                    // traversal restricted to a frame's subtree (a lens): the
+                    // resolve kernel walks that subtree itself
+                    w.cand_count[slot] = kWalkInline;
+                    item = -1;
                 } else {
                     sd = dot(s, d);
-                    i = root;
-                    end = __ldg(&sc.node_meta[root].x);
                     nc = 0;
+                    overflow = false;
+                    sp = 0;
+                    // merlict tests the root frame's own sphere first
+                    const double2* np = reinterpret_cast<const double2*>(sc.node);
+                    const double2 n01 = __ldg(np), n23 = __ldg(np + 1);
+                    if (sphere_cull(make_double4(n01.x, n01.y, n23.x, n23.y), s, d, sd)) {
+                        stack[sp++] = 0;
+                        ox = (float)s.x; oy = (float)s.y; oz = (float)s.z;
+                        float fdx = (float)d.x, fdy = (float)d.y, fdz = (float)d.z;
+                        if (fabsf(fdx) < 1e-30f) fdx = copysignf(1e-30f, fdx);
+                        if (fabsf(fdy) < 1e-30f) fdy = copysignf(1e-30f, fdy);
+                        if (fabsf(fdz) < 1e-30f) fdz = copysignf(1e-30f, fdz);
+                        idx = 1.0f/fdx; idy = 1.0f/fdy; idz = 1.0f/fdz;
+                        eps = sc.bvh_eps + 4e-7f*(fabsf(ox) + fabsf(oy) + fabsf(oz));
+                    }
                 }
             }
             chunk_begin += take;
@@ -133,24 +160,49 @@ wave_walk_kernel(const TraceArgs a, const WaveBuffers w, const RayPool cur) {
         }
         if (__ballot_sync(kFull, item >= 0) == 0) break;
         if (item >= 0) {
-            // merlict's walk over the frame tree, recording candidates
+            // BVH traversal; each leaf it reaches gets merlict's own sphere
+            // test (RayAndFrame.cpp:16-107) and, if it passes, becomes a
+            // candidate.  The resolve kernel breaks ties in merlict's
+            // visiting order, so the order here does not matter.
             int32_t* cand = w.cand + (size_t)item*kWaveCandidates;
-            for (int it = 0; it < kWalkBurst && i < end; it++) {
-                const double2* np = reinterpret_cast<const double2*>(sc.node + i);
-                const double2 n01 = __ldg(np), n23 = __ldg(np + 1);
-                const int2 meta = __ldg(&sc.node_meta[i]);
-                if (!sphere_cull(make_double4(n01.x, n01.y, n23.x, n23.y), s, d, sd)) {
-                    i = meta.x;
+            for (int it = 0; it < kWalkBurst && sp > 0; it++) {
+                const int32_t ref = stack[--sp];
+                if (ref < 0) {
+                    const int32_t start = (ref & 0x7fffffff) >> 3;
+                    const int32_t count = (ref & 7) + 1;
+                    for (int32_t j = start; j < start + count; j++) {
+                        const double2* q = reinterpret_cast<const double2*>(sc.bvh_sphere + j);
+                        const double2 c01 = __ldg(q), c23 = __ldg(q + 1);
+                        if (sphere_cull(make_double4(c01.x, c01.y, c23.x, c23.y), s, d, sd)) {
+                            if (nc < kWaveCandidates) cand[nc] = __ldg(sc.bvh_leaf + j);
+                            nc++;
+                        }
+                    }
                     continue;
                 }
-                if (meta.y >= 0) {
-                    if (nc < kWaveCandidates) cand[nc] = meta.y;
-                    nc++;
+                const float4* nq = reinterpret_cast<const float4*>(sc.bvh + ref);
+                const float4 lx = __ldg(nq), ly = __ldg(nq + 1), lz = __ldg(nq + 2);
+                const float4 hx = __ldg(nq + 3), hy = __ldg(nq + 4), hz = __ldg(nq + 5);
+                const int4 ch = __ldg(reinterpret_cast<const int4*>(nq + 6));
+                const float lox[4] = {lx.x, lx.y, lx.z, lx.w}, loy[4] = {ly.x, ly.y, ly.z, ly.w};
+                const float loz[4] = {lz.x, lz.y, lz.z, lz.w}, hix[4] = {hx.x, hx.y, hx.z, hx.w};
+                const float hiy[4] = {hy.x, hy.y, hy.z, hy.w}, hiz[4] = {hz.x, hz.y, hz.z, hz.w};
+                const int32_t child[4] = {ch.x, ch.y, ch.z, ch.w};
+#pragma unroll
+                for (int k = 0; k < 4; k++) {
+                    const float ax = (lox[k] - eps - ox)*idx, bx = (hix[k] + eps - ox)*idx;
+                    const float ay = (loy[k] - eps - oy)*idy, by = (hiy[k] + eps - oy)*idy;
+                    const float az = (loz[k] - eps - oz)*idz, bz = (hiz[k] + eps - oz)*idz;
+                    const float tmin = fmaxf(fmaxf(fminf(ax, bx), fminf(ay, by)), fmaxf(fminf(az, bz), 0.0f));
+                    const float tmax = fminf(fminf(fmaxf(ax, bx), fmaxf(ay, by)), fmaxf(az, bz));
+                    if (tmin <= tmax && child[k] != kBvhEmpty) {
+                        if (sp < kBvhStack) stack[sp++] = child[k];
+                        else overflow = true;
+                    }
                 }
-                i++;
             }
-            if (i >= end) {
-                w.cand_count[item] = nc;
+            if (sp == 0) {
+                w.cand_count[item] = overflow ? kWaveCandidates + 1 : nc;
                 item = -1;
             }
         }
@@ -202,7 +254,7 @@ wave_resolve_kernel(const TraceArgs a, const WaveBuffers w, const RayPool cur, c
             for (int k = 0; k < 12; k++) T[k] = IDENTITY[k];
         } else {
             // merlict's closest hit among the candidates, in visiting order
-            if (count > kWaveCandidates) {
+            if (count > kWaveCandidates || count == kWalkInline) {
                 is = first_intersection_tree(sc, root, s, d);
             } else {
                 bool have = false;

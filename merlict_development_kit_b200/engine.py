@@ -175,6 +175,12 @@ class Scene:
         del keep
         return out
 
+    def kernel_launches(self) -> int:
+        """Kernels this scene has launched so far."""
+        v = C.c_uint64(0)
+        check(lib().mlgpu_scene_kernel_launches(self._h, C.byref(v)))
+        return int(v.value)
+
     def sync_errors(self, stream=None) -> None:
         check(lib().mlgpu_scene_sync_errors(self._h, C.c_void_p(_stream_handle(stream))))
 
