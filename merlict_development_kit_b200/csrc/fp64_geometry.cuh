@@ -334,6 +334,22 @@ __device__ __forceinline__ void test_candidate(const DevScene& sc, int32_t leaf,
     }
 }
 
+// merlict's intersection of one leaf with a world ray; leaf < 0 if none.
+__device__ __forceinline__ Isec leaf_hit(const DevScene& sc, int32_t leaf, v3 s, v3 d) {
+    const LeafRec* L = sc.leaf + leaf;
+    double T[12], ti[3], pr[MLGPU_LEAF_PARAMS];
+#pragma unroll
+    for (int k = 0; k < 12; k++) T[k] = __ldg(&L->T[k]);
+#pragma unroll
+    for (int k = 0; k < 3; k++) ti[k] = __ldg(&L->tinv[k]);
+#pragma unroll
+    for (int k = 0; k < MLGPU_LEAF_PARAMS; k++) pr[k] = __ldg(&L->params[k]);
+    Isec h;
+    intersect_leaf(sc, leaf, __ldg(&L->primitive), pr, __ldg(&L->r2), position_inverse(T, ti, s),
+                   orientation_inverse(T, d), &h);
+    return h;
+}
+
 constexpr int kCandidates = 16;
 
 __device__ __forceinline__ void set_void(Isec* is, v3 s, v3 d) {

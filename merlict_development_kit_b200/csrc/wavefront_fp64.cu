@@ -35,7 +35,6 @@ constexpr int kWaveCandidates = 32;     // candidate leaves recorded per ray ste
 constexpr int kWalkChunk = 64;          // slots a warp takes at a time
 constexpr int kWalkBurst = 16;          // tree nodes a lane visits between refills
 constexpr int kNoStep = -2;             // candidate count: photon takes no step
-constexpr int kWalkInline = -3;         // candidate count: resolve walks the frame tree itself
 
 template <typename T>
 __device__ __forceinline__ double load_in(const void* p, uint64_t i) {
@@ -75,6 +74,8 @@ wave_walk_kernel(const TraceArgs a, const WaveBuffers w, const RayPool cur) {
     double sd = 0.0;
     int nc = 0;
     bool overflow = false;
+    bool tree_mode = false;                    // walking a frame's subtree
+    int32_t i = 0, end = 0;                    // frame-tree walk cursor
     // BVH traversal state (single precision slab tests)
     float ox = 0.f, oy = 0.f, oz = 0.f, idx = 0.f, idy = 0.f, idz = 0.f, eps = 0.f;
     int32_t stack[kBvhStack];
@@ -131,14 +132,19 @@ wave_walk_kernel(const TraceArgs a, const WaveBuffers w, const RayPool cur) {
                     item = -1;
                 } else if (root != 0 || sc.bvh_nodes == 0 ||
                            a.traversal == MLGPU_TRAVERSAL_FRAME_TREE) {
-                    // traversal restricted to a frame's subtree (a lens): the
-                    // resolve kernel walks that subtree itself
-                    w.cand_count[slot] = kWalkInline;
-                    item = -1;
+                    // traversal restricted to a frame's subtree (inside a
+                    // lens): merlict's own walk of that subtree
+                    sd = dot(s, d);
+                    nc = 0;
+                    overflow = false;
+                    tree_mode = true;
+                    i = root;
+                    end = __ldg(&sc.node_meta[root].x);
                 } else {
                     sd = dot(s, d);
                     nc = 0;
                     overflow = false;
+                    tree_mode = false;
                     sp = 0;
                     // merlict tests the root frame's own sphere first
                     const double2* np = reinterpret_cast<const double2*>(sc.node);
@@ -165,6 +171,27 @@ wave_walk_kernel(const TraceArgs a, const WaveBuffers w, const RayPool cur) {
             // candidate.  The resolve kernel breaks ties in merlict's
             // visiting order, so the order here does not matter.
             int32_t* cand = w.cand + (size_t)item*kWaveCandidates;
+            if (tree_mode) {
+                // merlict's walk (RayAndFrame.cpp:137-149), candidates in its order
+                for (int it = 0; it < kWalkBurst && i < end; it++) {
+                    const double2* np = reinterpret_cast<const double2*>(sc.node + i);
+                    const double2 n01 = __ldg(np), n23 = __ldg(np + 1);
+                    const int2 meta = __ldg(&sc.node_meta[i]);
+                    if (!sphere_cull(make_double4(n01.x, n01.y, n23.x, n23.y), s, d, sd)) {
+                        i = meta.x;
+                        continue;
+                    }
+                    if (meta.y >= 0) {
+                        if (nc < kWaveCandidates) cand[nc] = meta.y;
+                        nc++;
+                    }
+                    i++;
+                }
+                if (i >= end) {
+                    w.cand_count[item] = nc;
+                    item = -1;
+                }
+            } else {
             for (int it = 0; it < kWalkBurst && sp > 0; it++) {
                 const int32_t ref = stack[--sp];
                 if (ref < 0) {
@@ -205,6 +232,7 @@ wave_walk_kernel(const TraceArgs a, const WaveBuffers w, const RayPool cur) {
                 w.cand_count[item] = overflow ? kWaveCandidates + 1 : nc;
                 item = -1;
             }
+            }
         }
     }
 }
@@ -225,10 +253,15 @@ wave_resolve_kernel(const TraceArgs a, const WaveBuffers w, const RayPool cur, c
     int32_t photon = 0, root = 0, n_next = 0, k_draw = 0, err = 0;
     v3 s = mk(0, 0, 0), d = mk(0, 0, 0);
     double lambda = 0.0, tof = 0.0;
+    int32_t count = 0;
     if (valid) {
-        photon = cur.photon[slot];
         s = mk(cur.sx[slot], cur.sy[slot], cur.sz[slot]);
         d = mk(cur.dx[slot], cur.dy[slot], cur.dz[slot]);
+        count = w.cand_count[slot];
+    }
+
+    if (valid) {
+        photon = cur.photon[slot];
         lambda = cur.lambda[slot];
         tof = cur.tof[slot];
         root = cur.root[slot];
@@ -237,7 +270,6 @@ wave_resolve_kernel(const TraceArgs a, const WaveBuffers w, const RayPool cur, c
         const int32_t err_word = cur.err[slot];
         err = err_word & 0xff;
         int tof_error = (err_word >> 8) & 0xff;
-        const int32_t count = w.cand_count[slot];
         const uint64_t stream = a.rng.photon_offset + (uint64_t)photon;
         mlgpu_history_entry* hist =
             a.results.history ? a.results.history + (uint64_t)photon*hist_len : nullptr;
@@ -253,8 +285,9 @@ wave_resolve_kernel(const TraceArgs a, const WaveBuffers w, const RayPool cur, c
 #pragma unroll
             for (int k = 0; k < 12; k++) T[k] = IDENTITY[k];
         } else {
-            // merlict's closest hit among the candidates, in visiting order
-            if (count > kWaveCandidates || count == kWalkInline) {
+            // merlict's closest hit among the candidates: minimum distance,
+            // ties to merlict's visiting order (RayAndFrame.cpp:160-173)
+            if (count > kWaveCandidates) {
                 is = first_intersection_tree(sc, root, s, d);
             } else {
                 bool have = false;
