@@ -144,19 +144,10 @@ int build_device_scene(mlgpu_scene* s, const mlgpu_flat_scene* f) {
     const int32_t nn = f->num_nodes, nl = f->num_leaves, nf = f->num_functions;
     std::vector<double4> node(nn);
     std::vector<int2> meta(nn);
-    std::vector<float4> node_f(nn);
     for (int32_t i = 0; i < nn; i++) {
         const double* c = f->node_sphere + 4*(size_t)i;
         node[i] = make_double4(c[0], c[1], c[2], c[3]*c[3]);
         meta[i] = make_int2(f->node_skip[i], f->node_leaf[i]);
-        // FP32 cull sphere: centre rounded, radius widened by the rounding
-        // of the centre and of the ray so the cull stays conservative.
-        const float fx = (float)c[0], fy = (float)c[1], fz = (float)c[2];
-        const double dc = std::sqrt((fx - c[0])*(fx - c[0]) + (fy - c[1])*(fy - c[1]) +
-                                    (fz - c[2])*(fz - c[2]));
-        const double mag = std::fabs(c[0]) + std::fabs(c[1]) + std::fabs(c[2]);
-        const double r = c[3]*(1.0 + 1e-5) + dc + 4e-7*mag + 1e-6;
-        node_f[i] = make_float4(fx, fy, fz, (float)(r*r));
     }
     std::vector<LeafRec> leaf(nl > 0 ? nl : 1);
     std::vector<LeafRecF> leaf_f(nl > 0 ? nl : 1);
@@ -196,8 +187,6 @@ int build_device_scene(mlgpu_scene* s, const mlgpu_flat_scene* f) {
         origin[3*(size_t)l + 2] = t[11];
     }
     const int32_t npts = f->function_offset[nf];
-    std::vector<float> pts_f(3*(size_t)npts);
-    for (int32_t k = 0; k < 3*npts; k++) pts_f[k] = (float)f->function_points[k];
 
     int st;
     if ((st = upload(s, node.data(), nn, &s->dev.node))) return st;
@@ -205,10 +194,8 @@ int build_device_scene(mlgpu_scene* s, const mlgpu_flat_scene* f) {
     if ((st = upload(s, leaf.data(), leaf.size(), &s->dev.leaf))) return st;
     if ((st = upload(s, f->function_points, 3*(size_t)npts, &s->dev.fn_points))) return st;
     if ((st = upload(s, f->function_offset, (size_t)nf + 1, &s->dev.fn_offset))) return st;
-    if ((st = upload(s, node_f.data(), nn, &s->dev.node_f))) return st;
     if ((st = upload(s, leaf_f.data(), leaf_f.size(), &s->dev.leaf_f))) return st;
     if ((st = upload(s, origin.data(), origin.size(), &s->dev.leaf_origin))) return st;
-    if ((st = upload(s, pts_f.data(), pts_f.size(), &s->dev.fn_points_f))) return st;
     {
         // BVH over the leaves; boxes widened for single-precision slab tests
         const double* root = f->node_sphere;
@@ -271,8 +258,6 @@ int check_propagate_args(const mlgpu_scene* scene, const mlgpu_photons* ph,
         return fail(MLGPU_ERR_INVALID_ARGUMENT, "unknown tracer %d", st->tracer);
     if (st->traversal != MLGPU_TRAVERSAL_BVH && st->traversal != MLGPU_TRAVERSAL_FRAME_TREE)
         return fail(MLGPU_ERR_INVALID_ARGUMENT, "unknown traversal %d", st->traversal);
-    if (st->tracer != MLGPU_TRACER_FP64 && st->tracer != MLGPU_TRACER_FP64_PLAIN && res->history)
-        return fail(MLGPU_ERR_INVALID_ARGUMENT, "histories are recorded by the FP64 tracer only");
     return MLGPU_OK;
 }
 
@@ -329,13 +314,14 @@ int wave_buffers(mlgpu_scene* scene, uint32_t pool, WaveBuffers* w, RayPool* p0,
     return MLGPU_OK;
 }
 
-// Runs iterations of the wavefront tracer until every photon has finished,
-// checking the counters after every few iterations.
-int run_wavefront(mlgpu_scene* scene, const TraceArgs& a, cudaStream_t stream) {
+// Runs iterations of a wavefront tracer until every photon has finished,
+// checking the counters after every few iterations.  `resolve` selects the
+// intersection arithmetic of the resolve step (FP64 or one of the FP32 forms).
+int run_wavefront(mlgpu_scene* scene, const TraceArgs& a, int resolve, cudaStream_t stream) {
     const uint32_t pool = (uint32_t)std::min<uint64_t>(a.num_photons, kWavePool);
     WaveBuffers w;
     RayPool pools[2];
-    int st = wave_buffers(scene, pool, &w, &pools[0], &pools[1]);
+    const int st = wave_buffers(scene, pool, &w, &pools[0], &pools[1]);
     if (st) return st;
     MLGPU_CUDA(cudaMemsetAsync(w.counters, 0, sizeof(WaveCounters), stream));
     // every iteration advances each live photon by one step
@@ -345,8 +331,17 @@ int run_wavefront(mlgpu_scene* scene, const TraceArgs& a, cudaStream_t stream) {
     const int group = 4;
     while (true) {
         for (int g = 0; g < group; g++, iteration++) {
-            const cudaError_t e = launch_wave_fp64_iteration(
-                a, w, pools[iteration & 1], pools[(iteration + 1) & 1], scene->wave_walk_blocks, stream);
+            const RayPool& cur = pools[iteration & 1];
+            const RayPool& nxt = pools[(iteration + 1) & 1];
+            cudaError_t e;
+            if (resolve == MLGPU_TRACER_FP64) {
+                e = launch_wave_fp64_iteration(a, w, cur, nxt, scene->wave_walk_blocks, stream);
+            } else {
+                e = launch_wave_walk(a, w, cur, scene->wave_walk_blocks, stream);
+                if (e == cudaSuccess)
+                    e = launch_wave32_resolve(a, w, cur, nxt, resolve == MLGPU_TRACER_FP32_PURE, stream);
+                if (e == cudaSuccess) e = launch_wave_after_resolve(w, stream);
+            }
             if (e != cudaSuccess) return cuda_fail(e, "wavefront kernels");
             scene->launches += 4;
         }
@@ -364,10 +359,10 @@ int launch(mlgpu_scene* scene, const TraceArgs& a, const mlgpu_settings* st,
            cudaStream_t stream) {
     cudaError_t e;
     switch (st->tracer) {
-    case MLGPU_TRACER_FP64: return run_wavefront(scene, a, stream);
-    case MLGPU_TRACER_FP64_PLAIN: e = launch_trace_fp64(a, st->block_size, stream); scene->launches++; break;
-    case MLGPU_TRACER_FP32: e = launch_trace_fp32(a, st->block_size, false, stream); break;
-    default: e = launch_trace_fp32(a, st->block_size, true, stream); break;
+    case MLGPU_TRACER_FP64:
+    case MLGPU_TRACER_FP32:
+    case MLGPU_TRACER_FP32_PURE: return run_wavefront(scene, a, st->tracer, stream);
+    default: e = launch_trace_fp64(a, st->block_size, stream); scene->launches++; break;
     }
     if (e != cudaSuccess) return cuda_fail(e, "trace kernel launch");
     return MLGPU_OK;

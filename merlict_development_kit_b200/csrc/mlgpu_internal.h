@@ -64,10 +64,8 @@ struct DevScene {
     const double* fn_points;    // (x, y, slope) triplets
     const int32_t* fn_offset;
     // FP32 copies for the batched tracer
-    const float4* node_f;       // x, y, z (relative to the scene origin), radius^2 (rounded up)
     const LeafRecF* leaf_f;
     const double* leaf_origin;  // [num_leaves][3] translation of each leaf, FP64
-    const float* fn_points_f;
     int32_t num_nodes;
     int32_t num_leaves;
     int32_t num_functions;
@@ -156,12 +154,19 @@ struct WaveBuffers {
     uint32_t pool;
 };
 
+// the walk kernel and counter updates, shared by the FP64 and FP32 forms
+cudaError_t launch_wave_walk(const TraceArgs& a, const WaveBuffers& w, const RayPool& cur,
+                             int walk_blocks, cudaStream_t s);
+cudaError_t launch_wave_after_resolve(const WaveBuffers& w, cudaStream_t s);
+// resolve in single precision (batched FP32 tracer)
+cudaError_t launch_wave32_resolve(const TraceArgs& a, const WaveBuffers& w, const RayPool& cur,
+                                  const RayPool& nxt, bool pure, cudaStream_t s);
+
 cudaError_t launch_trace_fp64(const TraceArgs& a, int block, cudaStream_t s);
 cudaError_t launch_wave_fp64_iteration(const TraceArgs& a, const WaveBuffers& w,
                                        const RayPool& cur, const RayPool& nxt,
                                        int walk_blocks, cudaStream_t s);
 int wave_fp64_walk_blocks();
-cudaError_t launch_trace_fp32(const TraceArgs& a, int block, bool pure, cudaStream_t s);
 cudaError_t launch_bin_arrivals(const DevScene& sc, const int32_t* sensor,
                                 const double* time, uint64_t n, uint32_t* counts,
                                 uint32_t* time_hist, uint32_t num_bins,

@@ -264,7 +264,8 @@ def reflector_camera(focal_length=4.9, davies_cotton=1.0, max_aperture_radius=2.
     if len(order) < num_pixels:
         raise RuntimeError("pixel grid too small")
     for i in range(num_pixels):
-        pix = cam.add(HexPlane(f"pixel_{i}", cells[order[i]], Rot3(0.0, 0.0, deg2rad(30.0))))
+        # unrotated: flat sides face the grid neighbours, pixels tile without overlap
+        pix = cam.add(HexPlane(f"pixel_{i}", cells[order[i]], ROT3_UNITY))
         pix.set_outer_hex_radius(pixel_flat2flat / math.sqrt(3.0))
         sc.add_sensor(i, pix)
     if shield_radius > 0.0:

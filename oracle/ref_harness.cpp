@@ -244,8 +244,7 @@ void build_primitive_zoo(Handle* h) {
     const std::vector<ml::Vec3> cells = grid.get_grid();
     for (size_t i = 0; i < cells.size(); i++) {
         ml::HexPlane* pix = cam->add<ml::HexPlane>();
-        pix->set_name_pos_rot("pixel_" + std::to_string(i), cells[i],
-                              ml::Rot3(0.0, 0.0, 30*deg));
+        pix->set_name_pos_rot("pixel_" + std::to_string(i), cells[i], ml::ROT3_UNITY);
         pix->set_outer_hex_radius(0.25/std::sqrt(3.0));
         sense(pix);
     }
@@ -293,8 +292,9 @@ void build_reflector_camera(Handle* h, const double* p, int n) {
     if (order.size() < num_pixels) throw std::runtime_error("pixel grid too small");
     for (unsigned i = 0; i < num_pixels; i++) {
         ml::HexPlane* pix = cam->add<ml::HexPlane>();
-        pix->set_name_pos_rot("pixel_" + std::to_string(i), cells[order[i]],
-                              ml::Rot3(0.0, 0.0, ml::deg2rad(30.0)));
+        // unrotated: the hexagons' flat sides face the grid's neighbours, so
+        // the pixels tile the focal plane without overlap
+        pix->set_name_pos_rot("pixel_" + std::to_string(i), cells[order[i]], ml::ROT3_UNITY);
         pix->set_outer_hex_radius(pixel_f2f/std::sqrt(3.0));
         h->owned_sensors.push_back(new ml::sensor::Sensor(i, pix));
     }

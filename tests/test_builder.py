@@ -33,6 +33,26 @@ def test_reflector_camera_matches_reference_factory():
     assert flat_diff(mine, ref) == []
 
 
+def test_reflector_camera_pixels_tile_without_overlap():
+    """Every point of the focal plane lies in at most one pixel hexagon: the
+    closest hit never has to choose between two coplanar pixels at the same
+    distance."""
+    flat = F.reflector_camera().flatten()
+    T = np.asarray(flat.leaf_frame2world).reshape(-1, 3, 4)
+    P = np.asarray(flat.leaf_params).reshape(-1, abi.LEAF_PARAMS)
+    U = np.array([flat.hex_unit_u, flat.hex_unit_v, flat.hex_unit_w])
+    pixels = [l for l in range(flat.num_leaves) if flat.leaf_sensor[l] >= 0]
+    assert len(pixels) == 1440
+    rng = np.random.default_rng(1)
+    pts = np.c_[rng.uniform(-0.15, 0.15, (100_000, 2)), np.full(100_000, 4.9)]
+    covered = np.zeros(len(pts), int)
+    for l in pixels:
+        local = (pts - T[l][:, 3]) @ T[l][:, :3]
+        covered += (np.abs(local @ U.T) < P[l][0]).all(1)
+    assert covered.max() == 1
+    assert covered.mean() > 0.2
+
+
 @needs_ref
 def test_light_field_telescope_matches_reference_factory():
     """The full config-1 scene: 93,459 nodes, 78,378 leaves, 63,379 lixels."""
