@@ -42,6 +42,11 @@ BYTES_PER_PHOTON = {"fp64": 88, "fp64_plain": 88, "fp32": 52}
 # Fresnel steps, time-of-flight segments, table look-ups)
 FLOP_WEIGHTS = {"nodes": 26, "leaves": 48, "caps": 29, "cap_bounds": 85, "planes": 36,
                 "others": 29, "reflections": 91, "fresnels": 110, "segments": 3, "funcs": 4}
+# the kernel class that does each counted operation
+FLOP_STAGE = {"nodes": "walk", "leaves": "intersect", "caps": "intersect",
+              "cap_bounds": "intersect", "planes": "intersect", "others": "intersect",
+              "reflections": "resolve", "fresnels": "resolve", "segments": "resolve",
+              "funcs": "resolve"}
 FP64_PEAK_TFLOPS_NOMINAL = 37.0   # B200 vector FP64, nominal (no measured figure)
 FP32_PEAK_TFLOPS_NOMINAL = 75.0   # B200 vector FP32 (non-tensor), nominal
 WORKLOAD = "light-field telescope, 1039 lenses x 61 lixels (config 1)"
@@ -246,8 +251,7 @@ def run_ours(args, world, rank, local):
         if ev is not None:
             ev[0].record(stream)
         out = scene.propagate(dev, cfg, rng, tracer=tracer, outputs=("sensor", "x", "y", "time"),
-                              out_dtype=out_dtype, sync=False, results=results,
-                              traversal="frame_tree")
+                              out_dtype=out_dtype, sync=False, results=results)
         if ev is not None:
             ev[1].record(stream)
         scene.bin_arrivals(out["sensor"])
@@ -267,6 +271,7 @@ def run_ours(args, world, rank, local):
     t_start = torch.cuda.Event(enable_timing=True)
     t_stop = torch.cuda.Event(enable_timing=True)
     launches0 = scene.kernel_launches()
+    scene.set_profiling(True)   # CUDA events around every kernel class
     t_start.record(stream)
     for k in range(args.steps):
         step(kernel_events[k])
@@ -275,6 +280,8 @@ def run_ours(args, world, rank, local):
     torch.cuda.synchronize()
     barrier(world)
     clk = clocks.stop()
+    stage = scene.kernel_times()
+    scene.set_profiling(False)
     scene.sync_errors()
     elapsed_ms = t_start.elapsed_time(t_stop)
     kernel_ms = float(np.mean([a.elapsed_time(b) for a, b in kernel_events]))
@@ -298,7 +305,7 @@ def run_ours(args, world, rank, local):
     res.dtype = abi.F64 if out_dtype == torch.float64 else abi.F32
     res.sensor, res.x, res.y, res.time = (h_sensor.data_ptr(), h_x.data_ptr(), h_y.data_ptr(),
                                           h_t.data_ptr())
-    st = abi.mlgpu_settings(MAX_INTERACTIONS, 0, engine.TRACERS[tracer], 0, abi.TRAVERSAL_FRAME_TREE)
+    st = abi.mlgpu_settings(MAX_INTERACTIONS, 0, engine.TRACERS[tracer], 0, abi.TRAVERSAL_BVH)
     r = abi.mlgpu_rng()
     r.mode = abi.RNG_PHILOX
     r.seed = 99 + rank
@@ -323,21 +330,45 @@ def run_ours(args, world, rank, local):
         return
     hbm_peak, peak_kind = load_peaks()
     bpp = BYTES_PER_PHOTON[tracer]
-    achieved_gbs = bpp * n / (kernel_ms * 1e-3) / 1e9
-    roofline = {"bound": "hbm", "achieved": achieved_gbs, "peak": hbm_peak, "unit": "GB/s",
-                "frac": achieved_gbs / hbm_peak, "traffic": None,
-                "peak_source": f"{peak_kind} MEASURED_PEAKS.json hbm_gbs",
-                "bytes_per_photon": bpp}
+    fp32 = tracer == "fp32"
+    vec_peak = FP32_PEAK_TFLOPS_NOMINAL if fp32 else FP64_PEAK_TFLOPS_NOMINAL
     counts = flop_counts()
-    compute = None
-    if counts:
-        per = counts["per_photon"]
-        flops = sum(FLOP_WEIGHTS[k] * per.get(k, 0.0) for k in FLOP_WEIGHTS)
-        peak = FP32_PEAK_TFLOPS_NOMINAL if tracer == "fp32" else FP64_PEAK_TFLOPS_NOMINAL
-        achieved = flops * n / (kernel_ms * 1e-3) / 1e12
-        compute = {"bound": "fp32" if tracer == "fp32" else "fp64", "flops_per_photon": flops,
-                   "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
-                   "frac": achieved / peak, "peak_source": "nominal B200 vector peak"}
+    per = counts["per_photon"] if counts else {}
+    stage_flops = {}
+    for k, w in FLOP_WEIGHTS.items():
+        stage_flops[FLOP_STAGE[k]] = stage_flops.get(FLOP_STAGE[k], 0.0) + w * per.get(k, 0.0)
+    total_stage_ms = sum(ms for ms, _ in stage.values())
+    kernels = {}
+    for name, (ms, nl) in stage.items():
+        if nl == 0:
+            continue
+        f = stage_flops.get(name, 0.0) * n * args.steps
+        kernels[name] = {"ms_per_step": ms / args.steps, "launches": nl,
+                         "avg_launch_ms": ms / nl, "share": ms / total_stage_ms,
+                         "flops_per_photon": stage_flops.get(name, 0.0),
+                         "tflops": f / (ms * 1e-3) / 1e12 if ms > 0 else None}
+    dominant = max(kernels, key=lambda k: kernels[k]["ms_per_step"])
+    dk = kernels[dominant]
+    # the dominant stage against the vector pipe that bounds it: the
+    # reference's operation counts for that stage, per photon, times the
+    # photons of a step, over the stage's device time per step
+    achieved = dk["flops_per_photon"] * n / (dk["ms_per_step"] * 1e-3) / 1e12
+    roofline = {"bound": "fp32" if fp32 else "fp64", "kernel": dominant,
+                "achieved": achieved, "peak": vec_peak, "unit": "TFLOP/s",
+                "frac": achieved / vec_peak, "traffic": None,
+                "peak_source": "nominal B200 vector %s peak (no measured figure)" %
+                               ("FP32" if fp32 else "FP64"),
+                "flops_per_photon": dk["flops_per_photon"]}
+    flops = sum(stage_flops.values())
+    whole = flops * n / (kernel_ms * 1e-3) / 1e12
+    compute = {"bound": roofline["bound"], "flops_per_photon": flops, "achieved": whole,
+               "peak": vec_peak, "unit": "TFLOP/s", "frac": whole / vec_peak,
+               "scope": "whole propagate call"}
+    achieved_gbs = bpp * n / (kernel_ms * 1e-3) / 1e9
+    hbm = {"bound": "hbm", "achieved": achieved_gbs, "peak": hbm_peak, "unit": "GB/s",
+           "frac": achieved_gbs / hbm_peak,
+           "peak_source": f"{peak_kind} MEASURED_PEAKS.json hbm_gbs",
+           "bytes_per_photon": bpp, "scope": "whole propagate call"}
     cpu = None
     if world == 1 and not args.no_cpu_baseline:
         v, secs, cores, kind, sample = cpu_reference_run(args.ref_photons, 2, 1)
@@ -346,7 +377,7 @@ def run_ours(args, world, rank, local):
         "metric": "photons/s", "value": value, "unit": "photons/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": elapsed_ms / args.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-        "dtype": "f32" if tracer == "fp32" else "f64",
+        "dtype": "f32" if fp32 else "f64",
         "data": "synthetic",
         "config": {"workload": WORKLOAD, "scene": scene_config_name(), "tracer": tracer,
                    "photons_per_step_per_gpu": n, "max_interactions": MAX_INTERACTIONS,
@@ -354,6 +385,8 @@ def run_ours(args, world, rank, local):
         "kernel_ms": kernel_ms,
         "roofline": roofline,
         "compute_roofline": compute,
+        "hbm_roofline": hbm,
+        "kernels": kernels,
         "cpu_baseline": cpu,
         "e2e": {"value": e2e_value, "unit": "photons/s", "h2d_bytes_per_step": h2d,
                 "d2h_bytes_per_step": d2h},

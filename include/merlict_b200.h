@@ -245,6 +245,29 @@ int mlgpu_scene_destroy(mlgpu_scene* scene);
  * callers that account for GPU work.                                      */
 int mlgpu_scene_kernel_launches(const mlgpu_scene* scene, uint64_t* launches);
 
+/* Kernel classes timed by the profiling hook below.  No counterpart in the
+ * reference: it exists so that callers can put a roofline on each stage of
+ * the device pipeline.                                                    */
+enum {
+    MLGPU_KERNEL_WALK = 0,       /* tree walk, candidate lists, photon intake */
+    MLGPU_KERNEL_QUEUE = 1,      /* candidate queue and pool counters         */
+    MLGPU_KERNEL_INTERSECT = 2,  /* one thread per queued candidate           */
+    MLGPU_KERNEL_RESOLVE = 3,    /* closest hit, interaction, compaction      */
+    MLGPU_KERNEL_PLAIN = 4,      /* one-thread-per-photon tracer              */
+    MLGPU_KERNEL_BIN = 5,        /* arrival binning                           */
+    MLGPU_KERNEL_CLASSES = 6
+};
+
+/* Turns CUDA-event timing of every kernel class on (enable != 0) or off
+ * and clears the totals.  While on, each launch is bracketed by events on
+ * the caller's stream, which costs a few microseconds per launch.        */
+int mlgpu_scene_set_profiling(mlgpu_scene* scene, int enable);
+
+/* Device milliseconds and launches per kernel class since profiling was
+ * last turned on; waits for the outstanding timed launches.  `ms` and
+ * `launches` hold MLGPU_KERNEL_CLASSES entries each (either may be NULL). */
+int mlgpu_scene_kernel_times(mlgpu_scene* scene, double* ms, uint64_t* launches);
+
 /* ---- propagation ------------------------------------------------------ *
  * Replaces propagate_photons_in_frame_with_config (merlict/Photons.cpp:9-22)
  * and its thread-pool twin (merlict_multi_thread.cpp:28-55).

@@ -59,6 +59,9 @@ def lib():
             C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint64, C.c_void_p, C.c_void_p,
             C.c_uint32, C.c_double, C.c_double, C.c_void_p]
         L.mlgpu_scene_kernel_launches.argtypes = [C.c_void_p, C.POINTER(C.c_uint64)]
+        L.mlgpu_scene_set_profiling.argtypes = [C.c_void_p, C.c_int]
+        L.mlgpu_scene_kernel_times.argtypes = [C.c_void_p, C.POINTER(C.c_double),
+                                               C.POINTER(C.c_uint64)]
         L.mlgpu_bin_arrivals_noalloc.argtypes = [
             C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint64, C.c_void_p, C.c_void_p,
             C.c_uint32, C.c_double, C.c_double, C.c_void_p]
@@ -88,4 +91,5 @@ EXPORTED = (
     "mlgpu_abi_version", "mlgpu_last_error", "mlgpu_scene_create", "mlgpu_scene_destroy",
     "mlgpu_propagate", "mlgpu_scene_sync_errors", "mlgpu_propagate_host",
     "mlgpu_bin_arrivals", "mlgpu_bin_arrivals_noalloc", "mlgpu_scene_kernel_launches",
+    "mlgpu_scene_set_profiling", "mlgpu_scene_kernel_times",
 )

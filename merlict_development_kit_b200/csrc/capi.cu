@@ -55,6 +55,72 @@ struct DeviceBuffer {
     }
 };
 
+// CUDA-event timing of the kernel classes (mlgpu_scene_set_profiling).
+// A chain is a run of events recorded on one stream with one kernel class
+// between each neighbouring pair; chains stay pending until flushed.
+struct Profiler {
+    static constexpr int kMaxChain = 6;
+    struct Chain {
+        int n = 0;                          // events in the chain
+        cudaEvent_t ev[kMaxChain];
+        int cls[kMaxChain - 1];             // class between ev[k] and ev[k + 1]
+        int launches[kMaxChain - 1];
+    };
+    bool on = false;
+    std::vector<Chain> pending;
+    std::vector<cudaEvent_t> spare;
+    double ms[MLGPU_KERNEL_CLASSES] = {};
+    uint64_t launches[MLGPU_KERNEL_CLASSES] = {};
+
+    cudaEvent_t take() {
+        if (!spare.empty()) { cudaEvent_t e = spare.back(); spare.pop_back(); return e; }
+        cudaEvent_t e = nullptr;
+        if (cudaEventCreate(&e) != cudaSuccess) return nullptr;
+        return e;
+    }
+    // Takes n events; false (and none taken) if one cannot be created.
+    bool take(int n, cudaEvent_t* out) {
+        for (int k = 0; k < n; k++) {
+            out[k] = take();
+            if (!out[k]) {
+                for (int j = 0; j < k; j++) spare.push_back(out[j]);
+                return false;
+            }
+        }
+        return true;
+    }
+    void add(const Chain& c) {
+        pending.push_back(c);
+        if (pending.size() > 4096) flush();   // bounds the pool of events
+    }
+    // Folds the pending chains into the totals (waits for their last events).
+    cudaError_t flush() {
+        cudaError_t err = cudaSuccess;
+        for (const Chain& c : pending) {
+            cudaError_t e = cudaEventSynchronize(c.ev[c.n - 1]);
+            for (int k = 0; e == cudaSuccess && k + 1 < c.n; k++) {
+                float t = 0.0f;
+                e = cudaEventElapsedTime(&t, c.ev[k], c.ev[k + 1]);
+                if (e == cudaSuccess) { ms[c.cls[k]] += t; launches[c.cls[k]] += c.launches[k]; }
+            }
+            if (e != cudaSuccess && err == cudaSuccess) err = e;
+            for (int k = 0; k < c.n; k++) spare.push_back(c.ev[k]);
+        }
+        pending.clear();
+        return err;
+    }
+    cudaError_t reset() {
+        const cudaError_t e = flush();
+        for (int k = 0; k < MLGPU_KERNEL_CLASSES; k++) { ms[k] = 0.0; launches[k] = 0; }
+        return e;
+    }
+    void release() {
+        flush();
+        for (cudaEvent_t e : spare) cudaEventDestroy(e);
+        spare.clear();
+    }
+};
+
 }  // namespace
 
 struct mlgpu_scene {
@@ -68,7 +134,9 @@ struct mlgpu_scene {
     DeviceBuffer wave;
     WaveCounters* wave_host = nullptr;   // pinned copy of the counters
     int wave_walk_blocks = 0;
+    int wave_isect_blocks = 0;
     uint64_t launches = 0;               // kernels launched for this scene
+    Profiler prof;
 };
 
 namespace {
@@ -187,6 +255,7 @@ int build_device_scene(mlgpu_scene* s, const mlgpu_flat_scene* f) {
         origin[3*(size_t)l + 2] = t[11];
     }
     const int32_t npts = f->function_offset[nf];
+    s->dev.num_fn_points = npts;
 
     int st;
     if ((st = upload(s, node.data(), nn, &s->dev.node))) return st;
@@ -292,25 +361,41 @@ constexpr uint32_t kWavePool = 1u << 21;   // ray slots of the wavefront tracers
 // Carves the two ray pools, the candidate lists and the counters out of
 // one device buffer.
 int wave_buffers(mlgpu_scene* scene, uint32_t pool, WaveBuffers* w, RayPool* p0, RayPool* p1) {
-    const size_t per_pool = (size_t)pool*(8*8 + 5*4);
-    const size_t bytes = 2*per_pool + (size_t)pool*(4*32 + 4) + 4096;
-    MLGPU_CUDA(scene->wave.reserve(bytes));
+    auto up = [](size_t x) { return (x + 255) & ~size_t(255); };
+    const size_t per_pool = 8*up((size_t)pool*8) + 5*up((size_t)pool*4);
+    const size_t spills = (size_t)kSpillRows*kSpillCap;
+    const size_t lists = up((size_t)pool*32*4) + up((size_t)pool*4) + up((size_t)pool*32*8) +
+        up(((size_t)pool*32 + spills)*4) + up((size_t)pool*4) + up(spills*4) + up(spills*8) +
+        up((size_t)pool*4) + up((size_t)kSpillRows*4);
+    MLGPU_CUDA(scene->wave.reserve(256 + 2*per_pool + lists));
     if (!scene->wave_host) MLGPU_CUDA(cudaMallocHost(&scene->wave_host, sizeof(WaveCounters)));
     if (!scene->wave_walk_blocks) scene->wave_walk_blocks = wave_fp64_walk_blocks();
+    if (!scene->wave_isect_blocks) scene->wave_isect_blocks = wave_isect_blocks();
     char* b = static_cast<char*>(scene->wave.ptr);
     w->counters = reinterpret_cast<WaveCounters*>(b);
     b += 256;
+    auto take = [&](size_t bytes) { char* p = b; b += up(bytes); return p; };
     RayPool* pools[2] = {p0, p1};
     for (RayPool* p : pools) {
         double** d[8] = {&p->sx, &p->sy, &p->sz, &p->dx, &p->dy, &p->dz, &p->lambda, &p->tof};
-        for (double** q : d) { *q = reinterpret_cast<double*>(b); b += (size_t)pool*8; }
+        for (double** q : d) *q = reinterpret_cast<double*>(take((size_t)pool*8));
         int32_t** i[5] = {&p->photon, &p->root, &p->n_int, &p->k_draw, &p->err};
-        for (int32_t** q : i) { *q = reinterpret_cast<int32_t*>(b); b += ((size_t)pool*4 + 255) & ~size_t(255); }
+        for (int32_t** q : i) *q = reinterpret_cast<int32_t*>(take((size_t)pool*4));
     }
-    w->cand = reinterpret_cast<int32_t*>(b);
-    b += (size_t)pool*32*4;
-    w->cand_count = reinterpret_cast<int32_t*>(b);
+    w->cand = reinterpret_cast<int32_t*>(take((size_t)pool*32*4));
+    w->cand_count = reinterpret_cast<int32_t*>(take((size_t)pool*4));
+    w->cand_dist = reinterpret_cast<double*>(take((size_t)pool*32*8));
+    w->queue = reinterpret_cast<uint32_t*>(take(((size_t)pool*32 + spills)*4));
+    w->overflow = reinterpret_cast<uint32_t*>(take((size_t)pool*4));
+    w->spill = reinterpret_cast<int32_t*>(take(spills*4));
+    w->spill_dist = reinterpret_cast<double*>(take(spills*8));
+    w->spill_row = reinterpret_cast<int32_t*>(take((size_t)pool*4));
+    w->spill_slot = reinterpret_cast<uint32_t*>(take((size_t)kSpillRows*4));
     w->pool = pool;
+    const size_t fn_bytes = (size_t)scene->dev.num_fn_points*3*sizeof(double) +
+        ((size_t)scene->dev.num_functions + 1)*sizeof(int32_t);
+    w->fn_smem_bytes = fn_bytes <= 16384 ? (int)fn_bytes : 0;
+    w->isect_blocks = scene->wave_isect_blocks;
     return MLGPU_OK;
 }
 
@@ -333,17 +418,20 @@ int run_wavefront(mlgpu_scene* scene, const TraceArgs& a, int resolve, cudaStrea
         for (int g = 0; g < group; g++, iteration++) {
             const RayPool& cur = pools[iteration & 1];
             const RayPool& nxt = pools[(iteration + 1) & 1];
-            cudaError_t e;
-            if (resolve == MLGPU_TRACER_FP64) {
-                e = launch_wave_fp64_iteration(a, w, cur, nxt, scene->wave_walk_blocks, stream);
-            } else {
-                e = launch_wave_walk(a, w, cur, scene->wave_walk_blocks, stream);
-                if (e == cudaSuccess)
-                    e = launch_wave32_resolve(a, w, cur, nxt, resolve == MLGPU_TRACER_FP32_PURE, stream);
-                if (e == cudaSuccess) e = launch_wave_after_resolve(w, stream);
-            }
+            Profiler::Chain ch;
+            const bool timed = scene->prof.on && scene->prof.take(5, ch.ev);
+            const cudaError_t e = launch_wave_iteration(a, w, cur, nxt, scene->wave_walk_blocks,
+                                                        resolve, stream, timed ? ch.ev : nullptr);
             if (e != cudaSuccess) return cuda_fail(e, "wavefront kernels");
-            scene->launches += 4;
+            scene->launches += 7;
+            if (timed) {
+                ch.n = 5;
+                const int cls[4] = {MLGPU_KERNEL_WALK, MLGPU_KERNEL_QUEUE, MLGPU_KERNEL_INTERSECT,
+                                    MLGPU_KERNEL_RESOLVE};
+                const int launches[4] = {1, 3, 1, 2};
+                for (int k = 0; k < 4; k++) { ch.cls[k] = cls[k]; ch.launches[k] = launches[k]; }
+                scene->prof.add(ch);
+            }
         }
         MLGPU_CUDA(cudaMemcpyAsync(scene->wave_host, w.counters, sizeof(WaveCounters),
                                    cudaMemcpyDeviceToHost, stream));
@@ -362,7 +450,19 @@ int launch(mlgpu_scene* scene, const TraceArgs& a, const mlgpu_settings* st,
     case MLGPU_TRACER_FP64:
     case MLGPU_TRACER_FP32:
     case MLGPU_TRACER_FP32_PURE: return run_wavefront(scene, a, st->tracer, stream);
-    default: e = launch_trace_fp64(a, st->block_size, stream); scene->launches++; break;
+    default: {
+        Profiler::Chain ch;
+        const bool timed = scene->prof.on && scene->prof.take(2, ch.ev);
+        if (timed) cudaEventRecord(ch.ev[0], stream);
+        e = launch_trace_fp64(a, st->block_size, stream);
+        scene->launches++;
+        if (timed) {
+            cudaEventRecord(ch.ev[1], stream);
+            ch.n = 2; ch.cls[0] = MLGPU_KERNEL_PLAIN; ch.launches[0] = 1;
+            scene->prof.add(ch);
+        }
+        break;
+    }
     }
     if (e != cudaSuccess) return cuda_fail(e, "trace kernel launch");
     return MLGPU_OK;
@@ -430,6 +530,7 @@ int mlgpu_scene_destroy(mlgpu_scene* scene) {
     scene->bin_scratch.release();
     scene->wave.release();
     if (scene->wave_host) cudaFreeHost(scene->wave_host);
+    scene->prof.release();
     delete scene;
     return MLGPU_OK;
 }
@@ -552,10 +653,19 @@ int mlgpu_bin_arrivals(mlgpu_scene* scene, const int32_t* sensor, const double* 
     // partial histograms: one slice of `keys` words per photon slice
     const size_t slices = 32;
     MLGPU_CUDA(scene->bin_scratch.reserve(slices*keys*sizeof(uint32_t) + 256));
+    const cudaStream_t stream = static_cast<cudaStream_t>(cuda_stream);
+    Profiler::Chain ch;
+    const bool timed = scene->prof.on && scene->prof.take(2, ch.ev);
+    if (timed) cudaEventRecord(ch.ev[0], stream);
     const cudaError_t e = launch_bin_arrivals(
         scene->dev, sensor, time, n, counts, num_time_bins ? time_hist : nullptr,
         num_time_bins, t_min, t_max, static_cast<uint32_t*>(scene->bin_scratch.ptr),
-        scene->bin_scratch.bytes / sizeof(uint32_t), static_cast<cudaStream_t>(cuda_stream));
+        scene->bin_scratch.bytes / sizeof(uint32_t), stream);
+    if (timed) {
+        cudaEventRecord(ch.ev[1], stream);
+        ch.n = 2; ch.cls[0] = MLGPU_KERNEL_BIN; ch.launches[0] = 2;
+        scene->prof.add(ch);
+    }
     if (e != cudaSuccess) return cuda_fail(e, "binning kernels");
     scene->launches += 2;
     return MLGPU_OK;
@@ -564,6 +674,25 @@ int mlgpu_bin_arrivals(mlgpu_scene* scene, const int32_t* sensor, const double* 
 int mlgpu_scene_kernel_launches(const mlgpu_scene* scene, uint64_t* launches) {
     if (!scene || !launches) return fail(MLGPU_ERR_INVALID_ARGUMENT, "NULL argument");
     *launches = scene->launches;
+    return MLGPU_OK;
+}
+
+int mlgpu_scene_set_profiling(mlgpu_scene* scene, int enable) {
+    if (!scene) return fail(MLGPU_ERR_INVALID_ARGUMENT, "NULL argument");
+    const cudaError_t e = scene->prof.reset();
+    scene->prof.on = enable != 0;
+    if (e != cudaSuccess) return cuda_fail(e, "profiling events");
+    return MLGPU_OK;
+}
+
+int mlgpu_scene_kernel_times(mlgpu_scene* scene, double* ms, uint64_t* launches) {
+    if (!scene) return fail(MLGPU_ERR_INVALID_ARGUMENT, "NULL argument");
+    const cudaError_t e = scene->prof.flush();
+    if (e != cudaSuccess) return cuda_fail(e, "profiling events");
+    for (int k = 0; k < MLGPU_KERNEL_CLASSES; k++) {
+        if (ms) ms[k] = scene->prof.ms[k];
+        if (launches) launches[k] = scene->prof.launches[k];
+    }
     return MLGPU_OK;
 }
 

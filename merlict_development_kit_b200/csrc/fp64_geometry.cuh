@@ -101,6 +101,33 @@ __device__ double func_eval(const DevScene& sc, int32_t f, double x, int* err) {
     return slope*x + __ldg(p0 + 1) - slope*__ldg(p0);
 }
 
+// func_eval on tables at `pts` / `off` (a shared-memory copy, say); the
+// same arithmetic, so the same bits.
+__device__ double func_eval_tab(const double* pts, const int32_t* off, int32_t f, double x,
+                                int* err) {
+    const int32_t b = off[f];
+    const int32_t n = off[f + 1] - b;
+    const double* p = pts + 3*(size_t)b;
+    if (x < p[0] || x >= p[3*(n - 1)]) {
+        if (!*err) *err = MLGPU_ERR_OUT_OF_RANGE;
+        return 0.0;
+    }
+    int32_t first = 0, count = n;
+    while (count > 0) {
+        const int32_t step = count >> 1;
+        const int32_t it = first + step;
+        if (!(p[3*it] > x)) { first = it + 1; count -= step + 1; }
+        else { count = step; }
+    }
+    if (first == 0 || (first == n && x > p[3*(n - 1)])) {
+        if (!*err) *err = MLGPU_ERR_OUT_OF_RANGE;
+        return 0.0;
+    }
+    const double* p0 = p + 3*(first - 1);
+    const double slope = p0[2];
+    return slope*x + p0[1] - slope*p0[0];
+}
+
 // HexagonalPrismZ::is_inside, HexagonalPrismZ.cpp:14-30
 __device__ __forceinline__ bool hex_inside(const DevScene& sc, double inner, v3 v) {
     const double u = dot(mk(sc.hex_u[0], sc.hex_u[1], sc.hex_u[2]), v);

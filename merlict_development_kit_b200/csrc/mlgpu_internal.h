@@ -69,6 +69,7 @@ struct DevScene {
     int32_t num_nodes;
     int32_t num_leaves;
     int32_t num_functions;
+    int32_t num_fn_points;      // fn_offset[num_functions]
     int32_t default_refraction;
     int32_t num_sensors;
     double hex_u[3], hex_v[3], hex_w[3];
@@ -133,7 +134,16 @@ struct WaveCounters {
     unsigned int total;              // active + new photons of this iteration
     unsigned int next;               // survivors written to the next pool
     unsigned int walk_fetch;         // slots handed out by the walk kernel
+    unsigned int queue_len;          // (slot, candidate) pairs queued for intersection
+    unsigned int overflow_len;       // slots whose candidate list overflowed
+    unsigned int spill_used;         // spill rows handed out in this iteration
 };
+
+// A slot with more than 32 candidates continues its list in a spill row
+// of kSpillCap entries; a list longer than both is resolved by merlict's
+// own walk of the frame tree.
+constexpr int kSpillCap = 992;
+constexpr uint32_t kSpillRows = 16384;
 
 struct RayPool {
     int32_t* photon;
@@ -151,21 +161,34 @@ struct WaveBuffers {
     WaveCounters* counters;
     int32_t* cand;           // [pool][32] candidate leaves of the current step
     int32_t* cand_count;     // [pool]
+    double* cand_dist;       // [pool][32] distance to each candidate's hit, -1: none
+    uint32_t* queue;         // slot * 32 + k of every candidate to intersect
+    uint32_t* overflow;      // [pool] slots whose candidate list overflowed
+    int32_t* spill;          // [kSpillRows][kSpillCap] candidates 33 and up
+    double* spill_dist;      // [kSpillRows][kSpillCap]
+    int32_t* spill_row;      // [pool] spill row of a slot (valid when its count > 32)
+    uint32_t* spill_slot;    // [kSpillRows] slot of each spill row
     uint32_t pool;
+    int isect_blocks;        // persistent grid of the intersection kernel
+    int fn_smem_bytes;       // property tables staged in shared memory (0: read from global)
 };
 
-// the walk kernel and counter updates, shared by the FP64 and FP32 forms
-cudaError_t launch_wave_walk(const TraceArgs& a, const WaveBuffers& w, const RayPool& cur,
-                             int walk_blocks, cudaStream_t s);
-cudaError_t launch_wave_after_resolve(const WaveBuffers& w, cudaStream_t s);
-// resolve in single precision (batched FP32 tracer)
-cudaError_t launch_wave32_resolve(const TraceArgs& a, const WaveBuffers& w, const RayPool& cur,
-                                  const RayPool& nxt, bool pure, cudaStream_t s);
+// One iteration of a wavefront tracer: walk, queue and intersect the
+// candidates, resolve.  `form` is MLGPU_TRACER_FP64, _FP32 or _FP32_PURE;
+// the FP32 forms' kernels live in wavefront_fp32.cu.
+// With `ev` non-null, events ev[0..4] are recorded before the walk, after
+// it, after the queue, after the intersections and after the resolve step.
+cudaError_t launch_wave_iteration(const TraceArgs& a, const WaveBuffers& w, const RayPool& cur,
+                                  const RayPool& nxt, int walk_blocks, int form, cudaStream_t s,
+                                  cudaEvent_t* ev);
+// the FP32 forms' intersection and resolve kernels; `mid` (may be null) is
+// recorded between them
+cudaError_t launch_wave32_isect_resolve(const TraceArgs& a, const WaveBuffers& w,
+                                        const RayPool& cur, const RayPool& nxt, bool pure,
+                                        cudaStream_t s, cudaEvent_t mid);
+int wave_isect_blocks();
 
 cudaError_t launch_trace_fp64(const TraceArgs& a, int block, cudaStream_t s);
-cudaError_t launch_wave_fp64_iteration(const TraceArgs& a, const WaveBuffers& w,
-                                       const RayPool& cur, const RayPool& nxt,
-                                       int walk_blocks, cudaStream_t s);
 int wave_fp64_walk_blocks();
 cudaError_t launch_bin_arrivals(const DevScene& sc, const int32_t* sensor,
                                 const double* time, uint64_t n, uint32_t* counts,

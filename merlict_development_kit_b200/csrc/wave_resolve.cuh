@@ -27,6 +27,7 @@ constexpr int kWaveCandidates = 32;     // candidate leaves recorded per ray ste
 constexpr int kWalkChunk = 64;          // slots a warp takes at a time
 constexpr int kWalkBurst = 16;          // tree nodes a lane visits between refills
 constexpr int kNoStep = -2;             // candidate count: photon takes no step
+constexpr int kOverflowBlocks = 148;    // grid of the overflow kernel
 
 template <typename T>
 __device__ __forceinline__ double load_in(const void* p, uint64_t i) {
@@ -48,10 +49,115 @@ constexpr int kIsectFp64 = 0;
 constexpr int kIsectFp32 = 1;
 constexpr int kIsectFp32Pure = 2;
 
+// Queues every (slot, candidate) pair of this step for the intersection
+// kernel: a block-wide scan of the candidate counts and one atomic per block.
+// Slots without a step or whose list overflowed queue nothing.
+__global__ void __launch_bounds__(256)
+wave_enqueue_kernel(const WaveBuffers w) {
+    __shared__ uint32_t warp_sum[8];
+    __shared__ uint32_t block_base;
+    const uint32_t total = w.counters->total;
+    const uint32_t slot = blockIdx.x*blockDim.x + threadIdx.x;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    int32_t c = slot < total ? w.cand_count[slot] : 0;
+    if (c > kWaveCandidates + kSpillCap) w.overflow[atomicAdd(&w.counters->overflow_len, 1u)] = slot;
+    if (c < 0 || c > kWaveCandidates + kSpillCap) c = 0;
+    // inclusive scan within the warp
+    uint32_t x = (uint32_t)c;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t y = __shfl_up_sync(kFull, x, o);
+        if (lane >= o) x += y;
+    }
+    if (lane == 31) warp_sum[warp] = x;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        uint32_t run = 0;
+        for (int k = 0; k < 8; k++) { const uint32_t t = warp_sum[k]; warp_sum[k] = run; run += t; }
+        block_base = run ? atomicAdd(&w.counters->queue_len, run) : 0u;
+    }
+    __syncthreads();
+    const uint32_t first = block_base + warp_sum[warp] + x - (uint32_t)c;
+    const int own = c < kWaveCandidates ? c : kWaveCandidates;
+    for (int k = 0; k < own; k++) w.queue[first + k] = slot*kWaveCandidates + (uint32_t)k;
+    if (c > kWaveCandidates) {
+        // spill entries are numbered after the pool's own lists
+        const uint32_t base = w.pool*kWaveCandidates + (uint32_t)w.spill_row[slot]*kSpillCap;
+        for (int k = kWaveCandidates; k < c; k++)
+            w.queue[first + k] = base + (uint32_t)(k - kWaveCandidates);
+    }
+}
+
+// One thread per queued candidate: the distance to the candidate's hit, or
+// -1 for none.  A slot's candidates sit next to each other in the queue, so
+// a warp shares the few rays it reads.
+template <int kIsect>
+__global__ void __launch_bounds__(256)
+wave_isect_kernel(const TraceArgs a, const WaveBuffers w, const RayPool cur) {
+    const DevScene& sc = a.scene;
+    const uint32_t n = w.counters->queue_len;
+    for (uint32_t e = blockIdx.x*blockDim.x + threadIdx.x; e < n; e += gridDim.x*blockDim.x) {
+        const uint32_t idx = w.queue[e];
+        const uint32_t own = w.pool*kWaveCandidates;
+        const bool spilled = idx >= own;
+        const uint32_t slot = spilled ? w.spill_slot[(idx - own)/kSpillCap] : idx/kWaveCandidates;
+        const int32_t leaf = spilled ? w.spill[idx - own] : w.cand[idx];
+        const v3 s = mk(cur.sx[slot], cur.sy[slot], cur.sz[slot]);
+        const v3 d = mk(cur.dx[slot], cur.dy[slot], cur.dz[slot]);
+        double dist = -1.0;
+        if (kIsect == kIsectFp64) {
+            const Isec h = leaf_hit(sc, leaf, s, d);
+            if (h.leaf >= 0) dist = h.dist;
+        } else {
+            const fp32::Hit32 h = fp32::intersect32(sc, leaf, fp32::dmk(s.x, s.y, s.z),
+                                                    fp32::dmk(d.x, d.y, d.z),
+                                                    kIsect == kIsectFp32Pure);
+            if (h.leaf >= 0) dist = h.v;
+        }
+        if (spilled) w.spill_dist[idx - own] = dist;
+        else w.cand_dist[idx] = dist;
+    }
+}
+
+// Slots whose candidate list overflowed: merlict's own walk of the frame
+// tree (FP64, in merlict's order) finds the closest hit, which becomes the
+// slot's only candidate (none for a miss).  Runs before the resolve step.
+__global__ void __launch_bounds__(128)
+wave_overflow_kernel(const TraceArgs a, const WaveBuffers w, const RayPool cur) {
+    const uint32_t n = w.counters->overflow_len;
+    for (uint32_t e = blockIdx.x*blockDim.x + threadIdx.x; e < n; e += gridDim.x*blockDim.x) {
+        const uint32_t slot = w.overflow[e];
+        const v3 s = mk(cur.sx[slot], cur.sy[slot], cur.sz[slot]);
+        const v3 d = mk(cur.dx[slot], cur.dy[slot], cur.dz[slot]);
+        const Isec is = first_intersection_tree(a.scene, cur.root[slot], s, d);
+        const size_t row = (size_t)slot*kWaveCandidates;
+        if (is.leaf >= 0) {
+            w.cand[row] = is.leaf;
+            w.cand_dist[row] = is.dist;
+            w.cand_count[slot] = 1;
+        } else {
+            w.cand_count[slot] = 0;
+        }
+    }
+}
+
 template <typename Out, int kIsect>
 __global__ void __launch_bounds__(256)
 wave_resolve_kernel(const TraceArgs a, const WaveBuffers w, const RayPool cur, const RayPool nxt) {
     const DevScene& sc = a.scene;
+    // the property tables, staged in shared memory when they fit
+    extern __shared__ double s_fn[];
+    const double* fn_pts = sc.fn_points;
+    const int32_t* fn_off = sc.fn_offset;
+    if (w.fn_smem_bytes) {
+        const int np = 3*sc.num_fn_points;
+        int32_t* s_off = reinterpret_cast<int32_t*>(s_fn + np);
+        for (int k = threadIdx.x; k < np; k += blockDim.x) s_fn[k] = __ldg(sc.fn_points + k);
+        for (int k = threadIdx.x; k <= sc.num_functions; k += blockDim.x) s_off[k] = __ldg(sc.fn_offset + k);
+        __syncthreads();
+        fn_pts = s_fn;
+        fn_off = s_off;
+    }
     const uint32_t total = w.counters->total;
     const uint32_t slot = blockIdx.x*blockDim.x + threadIdx.x;
     const int lane = threadIdx.x & 31;
@@ -98,36 +204,49 @@ wave_resolve_kernel(const TraceArgs a, const WaveBuffers w, const RayPool cur, c
         } else {
             // merlict's closest hit among the candidates: minimum distance,
             // ties to merlict's visiting order (RayAndFrame.cpp:160-173)
-            if (count > kWaveCandidates) {
-                is = first_intersection_tree(sc, root, s, d);
-            } else {
-                bool have = false;
-                is.leaf = -1;
-                const double sd = dot(s, d);
-                const int32_t* cand = w.cand + (size_t)slot*kWaveCandidates;
-                if (kIsect == kIsectFp64) {
-                    for (int k = 0; k < count; k++)
-                        test_candidate(sc, cand[k], s, d, false, sd, &is, &have);
+            {
+                // merlict's closest hit among the candidates, whose distances
+                // the intersection kernel left in cand_dist: minimum
+                // distance, ties to the lower leaf index, which is the one
+                // merlict visits first (RayAndFrame.cpp:160-173); then the
+                // winner's full intersection, recomputed by the same code.
+                // A list longer than 32 continues in its spill row; an
+                // overflowed one holds the winner of merlict's own walk.
+                int32_t best = -1;
+                double best_dist = 0.0;
+                auto consider = [&](double dk, int32_t lk) {
+                    if (dk >= 0.0 && (best < 0 || dk < best_dist || (dk == best_dist && lk < best))) {
+                        best = lk;
+                        best_dist = dk;
+                    }
+                };
+                const size_t row = (size_t)slot*kWaveCandidates;
+                const int own = count < kWaveCandidates ? count : kWaveCandidates;
+#pragma unroll 4
+                for (int k = 0; k < own; k++) consider(w.cand_dist[row + k], w.cand[row + k]);
+                if (count > kWaveCandidates) {
+                    const size_t sr = (size_t)w.spill_row[slot]*kSpillCap;
+                    for (int k = 0; k < count - kWaveCandidates; k++)
+                        consider(w.spill_dist[sr + k], w.spill[sr + k]);
+                }
+                if (best < 0) {
+                    set_void(&is, s, d);
+                } else if (kIsect == kIsectFp64) {
+                    is = leaf_hit(sc, best, s, d);
                 } else {
-                    // single-precision intersections (fp32_geometry.cuh); the
-                    // closest hit with ties to the lower leaf index
-                    const fp32::d3 s32 = fp32::dmk(s.x, s.y, s.z);
-                    const fp32::d3 d32 = fp32::dmk(d.x, d.y, d.z);
-                    for (int k = 0; k < count; k++) {
-                        const fp32::Hit32 h =
-                            fp32::intersect32(sc, cand[k], s32, d32, kIsect == kIsectFp32Pure);
-                        if (h.leaf >= 0 && (!have || h.v < is.dist ||
-                                            (h.v == is.dist && h.leaf < is.leaf))) {
-                            is.leaf = h.leaf;
-                            is.pos = mk(h.p.x, h.p.y, h.p.z);
-                            is.normal = mk(h.n.x, h.n.y, h.n.z);
-                            is.dist = h.v;
-                            is.outside = h.outside;
-                            have = true;
-                        }
+                    const fp32::Hit32 h = fp32::intersect32(sc, best, fp32::dmk(s.x, s.y, s.z),
+                                                            fp32::dmk(d.x, d.y, d.z),
+                                                            kIsect == kIsectFp32Pure);
+                    if (h.leaf < 0) {
+                        set_void(&is, s, d);
+                    } else {
+                        is.leaf = h.leaf;
+                        is.pos = mk(h.p.x, h.p.y, h.p.z);
+                        is.normal = mk(h.n.x, h.n.y, h.n.z);
+                        is.dist = h.v;
+                        is.outside = h.outside;
                     }
                 }
-                if (!have) set_void(&is, s, d);
             }
             const bool hit = is.leaf >= 0;
             const LeafRec* L = hit ? sc.leaf + is.leaf : nullptr;
@@ -157,7 +276,7 @@ wave_resolve_kernel(const TraceArgs a, const WaveBuffers w, const RayPool cur, c
             bool absorbed = false;
             if (hit) {
                 // absorbed_in_medium_before_reaching_surface, PhotonAndFrame.cpp:32-38
-                const double depth = func_eval(sc, fn[is.outside ? MLGPU_SURF_OUTER_ABSORPTION
+                const double depth = func_eval_tab(fn_pts, fn_off, fn[is.outside ? MLGPU_SURF_OUTER_ABSORPTION
                                                                   : MLGPU_SURF_INNER_ABSORPTION], lambda, &err);
                 const double survival = exp(-is.dist/depth);
                 absorbed = draw() > survival;
@@ -165,7 +284,7 @@ wave_resolve_kernel(const TraceArgs a, const WaveBuffers w, const RayPool cur, c
             if (!hit || absorbed) {
                 kind = MLGPU_ABSORPTION_IN_VOID;
             } else {
-                const double refl = func_eval(sc, fn[is.outside ? MLGPU_SURF_OUTER_REFLECTION
+                const double refl = func_eval_tab(fn_pts, fn_off, fn[is.outside ? MLGPU_SURF_OUTER_REFLECTION
                                                                  : MLGPU_SURF_INNER_REFLECTION], lambda, &err);
                 if (refl >= draw()) {
                     kind = MLGPU_REFLECTION_ON_SURFACE;
@@ -177,9 +296,9 @@ wave_resolve_kernel(const TraceArgs a, const WaveBuffers w, const RayPool cur, c
                 } else {
                     const v3 inc = orientation_inverse(T, d);
                     const v3 nrm = is.outside ? is.normal : scale(is.normal, -1.0);
-                    const double n_from = func_eval(sc, fn[is.outside ? MLGPU_SURF_OUTER_REFRACTION
+                    const double n_from = func_eval_tab(fn_pts, fn_off, fn[is.outside ? MLGPU_SURF_OUTER_REFRACTION
                                                                        : MLGPU_SURF_INNER_REFRACTION], lambda, &err);
-                    const double n_to = func_eval(sc, fn[is.outside ? MLGPU_SURF_INNER_REFRACTION
+                    const double n_to = func_eval_tab(fn_pts, fn_off, fn[is.outside ? MLGPU_SURF_INNER_REFRACTION
                                                                      : MLGPU_SURF_OUTER_REFRACTION], lambda, &err);
                     const double cosI = dot(nrm, inc)*(-1.0);
                     const double ratio = n_from/n_to;
@@ -218,7 +337,7 @@ wave_resolve_kernel(const TraceArgs a, const WaveBuffers w, const RayPool cur, c
                     ? fn[is.outside ? MLGPU_SURF_OUTER_REFRACTION : MLGPU_SURF_INNER_REFRACTION]
                     : sc.default_refraction;
                 int terr = 0;
-                const double n = func_eval(sc, f, lambda, &terr);
+                const double n = func_eval_tab(fn_pts, fn_off, f, lambda, &terr);
                 if (terr && !tof_error) tof_error = terr;
                 tof += n*is.dist/299792458.0;
             }

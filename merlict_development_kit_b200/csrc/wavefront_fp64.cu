@@ -48,6 +48,7 @@ wave_walk_kernel(const TraceArgs a, const WaveBuffers w, const RayPool cur) {
     v3 s = mk(0, 0, 0), d = mk(0, 0, 0);
     double sd = 0.0;
     int nc = 0;
+    int32_t spill = -1;                        // spill row of the current slot
     bool overflow = false;
     bool tree_mode = false;                    // walking a frame's subtree
     int32_t i = 0, end = 0;                    // frame-tree walk cursor
@@ -111,6 +112,7 @@ wave_walk_kernel(const TraceArgs a, const WaveBuffers w, const RayPool cur) {
                     // lens): merlict's own walk of that subtree
                     sd = dot(s, d);
                     nc = 0;
+                    spill = -1;
                     overflow = false;
                     tree_mode = true;
                     i = root;
@@ -118,6 +120,7 @@ wave_walk_kernel(const TraceArgs a, const WaveBuffers w, const RayPool cur) {
                 } else {
                     sd = dot(s, d);
                     nc = 0;
+                    spill = -1;
                     overflow = false;
                     tree_mode = false;
                     sp = 0;
@@ -146,6 +149,32 @@ wave_walk_kernel(const TraceArgs a, const WaveBuffers w, const RayPool cur) {
             // candidate.  The resolve kernel breaks ties in merlict's
             // visiting order, so the order here does not matter.
             int32_t* cand = w.cand + (size_t)item*kWaveCandidates;
+            // appends a candidate: the slot's own 32 entries, then a spill row
+            auto push = [&](int32_t leaf) {
+                if (nc < kWaveCandidates) {
+                    cand[nc] = leaf;
+                } else {
+                    const int j = nc - kWaveCandidates;
+                    if (j == 0) {
+                        const uint32_t r = atomicAdd(&w.counters->spill_used, 1u);
+                        if (r < kSpillRows) {
+                            spill = (int32_t)r;
+                            w.spill_slot[r] = (uint32_t)item;
+                            w.spill_row[item] = spill;
+                        }
+                    }
+                    if (spill >= 0 && j < kSpillCap) w.spill[(size_t)spill*kSpillCap + j] = leaf;
+                }
+                nc++;
+            };
+            // the count the queue sees: > 32 + kSpillCap sends the slot to
+            // the overflow walk
+            auto final_count = [&]() -> int32_t {
+                if (overflow) return kWaveCandidates + kSpillCap + 1;
+                if (nc > kWaveCandidates && (spill < 0 || nc > kWaveCandidates + kSpillCap))
+                    return kWaveCandidates + kSpillCap + 1;
+                return nc;
+            };
             if (tree_mode) {
                 // merlict's walk (RayAndFrame.cpp:137-149), candidates in its order
                 for (int it = 0; it < kWalkBurst && i < end; it++) {
@@ -156,14 +185,11 @@ wave_walk_kernel(const TraceArgs a, const WaveBuffers w, const RayPool cur) {
                         i = meta.x;
                         continue;
                     }
-                    if (meta.y >= 0) {
-                        if (nc < kWaveCandidates) cand[nc] = meta.y;
-                        nc++;
-                    }
+                    if (meta.y >= 0) push(meta.y);
                     i++;
                 }
                 if (i >= end) {
-                    w.cand_count[item] = nc;
+                    w.cand_count[item] = final_count();
                     item = -1;
                 }
             } else {
@@ -175,10 +201,8 @@ wave_walk_kernel(const TraceArgs a, const WaveBuffers w, const RayPool cur) {
                     for (int32_t j = start; j < start + count; j++) {
                         const double2* q = reinterpret_cast<const double2*>(sc.bvh_sphere + j);
                         const double2 c01 = __ldg(q), c23 = __ldg(q + 1);
-                        if (sphere_cull(make_double4(c01.x, c01.y, c23.x, c23.y), s, d, sd)) {
-                            if (nc < kWaveCandidates) cand[nc] = __ldg(sc.bvh_leaf + j);
-                            nc++;
-                        }
+                        if (sphere_cull(make_double4(c01.x, c01.y, c23.x, c23.y), s, d, sd))
+                            push(__ldg(sc.bvh_leaf + j));
                     }
                     continue;
                 }
@@ -204,7 +228,7 @@ wave_walk_kernel(const TraceArgs a, const WaveBuffers w, const RayPool cur) {
                 }
             }
             if (sp == 0) {
-                w.cand_count[item] = overflow ? kWaveCandidates + 1 : nc;
+                w.cand_count[item] = final_count();
                 item = -1;
             }
             }
@@ -220,45 +244,57 @@ __global__ void wave_after_walk_kernel(WaveCounters* c, uint32_t pool, uint64_t 
     c->total = c->active + fresh;
     c->next_input += fresh;
     c->next = 0;
+    c->queue_len = 0;
+    c->overflow_len = 0;
 }
 
 __global__ void wave_after_resolve_kernel(WaveCounters* c) {
     c->active = c->next;
     c->walk_fetch = 0;
+    c->spill_used = 0;
 }
 
 }  // namespace
 
-cudaError_t launch_wave_fp64_iteration(const TraceArgs& a, const WaveBuffers& w,
-                                       const RayPool& cur, const RayPool& nxt,
-                                       int walk_blocks, cudaStream_t s) {
-    const int resolve_blocks = (int)((w.pool + 255)/256);
+cudaError_t launch_wave_iteration(const TraceArgs& a, const WaveBuffers& w, const RayPool& cur,
+                                  const RayPool& nxt, int walk_blocks, int form, cudaStream_t s,
+                                  cudaEvent_t* ev) {
+    const int slot_blocks = (int)((w.pool + 255)/256);
+    if (ev) cudaEventRecord(ev[0], s);
     if (a.in_dtype == MLGPU_F64)
         wave_walk_kernel<double><<<walk_blocks, 256, 0, s>>>(a, w, cur);
     else
         wave_walk_kernel<float><<<walk_blocks, 256, 0, s>>>(a, w, cur);
+    if (ev) cudaEventRecord(ev[1], s);
     wave_after_walk_kernel<<<1, 1, 0, s>>>(w.counters, w.pool, a.num_photons);
-    if (a.out_dtype == MLGPU_F64)
-        wave_resolve_kernel<double, kIsectFp64><<<resolve_blocks, 256, 0, s>>>(a, w, cur, nxt);
-    else
-        wave_resolve_kernel<float, kIsectFp64><<<resolve_blocks, 256, 0, s>>>(a, w, cur, nxt);
+    wave_enqueue_kernel<<<slot_blocks, 256, 0, s>>>(w);
+    wave_overflow_kernel<<<kOverflowBlocks, 128, 0, s>>>(a, w, cur);
+    if (ev) cudaEventRecord(ev[2], s);
+    if (form == MLGPU_TRACER_FP64) {
+        wave_isect_kernel<kIsectFp64><<<w.isect_blocks, 256, 0, s>>>(a, w, cur);
+        if (ev) cudaEventRecord(ev[3], s);
+        if (a.out_dtype == MLGPU_F64)
+            wave_resolve_kernel<double, kIsectFp64><<<slot_blocks, 256, w.fn_smem_bytes, s>>>(a, w, cur, nxt);
+        else
+            wave_resolve_kernel<float, kIsectFp64><<<slot_blocks, 256, w.fn_smem_bytes, s>>>(a, w, cur, nxt);
+    } else {
+        const cudaError_t e = launch_wave32_isect_resolve(a, w, cur, nxt,
+                                                          form == MLGPU_TRACER_FP32_PURE, s,
+                                                          ev ? ev[3] : nullptr);
+        if (e != cudaSuccess) return e;
+    }
     wave_after_resolve_kernel<<<1, 1, 0, s>>>(w.counters);
+    if (ev) cudaEventRecord(ev[4], s);
     return cudaGetLastError();
 }
 
-cudaError_t launch_wave_walk(const TraceArgs& a, const WaveBuffers& w, const RayPool& cur,
-                             int walk_blocks, cudaStream_t s) {
-    if (a.in_dtype == MLGPU_F64)
-        wave_walk_kernel<double><<<walk_blocks, 256, 0, s>>>(a, w, cur);
-    else
-        wave_walk_kernel<float><<<walk_blocks, 256, 0, s>>>(a, w, cur);
-    wave_after_walk_kernel<<<1, 1, 0, s>>>(w.counters, w.pool, a.num_photons);
-    return cudaGetLastError();
-}
-
-cudaError_t launch_wave_after_resolve(const WaveBuffers& w, cudaStream_t s) {
-    wave_after_resolve_kernel<<<1, 1, 0, s>>>(w.counters);
-    return cudaGetLastError();
+int wave_isect_blocks() {
+    int per_sm = 0, sms = 0, dev = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, wave_isect_kernel<kIsectFp64>, 256, 0);
+    if (per_sm < 1) per_sm = 1;
+    return per_sm*sms;
 }
 
 int wave_fp64_walk_blocks() {

@@ -181,6 +181,21 @@ class Scene:
         check(lib().mlgpu_scene_kernel_launches(self._h, C.byref(v)))
         return int(v.value)
 
+    KERNEL_CLASSES = ("walk", "queue", "intersect", "resolve", "plain", "bin")
+
+    def set_profiling(self, enable: bool) -> None:
+        """Turns CUDA-event timing of the kernel classes on or off (and
+        clears the totals)."""
+        check(lib().mlgpu_scene_set_profiling(self._h, int(bool(enable))))
+
+    def kernel_times(self) -> dict:
+        """{class: (device ms, launches)} since profiling was turned on."""
+        n = len(self.KERNEL_CLASSES)
+        ms = (C.c_double * n)()
+        launches = (C.c_uint64 * n)()
+        check(lib().mlgpu_scene_kernel_times(self._h, ms, launches))
+        return {k: (float(ms[i]), int(launches[i])) for i, k in enumerate(self.KERNEL_CLASSES)}
+
     def sync_errors(self, stream=None) -> None:
         check(lib().mlgpu_scene_sync_errors(self._h, C.c_void_p(_stream_handle(stream))))
 

@@ -35,6 +35,9 @@ typedef struct oracle_counters {
     uint64_t segments;     /* time-of-flight segments, Photon.cpp:44-56 */
     uint64_t funcs;        /* Func1 evaluations */
     uint64_t steps;        /* propagation steps */
+    /* steps by the number of leaves merlict intersects in them: [k] for k
+     * leaves, [64] for 64 or more */
+    uint64_t leaves_per_step[65];
 } oracle_counters;
 
 typedef struct { double x, y, z; } v3;
@@ -381,6 +384,7 @@ static isec_t first_intersection(ctx* c, int32_t root, v3 s, v3 d) {
     int have = 0;
     int32_t i = root;
     const int32_t end = sc->node_skip[root];
+    uint32_t tested = 0;
     while (i < end) {
         const double* sph = sc->node_sphere + 4*(size_t)i;
         if (c->cnt) c->cnt->nodes++;
@@ -392,6 +396,7 @@ static isec_t first_intersection(ctx* c, int32_t root, v3 s, v3 d) {
             const v3 dobj = orientation_inverse(t, d);
             isec_t cand;
             if (c->cnt) c->cnt->leaves++;
+            tested++;
             intersect_leaf(c, leaf, so, dobj, sph[3], &cand);
             if (cand.hit && (!have || cand.dist < best.dist)) {
                 best = cand;
@@ -400,6 +405,7 @@ static isec_t first_intersection(ctx* c, int32_t root, v3 s, v3 d) {
         }
         i++;
     }
+    if (c->cnt) c->cnt->leaves_per_step[tested < 64 ? tested : 64]++;
     if (!have) {
         best.hit = 0;
         best.leaf = MLGPU_LEAF_VOID;

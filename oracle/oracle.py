@@ -28,10 +28,13 @@ REFERENCE_DIR = os.environ.get("MERLICT_REFERENCE_DIR", "/root/reference")
 class OracleCounters(C.Structure):
     _fields_ = [(k, C.c_uint64) for k in (
         "nodes", "leaves", "caps", "cap_bounds", "planes", "others",
-        "reflections", "fresnels", "segments", "funcs", "steps")]
+        "reflections", "fresnels", "segments", "funcs", "steps")] + [
+        ("leaves_per_step", C.c_uint64 * 65)]
 
     def as_dict(self) -> dict:
-        return {k: int(getattr(self, k)) for k, _ in self._fields_}
+        d = {k: int(getattr(self, k)) for k, _ in self._fields_ if k != "leaves_per_step"}
+        d["leaves_per_step"] = [int(v) for v in self.leaves_per_step]
+        return d
 
 
 def build(reference: bool = True) -> None:
