@@ -249,10 +249,10 @@ int mlgpu_scene_kernel_launches(const mlgpu_scene* scene, uint64_t* launches);
  * reference: it exists so that callers can put a roofline on each stage of
  * the device pipeline.                                                    */
 enum {
-    MLGPU_KERNEL_WALK = 0,       /* tree walk, candidate lists, photon intake */
-    MLGPU_KERNEL_QUEUE = 1,      /* candidate queue and pool counters         */
-    MLGPU_KERNEL_INTERSECT = 2,  /* one thread per queued candidate           */
-    MLGPU_KERNEL_RESOLVE = 3,    /* closest hit, interaction, compaction      */
+    MLGPU_KERNEL_WALK = 0,       /* BVH levels and leaf-sphere tests          */
+    MLGPU_KERNEL_INTAKE = 1,     /* photon intake, lens walks, pool counters  */
+    MLGPU_KERNEL_INTERSECT = 2,  /* one thread per candidate, closest hit     */
+    MLGPU_KERNEL_RESOLVE = 3,    /* interaction, compaction, results          */
     MLGPU_KERNEL_PLAIN = 4,      /* one-thread-per-photon tracer              */
     MLGPU_KERNEL_BIN = 5,        /* arrival binning                           */
     MLGPU_KERNEL_CLASSES = 6

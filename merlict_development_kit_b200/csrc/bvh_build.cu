@@ -142,6 +142,7 @@ float round_up(double x) {
 void build_bvh4(const mlgpu_flat_scene* f, double inflate, BvhHost* out) {
     out->nodes.clear();
     out->leaf_ids.clear();
+    out->levels = 0;
     Builder b;
     for (int32_t l = 0; l < f->num_leaves; l++) {
         if (f->leaf_primitive[l] == MLGPU_PRIM_NONE) continue;
@@ -169,8 +170,10 @@ void build_bvh4(const mlgpu_flat_scene* f, double inflate, BvhHost* out) {
     // collapse to 4-wide nodes, breadth first from the root
     std::vector<int32_t> queue = {0};
     std::vector<int32_t> wide_of(b.nodes.size(), -1);
+    std::vector<int32_t> level = {0};   // per wide node
     wide_of[0] = 0;
     out->nodes.emplace_back();
+    out->levels = 1;
     for (size_t qi = 0; qi < queue.size(); qi++) {
         const int32_t bn = queue[qi];
         const int32_t w = wide_of[bn];
@@ -213,6 +216,8 @@ void build_bvh4(const mlgpu_flat_scene* f, double inflate, BvhHost* out) {
             } else {
                 const int32_t idx = (int32_t)out->nodes.size();
                 out->nodes.emplace_back();
+                level.push_back(level[w] + 1);
+                out->levels = std::max(out->levels, level[w] + 2);
                 wide_of[kids[k]] = idx;
                 queue.push_back(kids[k]);
                 node.child[k] = idx;

@@ -133,8 +133,7 @@ struct mlgpu_scene {
     // ray pools of the wavefront tracers
     DeviceBuffer wave;
     WaveCounters* wave_host = nullptr;   // pinned copy of the counters
-    int wave_walk_blocks = 0;
-    int wave_isect_blocks = 0;
+    int wave_grid = 0;                   // blocks of the persistent kernels
     uint64_t launches = 0;               // kernels launched for this scene
     Profiler prof;
 };
@@ -280,6 +279,12 @@ int build_device_scene(mlgpu_scene* s, const mlgpu_flat_scene* f) {
             for (size_t j = 0; j < sph.size(); j++) sph[j] = node[f->leaf_node[bvh.leaf_ids[j]]];
             if ((st = upload(s, sph.data(), sph.size(), &s->dev.bvh_sphere))) return st;
             s->dev.bvh_nodes = (int32_t)bvh.nodes.size();
+            s->dev.bvh_levels = bvh.levels;
+        }
+        // a tree deeper than the walk's level queues: merlict's frame walk
+        if (s->dev.bvh_levels >= kMaxBvhLevels) {
+            s->dev.bvh_nodes = 0;
+            s->dev.bvh_levels = 0;
         }
         s->dev.bvh_eps = (float)(1e-6 + 4e-7*extent);
     }
@@ -362,15 +367,14 @@ constexpr uint32_t kWavePool = 1u << 21;   // ray slots of the wavefront tracers
 // one device buffer.
 int wave_buffers(mlgpu_scene* scene, uint32_t pool, WaveBuffers* w, RayPool* p0, RayPool* p1) {
     auto up = [](size_t x) { return (x + 255) & ~size_t(255); };
-    const size_t per_pool = 8*up((size_t)pool*8) + 5*up((size_t)pool*4);
-    const size_t spills = (size_t)kSpillRows*kSpillCap;
-    const size_t lists = up((size_t)pool*32*4) + up((size_t)pool*4) + up((size_t)pool*32*8) +
-        up(((size_t)pool*32 + spills)*4) + up((size_t)pool*4) + up(spills*4) + up(spills*8) +
-        up((size_t)pool*4) + up((size_t)kSpillRows*4);
-    MLGPU_CUDA(scene->wave.reserve(256 + 2*per_pool + lists));
+    const size_t P = pool;
+    const size_t level_cap = 8*P, range_cap = 16*P, isect_cap = 16*P;
+    const size_t per_pool = 8*up(P*8) + 5*up(P*4);
+    const size_t rest = up(P*4) + 2*up(P*16) + 2*up(level_cap*8) + up(range_cap*8) +
+        up(isect_cap*8) + up(isect_cap*8) + up(P*8) + 3*up(P*4);
+    MLGPU_CUDA(scene->wave.reserve(256 + 2*per_pool + rest));
     if (!scene->wave_host) MLGPU_CUDA(cudaMallocHost(&scene->wave_host, sizeof(WaveCounters)));
-    if (!scene->wave_walk_blocks) scene->wave_walk_blocks = wave_fp64_walk_blocks();
-    if (!scene->wave_isect_blocks) scene->wave_isect_blocks = wave_isect_blocks();
+    if (!scene->wave_grid) scene->wave_grid = wave_persistent_blocks();
     char* b = static_cast<char*>(scene->wave.ptr);
     w->counters = reinterpret_cast<WaveCounters*>(b);
     b += 256;
@@ -378,24 +382,30 @@ int wave_buffers(mlgpu_scene* scene, uint32_t pool, WaveBuffers* w, RayPool* p0,
     RayPool* pools[2] = {p0, p1};
     for (RayPool* p : pools) {
         double** d[8] = {&p->sx, &p->sy, &p->sz, &p->dx, &p->dy, &p->dz, &p->lambda, &p->tof};
-        for (double** q : d) *q = reinterpret_cast<double*>(take((size_t)pool*8));
+        for (double** q : d) *q = reinterpret_cast<double*>(take(P*8));
         int32_t** i[5] = {&p->photon, &p->root, &p->n_int, &p->k_draw, &p->err};
-        for (int32_t** q : i) *q = reinterpret_cast<int32_t*>(take((size_t)pool*4));
+        for (int32_t** q : i) *q = reinterpret_cast<int32_t*>(take(P*4));
     }
-    w->cand = reinterpret_cast<int32_t*>(take((size_t)pool*32*4));
-    w->cand_count = reinterpret_cast<int32_t*>(take((size_t)pool*4));
-    w->cand_dist = reinterpret_cast<double*>(take((size_t)pool*32*8));
-    w->queue = reinterpret_cast<uint32_t*>(take(((size_t)pool*32 + spills)*4));
-    w->overflow = reinterpret_cast<uint32_t*>(take((size_t)pool*4));
-    w->spill = reinterpret_cast<int32_t*>(take(spills*4));
-    w->spill_dist = reinterpret_cast<double*>(take(spills*8));
-    w->spill_row = reinterpret_cast<int32_t*>(take((size_t)pool*4));
-    w->spill_slot = reinterpret_cast<uint32_t*>(take((size_t)kSpillRows*4));
     w->pool = pool;
+    w->grid = scene->wave_grid;
+    w->step = reinterpret_cast<int32_t*>(take(P*4));
+    w->ray_o = reinterpret_cast<float4*>(take(P*16));
+    w->ray_i = reinterpret_cast<float4*>(take(P*16));
+    w->level_q[0] = reinterpret_cast<uint2*>(take(level_cap*8));
+    w->level_q[1] = reinterpret_cast<uint2*>(take(level_cap*8));
+    w->level_cap = (uint32_t)level_cap;
+    w->range_q = reinterpret_cast<uint2*>(take(range_cap*8));
+    w->range_cap = (uint32_t)range_cap;
+    w->isect_q = reinterpret_cast<uint2*>(take(isect_cap*8));
+    w->isect_dist = reinterpret_cast<double*>(take(isect_cap*8));
+    w->isect_cap = (uint32_t)isect_cap;
+    w->best_key = reinterpret_cast<unsigned long long*>(take(P*8));
+    w->best_leaf = reinterpret_cast<int32_t*>(take(P*4));
+    w->overflow = reinterpret_cast<uint32_t*>(take(P*4));
+    w->overflow_flag = reinterpret_cast<uint32_t*>(take(P*4));
     const size_t fn_bytes = (size_t)scene->dev.num_fn_points*3*sizeof(double) +
         ((size_t)scene->dev.num_functions + 1)*sizeof(int32_t);
     w->fn_smem_bytes = fn_bytes <= 16384 ? (int)fn_bytes : 0;
-    w->isect_blocks = scene->wave_isect_blocks;
     return MLGPU_OK;
 }
 
@@ -420,15 +430,16 @@ int run_wavefront(mlgpu_scene* scene, const TraceArgs& a, int resolve, cudaStrea
             const RayPool& nxt = pools[(iteration + 1) & 1];
             Profiler::Chain ch;
             const bool timed = scene->prof.on && scene->prof.take(5, ch.ev);
-            const cudaError_t e = launch_wave_iteration(a, w, cur, nxt, scene->wave_walk_blocks,
-                                                        resolve, stream, timed ? ch.ev : nullptr);
+            const cudaError_t e = launch_wave_iteration(a, w, cur, nxt, resolve, stream,
+                                                        timed ? ch.ev : nullptr);
             if (e != cudaSuccess) return cuda_fail(e, "wavefront kernels");
-            scene->launches += 7;
+            const int levels = scene->dev.bvh_levels;
+            scene->launches += (uint64_t)levels + 8;
             if (timed) {
                 ch.n = 5;
-                const int cls[4] = {MLGPU_KERNEL_WALK, MLGPU_KERNEL_QUEUE, MLGPU_KERNEL_INTERSECT,
+                const int cls[4] = {MLGPU_KERNEL_INTAKE, MLGPU_KERNEL_WALK, MLGPU_KERNEL_INTERSECT,
                                     MLGPU_KERNEL_RESOLVE};
-                const int launches[4] = {1, 3, 1, 2};
+                const int launches[4] = {2, levels + 1, 2, 3};
                 for (int k = 0; k < 4; k++) { ch.cls[k] = cls[k]; ch.launches[k] = launches[k]; }
                 scene->prof.add(ch);
             }

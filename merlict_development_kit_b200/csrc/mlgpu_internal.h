@@ -79,6 +79,7 @@ struct DevScene {
     const int32_t* bvh_leaf;
     const double4* bvh_sphere;  // per BVH leaf slot: world centre and radius^2 of that leaf
     int32_t bvh_nodes;
+    int32_t bvh_levels;         // node levels of the BVH (nodes of level k are visited by pass k)
     float bvh_eps;              // box inflation per ray: bvh_eps + 4e-7 |origin|_1
 };
 
@@ -124,26 +125,22 @@ struct TraceArgs {
 struct BvhHost {
     std::vector<BvhNode4> nodes;
     std::vector<int32_t> leaf_ids;
+    int levels = 0;              // depth of the 4-wide tree (root alone: 1)
 };
 void build_bvh4(const mlgpu_flat_scene* f, double inflate, BvhHost* out);
 
 // wavefront tracers: a pool of ray slots, two of them (current, next)
+constexpr int kMaxBvhLevels = 48;
 struct WaveCounters {
     unsigned long long next_input;   // photons taken into the pool so far
     unsigned int active;             // rays carried over into the current pool
     unsigned int total;              // active + new photons of this iteration
     unsigned int next;               // survivors written to the next pool
-    unsigned int walk_fetch;         // slots handed out by the walk kernel
-    unsigned int queue_len;          // (slot, candidate) pairs queued for intersection
-    unsigned int overflow_len;       // slots whose candidate list overflowed
-    unsigned int spill_used;         // spill rows handed out in this iteration
+    unsigned int range_len;          // (slot, BVH leaf range) pairs for the sphere tests
+    unsigned int isect_len;          // (slot, leaf) candidates to intersect
+    unsigned int overflow_len;       // slots sent to merlict's own walk
+    unsigned int level_len[kMaxBvhLevels];   // (slot, node) pairs of each BVH level
 };
-
-// A slot with more than 32 candidates continues its list in a spill row
-// of kSpillCap entries; a list longer than both is resolved by merlict's
-// own walk of the frame tree.
-constexpr int kSpillCap = 992;
-constexpr uint32_t kSpillRows = 16384;
 
 struct RayPool {
     int32_t* photon;
@@ -159,37 +156,40 @@ struct RayPool {
 
 struct WaveBuffers {
     WaveCounters* counters;
-    int32_t* cand;           // [pool][32] candidate leaves of the current step
-    int32_t* cand_count;     // [pool]
-    double* cand_dist;       // [pool][32] distance to each candidate's hit, -1: none
-    uint32_t* queue;         // slot * 32 + k of every candidate to intersect
-    uint32_t* overflow;      // [pool] slots whose candidate list overflowed
-    int32_t* spill;          // [kSpillRows][kSpillCap] candidates 33 and up
-    double* spill_dist;      // [kSpillRows][kSpillCap]
-    int32_t* spill_row;      // [pool] spill row of a slot (valid when its count > 32)
-    uint32_t* spill_slot;    // [kSpillRows] slot of each spill row
     uint32_t pool;
-    int isect_blocks;        // persistent grid of the intersection kernel
+    int grid;                // blocks of the persistent (grid-stride) kernels
     int fn_smem_bytes;       // property tables staged in shared memory (0: read from global)
+    int32_t* step;           // [pool] 0, or kNoStep: the photon takes no step
+    float4* ray_o;           // [pool] single-precision origin, box inflation
+    float4* ray_i;           // [pool] reciprocal direction
+    uint2* level_q[2];       // (slot, node) pairs, ping-pong between BVH levels
+    uint32_t level_cap;
+    uint2* range_q;          // (slot, BVH leaf-range reference)
+    uint32_t range_cap;
+    uint2* isect_q;          // (slot, leaf) candidates
+    double* isect_dist;      // distance to each candidate's hit, -1: none
+    uint32_t isect_cap;
+    unsigned long long* best_key;   // [pool] smallest hit distance (bits of a positive double)
+    int32_t* best_leaf;      // [pool] leaf of the closest hit, lowest index on ties
+    uint32_t* overflow;      // [pool] slots for merlict's own walk
+    uint32_t* overflow_flag; // [pool]
 };
 
 // One iteration of a wavefront tracer: walk, queue and intersect the
 // candidates, resolve.  `form` is MLGPU_TRACER_FP64, _FP32 or _FP32_PURE;
 // the FP32 forms' kernels live in wavefront_fp32.cu.
-// With `ev` non-null, events ev[0..4] are recorded before the walk, after
-// it, after the queue, after the intersections and after the resolve step.
+// With `ev` non-null, events ev[0..4] are recorded before the intake, after
+// it, after the BVH walk, after the intersections and after the resolve step.
 cudaError_t launch_wave_iteration(const TraceArgs& a, const WaveBuffers& w, const RayPool& cur,
-                                  const RayPool& nxt, int walk_blocks, int form, cudaStream_t s,
-                                  cudaEvent_t* ev);
+                                  const RayPool& nxt, int form, cudaStream_t s, cudaEvent_t* ev);
 // the FP32 forms' intersection and resolve kernels; `mid` (may be null) is
 // recorded between them
 cudaError_t launch_wave32_isect_resolve(const TraceArgs& a, const WaveBuffers& w,
                                         const RayPool& cur, const RayPool& nxt, bool pure,
                                         cudaStream_t s, cudaEvent_t mid);
-int wave_isect_blocks();
 
 cudaError_t launch_trace_fp64(const TraceArgs& a, int block, cudaStream_t s);
-int wave_fp64_walk_blocks();
+int wave_persistent_blocks();
 cudaError_t launch_bin_arrivals(const DevScene& sc, const int32_t* sensor,
                                 const double* time, uint64_t n, uint32_t* counts,
                                 uint32_t* time_hist, uint32_t num_bins,

@@ -1,8 +1,20 @@
-// wave_resolve.cuh -- the resolve step of the wavefront tracers: merlict's
-// closest hit among a ray's candidate leaves, the interaction with the
-// surface (merlict/PhotonAndFrame.cpp:13-124), the history entry and the
-// time-of-flight term; survivors are compacted into the next pool with a
-// warp ballot and one atomic per warp, finished photons write their results.
+// wave_resolve.cuh -- the per-candidate and per-slot steps of the wavefront
+// tracers, shared by the FP64 and FP32 forms:
+//   intersect  one thread per (ray, candidate leaf): the distance to the
+//              leaf's hit; the smallest distance of each ray is kept with a
+//              64-bit atomic minimum on its bits (positive doubles order like
+//              their bit patterns);
+//   ties       one thread per candidate: among the candidates at exactly that
+//              distance the lowest leaf index wins, which is the leaf merlict
+//              visits first (RayAndFrame.cpp:160-173);
+//   overflow   rays whose walk overflowed a queue get merlict's own walk of
+//              the frame tree;
+//   resolve    one thread per ray: the winner's full intersection, recomputed
+//              by the same code, the interaction with the surface
+//              (merlict/PhotonAndFrame.cpp:13-124), the history entry and the
+//              time-of-flight term; survivors are compacted into the next
+//              pool with a warp ballot and one atomic per warp, finished
+//              photons write their results.
 //
 // kIsect selects the intersection arithmetic: FP64 (merlict's, bit-identical
 // when the translation unit is compiled with --fmad=false), or the FP32
@@ -11,6 +23,7 @@
 #ifndef MLGPU_WAVE_RESOLVE_CUH_
 #define MLGPU_WAVE_RESOLVE_CUH_
 
+#include <climits>
 #include <cstdint>
 
 #include "fp64_geometry.cuh"
@@ -23,11 +36,13 @@ namespace {
 using namespace fp64;
 
 constexpr unsigned kFull = 0xffffffffu;
-constexpr int kWaveCandidates = 32;     // candidate leaves recorded per ray step
-constexpr int kWalkChunk = 64;          // slots a warp takes at a time
-constexpr int kWalkBurst = 16;          // tree nodes a lane visits between refills
-constexpr int kNoStep = -2;             // candidate count: photon takes no step
-constexpr int kOverflowBlocks = 148;    // grid of the overflow kernel
+constexpr int kNoStep = -2;             // step state: the photon takes no step
+constexpr int32_t kNoLeaf = INT32_MAX;  // best_leaf of a ray without a hit
+constexpr unsigned long long kNoKey = ~0ull;
+
+constexpr int kIsectFp64 = 0;
+constexpr int kIsectFp32 = 1;
+constexpr int kIsectFp32Pure = 2;
 
 template <typename T>
 __device__ __forceinline__ double load_in(const void* p, uint64_t i) {
@@ -45,63 +60,44 @@ __device__ __forceinline__ void store_hist(mlgpu_history_entry* h, v3 pos, v3 nr
     h->pad[0] = 0; h->pad[1] = 0;
 }
 
-constexpr int kIsectFp64 = 0;
-constexpr int kIsectFp32 = 1;
-constexpr int kIsectFp32Pure = 2;
-
-// Queues every (slot, candidate) pair of this step for the intersection
-// kernel: a block-wide scan of the candidate counts and one atomic per block.
-// Slots without a step or whose list overflowed queue nothing.
-__global__ void __launch_bounds__(256)
-wave_enqueue_kernel(const WaveBuffers w) {
-    __shared__ uint32_t warp_sum[8];
-    __shared__ uint32_t block_base;
-    const uint32_t total = w.counters->total;
-    const uint32_t slot = blockIdx.x*blockDim.x + threadIdx.x;
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    int32_t c = slot < total ? w.cand_count[slot] : 0;
-    if (c > kWaveCandidates + kSpillCap) w.overflow[atomicAdd(&w.counters->overflow_len, 1u)] = slot;
-    if (c < 0 || c > kWaveCandidates + kSpillCap) c = 0;
-    // inclusive scan within the warp
-    uint32_t x = (uint32_t)c;
+// Reserves n consecutive entries of a queue for every lane of the (full,
+// converged) warp with one atomic; returns this lane's first index.
+__device__ __forceinline__ uint32_t warp_reserve(unsigned int* counter, uint32_t n) {
+    const int lane = threadIdx.x & 31;
+    uint32_t x = n;
 #pragma unroll
     for (int o = 1; o < 32; o <<= 1) {
         const uint32_t y = __shfl_up_sync(kFull, x, o);
         if (lane >= o) x += y;
     }
-    if (lane == 31) warp_sum[warp] = x;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        uint32_t run = 0;
-        for (int k = 0; k < 8; k++) { const uint32_t t = warp_sum[k]; warp_sum[k] = run; run += t; }
-        block_base = run ? atomicAdd(&w.counters->queue_len, run) : 0u;
-    }
-    __syncthreads();
-    const uint32_t first = block_base + warp_sum[warp] + x - (uint32_t)c;
-    const int own = c < kWaveCandidates ? c : kWaveCandidates;
-    for (int k = 0; k < own; k++) w.queue[first + k] = slot*kWaveCandidates + (uint32_t)k;
-    if (c > kWaveCandidates) {
-        // spill entries are numbered after the pool's own lists
-        const uint32_t base = w.pool*kWaveCandidates + (uint32_t)w.spill_row[slot]*kSpillCap;
-        for (int k = kWaveCandidates; k < c; k++)
-            w.queue[first + k] = base + (uint32_t)(k - kWaveCandidates);
-    }
+    const uint32_t sum = __shfl_sync(kFull, x, 31);
+    uint32_t base = 0;
+    if (lane == 31 && sum) base = atomicAdd(counter, sum);
+    base = __shfl_sync(kFull, base, 31);
+    return base + x - n;
 }
 
-// One thread per queued candidate: the distance to the candidate's hit, or
-// -1 for none.  A slot's candidates sit next to each other in the queue, so
-// a warp shares the few rays it reads.
+// Sends a slot to merlict's own walk (once per iteration).
+__device__ __forceinline__ void mark_overflow(const WaveBuffers& w, uint32_t slot) {
+    if (atomicExch(&w.overflow_flag[slot], 1u) == 0u)
+        w.overflow[atomicAdd(&w.counters->overflow_len, 1u)] = slot;
+}
+
+// The first index of this warp in a grid-stride loop whose trip count is
+// the same for every lane of a warp (so that warp_reserve sees full warps).
+__device__ __forceinline__ uint32_t warp_first() {
+    return blockIdx.x*blockDim.x + (threadIdx.x & ~31u);
+}
+
 template <int kIsect>
 __global__ void __launch_bounds__(256)
 wave_isect_kernel(const TraceArgs a, const WaveBuffers w, const RayPool cur) {
     const DevScene& sc = a.scene;
-    const uint32_t n = w.counters->queue_len;
+    const uint32_t n = w.counters->isect_len < w.isect_cap ? w.counters->isect_len : w.isect_cap;
     for (uint32_t e = blockIdx.x*blockDim.x + threadIdx.x; e < n; e += gridDim.x*blockDim.x) {
-        const uint32_t idx = w.queue[e];
-        const uint32_t own = w.pool*kWaveCandidates;
-        const bool spilled = idx >= own;
-        const uint32_t slot = spilled ? w.spill_slot[(idx - own)/kSpillCap] : idx/kWaveCandidates;
-        const int32_t leaf = spilled ? w.spill[idx - own] : w.cand[idx];
+        const uint2 q = w.isect_q[e];
+        const uint32_t slot = q.x;
+        const int32_t leaf = (int32_t)q.y;
         const v3 s = mk(cur.sx[slot], cur.sy[slot], cur.sz[slot]);
         const v3 d = mk(cur.dx[slot], cur.dy[slot], cur.dz[slot]);
         double dist = -1.0;
@@ -114,14 +110,25 @@ wave_isect_kernel(const TraceArgs a, const WaveBuffers w, const RayPool cur) {
                                                     kIsect == kIsectFp32Pure);
             if (h.leaf >= 0) dist = h.v;
         }
-        if (spilled) w.spill_dist[idx - own] = dist;
-        else w.cand_dist[idx] = dist;
+        w.isect_dist[e] = dist;
+        if (dist >= 0.0) atomicMin(&w.best_key[slot], (unsigned long long)__double_as_longlong(dist));
     }
 }
 
-// Slots whose candidate list overflowed: merlict's own walk of the frame
-// tree (FP64, in merlict's order) finds the closest hit, which becomes the
-// slot's only candidate (none for a miss).  Runs before the resolve step.
+__global__ void __launch_bounds__(256)
+wave_tie_kernel(const WaveBuffers w) {
+    const uint32_t n = w.counters->isect_len < w.isect_cap ? w.counters->isect_len : w.isect_cap;
+    for (uint32_t e = blockIdx.x*blockDim.x + threadIdx.x; e < n; e += gridDim.x*blockDim.x) {
+        const double dist = w.isect_dist[e];
+        if (!(dist >= 0.0)) continue;
+        const uint2 q = w.isect_q[e];
+        if ((unsigned long long)__double_as_longlong(dist) == w.best_key[q.x])
+            atomicMin(&w.best_leaf[q.x], (int32_t)q.y);
+    }
+}
+
+// Rays whose walk overflowed a queue: merlict's own walk of the frame tree
+// (FP64, in merlict's order) finds the closest hit.
 __global__ void __launch_bounds__(128)
 wave_overflow_kernel(const TraceArgs a, const WaveBuffers w, const RayPool cur) {
     const uint32_t n = w.counters->overflow_len;
@@ -130,14 +137,7 @@ wave_overflow_kernel(const TraceArgs a, const WaveBuffers w, const RayPool cur) 
         const v3 s = mk(cur.sx[slot], cur.sy[slot], cur.sz[slot]);
         const v3 d = mk(cur.dx[slot], cur.dy[slot], cur.dz[slot]);
         const Isec is = first_intersection_tree(a.scene, cur.root[slot], s, d);
-        const size_t row = (size_t)slot*kWaveCandidates;
-        if (is.leaf >= 0) {
-            w.cand[row] = is.leaf;
-            w.cand_dist[row] = is.dist;
-            w.cand_count[slot] = 1;
-        } else {
-            w.cand_count[slot] = 0;
-        }
+        w.best_leaf[slot] = is.leaf >= 0 ? is.leaf : kNoLeaf;
     }
 }
 
@@ -174,7 +174,7 @@ wave_resolve_kernel(const TraceArgs a, const WaveBuffers w, const RayPool cur, c
     if (valid) {
         s = mk(cur.sx[slot], cur.sy[slot], cur.sz[slot]);
         d = mk(cur.dx[slot], cur.dy[slot], cur.dz[slot]);
-        count = w.cand_count[slot];
+        count = w.step[slot];
     }
 
     if (valid) {
@@ -205,31 +205,10 @@ wave_resolve_kernel(const TraceArgs a, const WaveBuffers w, const RayPool cur, c
             // merlict's closest hit among the candidates: minimum distance,
             // ties to merlict's visiting order (RayAndFrame.cpp:160-173)
             {
-                // merlict's closest hit among the candidates, whose distances
-                // the intersection kernel left in cand_dist: minimum
-                // distance, ties to the lower leaf index, which is the one
-                // merlict visits first (RayAndFrame.cpp:160-173); then the
-                // winner's full intersection, recomputed by the same code.
-                // A list longer than 32 continues in its spill row; an
-                // overflowed one holds the winner of merlict's own walk.
-                int32_t best = -1;
-                double best_dist = 0.0;
-                auto consider = [&](double dk, int32_t lk) {
-                    if (dk >= 0.0 && (best < 0 || dk < best_dist || (dk == best_dist && lk < best))) {
-                        best = lk;
-                        best_dist = dk;
-                    }
-                };
-                const size_t row = (size_t)slot*kWaveCandidates;
-                const int own = count < kWaveCandidates ? count : kWaveCandidates;
-#pragma unroll 4
-                for (int k = 0; k < own; k++) consider(w.cand_dist[row + k], w.cand[row + k]);
-                if (count > kWaveCandidates) {
-                    const size_t sr = (size_t)w.spill_row[slot]*kSpillCap;
-                    for (int k = 0; k < count - kWaveCandidates; k++)
-                        consider(w.spill_dist[sr + k], w.spill[sr + k]);
-                }
-                if (best < 0) {
+                // the winner of the intersection and tie kernels (or of
+                // merlict's own walk), recomputed by the same code
+                const int32_t best = w.best_leaf[slot];
+                if (best == kNoLeaf) {
                     set_void(&is, s, d);
                 } else if (kIsect == kIsectFp64) {
                     is = leaf_hit(sc, best, s, d);

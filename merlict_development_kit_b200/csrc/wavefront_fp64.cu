@@ -2,24 +2,20 @@
 // (merlict/PhotonAndFrame.cpp:13-124) split into per-step kernels over a
 // fixed pool of ray slots, bit-identical to the plain tracer.
 //
-// One iteration over the pool:
-//   walk     persistent kernel; every warp refills its idle lanes from a
-//            per-warp chunk of slots (one atomic per 64 slots), takes new
-//            photons into free slots, and walks the BVH of the scene,
-//            recording the leaves that pass merlict's own bounding-sphere
-//            test (RayAndFrame.cpp:16-107) as candidates;
-//   resolve  one thread per slot: merlict's intersection of the candidates
-//            (closest hit, ties in merlict's visiting order,
-//            RayAndFrame.cpp:151-173) -- or, for a ray inside a lens,
-//            merlict's walk of that lens's subtree -- the
-//            interaction (absorption, reflection, Fresnel), the history
-//            entry and the time-of-flight term; survivors are compacted
-//            into the next pool with a warp ballot and one atomic per warp,
-//            finished photons write their results.
-// Separating the cheap, uniform tree walk from the heavy per-step work keeps
-// a warp's lanes doing the same thing, which the one-thread-per-photon
-// tracer cannot.  The arithmetic is the shared FP64 code, compiled with
-// --fmad=false.
+// One iteration over the pool, every stage a flat loop over uniform work
+// items so that a warp's lanes do the same thing:
+//   intake     one thread per slot: new photons enter free slots; a ray
+//              inside a lens gets merlict's walk of that lens's subtree
+//              (RayAndFrame.cpp:137-149), every other ray queues the root
+//              of the BVH;
+//   levels     one pass per BVH level, one thread per (ray, node) pair: the
+//              four child boxes; hit children go to the next level's queue,
+//              hit leaf ranges to the sphere queue;
+//   spheres    one thread per (ray, leaf range): merlict's own bounding-sphere
+//              test of each leaf (RayAndFrame.cpp:16-107); the leaves that
+//              pass are the ray's candidates;
+//   intersect, ties, overflow, resolve: wave_resolve.cuh.
+// The arithmetic is the shared FP64 code, compiled with --fmad=false.
 #include <cstdint>
 
 #include "wave_resolve.cuh"
@@ -27,9 +23,11 @@
 namespace mlgpu {
 namespace {
 
+constexpr int kTreeCands = 16;   // candidates of a frame-tree walk before it overflows
+
 template <typename In>
 __global__ void __launch_bounds__(256)
-wave_walk_kernel(const TraceArgs a, const WaveBuffers w, const RayPool cur) {
+wave_intake_kernel(const TraceArgs a, const WaveBuffers w, const RayPool cur) {
     const DevScene& sc = a.scene;
     const uint32_t active = w.counters->active;
     const unsigned long long next_input = w.counters->next_input;
@@ -37,147 +35,59 @@ wave_walk_kernel(const TraceArgs a, const WaveBuffers w, const RayPool cur) {
     const uint32_t room = w.pool - active;
     const uint32_t fresh = (uint32_t)(remaining < room ? remaining : room);
     const uint32_t total = active + fresh;
-    const int lane = threadIdx.x & 31;
-    const unsigned lower = (1u << lane) - 1u;
+    const uint32_t slot = blockIdx.x*blockDim.x + threadIdx.x;
     const uint32_t max_int = a.max_interactions;
     const uint32_t hist_len = max_int + 1;
-
-    uint32_t chunk_begin = 0, chunk_end = 0;   // warp-uniform
-    bool exhausted = false;                    // warp-uniform
-    int64_t item = -1;
-    v3 s = mk(0, 0, 0), d = mk(0, 0, 0);
-    double sd = 0.0;
-    int nc = 0;
-    int32_t spill = -1;                        // spill row of the current slot
-    bool overflow = false;
-    bool tree_mode = false;                    // walking a frame's subtree
-    int32_t i = 0, end = 0;                    // frame-tree walk cursor
-    // BVH traversal state (single precision slab tests)
-    float ox = 0.f, oy = 0.f, oz = 0.f, idx = 0.f, idy = 0.f, idz = 0.f, eps = 0.f;
-    int32_t stack[kBvhStack];
-    int sp = 0;
-    while (true) {
-        // hand idle lanes new slots from the warp's chunk
-        unsigned idle = __ballot_sync(kFull, item < 0);
-        while (idle && !exhausted) {
-            if (chunk_begin >= chunk_end) {
-                uint32_t b = 0;
-                if (lane == 0) b = atomicAdd(&w.counters->walk_fetch, (unsigned)kWalkChunk);
-                b = __shfl_sync(kFull, b, 0);
-                if (b >= total) { exhausted = true; break; }
-                chunk_begin = b;
-                chunk_end = min(b + (uint32_t)kWalkChunk, total);
-            }
-            const uint32_t take = min((uint32_t)__popc(idle), chunk_end - chunk_begin);
-            const int rank = __popc(idle & lower);
-            if (item < 0 && rank < (int)take) {
-                const uint32_t slot = chunk_begin + rank;
-                item = slot;
-                int32_t root;
-                uint32_t n_int;
-                if (slot >= active) {
-                    // a new photon: merlict::Photon's constructor (Ray.cpp:16-20,
-                    // RayForPropagation.cpp:52-64)
-                    const uint64_t p = next_input + (slot - active);
-                    s = mk(load_in<In>(a.photons.sx, p), load_in<In>(a.photons.sy, p),
-                           load_in<In>(a.photons.sz, p));
-                    d = normalized(mk(load_in<In>(a.photons.dx, p), load_in<In>(a.photons.dy, p),
-                                      load_in<In>(a.photons.dz, p)));
-                    root = a.start_node;
-                    n_int = 1;
-                    cur.photon[slot] = (int32_t)p;
-                    cur.sx[slot] = s.x; cur.sy[slot] = s.y; cur.sz[slot] = s.z;
-                    cur.dx[slot] = d.x; cur.dy[slot] = d.y; cur.dz[slot] = d.z;
-                    cur.lambda[slot] = load_in<In>(a.photons.wavelength, p);
-                    cur.tof[slot] = 0.0;
-                    cur.root[slot] = root;
-                    cur.n_int[slot] = 1;
-                    cur.k_draw[slot] = 0;
-                    cur.err[slot] = 0;
-                    if (a.results.history)
-                        store_hist(a.results.history + p*hist_len, s, d, 0.0,
-                                   MLGPU_LEAF_PHOTON_SOURCE, MLGPU_PRODUCTION, dot(d, d) < 0.0);
-                } else {
-                    s = mk(cur.sx[slot], cur.sy[slot], cur.sz[slot]);
-                    d = mk(cur.dx[slot], cur.dy[slot], cur.dz[slot]);
-                    root = cur.root[slot];
-                    n_int = (uint32_t)cur.n_int[slot];
-                }
-                if (n_int > max_int) {
-                    w.cand_count[slot] = kNoStep;
-                    item = -1;
-                } else if (root != 0 || sc.bvh_nodes == 0 ||
-                           a.traversal == MLGPU_TRAVERSAL_FRAME_TREE) {
-                    // traversal restricted to a frame's subtree (inside a
-                    // lens): merlict's own walk of that subtree
-                    sd = dot(s, d);
-                    nc = 0;
-                    spill = -1;
-                    overflow = false;
-                    tree_mode = true;
-                    i = root;
-                    end = __ldg(&sc.node_meta[root].x);
-                } else {
-                    sd = dot(s, d);
-                    nc = 0;
-                    spill = -1;
-                    overflow = false;
-                    tree_mode = false;
-                    sp = 0;
-                    // merlict tests the root frame's own sphere first
-                    const double2* np = reinterpret_cast<const double2*>(sc.node);
-                    const double2 n01 = __ldg(np), n23 = __ldg(np + 1);
-                    if (sphere_cull(make_double4(n01.x, n01.y, n23.x, n23.y), s, d, sd)) {
-                        stack[sp++] = 0;
-                        ox = (float)s.x; oy = (float)s.y; oz = (float)s.z;
-                        float fdx = (float)d.x, fdy = (float)d.y, fdz = (float)d.z;
-                        if (fabsf(fdx) < 1e-30f) fdx = copysignf(1e-30f, fdx);
-                        if (fabsf(fdy) < 1e-30f) fdy = copysignf(1e-30f, fdy);
-                        if (fabsf(fdz) < 1e-30f) fdz = copysignf(1e-30f, fdz);
-                        idx = 1.0f/fdx; idy = 1.0f/fdy; idz = 1.0f/fdz;
-                        eps = sc.bvh_eps + 4e-7f*(fabsf(ox) + fabsf(oy) + fabsf(oz));
-                    }
-                }
-            }
-            chunk_begin += take;
-            idle = __ballot_sync(kFull, item < 0);
+    bool bvh = false;          // queue the BVH root for this ray
+    int nc = 0;                // candidates of a frame-tree walk
+    int32_t cand[kTreeCands];
+    if (slot < total) {
+        v3 s, d;
+        int32_t root;
+        uint32_t n_int;
+        if (slot >= active) {
+            // a new photon: merlict::Photon's constructor (Ray.cpp:16-20,
+            // RayForPropagation.cpp:52-64)
+            const uint64_t p = next_input + (slot - active);
+            s = mk(load_in<In>(a.photons.sx, p), load_in<In>(a.photons.sy, p),
+                   load_in<In>(a.photons.sz, p));
+            d = normalized(mk(load_in<In>(a.photons.dx, p), load_in<In>(a.photons.dy, p),
+                              load_in<In>(a.photons.dz, p)));
+            root = a.start_node;
+            n_int = 1;
+            cur.photon[slot] = (int32_t)p;
+            cur.sx[slot] = s.x; cur.sy[slot] = s.y; cur.sz[slot] = s.z;
+            cur.dx[slot] = d.x; cur.dy[slot] = d.y; cur.dz[slot] = d.z;
+            cur.lambda[slot] = load_in<In>(a.photons.wavelength, p);
+            cur.tof[slot] = 0.0;
+            cur.root[slot] = root;
+            cur.n_int[slot] = 1;
+            cur.k_draw[slot] = 0;
+            cur.err[slot] = 0;
+            if (a.results.history)
+                store_hist(a.results.history + p*hist_len, s, d, 0.0,
+                           MLGPU_LEAF_PHOTON_SOURCE, MLGPU_PRODUCTION, dot(d, d) < 0.0);
+        } else {
+            s = mk(cur.sx[slot], cur.sy[slot], cur.sz[slot]);
+            d = mk(cur.dx[slot], cur.dy[slot], cur.dz[slot]);
+            root = cur.root[slot];
+            n_int = (uint32_t)cur.n_int[slot];
         }
-        if (__ballot_sync(kFull, item >= 0) == 0) break;
-        if (item >= 0) {
-            // BVH traversal; each leaf it reaches gets merlict's own sphere
-            // test (RayAndFrame.cpp:16-107) and, if it passes, becomes a
-            // candidate.  The resolve kernel breaks ties in merlict's
-            // visiting order, so the order here does not matter.
-            int32_t* cand = w.cand + (size_t)item*kWaveCandidates;
-            // appends a candidate: the slot's own 32 entries, then a spill row
-            auto push = [&](int32_t leaf) {
-                if (nc < kWaveCandidates) {
-                    cand[nc] = leaf;
-                } else {
-                    const int j = nc - kWaveCandidates;
-                    if (j == 0) {
-                        const uint32_t r = atomicAdd(&w.counters->spill_used, 1u);
-                        if (r < kSpillRows) {
-                            spill = (int32_t)r;
-                            w.spill_slot[r] = (uint32_t)item;
-                            w.spill_row[item] = spill;
-                        }
-                    }
-                    if (spill >= 0 && j < kSpillCap) w.spill[(size_t)spill*kSpillCap + j] = leaf;
-                }
-                nc++;
-            };
-            // the count the queue sees: > 32 + kSpillCap sends the slot to
-            // the overflow walk
-            auto final_count = [&]() -> int32_t {
-                if (overflow) return kWaveCandidates + kSpillCap + 1;
-                if (nc > kWaveCandidates && (spill < 0 || nc > kWaveCandidates + kSpillCap))
-                    return kWaveCandidates + kSpillCap + 1;
-                return nc;
-            };
-            if (tree_mode) {
-                // merlict's walk (RayAndFrame.cpp:137-149), candidates in its order
-                for (int it = 0; it < kWalkBurst && i < end; it++) {
+        w.best_key[slot] = kNoKey;
+        w.best_leaf[slot] = kNoLeaf;
+        w.overflow_flag[slot] = 0u;
+        if (n_int > max_int) {
+            w.step[slot] = kNoStep;
+        } else {
+            w.step[slot] = 0;
+            const double sd = dot(s, d);
+            if (root != 0 || sc.bvh_nodes == 0 || a.traversal == MLGPU_TRAVERSAL_FRAME_TREE) {
+                // traversal restricted to a frame's subtree (inside a lens):
+                // merlict's own walk of that subtree
+                bool over = false;
+                int32_t i = root;
+                const int32_t end = __ldg(&sc.node_meta[root].x);
+                while (i < end) {
                     const double2* np = reinterpret_cast<const double2*>(sc.node + i);
                     const double2 n01 = __ldg(np), n23 = __ldg(np + 1);
                     const int2 meta = __ldg(&sc.node_meta[i]);
@@ -185,94 +95,185 @@ wave_walk_kernel(const TraceArgs a, const WaveBuffers w, const RayPool cur) {
                         i = meta.x;
                         continue;
                     }
-                    if (meta.y >= 0) push(meta.y);
+                    if (meta.y >= 0) {
+                        if (nc < kTreeCands) cand[nc++] = meta.y;
+                        else over = true;
+                    }
                     i++;
                 }
-                if (i >= end) {
-                    w.cand_count[item] = final_count();
-                    item = -1;
+                if (over) {
+                    mark_overflow(w, slot);
+                    nc = 0;
                 }
             } else {
-            for (int it = 0; it < kWalkBurst && sp > 0; it++) {
-                const int32_t ref = stack[--sp];
-                if (ref < 0) {
-                    const int32_t start = (ref & 0x7fffffff) >> 3;
-                    const int32_t count = (ref & 7) + 1;
-                    for (int32_t j = start; j < start + count; j++) {
-                        const double2* q = reinterpret_cast<const double2*>(sc.bvh_sphere + j);
-                        const double2 c01 = __ldg(q), c23 = __ldg(q + 1);
-                        if (sphere_cull(make_double4(c01.x, c01.y, c23.x, c23.y), s, d, sd))
-                            push(__ldg(sc.bvh_leaf + j));
-                    }
-                    continue;
+                // merlict tests the root frame's own sphere first
+                const double2* np = reinterpret_cast<const double2*>(sc.node);
+                const double2 n01 = __ldg(np), n23 = __ldg(np + 1);
+                if (sphere_cull(make_double4(n01.x, n01.y, n23.x, n23.y), s, d, sd)) {
+                    bvh = true;
+                    const float ox = (float)s.x, oy = (float)s.y, oz = (float)s.z;
+                    float fdx = (float)d.x, fdy = (float)d.y, fdz = (float)d.z;
+                    if (fabsf(fdx) < 1e-30f) fdx = copysignf(1e-30f, fdx);
+                    if (fabsf(fdy) < 1e-30f) fdy = copysignf(1e-30f, fdy);
+                    if (fabsf(fdz) < 1e-30f) fdz = copysignf(1e-30f, fdz);
+                    const float eps = sc.bvh_eps + 4e-7f*(fabsf(ox) + fabsf(oy) + fabsf(oz));
+                    w.ray_o[slot] = make_float4(ox, oy, oz, eps);
+                    w.ray_i[slot] = make_float4(1.0f/fdx, 1.0f/fdy, 1.0f/fdz, 0.0f);
                 }
-                const float4* nq = reinterpret_cast<const float4*>(sc.bvh + ref);
-                const float4 lx = __ldg(nq), ly = __ldg(nq + 1), lz = __ldg(nq + 2);
-                const float4 hx = __ldg(nq + 3), hy = __ldg(nq + 4), hz = __ldg(nq + 5);
-                const int4 ch = __ldg(reinterpret_cast<const int4*>(nq + 6));
-                const float lox[4] = {lx.x, lx.y, lx.z, lx.w}, loy[4] = {ly.x, ly.y, ly.z, ly.w};
-                const float loz[4] = {lz.x, lz.y, lz.z, lz.w}, hix[4] = {hx.x, hx.y, hx.z, hx.w};
-                const float hiy[4] = {hy.x, hy.y, hy.z, hy.w}, hiz[4] = {hz.x, hz.y, hz.z, hz.w};
-                const int32_t child[4] = {ch.x, ch.y, ch.z, ch.w};
+            }
+        }
+    }
+    // queue the BVH root and the frame-tree candidates (all lanes take part)
+    const uint32_t qb = warp_reserve(&w.counters->level_len[0], bvh ? 1u : 0u);
+    if (bvh) {
+        if (qb < w.level_cap) w.level_q[0][qb] = make_uint2(slot, 0u);
+        else mark_overflow(w, slot);
+    }
+    const uint32_t cb = warp_reserve(&w.counters->isect_len, (uint32_t)nc);
+    for (int k = 0; k < nc; k++) {
+        if (cb + k < w.isect_cap) w.isect_q[cb + k] = make_uint2(slot, (uint32_t)cand[k]);
+        else mark_overflow(w, slot);
+    }
+}
+
+// One BVH level: the four child boxes of each queued (ray, node) pair, slab
+// tests in single precision on boxes widened by the ray's rounding.
+__global__ void __launch_bounds__(256)
+wave_level_kernel(const TraceArgs a, const WaveBuffers w, int level) {
+    const DevScene& sc = a.scene;
+    const uint2* in = w.level_q[level & 1];
+    uint2* out = w.level_q[(level + 1) & 1];
+    const uint32_t len = w.counters->level_len[level];
+    const uint32_t n = len < w.level_cap ? len : w.level_cap;
+    const bool last = level + 1 >= kMaxBvhLevels;
+    const int lane = threadIdx.x & 31;
+    for (uint32_t first = warp_first(); first < n; first += gridDim.x*blockDim.x) {
+        const uint32_t e = first + (uint32_t)lane;
+        uint32_t slot = 0;
+        int32_t child[4] = {kBvhEmpty, kBvhEmpty, kBvhEmpty, kBvhEmpty};
+        uint32_t hit = 0;   // bit k: child k hit
+        if (e < n) {
+            const uint2 q = in[e];
+            slot = q.x;
+            const float4 o = w.ray_o[slot], iv = w.ray_i[slot];
+            const float4* nq = reinterpret_cast<const float4*>(sc.bvh + q.y);
+            const float4 lx = __ldg(nq), ly = __ldg(nq + 1), lz = __ldg(nq + 2);
+            const float4 hx = __ldg(nq + 3), hy = __ldg(nq + 4), hz = __ldg(nq + 5);
+            const int4 ch = __ldg(reinterpret_cast<const int4*>(nq + 6));
+            const float lox[4] = {lx.x, lx.y, lx.z, lx.w}, loy[4] = {ly.x, ly.y, ly.z, ly.w};
+            const float loz[4] = {lz.x, lz.y, lz.z, lz.w}, hix[4] = {hx.x, hx.y, hx.z, hx.w};
+            const float hiy[4] = {hy.x, hy.y, hy.z, hy.w}, hiz[4] = {hz.x, hz.y, hz.z, hz.w};
+            child[0] = ch.x; child[1] = ch.y; child[2] = ch.z; child[3] = ch.w;
 #pragma unroll
-                for (int k = 0; k < 4; k++) {
-                    const float ax = (lox[k] - eps - ox)*idx, bx = (hix[k] + eps - ox)*idx;
-                    const float ay = (loy[k] - eps - oy)*idy, by = (hiy[k] + eps - oy)*idy;
-                    const float az = (loz[k] - eps - oz)*idz, bz = (hiz[k] + eps - oz)*idz;
-                    const float tmin = fmaxf(fmaxf(fminf(ax, bx), fminf(ay, by)), fmaxf(fminf(az, bz), 0.0f));
-                    const float tmax = fminf(fminf(fmaxf(ax, bx), fmaxf(ay, by)), fmaxf(az, bz));
-                    if (tmin <= tmax && child[k] != kBvhEmpty) {
-                        if (sp < kBvhStack) stack[sp++] = child[k];
-                        else overflow = true;
-                    }
-                }
+            for (int k = 0; k < 4; k++) {
+                const float ax = (lox[k] - o.w - o.x)*iv.x, bx = (hix[k] + o.w - o.x)*iv.x;
+                const float ay = (loy[k] - o.w - o.y)*iv.y, by = (hiy[k] + o.w - o.y)*iv.y;
+                const float az = (loz[k] - o.w - o.z)*iv.z, bz = (hiz[k] + o.w - o.z)*iv.z;
+                const float tmin = fmaxf(fmaxf(fminf(ax, bx), fminf(ay, by)), fmaxf(fminf(az, bz), 0.0f));
+                const float tmax = fminf(fminf(fmaxf(ax, bx), fmaxf(ay, by)), fmaxf(az, bz));
+                if (tmin <= tmax && child[k] != kBvhEmpty) hit |= 1u << k;
             }
-            if (sp == 0) {
-                w.cand_count[item] = final_count();
-                item = -1;
-            }
+        }
+        uint32_t nn = 0, nr = 0;
+#pragma unroll
+        for (int k = 0; k < 4; k++)
+            if (hit & (1u << k)) { if (child[k] < 0) nr++; else nn++; }
+        uint32_t nb = warp_reserve(&w.counters->level_len[last ? level : level + 1], last ? 0u : nn);
+        uint32_t rb = warp_reserve(&w.counters->range_len, nr);
+#pragma unroll
+        for (int k = 0; k < 4; k++) {
+            if (!(hit & (1u << k))) continue;
+            if (child[k] < 0) {
+                if (rb < w.range_cap) w.range_q[rb] = make_uint2(slot, (uint32_t)child[k]);
+                else mark_overflow(w, slot);
+                rb++;
+            } else {
+                if (!last && nb < w.level_cap) out[nb] = make_uint2(slot, (uint32_t)child[k]);
+                else mark_overflow(w, slot);
+                nb++;
             }
         }
     }
 }
 
+// merlict's bounding-sphere test (RayAndFrame.cpp:16-107) of every leaf in
+// the queued leaf ranges; the leaves that pass become candidates.
+__global__ void __launch_bounds__(256)
+wave_sphere_kernel(const TraceArgs a, const WaveBuffers w, const RayPool cur) {
+    const DevScene& sc = a.scene;
+    const uint32_t len = w.counters->range_len;
+    const uint32_t n = len < w.range_cap ? len : w.range_cap;
+    const int lane = threadIdx.x & 31;
+    for (uint32_t first = warp_first(); first < n; first += gridDim.x*blockDim.x) {
+        const uint32_t e = first + (uint32_t)lane;
+        uint32_t slot = 0;
+        int32_t pass[8];
+        uint32_t np = 0;
+        if (e < n) {
+            const uint2 q = w.range_q[e];
+            slot = q.x;
+            const int32_t ref = (int32_t)q.y;
+            const int32_t start = (ref & 0x7fffffff) >> 3;
+            const int32_t count = (ref & 7) + 1;
+            const v3 s = mk(cur.sx[slot], cur.sy[slot], cur.sz[slot]);
+            const v3 d = mk(cur.dx[slot], cur.dy[slot], cur.dz[slot]);
+            const double sd = dot(s, d);
+            for (int32_t j = start; j < start + count; j++) {
+                const double2* c = reinterpret_cast<const double2*>(sc.bvh_sphere + j);
+                const double2 c01 = __ldg(c), c23 = __ldg(c + 1);
+                if (sphere_cull(make_double4(c01.x, c01.y, c23.x, c23.y), s, d, sd))
+                    pass[np++] = __ldg(sc.bvh_leaf + j);
+            }
+        }
+        const uint32_t cb = warp_reserve(&w.counters->isect_len, np);
+        for (uint32_t k = 0; k < np; k++) {
+            if (cb + k < w.isect_cap) w.isect_q[cb + k] = make_uint2(slot, (uint32_t)pass[k]);
+            else mark_overflow(w, slot);
+        }
+    }
+}
+
 // counters between the kernels of an iteration
-__global__ void wave_after_walk_kernel(WaveCounters* c, uint32_t pool, uint64_t num_photons) {
+__global__ void wave_after_intake_kernel(WaveCounters* c, uint32_t pool, uint64_t num_photons) {
     const unsigned long long remaining = num_photons - c->next_input;
     const uint32_t room = pool - c->active;
     const uint32_t fresh = (uint32_t)(remaining < room ? remaining : room);
     c->total = c->active + fresh;
     c->next_input += fresh;
     c->next = 0;
-    c->queue_len = 0;
-    c->overflow_len = 0;
 }
 
 __global__ void wave_after_resolve_kernel(WaveCounters* c) {
-    c->active = c->next;
-    c->walk_fetch = 0;
-    c->spill_used = 0;
+    if (threadIdx.x == 0) {
+        c->active = c->next;
+        c->range_len = 0;
+        c->isect_len = 0;
+        c->overflow_len = 0;
+    }
+    for (int k = threadIdx.x; k < kMaxBvhLevels; k += blockDim.x) c->level_len[k] = 0;
 }
 
 }  // namespace
 
 cudaError_t launch_wave_iteration(const TraceArgs& a, const WaveBuffers& w, const RayPool& cur,
-                                  const RayPool& nxt, int walk_blocks, int form, cudaStream_t s,
-                                  cudaEvent_t* ev) {
+                                  const RayPool& nxt, int form, cudaStream_t s, cudaEvent_t* ev) {
     const int slot_blocks = (int)((w.pool + 255)/256);
     if (ev) cudaEventRecord(ev[0], s);
     if (a.in_dtype == MLGPU_F64)
-        wave_walk_kernel<double><<<walk_blocks, 256, 0, s>>>(a, w, cur);
+        wave_intake_kernel<double><<<slot_blocks, 256, 0, s>>>(a, w, cur);
     else
-        wave_walk_kernel<float><<<walk_blocks, 256, 0, s>>>(a, w, cur);
+        wave_intake_kernel<float><<<slot_blocks, 256, 0, s>>>(a, w, cur);
+    wave_after_intake_kernel<<<1, 1, 0, s>>>(w.counters, w.pool, a.num_photons);
     if (ev) cudaEventRecord(ev[1], s);
-    wave_after_walk_kernel<<<1, 1, 0, s>>>(w.counters, w.pool, a.num_photons);
-    wave_enqueue_kernel<<<slot_blocks, 256, 0, s>>>(w);
-    wave_overflow_kernel<<<kOverflowBlocks, 128, 0, s>>>(a, w, cur);
+    for (int k = 0; k < a.scene.bvh_levels; k++)
+        wave_level_kernel<<<w.grid, 256, 0, s>>>(a, w, k);
+    wave_sphere_kernel<<<w.grid, 256, 0, s>>>(a, w, cur);
     if (ev) cudaEventRecord(ev[2], s);
     if (form == MLGPU_TRACER_FP64) {
-        wave_isect_kernel<kIsectFp64><<<w.isect_blocks, 256, 0, s>>>(a, w, cur);
+        wave_isect_kernel<kIsectFp64><<<w.grid, 256, 0, s>>>(a, w, cur);
+        wave_tie_kernel<<<w.grid, 256, 0, s>>>(w);
         if (ev) cudaEventRecord(ev[3], s);
+        wave_overflow_kernel<<<148, 128, 0, s>>>(a, w, cur);
         if (a.out_dtype == MLGPU_F64)
             wave_resolve_kernel<double, kIsectFp64><<<slot_blocks, 256, w.fn_smem_bytes, s>>>(a, w, cur, nxt);
         else
@@ -283,27 +284,16 @@ cudaError_t launch_wave_iteration(const TraceArgs& a, const WaveBuffers& w, cons
                                                           ev ? ev[3] : nullptr);
         if (e != cudaSuccess) return e;
     }
-    wave_after_resolve_kernel<<<1, 1, 0, s>>>(w.counters);
+    wave_after_resolve_kernel<<<1, 64, 0, s>>>(w.counters);
     if (ev) cudaEventRecord(ev[4], s);
     return cudaGetLastError();
 }
 
-int wave_isect_blocks() {
-    int per_sm = 0, sms = 0, dev = 0;
+int wave_persistent_blocks() {
+    int sms = 0, dev = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, wave_isect_kernel<kIsectFp64>, 256, 0);
-    if (per_sm < 1) per_sm = 1;
-    return per_sm*sms;
-}
-
-int wave_fp64_walk_blocks() {
-    int per_sm = 0, sms = 0, dev = 0;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, wave_walk_kernel<double>, 256, 0);
-    if (per_sm < 1) per_sm = 1;
-    return per_sm*sms;
+    return 8*sms;
 }
 
 }  // namespace mlgpu

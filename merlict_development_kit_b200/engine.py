@@ -181,7 +181,7 @@ class Scene:
         check(lib().mlgpu_scene_kernel_launches(self._h, C.byref(v)))
         return int(v.value)
 
-    KERNEL_CLASSES = ("walk", "queue", "intersect", "resolve", "plain", "bin")
+    KERNEL_CLASSES = ("walk", "intake", "intersect", "resolve", "plain", "bin")
 
     def set_profiling(self, enable: bool) -> None:
         """Turns CUDA-event timing of the kernel classes on or off (and
