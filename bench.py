@@ -247,11 +247,17 @@ def run_ours(args, world, rank, local):
     stream = torch.cuda.current_stream()
     results = {}
 
+    tuning = None
+    if args.autotune and tracer != "fp64_plain":
+        sample = {k: v[:min(n, 2_000_000)].contiguous() for k, v in dev.items()}
+        tuning, _ = scene.autotune(sample, cfg, engine.Philox(3), tracer=tracer)
+        del sample
+
     def step(ev=None):
         if ev is not None:
             ev[0].record(stream)
         out = scene.propagate(dev, cfg, rng, tracer=tracer, outputs=("sensor", "x", "y", "time"),
-                              out_dtype=out_dtype, sync=False, results=results)
+                              out_dtype=out_dtype, sync=False, results=results, tuning=tuning)
         if ev is not None:
             ev[1].record(stream)
         scene.bin_arrivals(out["sensor"])
@@ -271,7 +277,6 @@ def run_ours(args, world, rank, local):
     t_start = torch.cuda.Event(enable_timing=True)
     t_stop = torch.cuda.Event(enable_timing=True)
     launches0 = scene.kernel_launches()
-    scene.set_profiling(True)   # CUDA events around every kernel class
     t_start.record(stream)
     for k in range(args.steps):
         step(kernel_events[k])
@@ -280,9 +285,15 @@ def run_ours(args, world, rank, local):
     torch.cuda.synchronize()
     barrier(world)
     clk = clocks.stop()
+    scene.sync_errors()
+    # per-stage device times: the same steps again with CUDA events around
+    # every kernel class (launched one by one, outside the timed region)
+    scene.set_profiling(True)
+    for k in range(args.steps):
+        step()
+    torch.cuda.synchronize()
     stage = scene.kernel_times()
     scene.set_profiling(False)
-    scene.sync_errors()
     elapsed_ms = t_start.elapsed_time(t_stop)
     kernel_ms = float(np.mean([a.elapsed_time(b) for a, b in kernel_events]))
     elapsed_ms = max_over_ranks(elapsed_ms, world)
@@ -305,7 +316,7 @@ def run_ours(args, world, rank, local):
     res.dtype = abi.F64 if out_dtype == torch.float64 else abi.F32
     res.sensor, res.x, res.y, res.time = (h_sensor.data_ptr(), h_x.data_ptr(), h_y.data_ptr(),
                                           h_t.data_ptr())
-    st = abi.mlgpu_settings(MAX_INTERACTIONS, 0, engine.TRACERS[tracer], 0, abi.TRAVERSAL_BVH)
+    st = engine._settings(cfg, 0, tracer, "bvh", tuning)
     r = abi.mlgpu_rng()
     r.mode = abi.RNG_PHILOX
     r.seed = 99 + rank
@@ -381,7 +392,9 @@ def run_ours(args, world, rank, local):
         "data": "synthetic",
         "config": {"workload": WORKLOAD, "scene": scene_config_name(), "tracer": tracer,
                    "photons_per_step_per_gpu": n, "max_interactions": MAX_INTERACTIONS,
-                   "l2": "inputs larger than L2 (photon planes %.0f MB)" % (7 * elt * n / 1e6)},
+                   "l2": "inputs larger than L2 (photon planes %.0f MB)" % (7 * elt * n / 1e6),
+                   "tuning": tuning or "defaults",
+                   "stage_times": "a second pass over the same steps, kernels timed one by one"},
         "kernel_ms": kernel_ms,
         "roofline": roofline,
         "compute_roofline": compute,
@@ -397,6 +410,134 @@ def run_ours(args, world, rank, local):
     scene.close()
 
 
+def run_bunches(args, world, rank, local):
+    """Batched uneven events: `args.events` air-shower-like events with
+    log-uniform sizes in [1e2, 1e6] photons on the light-field telescope,
+    traced (a) as one photon stream with autotuned knobs and CUDA-graph
+    launches and (b) with one propagate call per event (the reference's
+    per-event loop, plenoscope_propagation.cpp:206-210), same Philox streams,
+    so the two give identical results."""
+    import torch
+    from merlict_development_kit_b200 import engine, factories as F, photons as P
+
+    torch.cuda.set_device(local)
+    flat = F.light_field_telescope(**SCENE).flatten()
+    scene = engine.Scene(flat)
+    sizes = P.cherenkov_event_sizes(args.events, 2024 + rank)
+    dev, off = P.cherenkov_events(sizes, 4048 + rank, device=f"cuda:{local}")
+    n = int(off[-1])
+    cfg = engine.PropagationConfig(MAX_INTERACTIONS)
+    stream = torch.cuda.current_stream()
+    outs = ("sensor", "x", "y", "time")
+    sample = {k: v[:min(n, 4_000_000)].contiguous() for k, v in dev.items()}
+    tuning, _ = scene.autotune(sample, cfg, engine.Philox(3))
+    del sample
+    res_batched, res_events = {}, {}
+
+    def batched():
+        return scene.propagate(dev, cfg, engine.Philox(11), outputs=outs, sync=False,
+                               results=res_batched, tuning=tuning)
+
+    def per_event():
+        for e in range(len(sizes)):
+            a, b = int(off[e]), int(off[e + 1])
+            part = {k: v[a:b] for k, v in dev.items()}
+            r = {k: v[a:b] for k, v in res_events.items()}
+            scene.propagate(part, cfg, engine.Philox(11, photon_offset=a), outputs=outs,
+                            sync=False, results=r)
+
+    for _ in range(args.warmup):
+        batched()
+    scene.sync_errors()
+    for k, v in res_batched.items():
+        res_events[k] = torch.empty_like(v)
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
+    clocks = ClockSampler(local)
+    clocks.start()
+    barrier(world)
+    torch.cuda.synchronize()
+    ev[0].record(stream)
+    for _ in range(args.steps):
+        batched()
+    ev[1].record(stream)
+    torch.cuda.synchronize()
+    ev[2].record(stream)
+    per_event()
+    ev[3].record(stream)
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    scene.sync_errors()
+    identical = all(bool(torch.equal(res_batched[k], res_events[k])) for k in ("sensor", "x", "y"))
+    ms_b = max_over_ranks(ev[0].elapsed_time(ev[1]) / args.steps, world)
+    ms_e = max_over_ranks(ev[2].elapsed_time(ev[3]), world)
+    if rank == 0:
+        hit = float((res_batched["sensor"] >= 0).float().mean())
+        print(json.dumps({
+            "metric": "photons/s", "value": n * world / (ms_b * 1e-3), "unit": "photons/s",
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_b,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic",
+            "config": {"workload": f"{args.events} air-shower-like events, log-uniform 1e2-1e6 "
+                                   "photons, on the light-field telescope (config 2)",
+                       "photons_per_step_per_gpu": n, "events": int(len(sizes)),
+                       "max_interactions": MAX_INTERACTIONS, "tuning": tuning,
+                       "fraction_on_lixels": hit},
+            "one_call_per_event": {"value": n * world / (ms_e * 1e-3), "unit": "photons/s",
+                                   "ms": ms_e, "calls": int(len(sizes))},
+            "batched_over_per_event": ms_e / ms_b,
+            "identical_results": identical,
+            "clocks": clk,
+        }), flush=True)
+    scene.close()
+
+
+def run_precision(args, world, rank, local):
+    """Precision study (config 3): the large parabolic reflector (0.9 m facets
+    of curvature radius 213 m on a 35.5 m aperture) with 8,443 flat pixels at
+    106.5 m; photons within 3.5 degrees of the axis.  Photons/s of each form
+    and its errors against the FP64 tracer, photon by photon."""
+    import torch
+    from merlict_development_kit_b200 import engine, factories as F, photons as P, precision
+
+    torch.cuda.set_device(local)
+    flat = F.large_reflector_camera().flatten()
+    n = args.photons
+    ph = P.downward_disc_source_device(n, 303 + rank, 40.0, 110.0, 3.5, device=f"cuda:{local}",
+                                       dtype=torch.float32)
+    scene = engine.Scene(flat)
+    cfg = engine.PropagationConfig(5)
+    rates = {}
+    for form in ("fp64", "fp32", "fp32_pure"):
+        dt = torch.float32 if form.startswith("fp32") else torch.float64
+        planes = {k: v.to(dt) for k, v in ph.items()}
+        res = {}
+        for _ in range(args.warmup):
+            scene.propagate(planes, cfg, engine.Philox(5), tracer=form, sync=False, results=res,
+                            outputs=("sensor", "x", "y", "time"), out_dtype=dt)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(args.steps):
+            scene.propagate(planes, cfg, engine.Philox(5), tracer=form, sync=False, results=res,
+                            outputs=("sensor", "x", "y", "time"), out_dtype=dt)
+        e1.record()
+        torch.cuda.synchronize()
+        rates[form] = n * args.steps / (e0.elapsed_time(e1) * 1e-3)
+        del planes, res
+    scene.close()
+    errors = precision.study(flat, ph, seed=9, max_interactions=5)
+    if rank == 0:
+        print(json.dumps({
+            "metric": "photons/s", "value": rates["fp32"], "unit": "photons/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": "precision study: 5,388-facet parabolic reflector, R = 213 m, "
+                                   "8,443 pixels at 106.5 m (config 3)",
+                       "photons": n, "max_interactions": 5},
+            "photons_per_s": rates, "errors_vs_fp64": errors,
+        }), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -407,11 +548,23 @@ def main():
     ap.add_argument("--photons", type=int, default=10_000_000)
     ap.add_argument("--ref-photons", type=int, default=100_000)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-autotune", dest="autotune", action="store_false",
+                    help="default wavefront knobs instead of mlgpu_scene_autotune's")
+    ap.add_argument("--workload", choices=["telescope", "bunches", "precision"],
+                    default="telescope",
+                    help="telescope: the light-field telescope batch; bunches: 4096 "
+                         "air-shower-like events of uneven sizes, batched vs one call per event; "
+                         "precision: the FP32 forms against FP64 on the large reflector")
+    ap.add_argument("--events", type=int, default=4096)
     args = ap.parse_args()
     world, rank, local = init_dist()
     try:
         if args.impl == "reference":
             run_reference_arm(args, world, rank)
+        elif args.workload == "bunches":
+            run_bunches(args, world, rank, local)
+        elif args.workload == "precision":
+            run_precision(args, world, rank, local)
         else:
             run_ours(args, world, rank, local)
     finally:

@@ -32,7 +32,7 @@
 extern "C" {
 #endif
 
-#define MLGPU_ABI_VERSION 2
+#define MLGPU_ABI_VERSION 3
 
 /* ---- status codes ------------------------------------------------------ */
 enum {
@@ -218,14 +218,28 @@ enum {
  * frame) always walks the frame tree.                                     */
 enum { MLGPU_TRAVERSAL_BVH = 0, MLGPU_TRAVERSAL_FRAME_TREE = 1 };
 
-/* PropagationConfig (merlict/PropagationConfig.h:10-13) plus engine knobs. */
+/* PropagationConfig (merlict/PropagationConfig.h:10-13) plus engine knobs.
+ * The knobs after `traversal` tune the wavefront tracers and never change
+ * results; 0 selects the default.  mlgpu_scene_autotune picks them.       */
 typedef struct mlgpu_settings {
     uint32_t max_num_interactions_per_photon;
     int32_t start_node;     /* node of the `world` frame passed by the caller */
     int32_t tracer;         /* MLGPU_TRACER_*                                 */
     int32_t block_size;     /* 0 = default                                    */
     int32_t traversal;      /* MLGPU_TRAVERSAL_*                              */
+    uint32_t pool_size;     /* ray slots of the wavefront pool (2^21)         */
+    int32_t check_period;   /* iterations between host checks of the pool (4) */
+    int32_t use_graph;      /* 1: each check period is one CUDA-graph launch  */
+    int32_t grid_blocks;    /* blocks of the grid-stride kernels (8 per SM)   */
+    int32_t staged_levels;  /* top BVH levels read from shared memory (0)     */
+    int32_t photon_order;   /* MLGPU_ORDER_*: the order photons enter the pool */
 } mlgpu_settings;
+
+/* photon_order: COHERENT sorts the batch by a 4-D cell key of support and
+ * direction before tracing, so that neighbouring ray slots follow nearly
+ * the same path (results are the same in any order).  DEFAULT is COHERENT
+ * for batches of at least 65,536 photons and INPUT below.                  */
+enum { MLGPU_ORDER_DEFAULT = 0, MLGPU_ORDER_INPUT = 1, MLGPU_ORDER_COHERENT = 2 };
 
 typedef struct mlgpu_scene mlgpu_scene;
 
@@ -298,6 +312,28 @@ int mlgpu_propagate_host(
     const mlgpu_settings* settings,
     const mlgpu_rng* rng,
     mlgpu_results* results);
+
+/* ---- tuning ------------------------------------------------------------ *
+ * No counterpart in the reference (merlict has no device parameters).
+ * Picks the wavefront knobs of `base` (pool_size, check_period, use_graph,
+ * grid_blocks, staged_levels, photon_order) for this scene by timing
+ * mlgpu_propagate on a
+ * sample of photons (device pointers, as for mlgpu_propagate): coordinate
+ * descent from the defaults, each candidate timed with CUDA events on
+ * `cuda_stream` (best of two runs after one untimed run).  Writes the
+ * fastest settings to `best` (the other fields copied from `base`) and its
+ * time in milliseconds to `best_ms` (may be NULL).  Results of the sample
+ * runs are discarded; the tracer form is `base->tracer` (a wavefront
+ * form).  The knobs never change what a propagation computes.            */
+int mlgpu_scene_autotune(
+    mlgpu_scene* scene,
+    const mlgpu_photons* sample,
+    uint64_t num_photons,
+    const mlgpu_settings* base,
+    const mlgpu_rng* rng,
+    mlgpu_settings* best,
+    double* best_ms,
+    void* cuda_stream);
 
 /* ---- arrival binning ------------------------------------------------- *
  * Replaces Sensors::assign_photons (merlict/sensor/Sensors.cpp:79-81) for

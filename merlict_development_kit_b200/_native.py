@@ -65,7 +65,11 @@ def lib():
         L.mlgpu_bin_arrivals_noalloc.argtypes = [
             C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint64, C.c_void_p, C.c_void_p,
             C.c_uint32, C.c_double, C.c_double, C.c_void_p]
-        for name in ("mlgpu_scene_create", "mlgpu_scene_destroy", "mlgpu_propagate",
+        L.mlgpu_scene_autotune.argtypes = [
+            C.c_void_p, C.POINTER(abi.mlgpu_photons), C.c_uint64,
+            C.POINTER(abi.mlgpu_settings), C.POINTER(abi.mlgpu_rng),
+            C.POINTER(abi.mlgpu_settings), C.POINTER(C.c_double), C.c_void_p]
+        for name in ("mlgpu_scene_create", "mlgpu_scene_destroy", "mlgpu_propagate", "mlgpu_scene_autotune",
                      "mlgpu_propagate_host", "mlgpu_scene_sync_errors", "mlgpu_bin_arrivals",
                      "mlgpu_bin_arrivals_noalloc", "mlgpu_scene_kernel_launches"):
             getattr(L, name).restype = C.c_int
@@ -91,5 +95,5 @@ EXPORTED = (
     "mlgpu_abi_version", "mlgpu_last_error", "mlgpu_scene_create", "mlgpu_scene_destroy",
     "mlgpu_propagate", "mlgpu_scene_sync_errors", "mlgpu_propagate_host",
     "mlgpu_bin_arrivals", "mlgpu_bin_arrivals_noalloc", "mlgpu_scene_kernel_launches",
-    "mlgpu_scene_set_profiling", "mlgpu_scene_kernel_times",
+    "mlgpu_scene_set_profiling", "mlgpu_scene_kernel_times", "mlgpu_scene_autotune",
 )

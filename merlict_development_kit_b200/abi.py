@@ -11,7 +11,7 @@ from dataclasses import dataclass, field
 
 import numpy as np
 
-ABI_VERSION = 2
+ABI_VERSION = 3
 
 # status codes
 OK = 0
@@ -183,6 +183,10 @@ class mlgpu_rng(C.Structure):
 TRAVERSAL_BVH = 0
 TRAVERSAL_FRAME_TREE = 1
 
+ORDER_DEFAULT = 0
+ORDER_INPUT = 1
+ORDER_COHERENT = 2
+
 
 class mlgpu_settings(C.Structure):
     _fields_ = [
@@ -191,7 +195,19 @@ class mlgpu_settings(C.Structure):
         ("tracer", C.c_int32),
         ("block_size", C.c_int32),
         ("traversal", C.c_int32),
+        ("pool_size", C.c_uint32),
+        ("check_period", C.c_int32),
+        ("use_graph", C.c_int32),
+        ("grid_blocks", C.c_int32),
+        ("staged_levels", C.c_int32),
+        ("photon_order", C.c_int32),
     ]
+
+    TUNING = ("pool_size", "check_period", "use_graph", "grid_blocks", "staged_levels",
+              "photon_order")
+
+    def tuning(self) -> dict:
+        return {k: int(getattr(self, k)) for k in self.TUNING}
 
 
 def _ptr(a: np.ndarray, ctype):

@@ -225,6 +225,10 @@ void build_bvh4(const mlgpu_flat_scene* f, double inflate, BvhHost* out) {
         }
         out->nodes[w] = node;
     }
+    // nodes were numbered in breadth-first order, so each level is a range
+    out->level_start.assign((size_t)out->levels + 1, (int32_t)out->nodes.size());
+    for (int32_t i = (int32_t)level.size() - 1; i >= 0; i--) out->level_start[level[i]] = i;
+    out->level_start[0] = 0;
 }
 
 }  // namespace mlgpu

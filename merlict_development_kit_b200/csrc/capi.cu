@@ -129,11 +129,16 @@ struct mlgpu_scene {
     std::vector<void*> owned;        // device allocations of the scene
     unsigned int* error_word = nullptr;
     // staging for mlgpu_propagate_host and scratch for binning
-    DeviceBuffer staging_in, staging_out, staging_hist, staging_rng, bin_scratch;
+    DeviceBuffer staging_in, staging_out, staging_hist, staging_rng, bin_scratch, tune_out;
+    DeviceBuffer order;                  // tracing order of a batch and its sort scratch
     // ray pools of the wavefront tracers
     DeviceBuffer wave;
     WaveCounters* wave_host = nullptr;   // pinned copy of the counters
-    int wave_grid = 0;                   // blocks of the persistent kernels
+    int wave_grid = 0;                   // default blocks of the persistent kernels
+    // one check period of wavefront iterations as a CUDA graph, recorded on
+    // a private stream and replayed on the caller's
+    cudaGraphExec_t wave_graph = nullptr;
+    cudaStream_t capture_stream = nullptr;
     uint64_t launches = 0;               // kernels launched for this scene
     Profiler prof;
 };
@@ -280,6 +285,8 @@ int build_device_scene(mlgpu_scene* s, const mlgpu_flat_scene* f) {
             if ((st = upload(s, sph.data(), sph.size(), &s->dev.bvh_sphere))) return st;
             s->dev.bvh_nodes = (int32_t)bvh.nodes.size();
             s->dev.bvh_levels = bvh.levels;
+            for (int k = 0; k <= kMaxBvhLevels; k++)
+                s->dev.bvh_level_start[k] = k <= bvh.levels ? bvh.level_start[k] : s->dev.bvh_nodes;
         }
         // a tree deeper than the walk's level queues: merlict's frame walk
         if (s->dev.bvh_levels >= kMaxBvhLevels) {
@@ -332,6 +339,18 @@ int check_propagate_args(const mlgpu_scene* scene, const mlgpu_photons* ph,
         return fail(MLGPU_ERR_INVALID_ARGUMENT, "unknown tracer %d", st->tracer);
     if (st->traversal != MLGPU_TRAVERSAL_BVH && st->traversal != MLGPU_TRAVERSAL_FRAME_TREE)
         return fail(MLGPU_ERR_INVALID_ARGUMENT, "unknown traversal %d", st->traversal);
+    if (st->pool_size > (1u << 24) || (st->pool_size != 0 && st->pool_size < 1024))
+        return fail(MLGPU_ERR_INVALID_ARGUMENT, "pool_size must be 0 or in [1024, 2^24]");
+    if (st->check_period < 0 || st->check_period > 64)
+        return fail(MLGPU_ERR_INVALID_ARGUMENT, "check_period must be in [0, 64]");
+    if (st->grid_blocks < 0 || st->grid_blocks > 65535)
+        return fail(MLGPU_ERR_INVALID_ARGUMENT, "grid_blocks must be in [0, 65535]");
+    if (st->staged_levels < 0 || st->staged_levels > kMaxBvhLevels)
+        return fail(MLGPU_ERR_INVALID_ARGUMENT, "staged_levels must be in [0, %d]", kMaxBvhLevels);
+    if (st->use_graph != 0 && st->use_graph != 1)
+        return fail(MLGPU_ERR_INVALID_ARGUMENT, "use_graph must be 0 or 1");
+    if (st->photon_order < MLGPU_ORDER_DEFAULT || st->photon_order > MLGPU_ORDER_COHERENT)
+        return fail(MLGPU_ERR_INVALID_ARGUMENT, "unknown photon_order %d", st->photon_order);
     return MLGPU_OK;
 }
 
@@ -365,7 +384,8 @@ constexpr uint32_t kWavePool = 1u << 21;   // ray slots of the wavefront tracers
 
 // Carves the two ray pools, the candidate lists and the counters out of
 // one device buffer.
-int wave_buffers(mlgpu_scene* scene, uint32_t pool, WaveBuffers* w, RayPool* p0, RayPool* p1) {
+int wave_buffers(mlgpu_scene* scene, uint32_t pool, int grid, int staged, WaveBuffers* w,
+                 RayPool* p0, RayPool* p1) {
     auto up = [](size_t x) { return (x + 255) & ~size_t(255); };
     const size_t P = pool;
     const size_t level_cap = 8*P, range_cap = 16*P, isect_cap = 16*P;
@@ -387,7 +407,8 @@ int wave_buffers(mlgpu_scene* scene, uint32_t pool, WaveBuffers* w, RayPool* p0,
         for (int32_t** q : i) *q = reinterpret_cast<int32_t*>(take(P*4));
     }
     w->pool = pool;
-    w->grid = scene->wave_grid;
+    w->grid = grid > 0 ? grid : scene->wave_grid;
+    w->staged_levels = staged;
     w->step = reinterpret_cast<int32_t*>(take(P*4));
     w->ray_o = reinterpret_cast<float4*>(take(P*16));
     w->ray_i = reinterpret_cast<float4*>(take(P*16));
@@ -409,43 +430,117 @@ int wave_buffers(mlgpu_scene* scene, uint32_t pool, WaveBuffers* w, RayPool* p0,
     return MLGPU_OK;
 }
 
+// Records `period` wavefront iterations (starting from ray pool 0) and the
+// copy of the counters to the host as one CUDA graph, on the scene's private
+// stream, and makes it the scene's executable graph (updated in place when
+// the previous one has the same shape).
+int record_wave_graph(mlgpu_scene* scene, const TraceArgs& a, const WaveBuffers& w,
+                      const RayPool* pools, int form, int period) {
+    if (!scene->capture_stream)
+        MLGPU_CUDA(cudaStreamCreateWithFlags(&scene->capture_stream, cudaStreamNonBlocking));
+    cudaStream_t cs = scene->capture_stream;
+    MLGPU_CUDA(cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal));
+    cudaError_t e = cudaSuccess;
+    for (int g = 0; g < period && e == cudaSuccess; g++)
+        e = launch_wave_iteration(a, w, pools[g & 1], pools[(g + 1) & 1], form, cs, nullptr);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(scene->wave_host, w.counters, sizeof(WaveCounters),
+                            cudaMemcpyDeviceToHost, cs);
+    cudaGraph_t graph = nullptr;
+    const cudaError_t e2 = cudaStreamEndCapture(cs, &graph);
+    if (e != cudaSuccess || e2 != cudaSuccess) {
+        if (graph) cudaGraphDestroy(graph);
+        return cuda_fail(e != cudaSuccess ? e : e2, "recording the wavefront graph");
+    }
+    bool updated = false;
+    if (scene->wave_graph) {
+        cudaGraphExecUpdateResultInfo info;
+        if (cudaGraphExecUpdate(scene->wave_graph, graph, &info) == cudaSuccess) updated = true;
+        else {
+            cudaGetLastError();
+            cudaGraphExecDestroy(scene->wave_graph);
+            scene->wave_graph = nullptr;
+        }
+    }
+    if (!updated) e = cudaGraphInstantiate(&scene->wave_graph, graph, 0);
+    cudaGraphDestroy(graph);
+    if (e != cudaSuccess) {
+        scene->wave_graph = nullptr;
+        return cuda_fail(e, "instantiating the wavefront graph");
+    }
+    return MLGPU_OK;
+}
+
 // Runs iterations of a wavefront tracer until every photon has finished,
-// checking the counters after every few iterations.  `resolve` selects the
-// intersection arithmetic of the resolve step (FP64 or one of the FP32 forms).
-int run_wavefront(mlgpu_scene* scene, const TraceArgs& a, int resolve, cudaStream_t stream) {
-    const uint32_t pool = (uint32_t)std::min<uint64_t>(a.num_photons, kWavePool);
+// checking the counters on the host after every `check_period` iterations
+// (one CUDA-graph launch per period with use_graph).  `form` selects the
+// intersection arithmetic (FP64 or one of the FP32 forms).
+int run_wavefront(mlgpu_scene* scene, TraceArgs a, const mlgpu_settings* st,
+                  cudaStream_t stream) {
+    const int form = st->tracer;
+    const bool coherent = a.num_photons < (1ull << 32) &&
+        (st->photon_order == MLGPU_ORDER_COHERENT ||
+         (st->photon_order == MLGPU_ORDER_DEFAULT && a.num_photons >= 65536));
+    if (coherent) {
+        const size_t obytes = (size_t)a.num_photons*sizeof(uint32_t);
+        MLGPU_CUDA(scene->order.reserve(obytes + 256 + photon_order_scratch_bytes(a.num_photons)));
+        uint32_t* order = static_cast<uint32_t*>(scene->order.ptr);
+        char* scratch = static_cast<char*>(scene->order.ptr) + ((obytes + 255) & ~size_t(255));
+        if (!scene->wave_grid) scene->wave_grid = wave_persistent_blocks();
+        const cudaError_t e = launch_photon_order(a.photons, a.in_dtype, a.num_photons, order,
+                                                  scratch, scene->wave_grid, stream);
+        if (e != cudaSuccess) return cuda_fail(e, "photon order kernels");
+        scene->launches += 7;
+        a.order = order;
+    }
+    const uint32_t want = st->pool_size ? st->pool_size : kWavePool;
+    const uint32_t pool = (uint32_t)std::min<uint64_t>(a.num_photons, want);
     WaveBuffers w;
     RayPool pools[2];
-    const int st = wave_buffers(scene, pool, &w, &pools[0], &pools[1]);
-    if (st) return st;
+    const int rc = wave_buffers(scene, pool, st->grid_blocks, st->staged_levels, &w,
+                                &pools[0], &pools[1]);
+    if (rc) return rc;
+    // per-kernel events cannot be taken inside a graph: profiling runs launch by launch
+    const bool graph = st->use_graph != 0 && !scene->prof.on;
+    int period = st->check_period > 0 ? st->check_period : 4;
+    if (graph && (period & 1)) period++;   // a graph starts and ends on ray pool 0
+    if (graph) {
+        const int r = record_wave_graph(scene, a, w, pools, form, period);
+        if (r) return r;
+    }
     MLGPU_CUDA(cudaMemsetAsync(w.counters, 0, sizeof(WaveCounters), stream));
     // every iteration advances each live photon by one step
     const uint64_t bound = (a.num_photons*(uint64_t)(a.max_interactions + 1))/pool +
-        a.max_interactions + 16;
+        a.max_interactions + 16 + (uint64_t)period;
+    const int levels = scene->dev.bvh_levels;
     uint64_t iteration = 0;
-    const int group = 4;
     while (true) {
-        for (int g = 0; g < group; g++, iteration++) {
-            const RayPool& cur = pools[iteration & 1];
-            const RayPool& nxt = pools[(iteration + 1) & 1];
-            Profiler::Chain ch;
-            const bool timed = scene->prof.on && scene->prof.take(5, ch.ev);
-            const cudaError_t e = launch_wave_iteration(a, w, cur, nxt, resolve, stream,
-                                                        timed ? ch.ev : nullptr);
-            if (e != cudaSuccess) return cuda_fail(e, "wavefront kernels");
-            const int levels = scene->dev.bvh_levels;
-            scene->launches += (uint64_t)levels + 8;
-            if (timed) {
-                ch.n = 5;
-                const int cls[4] = {MLGPU_KERNEL_INTAKE, MLGPU_KERNEL_WALK, MLGPU_KERNEL_INTERSECT,
-                                    MLGPU_KERNEL_RESOLVE};
-                const int launches[4] = {2, levels + 1, 2, 3};
-                for (int k = 0; k < 4; k++) { ch.cls[k] = cls[k]; ch.launches[k] = launches[k]; }
-                scene->prof.add(ch);
+        if (graph) {
+            MLGPU_CUDA(cudaGraphLaunch(scene->wave_graph, stream));
+            iteration += (uint64_t)period;
+            scene->launches += (uint64_t)period*((uint64_t)levels + 8);
+        } else {
+            for (int g = 0; g < period; g++, iteration++) {
+                const RayPool& cur = pools[iteration & 1];
+                const RayPool& nxt = pools[(iteration + 1) & 1];
+                Profiler::Chain ch;
+                const bool timed = scene->prof.on && scene->prof.take(5, ch.ev);
+                const cudaError_t e = launch_wave_iteration(a, w, cur, nxt, form, stream,
+                                                            timed ? ch.ev : nullptr);
+                if (e != cudaSuccess) return cuda_fail(e, "wavefront kernels");
+                scene->launches += (uint64_t)levels + 8;
+                if (timed) {
+                    ch.n = 5;
+                    const int cls[4] = {MLGPU_KERNEL_INTAKE, MLGPU_KERNEL_WALK,
+                                        MLGPU_KERNEL_INTERSECT, MLGPU_KERNEL_RESOLVE};
+                    const int launches[4] = {2, levels + 1, 2, 3};
+                    for (int k = 0; k < 4; k++) { ch.cls[k] = cls[k]; ch.launches[k] = launches[k]; }
+                    scene->prof.add(ch);
+                }
             }
+            MLGPU_CUDA(cudaMemcpyAsync(scene->wave_host, w.counters, sizeof(WaveCounters),
+                                       cudaMemcpyDeviceToHost, stream));
         }
-        MLGPU_CUDA(cudaMemcpyAsync(scene->wave_host, w.counters, sizeof(WaveCounters),
-                                   cudaMemcpyDeviceToHost, stream));
         MLGPU_CUDA(cudaStreamSynchronize(stream));
         if (scene->wave_host->active == 0 && scene->wave_host->next_input >= a.num_photons) break;
         if (iteration > bound)
@@ -460,7 +555,7 @@ int launch(mlgpu_scene* scene, const TraceArgs& a, const mlgpu_settings* st,
     switch (st->tracer) {
     case MLGPU_TRACER_FP64:
     case MLGPU_TRACER_FP32:
-    case MLGPU_TRACER_FP32_PURE: return run_wavefront(scene, a, st->tracer, stream);
+    case MLGPU_TRACER_FP32_PURE: return run_wavefront(scene, a, st, stream);
     default: {
         Profiler::Chain ch;
         const bool timed = scene->prof.on && scene->prof.take(2, ch.ev);
@@ -539,8 +634,12 @@ int mlgpu_scene_destroy(mlgpu_scene* scene) {
     scene->staging_hist.release();
     scene->staging_rng.release();
     scene->bin_scratch.release();
+    scene->tune_out.release();
+    scene->order.release();
     scene->wave.release();
     if (scene->wave_host) cudaFreeHost(scene->wave_host);
+    if (scene->wave_graph) cudaGraphExecDestroy(scene->wave_graph);
+    if (scene->capture_stream) cudaStreamDestroy(scene->capture_stream);
     scene->prof.release();
     delete scene;
     return MLGPU_OK;
@@ -554,6 +653,95 @@ int mlgpu_propagate(mlgpu_scene* scene, const mlgpu_photons* photons, uint64_t n
     if (num_photons == 0) return MLGPU_OK;
     const TraceArgs a = make_args(scene, photons, num_photons, settings, rng, results);
     return launch(scene, a, settings, static_cast<cudaStream_t>(cuda_stream));
+}
+
+int mlgpu_scene_autotune(mlgpu_scene* scene, const mlgpu_photons* sample, uint64_t n,
+                         const mlgpu_settings* base, const mlgpu_rng* rng,
+                         mlgpu_settings* best, double* best_ms, void* cuda_stream) {
+    if (!best) return fail(MLGPU_ERR_INVALID_ARGUMENT, "NULL argument");
+    mlgpu_results res;
+    std::memset(&res, 0, sizeof(res));
+    res.dtype = MLGPU_F64;
+    res.sensor = reinterpret_cast<int32_t*>(1);   // checked below against NULL only
+    int st = check_propagate_args(scene, sample, base, rng, &res);
+    if (st) return st;
+    if (n == 0) return fail(MLGPU_ERR_INVALID_ARGUMENT, "empty sample");
+    if (base->tracer == MLGPU_TRACER_FP64_PLAIN)
+        return fail(MLGPU_ERR_INVALID_ARGUMENT, "only the wavefront tracers have knobs to tune");
+    MLGPU_CUDA(scene->tune_out.reserve(4*n));
+    res.sensor = static_cast<int32_t*>(scene->tune_out.ptr);
+    const cudaStream_t stream = static_cast<cudaStream_t>(cuda_stream);
+    const bool prof = scene->prof.on;
+    scene->prof.on = false;
+    cudaEvent_t ev[2] = {nullptr, nullptr};
+    MLGPU_CUDA(cudaEventCreate(&ev[0]));
+    MLGPU_CUDA(cudaEventCreate(&ev[1]));
+    // times one setting: best of two runs after an untimed one
+    auto time_of = [&](const mlgpu_settings& cand, double* ms) -> int {
+        const TraceArgs a = make_args(scene, sample, n, &cand, rng, &res);
+        double t_best = 1e300;
+        for (int rep = 0; rep < 3; rep++) {
+            if (cudaEventRecord(ev[0], stream) != cudaSuccess) return cuda_fail(cudaGetLastError(), "event");
+            const int r = launch(scene, a, &cand, stream);
+            if (r) return r;
+            if (cudaEventRecord(ev[1], stream) != cudaSuccess) return cuda_fail(cudaGetLastError(), "event");
+            const cudaError_t e = cudaEventSynchronize(ev[1]);
+            if (e != cudaSuccess) return cuda_fail(e, "autotune run");
+            float t = 0.0f;
+            cudaEventElapsedTime(&t, ev[0], ev[1]);
+            if (rep > 0) t_best = std::min(t_best, (double)t);
+        }
+        *ms = t_best;
+        return MLGPU_OK;
+    };
+    int sms = 0, dev = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    mlgpu_settings cur = *base;
+    cur.pool_size = 0; cur.check_period = 0; cur.use_graph = 1; cur.grid_blocks = 0;
+    cur.staged_levels = 0;
+    cur.photon_order = MLGPU_ORDER_DEFAULT;
+    double cur_ms = 0.0;
+    st = time_of(cur, &cur_ms);
+    // candidate values of each knob, tried one knob at a time
+    const uint32_t pools[] = {1u << 19, 1u << 20, 1u << 21, 1u << 22};
+    const int periods[] = {2, 4, 8, 16};
+    const int grids[] = {4*sms, 8*sms, 16*sms};
+    const int stages[] = {0, 3, 5};
+    const int graphs[] = {0, 1};
+    const int orders[] = {MLGPU_ORDER_INPUT, MLGPU_ORDER_COHERENT};
+    for (int pass = 0; pass < 2 && st == MLGPU_OK; pass++) {
+        const double start_ms = cur_ms;
+        for (int knob = 0; knob < 6 && st == MLGPU_OK; knob++) {
+            const int count = knob <= 1 ? 4 : knob <= 3 ? 3 : 2;
+            for (int c = 0; c < count && st == MLGPU_OK; c++) {
+                mlgpu_settings cand = cur;
+                switch (knob) {
+                case 0:
+                    if (pools[c] > 2*n && c > 0) continue;   // larger than the sample
+                    cand.pool_size = pools[c];
+                    break;
+                case 1: cand.check_period = periods[c]; break;
+                case 2: cand.grid_blocks = grids[c]; break;
+                case 3: cand.staged_levels = stages[c]; break;
+                case 4: cand.use_graph = graphs[c]; break;
+                default: cand.photon_order = orders[c]; break;
+                }
+                if (std::memcmp(&cand, &cur, sizeof(cand)) == 0) continue;
+                double ms = 0.0;
+                st = time_of(cand, &ms);
+                if (st == MLGPU_OK && ms < cur_ms) { cur = cand; cur_ms = ms; }
+            }
+        }
+        if (cur_ms > 0.98*start_ms) break;   // the pass gained little
+    }
+    cudaEventDestroy(ev[0]);
+    cudaEventDestroy(ev[1]);
+    scene->prof.on = prof;
+    if (st) return st;
+    *best = cur;
+    if (best_ms) *best_ms = cur_ms;
+    return MLGPU_OK;
 }
 
 int mlgpu_scene_sync_errors(mlgpu_scene* scene, void* cuda_stream) {

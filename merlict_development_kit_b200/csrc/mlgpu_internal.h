@@ -56,6 +56,7 @@ static_assert(sizeof(BvhNode4) == 128, "BvhNode4 must be 128 bytes");
 constexpr int32_t kBvhLeafFlag = (int32_t)0x80000000u;
 constexpr int32_t kBvhEmpty = 0x7fffffff;
 constexpr int kBvhStack = 48;
+constexpr int kMaxBvhLevels = 48;
 
 struct DevScene {
     const double4* node;        // x, y, z, radius^2
@@ -81,6 +82,7 @@ struct DevScene {
     int32_t bvh_nodes;
     int32_t bvh_levels;         // node levels of the BVH (nodes of level k are visited by pass k)
     float bvh_eps;              // box inflation per ray: bvh_eps + 4e-7 |origin|_1
+    int32_t bvh_level_start[kMaxBvhLevels + 1];   // nodes of level k: [start[k], start[k+1])
 };
 
 struct DevPhotons {
@@ -120,17 +122,18 @@ struct TraceArgs {
     uint32_t max_interactions;
     int32_t start_node;
     int32_t traversal;          // MLGPU_TRAVERSAL_*
+    const uint32_t* order;      // wavefront intake order of the photons, or null (input order)
 };
 
 struct BvhHost {
-    std::vector<BvhNode4> nodes;
+    std::vector<BvhNode4> nodes;         // breadth first: each level is an index range
     std::vector<int32_t> leaf_ids;
+    std::vector<int32_t> level_start;    // levels + 1 entries
     int levels = 0;              // depth of the 4-wide tree (root alone: 1)
 };
 void build_bvh4(const mlgpu_flat_scene* f, double inflate, BvhHost* out);
 
 // wavefront tracers: a pool of ray slots, two of them (current, next)
-constexpr int kMaxBvhLevels = 48;
 struct WaveCounters {
     unsigned long long next_input;   // photons taken into the pool so far
     unsigned int active;             // rays carried over into the current pool
@@ -158,6 +161,7 @@ struct WaveBuffers {
     WaveCounters* counters;
     uint32_t pool;
     int grid;                // blocks of the persistent (grid-stride) kernels
+    int staged_levels;       // BVH levels whose nodes each block stages in shared memory
     int fn_smem_bytes;       // property tables staged in shared memory (0: read from global)
     int32_t* step;           // [pool] 0, or kNoStep: the photon takes no step
     float4* ray_o;           // [pool] single-precision origin, box inflation
@@ -189,6 +193,11 @@ cudaError_t launch_wave32_isect_resolve(const TraceArgs& a, const WaveBuffers& w
                                         cudaStream_t s, cudaEvent_t mid);
 
 cudaError_t launch_trace_fp64(const TraceArgs& a, int block, cudaStream_t s);
+// A coherent tracing order of a photon batch (photon_order.cu): `order`
+// receives n photon indices; `scratch` holds photon_order_scratch_bytes(n).
+size_t photon_order_scratch_bytes(uint64_t n);
+cudaError_t launch_photon_order(const DevPhotons& p, int in_dtype, uint64_t n, uint32_t* order,
+                                void* scratch, int grid, cudaStream_t s);
 int wave_persistent_blocks();
 cudaError_t launch_bin_arrivals(const DevScene& sc, const int32_t* sensor,
                                 const double* time, uint64_t n, uint32_t* counts,

@@ -24,6 +24,7 @@ namespace mlgpu {
 namespace {
 
 constexpr int kTreeCands = 16;   // candidates of a frame-tree walk before it overflows
+constexpr int kMaxStagedNodes = 256;   // 32 KB of shared memory per block
 
 template <typename In>
 __global__ void __launch_bounds__(256)
@@ -48,7 +49,8 @@ wave_intake_kernel(const TraceArgs a, const WaveBuffers w, const RayPool cur) {
         if (slot >= active) {
             // a new photon: merlict::Photon's constructor (Ray.cpp:16-20,
             // RayForPropagation.cpp:52-64)
-            const uint64_t p = next_input + (slot - active);
+            const uint64_t q = next_input + (slot - active);
+            const uint64_t p = a.order ? (uint64_t)__ldg(a.order + q) : q;
             s = mk(load_in<In>(a.photons.sx, p), load_in<In>(a.photons.sy, p),
                    load_in<In>(a.photons.sz, p));
             d = normalized(mk(load_in<In>(a.photons.dx, p), load_in<In>(a.photons.dy, p),
@@ -137,9 +139,13 @@ wave_intake_kernel(const TraceArgs a, const WaveBuffers w, const RayPool cur) {
 }
 
 // One BVH level: the four child boxes of each queued (ray, node) pair, slab
-// tests in single precision on boxes widened by the ray's rounding.
+// tests in single precision on boxes widened by the ray's rounding.  With
+// `staged` > 0 the block first copies the level's `staged` nodes (a
+// contiguous range, the tree being numbered breadth first) into shared
+// memory and reads them from there.
 __global__ void __launch_bounds__(256)
-wave_level_kernel(const TraceArgs a, const WaveBuffers w, int level) {
+wave_level_kernel(const TraceArgs a, const WaveBuffers w, int level, int staged) {
+    extern __shared__ float4 stage[];
     const DevScene& sc = a.scene;
     const uint2* in = w.level_q[level & 1];
     uint2* out = w.level_q[(level + 1) & 1];
@@ -147,6 +153,12 @@ wave_level_kernel(const TraceArgs a, const WaveBuffers w, int level) {
     const uint32_t n = len < w.level_cap ? len : w.level_cap;
     const bool last = level + 1 >= kMaxBvhLevels;
     const int lane = threadIdx.x & 31;
+    const int32_t base = sc.bvh_level_start[level];
+    if (staged > 0) {
+        const float4* src = reinterpret_cast<const float4*>(sc.bvh + base);
+        for (int k = threadIdx.x; k < staged*8; k += blockDim.x) stage[k] = __ldg(src + k);
+        __syncthreads();
+    }
     for (uint32_t first = warp_first(); first < n; first += gridDim.x*blockDim.x) {
         const uint32_t e = first + (uint32_t)lane;
         uint32_t slot = 0;
@@ -156,10 +168,20 @@ wave_level_kernel(const TraceArgs a, const WaveBuffers w, int level) {
             const uint2 q = in[e];
             slot = q.x;
             const float4 o = w.ray_o[slot], iv = w.ray_i[slot];
-            const float4* nq = reinterpret_cast<const float4*>(sc.bvh + q.y);
-            const float4 lx = __ldg(nq), ly = __ldg(nq + 1), lz = __ldg(nq + 2);
-            const float4 hx = __ldg(nq + 3), hy = __ldg(nq + 4), hz = __ldg(nq + 5);
-            const int4 ch = __ldg(reinterpret_cast<const int4*>(nq + 6));
+            float4 lx, ly, lz, hx, hy, hz;
+            int4 ch;
+            if ((uint32_t)((int32_t)q.y - base) < (uint32_t)staged) {
+                const float4* nq = stage + 8*((int32_t)q.y - base);
+                lx = nq[0]; ly = nq[1]; lz = nq[2]; hx = nq[3]; hy = nq[4]; hz = nq[5];
+                const float4 c = nq[6];
+                ch = make_int4(__float_as_int(c.x), __float_as_int(c.y), __float_as_int(c.z),
+                               __float_as_int(c.w));
+            } else {
+                const float4* nq = reinterpret_cast<const float4*>(sc.bvh + q.y);
+                lx = __ldg(nq); ly = __ldg(nq + 1); lz = __ldg(nq + 2);
+                hx = __ldg(nq + 3); hy = __ldg(nq + 4); hz = __ldg(nq + 5);
+                ch = __ldg(reinterpret_cast<const int4*>(nq + 6));
+            }
             const float lox[4] = {lx.x, lx.y, lx.z, lx.w}, loy[4] = {ly.x, ly.y, ly.z, ly.w};
             const float loz[4] = {lz.x, lz.y, lz.z, lz.w}, hix[4] = {hx.x, hx.y, hx.z, hx.w};
             const float hiy[4] = {hy.x, hy.y, hy.z, hy.w}, hiz[4] = {hz.x, hz.y, hz.z, hz.w};
@@ -265,8 +287,11 @@ cudaError_t launch_wave_iteration(const TraceArgs& a, const WaveBuffers& w, cons
         wave_intake_kernel<float><<<slot_blocks, 256, 0, s>>>(a, w, cur);
     wave_after_intake_kernel<<<1, 1, 0, s>>>(w.counters, w.pool, a.num_photons);
     if (ev) cudaEventRecord(ev[1], s);
-    for (int k = 0; k < a.scene.bvh_levels; k++)
-        wave_level_kernel<<<w.grid, 256, 0, s>>>(a, w, k);
+    for (int k = 0; k < a.scene.bvh_levels; k++) {
+        const int count = a.scene.bvh_level_start[k + 1] - a.scene.bvh_level_start[k];
+        const int staged = k < w.staged_levels && count <= kMaxStagedNodes ? count : 0;
+        wave_level_kernel<<<w.grid, 256, (size_t)staged*sizeof(BvhNode4), s>>>(a, w, k, staged);
+    }
     wave_sphere_kernel<<<w.grid, 256, 0, s>>>(a, w, cur);
     if (ev) cudaEventRecord(ev[2], s);
     if (form == MLGPU_TRACER_FP64) {

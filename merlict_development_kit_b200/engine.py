@@ -89,6 +89,29 @@ def photons_to_device(batch: dict, dtype=torch.float64) -> dict:
     return out
 
 
+def _settings(config: PropagationConfig, start_node: int, tracer: str, traversal: str,
+              tuning: dict | None) -> abi.mlgpu_settings:
+    st = abi.mlgpu_settings(int(config.max_num_interactions_per_photon), int(start_node),
+                            TRACERS[tracer], 0, TRAVERSALS[traversal])
+    for k, v in (tuning or {}).items():
+        if k not in abi.mlgpu_settings.TUNING:
+            raise ValueError(f"unknown tuning knob {k!r}")
+        setattr(st, k, int(v))
+    return st
+
+
+def _photon_struct(photons: dict, n: int) -> abi.mlgpu_photons:
+    in_dtype = photons["wavelength"].dtype
+    ph = abi.mlgpu_photons()
+    ph.dtype = abi.F64 if in_dtype == torch.float64 else abi.F32
+    for k in PLANES:
+        t = photons[k]
+        if t.dtype != in_dtype or not t.is_cuda or not t.is_contiguous() or t.shape[0] != n:
+            raise ValueError(f"photon plane {k} must be a contiguous CUDA tensor of {in_dtype}")
+        setattr(ph, k, t.data_ptr())
+    return ph
+
+
 class Scene:
     """A flattened frame tree resident on the current CUDA device."""
 
@@ -123,25 +146,22 @@ class Scene:
                   rng=None, tracer: str = "fp64", start_node: int = 0,
                   outputs=("sensor", "x", "y", "time"), history: bool = False,
                   out_dtype=torch.float64, stream=None, sync: bool = True,
-                  results: dict | None = None, traversal: str = "bvh") -> dict:
+                  results: dict | None = None, traversal: str = "bvh",
+                  tuning: dict | None = None) -> dict:
         """Traces a batch of device-resident photons.
 
         `photons` is a dict of CUDA tensors (see photons.PLANES).  Returns a
         dict of CUDA tensors with the requested outputs.  With sync=True the
         call waits and raises on device-side errors (a wavelength outside a
         property table raises IndexError, like merlict's std::out_of_range).
+        `tuning` sets the wavefront knobs of mlgpu_settings (pool_size,
+        check_period, use_graph, grid_blocks, staged_levels), e.g. the dict
+        `autotune` returns; they never change the results.
         """
         config = config or PropagationConfig()
         rng = rng if rng is not None else Philox(0)
         n = int(photons["wavelength"].shape[0])
-        in_dtype = photons["wavelength"].dtype
-        ph = abi.mlgpu_photons()
-        ph.dtype = abi.F64 if in_dtype == torch.float64 else abi.F32
-        for k in PLANES:
-            t = photons[k]
-            if t.dtype != in_dtype or not t.is_cuda or not t.is_contiguous() or t.shape[0] != n:
-                raise ValueError(f"photon plane {k} must be a contiguous CUDA tensor of {in_dtype}")
-            setattr(ph, k, t.data_ptr())
+        ph = _photon_struct(photons, n)
         dev = photons["wavelength"].device
         res = abi.mlgpu_results()
         res.dtype = abi.F64 if out_dtype == torch.float64 else abi.F32
@@ -163,8 +183,7 @@ class Scene:
             m = config.max_num_interactions_per_photon + 1
             out["history"] = torch.empty((n, m, abi.HISTORY_DTYPE.itemsize), dtype=torch.uint8, device=dev)
             res.history = out["history"].data_ptr()
-        st = abi.mlgpu_settings(int(config.max_num_interactions_per_photon), int(start_node),
-                                TRACERS[tracer], 0, TRAVERSALS[traversal])
+        st = _settings(config, start_node, tracer, traversal, tuning)
         r, keep = rng._struct(n)
         sh = _stream_handle(stream)
         check(lib().mlgpu_propagate(self._h, C.byref(ph), n, C.byref(st), C.byref(r),
@@ -174,6 +193,25 @@ class Scene:
             check(lib().mlgpu_scene_sync_errors(self._h, C.c_void_p(sh)))
         del keep
         return out
+
+    def autotune(self, photons: dict, config: PropagationConfig | None = None,
+                 rng=None, tracer: str = "fp64", stream=None) -> tuple[dict, float]:
+        """Picks the wavefront knobs for this scene by timing propagations
+        of the sample `photons` (mlgpu_scene_autotune); returns the tuning
+        dict for `propagate` and the sample's best time in ms."""
+        config = config or PropagationConfig()
+        rng = rng if rng is not None else Philox(0)
+        n = int(photons["wavelength"].shape[0])
+        ph = _photon_struct(photons, n)
+        base = _settings(config, 0, tracer, "bvh", None)
+        best = abi.mlgpu_settings()
+        ms = C.c_double(0.0)
+        r, keep = rng._struct(n)
+        check(lib().mlgpu_scene_autotune(self._h, C.byref(ph), n, C.byref(base), C.byref(r),
+                                         C.byref(best), C.byref(ms),
+                                         C.c_void_p(_stream_handle(stream))))
+        del keep
+        return best.tuning(), float(ms.value)
 
     def kernel_launches(self) -> int:
         """Kernels this scene has launched so far."""

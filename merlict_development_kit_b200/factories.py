@@ -274,6 +274,34 @@ def reflector_camera(focal_length=4.9, davies_cotton=1.0, max_aperture_radius=2.
     return sc.init()
 
 
+def large_reflector_camera(focal_length=106.5, aperture_radius=35.5, davies_cotton=0.0,
+                           facet_inner_hex_radius=0.45, gap=0.01, fov_deg=6.5,
+                           pixel_fov_deg=0.06667, reflectivity=0.9) -> Scenery:
+    """A large parabolic segmented reflector (hexagonal spherical-cap facets
+    of curvature radius 2f = 213 m) with a flat camera of hexagonal pixels
+    in its focal plane.  The pixel grid is the one merlict_portal_plenoscope
+    lays out for its lens array (light_field_sensor/Geometry.cpp:13-77):
+    spacing 2 f tan(pixel_fov/2) out to f tan(fov/2) -- 8,443 pixels for
+    the default 0.06667 degree pixels and 6.5 degree field of view.  With
+    0.9 m facets the reflector layout yields 5,388 facets on the 35.5 m
+    aperture."""
+    sc = Scenery()
+    reflector = sc.root.add(SurfaceEntity("reflector", (0.0, 0.0, 0.0), ROT3_UNITY))
+    reflector.outer_reflection = constant(reflectivity)
+    segmented_reflector(reflector, ReflectorConfig(
+        focal_length, davies_cotton, aperture_radius, 0.0, facet_inner_hex_radius, gap))
+    inner = focal_length * math.tan(deg2rad(pixel_fov_deg) / 2.0)
+    outer = inner * 2.0 / math.sqrt(3.0)
+    max_radius = focal_length * math.tan(deg2rad(fov_deg) / 2.0)
+    cells = hex_grid_annulus(max_radius - outer, 0.0, 2.0 * inner)
+    cam = sc.root.add(Frame("camera", (0.0, 0.0, focal_length), ROT3_UNITY))
+    for i, pos in enumerate(cells):
+        pix = cam.add(HexPlane(f"pixel_{i}", pos, ROT3_UNITY))
+        pix.set_outer_hex_radius(outer)
+        sc.add_sensor(i, pix)
+    return sc.init()
+
+
 def light_field_telescope(focal_length=10.7, aperture_radius=5.35, fov_deg=6.5,
                           pixel_fov_deg=0.186, paxels_on_diagonal=9, housing_overhead=1.1,
                           reflectivity=0.9, davies_cotton=1.0, facet_inner_hex_radius=0.3,

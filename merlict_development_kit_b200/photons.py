@@ -82,3 +82,116 @@ def isotropic_shell_source(n: int, seed: int, radius: float, aim_radius: float,
     d = aim - sup
     lam = lambda_min + (lambda_max - lambda_min) * rng.random(n)
     return make_batch(sup, d, lam)
+
+
+SPEED_OF_LIGHT = 299792458.0             # merlict/PhysicalConstants.h:7
+PRODUCTION_DISTANCE_OFFSET = 1e3         # merlict_corsika/PhotonFactory.cpp:51-57
+
+
+def cherenkov_event_sizes(num_events: int, seed: int, min_photons: int = 100,
+                          max_photons: int = 10**6) -> np.ndarray:
+    """Photons per event, log-uniform in [min_photons, max_photons]."""
+    rng = np.random.default_rng(seed)
+    lo, hi = np.log(float(min_photons)), np.log(float(max_photons))
+    return np.rint(np.exp(lo + (hi - lo) * rng.random(num_events))).astype(np.int64)
+
+
+def cherenkov_events(sizes, seed: int, device="cpu", dtype=None, core_radius: float = 150.0,
+                     clip_radius: float = 40.0, max_axis_zenith_deg: float = 3.0,
+                     cone_deg: float = 1.0, cone_spread_deg: float = 0.2,
+                     time_sigma: float = 5e-9, lambda_min: float = 300e-9,
+                     lambda_max: float = 700e-9, chunk: int = 1 << 25):
+    """Air-shower-like photon events, concatenated, as torch planes on
+    `device` (returns (batch, offsets); event e is photons
+    [offsets[e], offsets[e + 1])).
+
+    Per event: a shower axis uniform in solid angle within
+    `max_axis_zenith_deg` of the zenith, a core uniform within `core_radius`
+    of the telescope and a Cherenkov angle uniform in cone_deg +-
+    cone_spread_deg.  Per photon: a ground point uniform within
+    `clip_radius` of the telescope, a direction on the event's cone about
+    its axis at the azimuth of the ground point seen from the core, an
+    arrival time ~ N(0, time_sigma) and a wavelength from the 1/lambda^2
+    Cherenkov spectrum.  The support is placed like merlict's CORSIKA
+    photon factory places it (merlict_corsika/PhotonFactory.cpp:31-62): up
+    the ray from the ground point by c*t plus a 1 km offset, so that the
+    arrival time is part of the time of flight.
+    """
+    import torch
+    dtype = dtype or torch.float64
+    sizes = np.asarray(sizes, dtype=np.int64)
+    offsets = np.zeros(len(sizes) + 1, dtype=np.int64)
+    np.cumsum(sizes, out=offsets[1:])
+    total = int(offsets[-1])
+    rng = np.random.default_rng(seed)
+    e = len(sizes)
+    cos_max = np.cos(np.deg2rad(max_axis_zenith_deg))
+    cz = 1.0 - rng.random(e) * (1.0 - cos_max)
+    sz = np.sqrt(np.maximum(0.0, 1.0 - cz * cz))
+    pa = 2.0 * np.pi * rng.random(e)
+    axis = np.stack([sz * np.cos(pa), sz * np.sin(pa), -cz], axis=1)
+    rc = core_radius * np.sqrt(rng.random(e))
+    pc = 2.0 * np.pi * rng.random(e)
+    core = np.stack([rc * np.cos(pc), rc * np.sin(pc)], axis=1)
+    cone = np.deg2rad(cone_deg + cone_spread_deg * (2.0 * rng.random(e) - 1.0))
+    # orthonormal basis (e1, e2) perpendicular to each axis
+    ref = np.where(np.abs(axis[:, 2:3]) < 0.9, [[0.0, 0.0, 1.0]], [[1.0, 0.0, 0.0]])
+    e1 = np.cross(axis, ref)
+    e1 /= np.linalg.norm(e1, axis=1)[:, None]
+    e2 = np.cross(axis, e1)
+    out = {k: torch.empty(total, dtype=dtype, device=device) for k in PLANES}
+    gen = torch.Generator(device=device)
+    gen.manual_seed(int(seed) & 0x7FFFFFFFFFFFFFFF)
+    ev_of = torch.repeat_interleave(torch.arange(e, device=device),
+                                    torch.as_tensor(sizes, device=device))
+    t_axis = torch.as_tensor(axis, device=device)
+    t_core = torch.as_tensor(core, device=device)
+    t_cone = torch.as_tensor(cone, device=device)
+    t_e1 = torch.as_tensor(e1, device=device)
+    t_e2 = torch.as_tensor(e2, device=device)
+    inv_lo, inv_hi = 1.0 / lambda_min, 1.0 / lambda_max
+    f64 = torch.float64
+    for a in range(0, total, chunk):
+        b = min(total, a + chunk)
+        m = b - a
+        ev = ev_of[a:b]
+        u = torch.rand((5, m), generator=gen, device=device, dtype=f64)
+        r = clip_radius * torch.sqrt(u[0])
+        phi = 2.0 * np.pi * u[1]
+        gx, gy = r * torch.cos(phi), r * torch.sin(phi)
+        psi = torch.atan2(gy - t_core[ev, 1], gx - t_core[ev, 0])
+        ca, sa = torch.cos(t_cone[ev]), torch.sin(t_cone[ev])
+        rad = (torch.cos(psi)[:, None] * t_e1[ev] + torch.sin(psi)[:, None] * t_e2[ev])
+        d = ca[:, None] * t_axis[ev] + sa[:, None] * rad
+        d = d / torch.linalg.norm(d, dim=1, keepdim=True)
+        t = time_sigma * torch.randn(m, generator=gen, device=device, dtype=f64)
+        back = t * SPEED_OF_LIGHT + PRODUCTION_DISTANCE_OFFSET
+        lam = 1.0 / (inv_lo - u[2] * (inv_lo - inv_hi))
+        planes = (gx - d[:, 0] * back, gy - d[:, 1] * back, -d[:, 2] * back,
+                  d[:, 0], d[:, 1], d[:, 2], lam)
+        for k, v in zip(PLANES, planes):
+            out[k][a:b] = v.to(dtype)
+        del u, r, phi, gx, gy, psi, ca, sa, rad, d, t, back, lam, planes
+    return out, offsets
+
+
+def downward_disc_source_device(n: int, seed: int, disc_radius: float, height: float,
+                                max_zenith_deg: float, device="cuda", lambda_min: float = 300e-9,
+                                lambda_max: float = 700e-9, dtype=None) -> dict:
+    """downward_disc_source's law, drawn with torch on `device` (for batches
+    too large to make on the host)."""
+    import torch
+    dtype = dtype or torch.float64
+    g = torch.Generator(device=device)
+    g.manual_seed(int(seed) & 0x7FFFFFFFFFFFFFFF)
+    u = torch.rand((5, n), generator=g, device=device, dtype=torch.float64)
+    r = disc_radius * torch.sqrt(u[0])
+    phi = 2.0 * np.pi * u[1]
+    cos_max = float(np.cos(np.deg2rad(max_zenith_deg)))
+    cos_t = 1.0 - u[2] * (1.0 - cos_max)
+    sin_t = torch.sqrt(torch.clamp(1.0 - cos_t * cos_t, min=0.0))
+    az = 2.0 * np.pi * u[3]
+    planes = (r * torch.cos(phi), r * torch.sin(phi), torch.full_like(r, float(height)),
+              sin_t * torch.cos(az), sin_t * torch.sin(az), -cos_t,
+              lambda_min + (lambda_max - lambda_min) * u[4])
+    return {k: v.to(dtype).contiguous() for k, v in zip(PLANES, planes)}
