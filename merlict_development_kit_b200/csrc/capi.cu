@@ -223,7 +223,8 @@ int build_device_scene(mlgpu_scene* s, const mlgpu_flat_scene* f) {
     }
     std::vector<LeafRec> leaf(nl > 0 ? nl : 1);
     std::vector<LeafRecF> leaf_f(nl > 0 ? nl : 1);
-    std::vector<double> origin(3*(size_t)(nl > 0 ? nl : 1), 0.0);
+    std::vector<LeafAnchor> anchor(nl > 0 ? nl : 1);
+    std::memset(anchor.data(), 0, anchor.size()*sizeof(LeafAnchor));
     std::memset(leaf.data(), 0, leaf.size()*sizeof(LeafRec));
     std::memset(leaf_f.data(), 0, leaf_f.size()*sizeof(LeafRecF));
     for (int32_t l = 0; l < nl; l++) {
@@ -254,9 +255,17 @@ int build_device_scene(mlgpu_scene* s, const mlgpu_flat_scene* f) {
         F.allowed_node = L.allowed_node;
         F.flags = L.flags;
         for (int k = 0; k < 6; k++) F.fn[k] = L.fn[k];
-        origin[3*(size_t)l] = t[3];
-        origin[3*(size_t)l + 1] = t[7];
-        origin[3*(size_t)l + 2] = t[11];
+        LeafAnchor& A = anchor[l];
+        A.origin[0] = t[3]; A.origin[1] = t[7]; A.origin[2] = t[11];
+        if (L.primitive == MLGPU_PRIM_SPHERE_CAP_HEX || L.primitive == MLGPU_PRIM_SPHERE_CAP_CYL ||
+            L.primitive == MLGPU_PRIM_SPHERE_CAP_RECT) {
+            // the cap's sphere: centre (0, 0, R) in the leaf frame
+            const double R = L.params[0];
+            A.R = R;
+            A.center[0] = t[3] + R*t[2];
+            A.center[1] = t[7] + R*t[6];
+            A.center[2] = t[11] + R*t[10];
+        }
     }
     const int32_t npts = f->function_offset[nf];
     s->dev.num_fn_points = npts;
@@ -268,7 +277,7 @@ int build_device_scene(mlgpu_scene* s, const mlgpu_flat_scene* f) {
     if ((st = upload(s, f->function_points, 3*(size_t)npts, &s->dev.fn_points))) return st;
     if ((st = upload(s, f->function_offset, (size_t)nf + 1, &s->dev.fn_offset))) return st;
     if ((st = upload(s, leaf_f.data(), leaf_f.size(), &s->dev.leaf_f))) return st;
-    if ((st = upload(s, origin.data(), origin.size(), &s->dev.leaf_origin))) return st;
+    if ((st = upload(s, anchor.data(), anchor.size(), &s->dev.leaf_anchor))) return st;
     {
         // BVH over the leaves; boxes widened for single-precision slab tests
         const double* root = f->node_sphere;
@@ -283,6 +292,13 @@ int build_device_scene(mlgpu_scene* s, const mlgpu_flat_scene* f) {
             std::vector<double4> sph(bvh.leaf_ids.size());
             for (size_t j = 0; j < sph.size(); j++) sph[j] = node[f->leaf_node[bvh.leaf_ids[j]]];
             if ((st = upload(s, sph.data(), sph.size(), &s->dev.bvh_sphere))) return st;
+            std::vector<float4> sph_f(sph.size());
+            for (size_t j = 0; j < sph.size(); j++) {
+                float r = (float)std::sqrt(sph[j].w);
+                if ((double)r*(double)r < sph[j].w) r = std::nextafter(r, 3.0e38f);
+                sph_f[j] = make_float4((float)sph[j].x, (float)sph[j].y, (float)sph[j].z, r);
+            }
+            if ((st = upload(s, sph_f.data(), sph_f.size(), &s->dev.bvh_sphere_f))) return st;
             s->dev.bvh_nodes = (int32_t)bvh.nodes.size();
             s->dev.bvh_levels = bvh.levels;
             for (int k = 0; k <= kMaxBvhLevels; k++)

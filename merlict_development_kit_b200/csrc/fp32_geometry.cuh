@@ -98,15 +98,23 @@ __device__ __forceinline__ double newton64(double a, double b, double c, double 
 // causal solutions only, the self-intersection guard (a distance of more
 // than 1e-7 m), strict bounds as in the reference.  `pure` selects the
 // textbook single-precision form throughout (no rebasing, textbook roots,
-// FP32 normals).
+// FP32 normals).  Without kNeedHit only the distance is wanted (the
+// candidate pass): the Newton step of a spherical cap is then taken on the
+// cap's sphere in world coordinates (the leaf's FP64 anchor), which needs
+// none of the FP64 transform; with kNeedHit (the closest candidate's full
+// hit) it is taken in the leaf frame of the FP64 transform, and the hit
+// point and normal follow in FP64.
+template <bool kNeedHit>
 __device__ Hit32 intersect32(const DevScene& sc, int32_t leaf, d3 s, d3 d, bool pure) {
     Hit32 h;
     h.leaf = -1;
     const LeafRecF* L = sc.leaf_f + leaf;
     const int32_t prim = __ldg(&L->primitive);
     if (prim == MLGPU_PRIM_NONE) return h;
-    const double* o = sc.leaf_origin + 3*(size_t)leaf;
-    const d3 c = dmk(__ldg(o), __ldg(o + 1), __ldg(o + 2));
+    const LeafAnchor* A = sc.leaf_anchor + leaf;
+    const double2 o01 = __ldg(reinterpret_cast<const double2*>(A) + 0);   // origin x, y
+    const double2 o2R = __ldg(reinterpret_cast<const double2*>(A) + 1);   // origin z, R
+    const d3 c = dmk(o01.x, o01.y, o2R.x);
     float R[9];
 #pragma unroll
     for (int k = 0; k < 9; k++) R[k] = __ldg(&L->R[k]);
@@ -190,7 +198,23 @@ __device__ Hit32 intersect32(const DevScene& sc, int32_t leaf, d3 s, d3 d, bool 
         if (!roots32(a, b, cc, !pure, &f1, &f2)) return h;
         double t1 = f1, t2 = f2;
         d3 s64 = dwiden(sl), d64 = dwiden(dl);
-        if (!pure) {
+        if (!pure && !kNeedHit && !ell) {
+            // one Newton step each on |m + t d|^2 - R^2, m = rebased support
+            // - sphere centre, in FP64 world coordinates
+            const double2 c01 = __ldg(reinterpret_cast<const double2*>(A) + 2);   // centre x, y
+            const double2 c2p = __ldg(reinterpret_cast<const double2*>(A) + 3);   // centre z, pad
+            const d3 m = dmk(s.x + d.x*t0 - c01.x, s.y + d.y*t0 - c01.y, s.z + d.z*t0 - c2p.x);
+            const double R = o2R.y;
+#pragma unroll
+            for (int k = 0; k < 2; k++) {
+                const double t = k == 0 ? t1 : t2;
+                const d3 v = dmk(m.x + d.x*t, m.y + d.y*t, m.z + d.z*t);
+                const double f = (v.x*v.x + v.y*v.y + v.z*v.z) - R*R;
+                const double df = 2.0*(v.x*d.x + v.y*d.y + v.z*d.z);
+                const double tn = df != 0.0 ? t - f/df : t;
+                if (k == 0) t1 = tn; else t2 = tn;
+            }
+        } else if (!pure) {
             // one Newton step each on the quadratic in FP64, in the leaf frame
             // of the FP64 transform
             const double* T = sc.leaf[leaf].T;
@@ -230,7 +254,9 @@ __device__ Hit32 intersect32(const DevScene& sc, int32_t leaf, d3 s, d3 d, bool 
         for (int k = 0; k < 2; k++) {
             const double tl = k == 0 ? lo : hi;
             if (ok || !(t0 + tl > v_min)) continue;
-            const f3 p = fmk((float)(s64.x + d64.x*tl), (float)(s64.y + d64.y*tl), (float)(s64.z + d64.z*tl));
+            const f3 p = (!pure && !kNeedHit && !ell)
+                ? fadd(sl, fscale(dl, (float)tl))
+                : fmk((float)(s64.x + d64.x*tl), (float)(s64.y + d64.y*tl), (float)(s64.z + d64.z*tl));
             bool in;
             switch (prim) {
             case MLGPU_PRIM_SPHERE_CAP_HEX: in = hex_inside32(sc, pr[1], p); break;
@@ -241,6 +267,10 @@ __device__ Hit32 intersect32(const DevScene& sc, int32_t leaf, d3 s, d3 d, bool 
             if (in && fdot(p, p) <= r2) { best = tl; ok = true; }
         }
         if (!ok) return h;
+        if (!kNeedHit) {
+            h.leaf = leaf; h.v = t0 + best;
+            return h;
+        }
         if (pure) {
             const f3 p = fadd(sl, fscale(dl, (float)best));
             f3 n;

@@ -3,6 +3,7 @@
 #ifndef MLGPU_INTERNAL_H_
 #define MLGPU_INTERNAL_H_
 
+#include <cstddef>
 #include <cstdint>
 #include <vector>
 #include <cuda_runtime.h>
@@ -43,6 +44,22 @@ struct __align__(128) LeafRecF {
 };
 static_assert(sizeof(LeafRecF) == 128, "LeafRecF must be 128 bytes");
 
+// FP64 anchor of a leaf for the FP32 forms (64 bytes): the leaf's origin
+// (the FP32 geometry is relative to it) and, for spherical caps, the world
+// centre and radius of the cap's sphere (origin + R * the frame's z axis),
+// on which the FP64 Newton step of a cap root is taken.
+// Laid out for 16-byte loads: (origin x, y), (origin z, R), (centre x, y),
+// (centre z, pad).
+struct __align__(64) LeafAnchor {
+    double origin[3];
+    double R;              // cap curvature radius (0: not a spherical cap)
+    double center[3];
+    double pad;
+};
+static_assert(sizeof(LeafAnchor) == 64, "LeafAnchor must be 64 bytes");
+static_assert(offsetof(LeafAnchor, R) == 24 && offsetof(LeafAnchor, center) == 32,
+              "LeafAnchor fields must sit where the 16-byte loads expect them");
+
 // 4-wide BVH node: child boxes as [axis][child] (float, rounded outwards)
 // and child references: a node index, a leaf range (kBvhLeafFlag | start << 3
 // | count - 1, into DevScene::bvh_leaf) or kBvhEmpty.
@@ -66,7 +83,7 @@ struct DevScene {
     const int32_t* fn_offset;
     // FP32 copies for the batched tracer
     const LeafRecF* leaf_f;
-    const double* leaf_origin;  // [num_leaves][3] translation of each leaf, FP64
+    const LeafAnchor* leaf_anchor;  // [num_leaves] FP64 origin and cap sphere of each leaf
     int32_t num_nodes;
     int32_t num_leaves;
     int32_t num_functions;
@@ -79,6 +96,7 @@ struct DevScene {
     const BvhNode4* bvh;
     const int32_t* bvh_leaf;
     const double4* bvh_sphere;  // per BVH leaf slot: world centre and radius^2 of that leaf
+    const float4* bvh_sphere_f; // the same in FP32: centre (rounded) and radius (rounded up)
     int32_t bvh_nodes;
     int32_t bvh_levels;         // node levels of the BVH (nodes of level k are visited by pass k)
     float bvh_eps;              // box inflation per ray: bvh_eps + 4e-7 |origin|_1

@@ -105,7 +105,7 @@ wave_isect_kernel(const TraceArgs a, const WaveBuffers w, const RayPool cur) {
             const Isec h = leaf_hit(sc, leaf, s, d);
             if (h.leaf >= 0) dist = h.dist;
         } else {
-            const fp32::Hit32 h = fp32::intersect32(sc, leaf, fp32::dmk(s.x, s.y, s.z),
+            const fp32::Hit32 h = fp32::intersect32<false>(sc, leaf, fp32::dmk(s.x, s.y, s.z),
                                                     fp32::dmk(d.x, d.y, d.z),
                                                     kIsect == kIsectFp32Pure);
             if (h.leaf >= 0) dist = h.v;
@@ -213,7 +213,7 @@ wave_resolve_kernel(const TraceArgs a, const WaveBuffers w, const RayPool cur, c
                 } else if (kIsect == kIsectFp64) {
                     is = leaf_hit(sc, best, s, d);
                 } else {
-                    const fp32::Hit32 h = fp32::intersect32(sc, best, fp32::dmk(s.x, s.y, s.z),
+                    const fp32::Hit32 h = fp32::intersect32<true>(sc, best, fp32::dmk(s.x, s.y, s.z),
                                                             fp32::dmk(d.x, d.y, d.z),
                                                             kIsect == kIsectFp32Pure);
                     if (h.leaf < 0) {

@@ -218,8 +218,27 @@ wave_level_kernel(const TraceArgs a, const WaveBuffers w, int level, int staged)
     }
 }
 
+// The FP32 forms' version of merlict's bounding-sphere test: the same
+// geometry in single precision on the walk's FP32 ray, with the radius
+// widened by the rounding of the ray, the centre and the distance along the
+// ray, so that every leaf the exact test passes also passes this one (the
+// extra candidates are then rejected by their intersection, whose hits lie
+// inside the sphere).
+__device__ __forceinline__ bool sphere_cull32(float4 c, float4 o, float3 dv) {
+    const float wx = c.x - o.x, wy = c.y - o.y, wz = c.z - o.z;
+    const float alpha = dv.x*wx + dv.y*wy + dv.z*wz;
+    const float m = o.w + 4e-7f*(fabsf(c.x) + fabsf(c.y) + fabsf(c.z) + fabsf(alpha)) + 1e-6f*c.w;
+    const float rr = (c.w + m)*(c.w + m);
+    const float sx = wx - dv.x*alpha, sy = wy - dv.y*alpha, sz = wz - dv.z*alpha;
+    if (sx*sx + sy*sy + sz*sz > rr) return false;
+    if (alpha < -m) return wx*wx + wy*wy + wz*wz <= rr;
+    return true;
+}
+
 // merlict's bounding-sphere test (RayAndFrame.cpp:16-107) of every leaf in
 // the queued leaf ranges; the leaves that pass become candidates.
+// kF32: the FP32 forms' conservative test (sphere_cull32).
+template <bool kF32>
 __global__ void __launch_bounds__(256)
 wave_sphere_kernel(const TraceArgs a, const WaveBuffers w, const RayPool cur) {
     const DevScene& sc = a.scene;
@@ -237,14 +256,22 @@ wave_sphere_kernel(const TraceArgs a, const WaveBuffers w, const RayPool cur) {
             const int32_t ref = (int32_t)q.y;
             const int32_t start = (ref & 0x7fffffff) >> 3;
             const int32_t count = (ref & 7) + 1;
-            const v3 s = mk(cur.sx[slot], cur.sy[slot], cur.sz[slot]);
-            const v3 d = mk(cur.dx[slot], cur.dy[slot], cur.dz[slot]);
-            const double sd = dot(s, d);
-            for (int32_t j = start; j < start + count; j++) {
-                const double2* c = reinterpret_cast<const double2*>(sc.bvh_sphere + j);
-                const double2 c01 = __ldg(c), c23 = __ldg(c + 1);
-                if (sphere_cull(make_double4(c01.x, c01.y, c23.x, c23.y), s, d, sd))
-                    pass[np++] = __ldg(sc.bvh_leaf + j);
+            if (kF32) {
+                const float4 o = w.ray_o[slot], iv = w.ray_i[slot];
+                const float3 dv = make_float3(1.0f/iv.x, 1.0f/iv.y, 1.0f/iv.z);
+                for (int32_t j = start; j < start + count; j++)
+                    if (sphere_cull32(__ldg(sc.bvh_sphere_f + j), o, dv))
+                        pass[np++] = __ldg(sc.bvh_leaf + j);
+            } else {
+                const v3 s = mk(cur.sx[slot], cur.sy[slot], cur.sz[slot]);
+                const v3 d = mk(cur.dx[slot], cur.dy[slot], cur.dz[slot]);
+                const double sd = dot(s, d);
+                for (int32_t j = start; j < start + count; j++) {
+                    const double2* c = reinterpret_cast<const double2*>(sc.bvh_sphere + j);
+                    const double2 c01 = __ldg(c), c23 = __ldg(c + 1);
+                    if (sphere_cull(make_double4(c01.x, c01.y, c23.x, c23.y), s, d, sd))
+                        pass[np++] = __ldg(sc.bvh_leaf + j);
+                }
             }
         }
         const uint32_t cb = warp_reserve(&w.counters->isect_len, np);
@@ -292,7 +319,8 @@ cudaError_t launch_wave_iteration(const TraceArgs& a, const WaveBuffers& w, cons
         const int staged = k < w.staged_levels && count <= kMaxStagedNodes ? count : 0;
         wave_level_kernel<<<w.grid, 256, (size_t)staged*sizeof(BvhNode4), s>>>(a, w, k, staged);
     }
-    wave_sphere_kernel<<<w.grid, 256, 0, s>>>(a, w, cur);
+    if (form == MLGPU_TRACER_FP64) wave_sphere_kernel<false><<<w.grid, 256, 0, s>>>(a, w, cur);
+    else wave_sphere_kernel<true><<<w.grid, 256, 0, s>>>(a, w, cur);
     if (ev) cudaEventRecord(ev[2], s);
     if (form == MLGPU_TRACER_FP64) {
         wave_isect_kernel<kIsectFp64><<<w.grid, 256, 0, s>>>(a, w, cur);
