@@ -69,6 +69,7 @@ def lib():
             C.c_void_p, C.POINTER(abi.mlgpu_photons), C.c_uint64,
             C.POINTER(abi.mlgpu_settings), C.POINTER(abi.mlgpu_rng),
             C.POINTER(abi.mlgpu_settings), C.POINTER(C.c_double), C.c_void_p]
+        _declare_surrogate(L)
         for name in ("mlgpu_scene_create", "mlgpu_scene_destroy", "mlgpu_propagate", "mlgpu_scene_autotune",
                      "mlgpu_propagate_host", "mlgpu_scene_sync_errors", "mlgpu_bin_arrivals",
                      "mlgpu_bin_arrivals_noalloc", "mlgpu_scene_kernel_launches"):
@@ -77,6 +78,39 @@ def lib():
             raise ImportError("libmerlict_b200.so ABI version mismatch")
         _lib = L
     return _lib
+
+
+class mlgpu_sg_sensor_grid(C.Structure):
+    _fields_ = [
+        ("num_sensors", C.c_uint32),
+        ("center", C.c_void_p), ("rotation", C.c_void_p), ("inner", C.c_void_p),
+        ("sensor_id", C.c_void_p),
+        ("x0", C.c_double), ("y0", C.c_double), ("cell", C.c_double),
+        ("nx", C.c_uint32), ("ny", C.c_uint32),
+        ("cell_start", C.c_void_p), ("cell_items", C.c_void_p),
+        ("hex_u", C.c_double * 2), ("hex_v", C.c_double * 2), ("hex_w", C.c_double * 2),
+    ]
+
+
+def _declare_surrogate(L) -> None:
+    """ctypes signatures of include/merlict_b200_surrogate.h."""
+    vp, u32, u64, f32 = C.c_void_p, C.c_uint32, C.c_uint64, C.c_float
+    L.mlgpu_sg_image_offset.argtypes = [u32, u32, u32]
+    L.mlgpu_sg_image_offset.restype = C.c_size_t
+    L.mlgpu_sg_param_count.restype = u64
+    L.mlgpu_sg_image_bytes.restype = u64
+    L.mlgpu_sg_workspace_bytes.argtypes = [u32, C.c_int]
+    L.mlgpu_sg_workspace_bytes.restype = u64
+    L.mlgpu_sg_gemm_f32.argtypes = [vp, u32, vp, u32, u32, u32, u32, vp, vp, vp]
+    L.mlgpu_sg_pack_weights.argtypes = [vp, vp, vp]
+    L.mlgpu_sg_forward.argtypes = [vp, vp, vp, u32, vp, vp, vp]
+    L.mlgpu_sg_train_step.argtypes = [vp, vp, vp, vp, vp, vp, vp, u32, u32, f32, vp, vp, vp, vp]
+    L.mlgpu_sg_sample.argtypes = [vp, vp, u32, vp, vp, f32, f32, u64, u64,
+                                  C.POINTER(mlgpu_sg_sensor_grid), vp, vp, vp, vp, vp, vp, vp]
+    L.mlgpu_sg_sync_errors.argtypes = [vp]
+    for name in ("mlgpu_sg_gemm_f32", "mlgpu_sg_pack_weights", "mlgpu_sg_forward",
+                 "mlgpu_sg_train_step", "mlgpu_sg_sample", "mlgpu_sg_sync_errors"):
+        getattr(L, name).restype = C.c_int
 
 
 def last_error() -> str:
@@ -96,4 +130,8 @@ EXPORTED = (
     "mlgpu_propagate", "mlgpu_scene_sync_errors", "mlgpu_propagate_host",
     "mlgpu_bin_arrivals", "mlgpu_bin_arrivals_noalloc", "mlgpu_scene_kernel_launches",
     "mlgpu_scene_set_profiling", "mlgpu_scene_kernel_times", "mlgpu_scene_autotune",
+    # include/merlict_b200_surrogate.h
+    "mlgpu_sg_image_offset", "mlgpu_sg_gemm_f32", "mlgpu_sg_param_count", "mlgpu_sg_image_bytes",
+    "mlgpu_sg_pack_weights", "mlgpu_sg_workspace_bytes", "mlgpu_sg_forward",
+    "mlgpu_sg_train_step", "mlgpu_sg_sample", "mlgpu_sg_sync_errors",
 )

@@ -1,5 +1,5 @@
-"""The C ABI: the shared library exports every symbol include/merlict_b200.h
-declares, and the ctypes mirror matches the C struct layouts."""
+"""The C ABI: the shared library exports every symbol the headers in include/
+declare, and the ctypes mirror matches the C struct layouts."""
 import ctypes as C
 import os
 import re
@@ -10,12 +10,15 @@ import pytest
 from conftest import REPO
 from merlict_development_kit_b200 import abi
 
-HEADER = os.path.join(REPO, "include", "merlict_b200.h")
+HEADERS = [os.path.join(REPO, "include", h) for h in ("merlict_b200.h", "merlict_b200_surrogate.h")]
 
 
 def declared_functions():
-    text = open(HEADER).read()
-    return sorted(set(re.findall(r"^\s*int\s+(mlgpu_\w+)\s*\(", text, flags=re.M)))
+    names = set()
+    for h in HEADERS:
+        text = open(h).read()
+        names |= set(re.findall(r"^\s*(?:int|uint64_t|size_t)\s+(mlgpu_\w+)\s*\(", text, flags=re.M))
+    return sorted(names)
 
 
 def test_library_exports_every_declared_symbol():
@@ -29,13 +32,16 @@ def test_library_exports_every_declared_symbol():
 
 
 def test_struct_layouts_match_header(tmp_path):
+    from merlict_development_kit_b200 import _native
     src = tmp_path / "sizes.c"
     src.write_text(
         '#include <stdio.h>\n#include <stddef.h>\n#include "merlict_b200.h"\n'
-        "int main(void){printf(\"%zu %zu %zu %zu %zu %zu %zu %zu\\n\","
+        '#include "merlict_b200_surrogate.h"\n'
+        "int main(void){printf(\"%zu %zu %zu %zu %zu %zu %zu %zu %zu %zu\\n\","
         "sizeof(mlgpu_flat_scene), sizeof(mlgpu_photons), sizeof(mlgpu_history_entry),"
         "sizeof(mlgpu_results), sizeof(mlgpu_rng), sizeof(mlgpu_settings),"
-        "offsetof(mlgpu_flat_scene, hex_unit_u), offsetof(mlgpu_flat_scene, num_sensors));"
+        "offsetof(mlgpu_flat_scene, hex_unit_u), offsetof(mlgpu_flat_scene, num_sensors),"
+        "sizeof(mlgpu_sg_sensor_grid), offsetof(mlgpu_sg_sensor_grid, hex_u));"
         "return 0;}\n")
     exe = tmp_path / "sizes"
     subprocess.run(["gcc", "-I" + os.path.join(REPO, "include"), str(src), "-o", str(exe)], check=True)
@@ -43,7 +49,8 @@ def test_struct_layouts_match_header(tmp_path):
     expected = [C.sizeof(abi.mlgpu_flat_scene), C.sizeof(abi.mlgpu_photons),
                 C.sizeof(abi.mlgpu_history_entry), C.sizeof(abi.mlgpu_results),
                 C.sizeof(abi.mlgpu_rng), C.sizeof(abi.mlgpu_settings),
-                abi.mlgpu_flat_scene.hex_unit_u.offset, abi.mlgpu_flat_scene.num_sensors.offset]
+                abi.mlgpu_flat_scene.hex_unit_u.offset, abi.mlgpu_flat_scene.num_sensors.offset,
+                C.sizeof(_native.mlgpu_sg_sensor_grid), _native.mlgpu_sg_sensor_grid.hex_u.offset]
     assert [int(x) for x in out] == expected
 
 

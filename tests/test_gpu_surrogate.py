@@ -1,0 +1,163 @@
+"""The learned surrogate's tensor-core kernels: the tcgen05 GEMM against a
+PyTorch FP32 matmul of the same BF16 operands, the weight images, the
+training step's gradients against the NumPy oracle (oracle/
+surrogate_oracle.py), training, and what the trained network gains over
+the same lookup without it."""
+import numpy as np
+import pytest
+
+from conftest import load_golden
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def sg():
+    import torch
+    assert torch.cuda.is_available()
+    from merlict_development_kit_b200 import surrogate
+    return surrogate
+
+
+@pytest.mark.parametrize("m,n,k", [(128, 256, 64), (384, 256, 192), (256, 128, 128),
+                                   (128, 80, 256), (512, 80, 64)])
+def test_gemm_matches_fp32_matmul(sg, m, n, k):
+    import torch
+    g = torch.Generator(device="cuda").manual_seed(m * 7 + n + k)
+    a = torch.randn((m, k), generator=g, device="cuda").to(torch.bfloat16)
+    b = torch.randn((n, k), generator=g, device="cuda").to(torch.bfloat16)
+    bias = torch.randn(n, generator=g, device="cuda")
+    c = sg.gemm(sg.to_image(a), m, sg.to_image(b), n, m, n, k // 64, bias=bias)
+    sg.sync_errors()
+    ref = a.float() @ b.float().T + bias
+    # FP32 accumulation of exact BF16 products: only the summation order differs
+    assert torch.allclose(c, ref, rtol=1e-4, atol=1e-3 * np.sqrt(k)), (c - ref).abs().max()
+
+
+def test_image_round_trip(sg):
+    import torch
+    a = torch.randn((256, 128), device="cuda").to(torch.bfloat16)
+    assert torch.equal(sg.from_image(sg.to_image(a), 256, 128), a)
+
+
+def test_packed_weight_images_match(sg):
+    import torch
+    from merlict_development_kit_b200._native import lib
+    p = sg.init_params(3)
+    img = torch.zeros(int(lib().mlgpu_sg_image_bytes()), dtype=torch.uint8, device="cuda")
+    assert lib().mlgpu_sg_pack_weights(p.data_ptr(), img.data_ptr(), None) == 0
+    torch.cuda.synchronize()
+    sl = sg.param_slices()
+    hh = 256 * 256 * 2
+    off = 0
+    for l in (1, 2, 3):
+        W = p[sl[l][0]].reshape(256, 256)
+        assert torch.equal(img[off:off + hh], sg.to_image(W))
+        assert torch.equal(img[off + hh:off + 2 * hh], sg.to_image(W.T.contiguous()))
+        off += 2 * hh
+    W4 = p[sl[4][0]].reshape(73, 256)
+    w4 = torch.zeros((80, 256), device="cuda")
+    w4[:73] = W4
+    assert torch.equal(img[off:off + 80 * 256 * 2], sg.to_image(w4))
+    off += 80 * 256 * 2
+    w4t = torch.zeros((256, 128), device="cuda")
+    w4t[:, :73] = W4.T
+    assert torch.equal(img[off:off + 256 * 128 * 2], sg.to_image(w4t))
+
+
+def random_batch(n, seed):
+    rng = np.random.default_rng(seed)
+    x = np.zeros((n, 8), np.float32)
+    x[:, :5] = rng.uniform(-1, 1, size=(n, 5))
+    t = rng.normal(size=(n, 4)).astype(np.float32)
+    r = (rng.random(n) < 0.6).astype(np.uint8)
+    return x, t, r
+
+
+@pytest.mark.parametrize("batch", [256, 1024])
+def test_training_step_gradients_match_oracle(sg, batch):
+    """One training step with lr = 0: the device's loss and gradient of every
+    layer agree with the float64 oracle (which rounds to BF16 where the
+    device stores BF16) to 1e-3 in relative Frobenius norm."""
+    import torch
+    from oracle import surrogate_oracle as O
+    flat = load_golden("light_field_small")[0]
+    model = sg.Surrogate(flat, seed=5)
+    # outputs of order one (the output layer starts near zero); the hidden
+    # layers keep their unit-gain initialisation, so that BF16 rounding
+    # differences are not amplified layer by layer
+    w4, _, b4 = sg.param_slices()[4]
+    model.params[w4] *= 30.0
+    model.params[b4] = torch.linspace(-1.0, 1.0, b4.stop - b4.start, device="cuda")
+    model.pack()
+    x, t, r = random_batch(batch, 11)
+    loss = torch.zeros(1, device="cuda")
+    grads = torch.zeros_like(model.params)
+    p0 = model.params.clone()
+    model.train_step(torch.as_tensor(x, device="cuda"), torch.as_tensor(t, device="cuda"),
+                     torch.as_tensor(r, device="cuda"), 0.0, loss=loss, grads=grads)
+    sg.sync_errors()
+    assert torch.equal(model.params, p0)
+    ref_loss, ref_g = O.gradients(p0.cpu().numpy(), x, t, r)
+    assert abs(float(loss) - ref_loss) <= 1e-4 * abs(ref_loss)
+    g = grads.cpu().numpy().astype(np.float64)
+    errors = {}
+    for l, (w, shape, b) in enumerate(sg.param_slices()):
+        for name, s in (("W", w), ("b", b)):
+            errors[f"{name}{l}"] = np.linalg.norm(g[s] - ref_g[s]) / np.linalg.norm(ref_g[s])
+    assert max(errors.values()) < 1e-3, errors
+
+
+def test_training_reduces_the_loss(sg):
+    import torch
+    from merlict_development_kit_b200 import engine
+    flat = load_golden("light_field_small")[0]
+    src = sg.Source(max_zenith_deg=0.5)
+    scene = engine.Scene(flat)
+    data = sg.training_data(scene, src, 1 << 20, seed=2)
+    model = sg.Surrogate(flat, source=src, seed=1)
+    hist = model.train(data, epochs=6, batch=8192, lr=2e-3)
+    assert np.all(np.isfinite(hist))
+    assert hist[-1] < hist[0] - 1.0, hist
+    scene.close()
+
+
+def js_divergence(a, b):
+    p = a / a.sum()
+    q = b / b.sum()
+    m = 0.5 * (p + q)
+
+    def kl(x, y):
+        k = x > 0
+        return float(np.sum(x[k] * np.log(x[k] / y[k])))
+    return 0.5 * kl(p, m) + 0.5 * kl(q, m)
+
+
+def test_trained_network_beats_the_lookup_without_it(sg):
+    """Per-lixel histograms of 2 M fresh photons against the exact tracer:
+    the trained network (with exact tracing of the photons it flags) is
+    closer than the same lookup fed by the linear map alone."""
+    import torch
+    from merlict_development_kit_b200 import engine
+    flat = load_golden("light_field_small")[0]
+    src = sg.Source(max_zenith_deg=0.5)
+    scene = engine.Scene(flat)
+    data = sg.training_data(scene, src, 1 << 22, seed=3)
+    model = sg.Surrogate(flat, source=src, seed=2)
+    model.train(data, epochs=8, batch=16384, lr=2e-3)
+    ph = src.photons(1 << 21, seed=99)
+    exact = scene.propagate(ph, engine.PropagationConfig(10), engine.Philox(7),
+                            outputs=("sensor",))["sensor"]
+    net = model.propagate(ph, seed=8, scene=scene)
+    null = model.propagate(ph, seed=8, use_network=False, sigma_limit=1e9)
+
+    def hist(s):
+        s = s[s >= 0].long()
+        return torch.bincount(s, minlength=flat.num_sensors).double().cpu().numpy()
+    h = hist(exact)
+    js_net, js_null = js_divergence(hist(net["sensor"]), h), js_divergence(hist(null["sensor"]), h)
+    fallback = float(net["fallback"].float().mean())
+    print(f"JS network {js_net:.2e}, without network {js_null:.2e}, fallback {fallback:.3f}")
+    assert js_net < 0.5 * js_null, (js_net, js_null, fallback)
+    assert fallback < 0.5
+    scene.close()
