@@ -299,6 +299,43 @@ def run_ours(args, world, rank, local):
     elapsed_ms = max_over_ranks(elapsed_ms, world)
     value = n * world * args.steps / (elapsed_ms * 1e-3)
 
+    # the FP32 form on the same photons (rounded to FP32) with the same
+    # Philox streams as one FP64 step: photons/s, replay-mode sensor
+    # agreement and the per-lixel histogram divergence against FP64
+    forms = None
+    if tracer == "fp64" and not args.no_forms:
+        from merlict_development_kit_b200.precision import js_divergence
+        dev32 = {k: v.float() for k, v in dev.items()}
+        dev64r = {k: v.double() for k, v in dev32.items()}
+        tune32, _ = (scene.autotune({k: v[:min(n, 2_000_000)].contiguous() for k, v in dev32.items()},
+                                    cfg, engine.Philox(3), tracer="fp32")
+                     if args.autotune else (None, 0.0))
+        ref = scene.propagate(dev64r, cfg, engine.Philox(31), outputs=("sensor",), tuning=tuning)
+        ref_sensor = ref["sensor"].clone()
+        res32 = {}
+        for _ in range(2):
+            scene.propagate(dev32, cfg, engine.Philox(31), tracer="fp32", outputs=("sensor",),
+                            out_dtype=torch.float32, results=res32, tuning=tune32, sync=False)
+        torch.cuda.synchronize()
+        f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        f0.record(stream)
+        for _ in range(args.steps):
+            scene.propagate(dev32, cfg, engine.Philox(31), tracer="fp32", outputs=("sensor",),
+                            out_dtype=torch.float32, results=res32, tuning=tune32, sync=False)
+        f1.record(stream)
+        torch.cuda.synchronize()
+        ms32 = max_over_ranks(f0.elapsed_time(f1) / args.steps, world)
+        s32 = res32["sensor"]
+
+        def hist(sn):
+            sn = sn[sn >= 0].long()
+            return torch.bincount(sn, minlength=flat.num_sensors).double().cpu().numpy()
+        forms = {"fp32": {"value": n * world / (ms32 * 1e-3), "unit": "photons/s",
+                          "replay_sensor_agreement": float((s32 == ref_sensor).float().mean()),
+                          "lixel_js_vs_fp64": js_divergence(hist(s32), hist(ref_sensor)),
+                          "tuning": tune32}}
+        del dev32, dev64r, ref, res32
+
     # e2e: the C-ABI host-buffer call (H2D of the batch, trace, D2H of the
     # results, synchronise), pinned host memory, same batch size
     pin = {k: torch.from_numpy(np.ascontiguousarray(host[k])).to(in_dtype).pin_memory()
@@ -403,6 +440,7 @@ def run_ours(args, world, rank, local):
         "cpu_baseline": cpu,
         "e2e": {"value": e2e_value, "unit": "photons/s", "h2d_bytes_per_step": h2d,
                 "d2h_bytes_per_step": d2h},
+        "forms": forms,
         "gpu_launches": launches,
         "clocks": clk,
     }
@@ -668,6 +706,8 @@ def main():
     ap.add_argument("--photons", type=int, default=10_000_000)
     ap.add_argument("--ref-photons", type=int, default=100_000)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-forms", action="store_true",
+                    help="skip the FP32 form's line items in the default workload")
     ap.add_argument("--no-autotune", dest="autotune", action="store_false",
                     help="default wavefront knobs instead of mlgpu_scene_autotune's")
     ap.add_argument("--workload", choices=["telescope", "bunches", "precision", "surrogate"],

@@ -313,6 +313,42 @@ int mlgpu_propagate_host(
     const mlgpu_rng* rng,
     mlgpu_results* results);
 
+/* ---- CORSIKA photon bunches --------------------------------------------- *
+ * Replaces merlict::EventIoPhotonFactory (merlict_corsika/PhotonFactory.cpp:
+ * 8-136) for a whole event at once, on the device.  `bunches` holds
+ * num_bunches rows of 8 floats (x, y [cm], u, v, time [ns], production
+ * height [cm], weight, wavelength [nm]); bunch i gives floor(weight) photons
+ * plus one if its uniform draw is <= the weight's fraction, each with the
+ * support, direction and wavelength merlict's factory gives it, and
+ * simulation_truth_id = bunch_ids[i] (or i if bunch_ids is NULL).  The
+ * draws: PHILOX stream (photon_offset + i), first uniform; REPLAY
+ * uniforms[i].  Photons are written in bunch order.  The call waits for
+ * `cuda_stream`; *num_photons receives the number of photons; if it exceeds
+ * out->capacity nothing is written and MLGPU_ERR_INVALID_ARGUMENT is
+ * returned (call again with larger buffers).  A weight outside [0, 16] is
+ * MLGPU_ERR_INVALID_ARGUMENT (merlict throws std::invalid_argument).     */
+typedef struct mlgpu_photon_buffers {
+    double* support_x;
+    double* support_y;
+    double* support_z;
+    double* direction_x;
+    double* direction_y;
+    double* direction_z;
+    double* wavelength;
+    int32_t* simulation_truth_id;     /* may be NULL                       */
+    uint64_t capacity;                /* photons each buffer holds          */
+} mlgpu_photon_buffers;
+
+int mlgpu_corsika_photons(
+    mlgpu_scene* scene,
+    const float* bunches,
+    uint64_t num_bunches,
+    const int32_t* bunch_ids,
+    const mlgpu_rng* rng,
+    mlgpu_photon_buffers* out,
+    uint64_t* num_photons,
+    void* cuda_stream);
+
 /* ---- tuning ------------------------------------------------------------ *
  * No counterpart in the reference (merlict has no device parameters).
  * Picks the wavefront knobs of `base` (pool_size, check_period, use_graph,

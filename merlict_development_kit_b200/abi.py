@@ -180,6 +180,12 @@ class mlgpu_rng(C.Structure):
     ]
 
 
+class mlgpu_photon_buffers(C.Structure):
+    _fields_ = [(k, C.c_void_p) for k in (
+        "support_x", "support_y", "support_z", "direction_x", "direction_y", "direction_z",
+        "wavelength", "simulation_truth_id")] + [("capacity", C.c_uint64)]
+
+
 TRAVERSAL_BVH = 0
 TRAVERSAL_FRAME_TREE = 1
 

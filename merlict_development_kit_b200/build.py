@@ -27,6 +27,7 @@ EXTRA = {
     "trace_fp64.cu": ["--fmad=false"],
     "bin.cu": ["--fmad=false"],
     "wavefront_fp64.cu": ["--fmad=false"],
+    "corsika.cu": ["--fmad=false"],
 }
 
 

@@ -131,6 +131,7 @@ struct mlgpu_scene {
     // staging for mlgpu_propagate_host and scratch for binning
     DeviceBuffer staging_in, staging_out, staging_hist, staging_rng, bin_scratch, tune_out;
     DeviceBuffer order;                  // tracing order of a batch and its sort scratch
+    DeviceBuffer corsika;                // bunch counts, offsets and the total
     // ray pools of the wavefront tracers
     DeviceBuffer wave;
     WaveCounters* wave_host = nullptr;   // pinned copy of the counters
@@ -652,6 +653,7 @@ int mlgpu_scene_destroy(mlgpu_scene* scene) {
     scene->bin_scratch.release();
     scene->tune_out.release();
     scene->order.release();
+    scene->corsika.release();
     scene->wave.release();
     if (scene->wave_host) cudaFreeHost(scene->wave_host);
     if (scene->wave_graph) cudaGraphExecDestroy(scene->wave_graph);
@@ -757,6 +759,61 @@ int mlgpu_scene_autotune(mlgpu_scene* scene, const mlgpu_photons* sample, uint64
     if (st) return st;
     *best = cur;
     if (best_ms) *best_ms = cur_ms;
+    return MLGPU_OK;
+}
+
+int mlgpu_corsika_photons(mlgpu_scene* scene, const float* bunches, uint64_t n,
+                          const int32_t* bunch_ids, const mlgpu_rng* rng,
+                          mlgpu_photon_buffers* out, uint64_t* num_photons, void* cuda_stream) {
+    if (!scene || !rng || !out || !num_photons)
+        return fail(MLGPU_ERR_INVALID_ARGUMENT, "NULL argument");
+    *num_photons = 0;
+    if (n == 0) return MLGPU_OK;
+    if (!bunches) return fail(MLGPU_ERR_INVALID_ARGUMENT, "bunches is NULL");
+    if (rng->mode != MLGPU_RNG_PHILOX && rng->mode != MLGPU_RNG_REPLAY)
+        return fail(MLGPU_ERR_INVALID_ARGUMENT, "unknown rng mode");
+    if (rng->mode == MLGPU_RNG_REPLAY && !rng->uniforms)
+        return fail(MLGPU_ERR_INVALID_ARGUMENT, "replay rng without uniforms");
+    double* planes[7] = {out->support_x, out->support_y, out->support_z, out->direction_x,
+                         out->direction_y, out->direction_z, out->wavelength};
+    for (double* p : planes)
+        if (!p) return fail(MLGPU_ERR_INVALID_ARGUMENT, "photon buffer is NULL");
+    const cudaStream_t stream = static_cast<cudaStream_t>(cuda_stream);
+    MLGPU_CUDA(scene->corsika.reserve(corsika_scratch_bytes(n) + 256));
+    if (!scene->wave_host) MLGPU_CUDA(cudaMallocHost(&scene->wave_host, sizeof(WaveCounters)));
+    if (!scene->wave_grid) scene->wave_grid = wave_persistent_blocks();
+    char* base = static_cast<char*>(scene->corsika.ptr);
+    uint64_t* total_dev = reinterpret_cast<uint64_t*>(base);
+    void* scratch = base + 256;
+    DevRng r;
+    r.mode = rng->mode; r.stride = rng->stride; r.seed = rng->seed;
+    r.photon_offset = rng->photon_offset; r.uniforms = rng->uniforms;
+    MLGPU_CUDA(cudaMemsetAsync(scene->error_word, 0, sizeof(unsigned int), stream));
+    cudaError_t e = launch_corsika_count(bunches, n, r, scratch, total_dev, scene->error_word,
+                                         scene->wave_grid, stream);
+    if (e != cudaSuccess) return cuda_fail(e, "bunch count kernels");
+    scene->launches += 4;
+    // the total and the error word, back on the host (pinned staging)
+    uint64_t* host = reinterpret_cast<uint64_t*>(scene->wave_host);
+    MLGPU_CUDA(cudaMemcpyAsync(host, total_dev, sizeof(uint64_t), cudaMemcpyDeviceToHost, stream));
+    MLGPU_CUDA(cudaMemcpyAsync(host + 1, scene->error_word, sizeof(unsigned int),
+                               cudaMemcpyDeviceToHost, stream));
+    MLGPU_CUDA(cudaStreamSynchronize(stream));
+    const uint64_t total = host[0];
+    const unsigned int err = static_cast<unsigned int>(host[1] & 0xffffffffu);
+    if (err) {
+        MLGPU_CUDA(cudaMemset(scene->error_word, 0, sizeof(unsigned int)));
+        return fail(MLGPU_ERR_INVALID_ARGUMENT,
+                    "a bunch weight is outside [0, 16] (EventIoPhotonFactory::assert_bunch_weight)");
+    }
+    *num_photons = total;
+    if (total > out->capacity)
+        return fail(MLGPU_ERR_INVALID_ARGUMENT, "the bunches give %llu photons, the buffers hold %llu",
+                    (unsigned long long)total, (unsigned long long)out->capacity);
+    e = launch_corsika_expand(bunches, n, bunch_ids, scratch, planes, out->simulation_truth_id,
+                              scene->wave_grid, stream);
+    if (e != cudaSuccess) return cuda_fail(e, "bunch expansion kernel");
+    scene->launches += 1;
     return MLGPU_OK;
 }
 

@@ -211,6 +211,15 @@ cudaError_t launch_wave32_isect_resolve(const TraceArgs& a, const WaveBuffers& w
                                         cudaStream_t s, cudaEvent_t mid);
 
 cudaError_t launch_trace_fp64(const TraceArgs& a, int block, cudaStream_t s);
+// CORSIKA bunches to photons (corsika.cu): counts and offsets into
+// `scratch` (corsika_scratch_bytes), the total to *total_dev; then the
+// expansion into the seven FP64 planes.
+size_t corsika_scratch_bytes(uint64_t n);
+cudaError_t launch_corsika_count(const float* bunches, uint64_t n, const DevRng& rng, void* scratch,
+                                 uint64_t* total_dev, unsigned int* err, int grid, cudaStream_t s);
+cudaError_t launch_corsika_expand(const float* bunches, uint64_t n, const int32_t* ids,
+                                  void* scratch, double* const* planes, int32_t* out_id, int grid,
+                                  cudaStream_t s);
 // A coherent tracing order of a photon batch (photon_order.cu): `order`
 // receives n photon indices; `scratch` holds photon_order_scratch_bytes(n).
 size_t photon_order_scratch_bytes(uint64_t n);

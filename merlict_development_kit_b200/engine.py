@@ -213,6 +213,39 @@ class Scene:
         del keep
         return best.tuning(), float(ms.value)
 
+    def corsika_photons(self, bunches: torch.Tensor, rng=None, bunch_ids: torch.Tensor | None = None,
+                        capacity: int | None = None, stream=None) -> dict:
+        """Photons of CORSIKA bunches ([n][8] float32 CUDA tensor: x, y [cm],
+        u, v, time [ns], production height [cm], weight, wavelength [nm]),
+        made on the device the way merlict's EventIoPhotonFactory makes them
+        (mlgpu_corsika_photons); planes as for `propagate`, plus "id".
+        A weight outside [0, 16] raises ValueError, like merlict."""
+        if bunches.dtype != torch.float32 or not bunches.is_cuda or bunches.dim() != 2 \
+                or bunches.shape[1] != 8:
+            raise ValueError("bunches must be a [n][8] float32 CUDA tensor")
+        b = bunches.contiguous()
+        n = int(b.shape[0])
+        rng = rng if rng is not None else Philox(0)
+        r, keep = rng._struct(n)
+        cap = 17 * n if capacity is None else int(capacity)
+        out = {k: torch.empty(cap, dtype=torch.float64, device=b.device) for k in PLANES}
+        out["id"] = torch.empty(cap, dtype=torch.int32, device=b.device)
+        buf = abi.mlgpu_photon_buffers()
+        for k in PLANES:
+            setattr(buf, k, out[k].data_ptr())
+        buf.simulation_truth_id = out["id"].data_ptr()
+        buf.capacity = cap
+        total = C.c_uint64(0)
+        ids = bunch_ids.contiguous() if bunch_ids is not None else None
+        check(lib().mlgpu_corsika_photons(self._h, C.c_void_p(b.data_ptr()), n,
+                                          C.c_void_p(ids.data_ptr() if ids is not None else None),
+                                          C.byref(r), C.byref(buf), C.byref(total),
+                                          C.c_void_p(_stream_handle(stream))))
+        rng.advance(n)
+        del keep
+        t = int(total.value)
+        return {k: v[:t] for k, v in out.items()}
+
     def kernel_launches(self) -> int:
         """Kernels this scene has launched so far."""
         v = C.c_uint64(0)

@@ -214,3 +214,52 @@ class RefScene:
         if status != 0 and out is None:
             raise RuntimeError(self.lib.ref_last_error().decode())
         return status, out, sec.value
+
+
+def corsika_photons_reference(bunches: np.ndarray, uniforms: np.ndarray) -> dict:
+    """merlict's own EventIoPhotonFactory (through the harness) on bunches
+    [n][8] float32, bunch i drawing uniforms[i]."""
+    L = C.CDLL(HARNESS_SO)
+    b = np.ascontiguousarray(bunches, dtype=np.float32)
+    u = np.ascontiguousarray(uniforms, dtype=np.float64)
+    n = b.shape[0]
+    cap = 17 * n
+    planes = {k: np.zeros(cap) for k in ("support_x", "support_y", "support_z", "direction_x",
+                                          "direction_y", "direction_z", "wavelength")}
+    ids = np.zeros(cap, np.int32)
+    total = C.c_uint64(0)
+    L.ref_corsika_photons.argtypes = [C.c_void_p, C.c_uint64, C.c_void_p] + [C.c_void_p] * 8 + [
+        C.c_uint64, C.POINTER(C.c_uint64)]
+    L.ref_last_error.restype = C.c_char_p
+    st = L.ref_corsika_photons(b.ctypes.data, n, u.ctypes.data, *[planes[k].ctypes.data for k in planes],
+                               ids.ctypes.data, cap, C.byref(total))
+    if st != 0:
+        raise ValueError(L.ref_last_error().decode())
+    t = int(total.value)
+    out = {k: v[:t] for k, v in planes.items()}
+    out["id"] = ids[:t]
+    return out
+
+
+def corsika_photons_numpy(bunches: np.ndarray, uniforms: np.ndarray) -> dict:
+    """A NumPy restatement of EventIoPhotonFactory (merlict_corsika/
+    PhotonFactory.cpp:8-136) in merlict's operation order; the direction is
+    returned as the Photon holds it (normalised, Ray.cpp:16-20)."""
+    b = np.asarray(bunches, dtype=np.float32).astype(np.float64)
+    w = b[:, 6]
+    if np.any((w < 0.0) | (w > 16.0)):
+        raise ValueError("bunch weight outside [0, 16]")
+    count = np.floor(w).astype(np.int64) + (np.asarray(uniforms) <= np.fmod(w, 1.0))
+    u, v = b[:, 2], b[:, 3]
+    z = np.sqrt(1.0 - u * u - v * v)
+    cx, cy, cz = u, v, -z
+    ux, uy, uz = cx * -1.0, cy * -1.0, cz * -1.0
+    un = np.sqrt(ux * ux + uy * uy + uz * uz)
+    par = (b[:, 4] * 1e-9) * 299792458.0 + 1e3
+    sx, sy, sz = b[:, 0] * 1e-2 + (ux / un) * par, b[:, 1] * 1e-2 + (uy / un) * par, 0.0 + (uz / un) * par
+    dn = np.sqrt(cx * cx + cy * cy + cz * cz)
+    rep = lambda a: np.repeat(a, count)
+    return {"support_x": rep(sx), "support_y": rep(sy), "support_z": rep(sz),
+            "direction_x": rep(cx / dn), "direction_y": rep(cy / dn), "direction_z": rep(cz / dn),
+            "wavelength": rep(np.abs(b[:, 7] * 1e-9)),
+            "id": rep(np.arange(b.shape[0], dtype=np.int32))}

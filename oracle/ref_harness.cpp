@@ -31,6 +31,7 @@
 
 #include "merlict/merlict.h"
 #include "merlict/scenery/segmented_imaging_reflector/segmented_imaging_reflector.h"
+#include "merlict_corsika/PhotonFactory.h"
 #include "merlict_multi_thread/merlict_multi_thread.h"
 #include "merlict_portal_plenoscope/light_field_sensor/LightFieldSensor.h"
 #include "merlict_b200.h"
@@ -594,6 +595,46 @@ int ref_propagate(void* handle, const mlgpu_photons* ph, uint64_t n,
     } catch (const std::exception& e) {
         last_error = e.what();
         return MLGPU_ERR_RUNTIME;
+    }
+}
+
+// merlict's EventIoPhotonFactory (merlict_corsika/PhotonFactory.cpp) on
+// given bunches (8 floats each), bunch i drawing uniforms[i] for its
+// weight's extra photon and getting id i.  Writes each photon's support,
+// direction (as the Photon holds it), wavelength and id, in bunch order, up
+// to `capacity` photons; *total = the number of photons made.
+int ref_corsika_photons(const float* bunches, uint64_t n, const double* uniforms, double* sx,
+                        double* sy, double* sz, double* dx, double* dy, double* dz, double* wl,
+                        int32_t* ids, uint64_t capacity, uint64_t* total) {
+    try {
+        ReplayGenerator g;
+        g.mode = 1;
+        g.stride = 1;
+        g.uniforms = uniforms;
+        uint64_t k = 0;
+        for (uint64_t i = 0; i < n; i++) {
+            std::array<float, 8> row;
+            for (int j = 0; j < 8; j++) row[j] = bunches[8*i + j];
+            g.stream = i;
+            g.used = 0;
+            ml::EventIoPhotonFactory factory(row, static_cast<unsigned int>(i), &g);
+            while (factory.has_still_photons_to_be_made()) {
+                const ml::Photon p = factory.make_photon();
+                if (k < capacity) {
+                    const ml::Vec3 s = p.support(), d = p.direction();
+                    sx[k] = s.x; sy[k] = s.y; sz[k] = s.z;
+                    dx[k] = d.x; dy[k] = d.y; dz[k] = d.z;
+                    wl[k] = p.wavelength;
+                    ids[k] = p.simulation_truth_id;
+                }
+                k++;
+            }
+        }
+        *total = k;
+        return 0;
+    } catch (const std::exception& e) {
+        last_error = e.what();
+        return MLGPU_ERR_INVALID_ARGUMENT;
     }
 }
 
