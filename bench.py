@@ -589,12 +589,18 @@ def run_surrogate(args, world, rank, local):
     flat = F.light_field_telescope(**SCENE).flatten()
     scene = engine.Scene(flat)
     src = S.Source(SOURCE["disc_radius"], SOURCE["height"], SOURCE["max_zenith_deg"])
+    plane = args.surrogate_mode == "plane"
+    plane_z = SCENE["focal_length"] - 0.05   # 5 cm below the lens array
     t0 = time.perf_counter()
-    data = S.training_data(scene, src, args.train_photons, seed=1 + rank,
-                           max_interactions=MAX_INTERACTIONS)
+    if plane:
+        data = S.training_data_plane(scene, src, args.train_photons, seed=1 + rank,
+                                     plane_z=plane_z)
+    else:
+        data = S.training_data(scene, src, args.train_photons, seed=1 + rank,
+                               max_interactions=MAX_INTERACTIONS)
     torch.cuda.synchronize()
     t_data = time.perf_counter() - t0
-    model = S.Surrogate(flat, source=src, seed=rank)
+    model = S.Surrogate(flat, source=src, seed=rank, plane_z=plane_z if plane else None)
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record()
     losses = model.train(data, epochs=args.epochs, batch=65536, lr=2e-3)
@@ -607,8 +613,12 @@ def run_surrogate(args, world, rank, local):
     ph = src.photons(n, seed=777 + rank)
     cfg = engine.PropagationConfig(MAX_INTERACTIONS)
 
+    tuning, _ = scene.autotune({k: v[:2_000_000].contiguous() for k, v in ph.items()}, cfg,
+                               engine.Philox(3))
+
     def exact():
-        return scene.propagate(ph, cfg, engine.Philox(4242), outputs=("sensor",))["sensor"]
+        return scene.propagate(ph, cfg, engine.Philox(4242), outputs=("sensor",),
+                               tuning=tuning)["sensor"]
 
     def learned(use_network=True):
         return model.propagate(ph, seed=99, scene=scene, max_interactions=MAX_INTERACTIONS,
@@ -622,21 +632,24 @@ def run_surrogate(args, world, rank, local):
     h_exact = hist(r_exact)
     # operating point: the widest component (in units of the smallest lixel's
     # inner radius) that still keeps the per-lixel JS within the target
+    # the unit of the fallback threshold: the smallest lixel's inner radius
+    # (lookup mode) or 1 mm on the plane (plane mode)
+    unit = model.grid.inner_min if model.grid is not None else 1e-3
     sweep = []
-    for mult in (0.0625, 0.125, 0.25, 0.5, 1.0, 2.0, 4.0):
+    for mult in (0.0625, 0.25, 1.0, 4.0, 16.0, 64.0):
         r = model.propagate(ph, seed=99, scene=scene, max_interactions=MAX_INTERACTIONS,
-                            sigma_limit=mult * model.grid.inner_min)
-        sweep.append({"sigma_limit_lixels": mult,
+                            sigma_limit=mult * unit, tuning=tuning)
+        sweep.append({"sigma_limit_m": mult * unit,
                       "js": js_divergence(hist(r["sensor"]), h_exact),
                       "fallback": float(r["fallback"].float().mean())})
     ok = [s_ for s_ in sweep if s_["js"] <= args.js_target]
-    chosen = (max(ok, key=lambda s_: s_["sigma_limit_lixels"]) if ok
+    chosen = (max(ok, key=lambda s_: s_["sigma_limit_m"]) if ok
               else min(sweep, key=lambda s_: s_["js"]))
-    limit = chosen["sigma_limit_lixels"] * model.grid.inner_min
+    limit = chosen["sigma_limit_m"]
 
     def learned(use_network=True):
         return model.propagate(ph, seed=99, scene=scene, max_interactions=MAX_INTERACTIONS,
-                               use_network=use_network, sigma_limit=limit)
+                               use_network=use_network, sigma_limit=limit, tuning=tuning)
 
     learned()
     ev = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
@@ -656,7 +669,7 @@ def run_surrogate(args, world, rank, local):
     ev[3].record()
     torch.cuda.synchronize()
     fwd_ms = ev[2].elapsed_time(ev[3]) / 5
-    tc_flops = 2.0 * (3 * 256 * 256 + 256 * 80) * x.shape[0]   # the tensor-core layers
+    tc_flops = 2.0 * (128 * 256 + 3 * 256 * 256 + 256 * 80) * x.shape[0]   # tensor-core layers
     r_null = model.propagate(ph, seed=99, use_network=False, sigma_limit=1e9)
     js_net = js_divergence(hist(r_net["sensor"]), h_exact)
     js_null = js_divergence(hist(r_null["sensor"]), h_exact)
@@ -676,9 +689,11 @@ def run_surrogate(args, world, rank, local):
             "n_gpus": world, "steps": 1, "warmup": 1, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "bf16", "data": "synthetic",
             "config": {"workload": "learned surrogate on the light-field telescope (config 4)",
+                       "mode": args.surrogate_mode,
                        "train_photons": args.train_photons, "epochs": args.epochs,
                        "eval_photons": n, "max_interactions": MAX_INTERACTIONS,
-                       "network": "5-256x4 SiLU-73, 8-component mixture, BF16 on tcgen05"},
+                       "network": "5 inputs (sin/cos-encoded to 128) -256x4 SiLU-73, 8-component "
+                                  "mixture, BF16 on tcgen05"},
             "exact_fp64": {"value": n / (ms_exact * 1e-3), "unit": "photons/s"},
             "speedup_over_exact": ms_exact / ms_net,
             "lixel_js": {"surrogate": js_net, "without_network": js_null,
@@ -719,6 +734,10 @@ def main():
     ap.add_argument("--train-photons", type=int, default=200_000_000)
     ap.add_argument("--epochs", type=int, default=8)
     ap.add_argument("--js-target", type=float, default=1e-3)
+    ap.add_argument("--surrogate-mode", choices=["plane", "lookup"], default="plane",
+                    help="plane: the network models the photon 5 cm below the lens array and the "
+                         "exact tracer carries it through the light-field sensor; lookup: the "
+                         "network models the final hit and the lixel is looked up")
     args = ap.parse_args()
     world, rank, local = init_dist()
     try:

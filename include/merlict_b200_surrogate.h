@@ -122,7 +122,9 @@ typedef struct mlgpu_sg_sensor_grid {
  * inputs lie outside [-in_limit, in_limit] or whose chosen component has a
  * position sigma (metres) above `sigma_limit` is flagged for exact tracing
  * (fallback[i] = 1, sensor -1).  Outputs: sensor, x, y (target plane),
- * direction x, y, fallback.                                              */
+ * direction x, y, fallback.  With grid = NULL there is no lookup: a photon
+ * that reaches gets sensor -2 and its sampled plane point and direction are
+ * for the caller to trace on (the exact tracer as the sensor lookup).    */
 int mlgpu_sg_sample(const float* outputs, const float* inputs, uint32_t n,
                     const float* linear, const float* scale, float in_limit, float sigma_limit,
                     uint64_t seed, uint64_t photon_offset, const mlgpu_sg_sensor_grid* grid,

@@ -875,7 +875,7 @@ sample_kernel(const float* __restrict__ out, const float* __restrict__ x, uint32
                 if (d < 2) sig_pos = fmaxf(sig_pos, s*scale[d]);
             }
             if (sig_pos > sigma_limit) fb = 1;
-            else sid = lookup_sensor(grid, t[0], t[1]);
+            else sid = grid.nx ? lookup_sensor(grid, t[0], t[1]) : -2;   // -2: reached the plane
         }
     }
     sensor[i] = fb ? -1 : sid;
@@ -1136,14 +1136,16 @@ int mlgpu_sg_sample(const float* outputs, const float* inputs, uint32_t n, const
                     uint64_t photon_offset, const mlgpu_sg_sensor_grid* grid, int32_t* sensor,
                     float* x, float* y, float* cx, float* cy, uint8_t* fallback,
                     void* cuda_stream) {
-    if (!outputs || !inputs || !linear || !scale || !grid || !sensor || !fallback)
+    if (!outputs || !inputs || !linear || !scale || !sensor || !fallback)
         return report_error(MLGPU_ERR_INVALID_ARGUMENT, "NULL argument");
-    if (!grid->center || !grid->rotation || !grid->inner || !grid->sensor_id ||
-        !grid->cell_start || !grid->cell_items || !(grid->cell > 0.0) || grid->nx == 0 ||
-        grid->ny == 0)
+    if (grid && (!grid->center || !grid->rotation || !grid->inner || !grid->sensor_id ||
+                 !grid->cell_start || !grid->cell_items || !(grid->cell > 0.0) ||
+                 grid->nx == 0 || grid->ny == 0))
         return report_error(MLGPU_ERR_INVALID_ARGUMENT, "incomplete sensor grid");
     if (n == 0) return MLGPU_OK;
     Grid g;
+    memset(&g, 0, sizeof(g));
+    if (grid) {
     g.num_sensors = grid->num_sensors;
     g.center = grid->center; g.rotation = grid->rotation; g.inner = grid->inner;
     g.sensor_id = grid->sensor_id;
@@ -1152,6 +1154,7 @@ int mlgpu_sg_sample(const float* outputs, const float* inputs, uint32_t n, const
     g.cell_start = grid->cell_start; g.cell_items = grid->cell_items;
     for (int k = 0; k < 2; k++) {
         g.hu[k] = (float)grid->hex_u[k]; g.hv[k] = (float)grid->hex_v[k]; g.hw[k] = (float)grid->hex_w[k];
+    }
     }
     sample_kernel<<<(n + 255)/256, 256, 0, static_cast<cudaStream_t>(cuda_stream)>>>(
         outputs, inputs, n, linear, scale, in_limit, sigma_limit, seed, photon_offset, g, sensor,

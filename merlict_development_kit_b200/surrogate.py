@@ -197,6 +197,30 @@ class Source:
                                            lambda_min=self.lambda_min, lambda_max=self.lambda_max)
 
 
+def training_data_plane(scene: engine.Scene, source: Source, n: int, seed: int, plane_z: float,
+                        chunk: int = 1 << 24) -> dict:
+    """Photons of `source` traced exactly (FP64) through their first
+    interaction: a photon "reaches" if it was reflected upwards below the
+    plane z = plane_z; its targets are where it crosses that plane and its
+    direction (x, y) there."""
+    xs, ts, rs = [], [], []
+    for a in range(0, n, chunk):
+        m = min(chunk, n - a)
+        ph = source.photons(m, seed * 1000003 + a)
+        out = scene.propagate(ph, engine.PropagationConfig(1), engine.Philox(seed, photon_offset=a),
+                              outputs=("sensor", "info", "final_position", "final_direction"))
+        p, d = out["final_position"], out["final_direction"]
+        kind = out["info"] & 0xFF
+        ok = (kind == abi.REFLECTION_ON_SURFACE) & (d[:, 2] > 0.0) & (p[:, 2] < plane_z)
+        t = torch.where(ok, (plane_z - p[:, 2]) / d[:, 2].clamp_min(1e-12), torch.zeros_like(p[:, 2]))
+        xs.append(source.inputs(ph))
+        ts.append(torch.stack([p[:, 0] + d[:, 0] * t, p[:, 1] + d[:, 1] * t, d[:, 0], d[:, 1]],
+                              dim=1).float())
+        rs.append(ok.to(torch.uint8))
+        del ph, out
+    return {"inputs": torch.cat(xs), "targets": torch.cat(ts), "reached": torch.cat(rs)}
+
+
 def training_data(scene: engine.Scene, source: Source, n: int, seed: int,
                   max_interactions: int = 10, chunk: int = 1 << 24) -> dict:
     """Photons of `source` traced exactly (FP64): inputs, the final position
@@ -223,10 +247,17 @@ class Surrogate:
     """Parameters, Adam state and normalisation of one trained network."""
 
     def __init__(self, flat: abi.FlatScene, source: Source | None = None, seed: int = 0,
-                 device="cuda"):
+                 device="cuda", plane_z: float | None = None):
+        """With plane_z the network models the photon where it crosses the
+        plane z = plane_z on its way to the sensors (hit point and
+        direction), and the exact tracer carries each sampled photon on from
+        there ("plane" mode, for sensors with optics of their own such as a
+        light-field sensor); without, it models the final hit on a plane of
+        hexagonal sensors looked up exactly ("lookup" mode)."""
         self.device = torch.device(device)
         self.source = source or Source()
-        self.grid = SensorGrid(flat, device=device)
+        self.plane_z = plane_z
+        self.grid = SensorGrid(flat, device=device) if plane_z is None else None
         self.params = init_params(seed, device)
         self.images = torch.zeros(int(lib().mlgpu_sg_image_bytes()), dtype=torch.uint8,
                                   device=device)
@@ -324,7 +355,9 @@ class Surrogate:
     def sample(self, y: torch.Tensor, x: torch.Tensor, seed: int, photon_offset: int = 0,
                sigma_limit: float | None = None, in_limit: float = 1.0001) -> dict:
         n = x.shape[0]
-        sl = self.grid.inner_min if sigma_limit is None else sigma_limit
+        if sigma_limit is None:
+            sigma_limit = self.grid.inner_min if self.grid is not None else 2e-3
+        sl = sigma_limit
         out = {"sensor": torch.empty(n, dtype=torch.int32, device=self.device),
                "x": torch.empty(n, dtype=torch.float32, device=self.device),
                "y": torch.empty(n, dtype=torch.float32, device=self.device),
@@ -334,7 +367,8 @@ class Surrogate:
         check(lib().mlgpu_sg_sample(
             y.contiguous().data_ptr(), x.contiguous().data_ptr(), n, self.linear.data_ptr(),
             self.scale.data_ptr(), float(in_limit), float(sl), seed & 0xFFFFFFFFFFFFFFFF,
-            photon_offset, C.byref(self.grid.struct), out["sensor"].data_ptr(),
+            photon_offset, C.byref(self.grid.struct) if self.grid is not None else None,
+            out["sensor"].data_ptr(),
             out["x"].data_ptr(), out["y"].data_ptr(), out["cx"].data_ptr(), out["cy"].data_ptr(),
             out["fallback"].data_ptr(), None))
         return out
@@ -350,13 +384,18 @@ class Surrogate:
         return y
 
     def propagate(self, photons: dict, seed: int, scene: engine.Scene | None = None,
-                  max_interactions: int = 10, chunk: int = 1 << 22, use_network: bool = True,
-                  sigma_limit: float | None = None) -> dict:
-        """Sensor of every photon: sampled from the network, with the photons
-        it flags traced exactly by `scene` (if given)."""
+                  max_interactions: int = 10, chunk: int = 1 << 23, use_network: bool = True,
+                  sigma_limit: float | None = None, tuning: dict | None = None) -> dict:
+        """Sensor of every photon: sampled from the network (in plane mode
+        carried on from the plane by `scene`'s exact tracer, in one call for
+        the whole batch), with the photons it flags traced exactly by
+        `scene` (if given).  `tuning` goes to those tracer calls."""
         n = int(photons["wavelength"].shape[0])
         sensor = torch.empty(n, dtype=torch.int32, device=self.device)
         fallback = torch.empty(n, dtype=torch.uint8, device=self.device)
+        plane = self.plane_z is not None and scene is not None
+        if plane:
+            pxy = torch.empty((n, 4), dtype=torch.float32, device=self.device)
         for a in range(0, n, chunk):
             b = min(n, a + chunk)
             part = {k: v[a:b] for k, v in photons.items()}
@@ -365,12 +404,35 @@ class Surrogate:
             s = self.sample(y, x, seed, a, sigma_limit=sigma_limit)
             sensor[a:b] = s["sensor"]
             fallback[a:b] = s["fallback"]
+            if plane:
+                pxy[a:b] = torch.stack([s["x"], s["y"], s["cx"], s["cy"]], dim=1)
+            del x, y, s
+        if plane:
+            # every sampled photon, carried on from the plane by the exact tracer
+            idx = torch.nonzero(sensor == -2, as_tuple=False).flatten()
+            if idx.numel():
+                q = pxy[idx].double()
+                cz = torch.sqrt(torch.clamp(1.0 - q[:, 2] * q[:, 2] - q[:, 3] * q[:, 3], min=0.0))
+                sub = {"support_x": q[:, 0].contiguous(), "support_y": q[:, 1].contiguous(),
+                       "support_z": torch.full_like(cz, self.plane_z),
+                       "direction_x": q[:, 2].contiguous(), "direction_y": q[:, 3].contiguous(),
+                       "direction_z": cz,
+                       "wavelength": photons["wavelength"][idx].double().contiguous()}
+                del q
+                r = scene.propagate(sub, engine.PropagationConfig(max(1, max_interactions - 1)),
+                                    engine.Philox(seed ^ 0x2545F491), outputs=("sensor",),
+                                    tuning=tuning)
+                sensor[idx] = r["sensor"]
+                del sub, r
+            sensor[sensor == -2] = -1
+            del pxy
         if scene is not None:
             idx = torch.nonzero(fallback, as_tuple=False).flatten()
             if idx.numel():
                 sub = {k: v[idx].contiguous() for k, v in photons.items()}
                 r = scene.propagate(sub, engine.PropagationConfig(max_interactions),
-                                    engine.Philox(seed ^ 0x5DEECE66D), outputs=("sensor",))
+                                    engine.Philox(seed ^ 0x5DEECE66D), outputs=("sensor",),
+                                    tuning=tuning)
                 sensor[idx] = r["sensor"]
         sync_errors()
         return {"sensor": sensor, "fallback": fallback}
