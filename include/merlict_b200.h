@@ -349,6 +349,30 @@ int mlgpu_corsika_photons(
     uint64_t* num_photons,
     void* cuda_stream);
 
+/* ---- calibration statistics ----------------------------------------------- *
+ * Replaces plenoscope::calibration::LixelStatisticsFiller (merlict_portal_
+ * plenoscope/calibration/LixelStatisticsFiller.cpp:20-62): for every sensor
+ * s, of the photons with sensor[i] == s in their order i, the count and the
+ * online mean and standard deviation (OnlineStatistics.cpp:15-50, variance
+ * m2/n) of cx, cy (incident direction), x, y (support on the aperture) and
+ * time_delay.  statistics[s][12] receives LixelStatistic's fields as merlict
+ * computes them: efficiency = count/photons_emitted_per_lixel,
+ * efficiency_std = sqrt(count)/photons_emitted_per_lixel, then cx, cy, x,
+ * y, time_delay as (mean, std) pairs (NaN where merlict's are NaN).
+ * Device pointers; asynchronous on `cuda_stream`.                        */
+int mlgpu_lixel_statistics(
+    mlgpu_scene* scene,
+    const int32_t* sensor,
+    const float* cx,
+    const float* cy,
+    const float* x,
+    const float* y,
+    const float* time_delay,
+    uint64_t num_photons,
+    double photons_emitted_per_lixel,
+    float* statistics,
+    void* cuda_stream);
+
 /* ---- tuning ------------------------------------------------------------ *
  * No counterpart in the reference (merlict has no device parameters).
  * Picks the wavefront knobs of `base` (pool_size, check_period, use_graph,

@@ -28,6 +28,7 @@ EXTRA = {
     "bin.cu": ["--fmad=false"],
     "wavefront_fp64.cu": ["--fmad=false"],
     "corsika.cu": ["--fmad=false"],
+    "lixel_stats.cu": ["--fmad=false"],
 }
 
 

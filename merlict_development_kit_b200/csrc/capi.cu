@@ -132,6 +132,7 @@ struct mlgpu_scene {
     DeviceBuffer staging_in, staging_out, staging_hist, staging_rng, bin_scratch, tune_out;
     DeviceBuffer order;                  // tracing order of a batch and its sort scratch
     DeviceBuffer corsika;                // bunch counts, offsets and the total
+    DeviceBuffer stats;                  // sort buffers of the calibration statistics
     // ray pools of the wavefront tracers
     DeviceBuffer wave;
     WaveCounters* wave_host = nullptr;   // pinned copy of the counters
@@ -654,6 +655,7 @@ int mlgpu_scene_destroy(mlgpu_scene* scene) {
     scene->tune_out.release();
     scene->order.release();
     scene->corsika.release();
+    scene->stats.release();
     scene->wave.release();
     if (scene->wave_host) cudaFreeHost(scene->wave_host);
     if (scene->wave_graph) cudaGraphExecDestroy(scene->wave_graph);
@@ -814,6 +816,30 @@ int mlgpu_corsika_photons(mlgpu_scene* scene, const float* bunches, uint64_t n,
                               scene->wave_grid, stream);
     if (e != cudaSuccess) return cuda_fail(e, "bunch expansion kernel");
     scene->launches += 1;
+    return MLGPU_OK;
+}
+
+int mlgpu_lixel_statistics(mlgpu_scene* scene, const int32_t* sensor, const float* cx,
+                           const float* cy, const float* x, const float* y,
+                           const float* time_delay, uint64_t n, double emitted,
+                           float* statistics, void* cuda_stream) {
+    if (!scene || !statistics) return fail(MLGPU_ERR_INVALID_ARGUMENT, "NULL argument");
+    if (n > 0 && (!sensor || !cx || !cy || !x || !y || !time_delay))
+        return fail(MLGPU_ERR_INVALID_ARGUMENT, "NULL photon array");
+    if (n >= (1ull << 31))
+        return fail(MLGPU_ERR_INVALID_ARGUMENT, "at most 2^31 - 1 photons per call");
+    if (!(emitted > 0.0))
+        return fail(MLGPU_ERR_INVALID_ARGUMENT, "photons_emitted_per_lixel must be > 0");
+    const size_t bytes = lixel_stats_scratch_bytes(n);
+    MLGPU_CUDA(scene->stats.reserve(bytes));
+    if (!scene->wave_grid) scene->wave_grid = wave_persistent_blocks();
+    const float* values[5] = {cx, cy, x, y, time_delay};
+    const cudaError_t e = launch_lixel_stats(sensor, values, n, (uint32_t)scene->dev.num_sensors,
+                                             emitted, statistics, scene->stats.ptr,
+                                             scene->stats.bytes, scene->wave_grid,
+                                             static_cast<cudaStream_t>(cuda_stream));
+    if (e != cudaSuccess) return cuda_fail(e, "calibration statistics");
+    scene->launches += 3;
     return MLGPU_OK;
 }
 

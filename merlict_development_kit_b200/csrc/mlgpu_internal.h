@@ -220,6 +220,12 @@ cudaError_t launch_corsika_count(const float* bunches, uint64_t n, const DevRng&
 cudaError_t launch_corsika_expand(const float* bunches, uint64_t n, const int32_t* ids,
                                   void* scratch, double* const* planes, int32_t* out_id, int grid,
                                   cudaStream_t s);
+// Per-sensor calibration statistics (lixel_stats.cu): `values` = cx, cy,
+// x, y, time delay; `out` [num_sensors][12].
+size_t lixel_stats_scratch_bytes(uint64_t n);
+cudaError_t launch_lixel_stats(const int32_t* sensor, const float* const* values, uint64_t n,
+                               uint32_t num_sensors, double emitted, float* out, void* scratch,
+                               size_t scratch_bytes, int grid, cudaStream_t s);
 // A coherent tracing order of a photon batch (photon_order.cu): `order`
 // receives n photon indices; `scratch` holds photon_order_scratch_bytes(n).
 size_t photon_order_scratch_bytes(uint64_t n);

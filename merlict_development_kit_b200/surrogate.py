@@ -436,3 +436,32 @@ class Surrogate:
                 sensor[idx] = r["sensor"]
         sync_errors()
         return {"sensor": sensor, "fallback": fallback}
+
+
+def _forward_probe(n: int, repeats: int = 3) -> None:
+    """Times the forward pass of an untrained network on the light-field
+    telescope on n random inputs (the tensor-core layers' throughput)."""
+    from . import factories
+    model = Surrogate(factories.light_field_telescope().flatten(), seed=1)
+    x = torch.rand((n, IN_LD), device=model.device) * 2.0 - 1.0
+    model.forward(x)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(repeats):
+        model.forward(x)
+    e1.record()
+    torch.cuda.synchronize()
+    sync_errors()
+    ms = e0.elapsed_time(e1) / repeats
+    flops = 2.0 * sum(fin * (80 if fout == 73 else fout) for fin, fout in LAYERS) * n
+    print(f"forward of {n} photons: {ms:.3f} ms, {flops / ms / 1e9:.1f} TFLOP/s on the "
+          f"tensor-core layers, {n / ms / 1e3:.1f} M photons/s")
+
+
+if __name__ == "__main__":
+    import sys
+    if len(sys.argv) >= 3 and sys.argv[1] == "forward":
+        _forward_probe(int(sys.argv[2]))
+    else:
+        print("usage: python -m merlict_development_kit_b200.surrogate forward N")

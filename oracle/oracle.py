@@ -263,3 +263,19 @@ def corsika_photons_numpy(bunches: np.ndarray, uniforms: np.ndarray) -> dict:
             "direction_x": rep(cx / dn), "direction_y": rep(cy / dn), "direction_z": rep(cz / dn),
             "wavelength": rep(np.abs(b[:, 7] * 1e-9)),
             "id": rep(np.arange(b.shape[0], dtype=np.int32))}
+
+
+def lixel_statistics_reference(sensor, cx, cy, x, y, t, num_lixel: int, num_blocks: int,
+                               photons_per_block: int) -> np.ndarray:
+    """merlict's own LixelStatisticsFiller (through the harness) on one block
+    of per-photon results; returns [num_lixel][12] float32."""
+    L = C.CDLL(HARNESS_SO)
+    arrs = [np.ascontiguousarray(sensor, dtype=np.int32)] + [
+        np.ascontiguousarray(a, dtype=np.float32) for a in (cx, cy, x, y, t)]
+    out = np.zeros((num_lixel, 12), np.float32)
+    L.ref_lixel_statistics.argtypes = [C.c_void_p] * 6 + [C.c_uint64] * 4 + [C.c_void_p]
+    st = L.ref_lixel_statistics(*[a.ctypes.data for a in arrs], arrs[0].size, num_lixel,
+                                num_blocks, photons_per_block, out.ctypes.data)
+    if st != 0:
+        raise RuntimeError("reference statistics failed")
+    return out

@@ -32,6 +32,7 @@
 #include "merlict/merlict.h"
 #include "merlict/scenery/segmented_imaging_reflector/segmented_imaging_reflector.h"
 #include "merlict_corsika/PhotonFactory.h"
+#include "merlict_portal_plenoscope/calibration/LixelStatisticsFiller.h"
 #include "merlict_multi_thread/merlict_multi_thread.h"
 #include "merlict_portal_plenoscope/light_field_sensor/LightFieldSensor.h"
 #include "merlict_b200.h"
@@ -635,6 +636,42 @@ int ref_corsika_photons(const float* bunches, uint64_t n, const double* uniforms
     } catch (const std::exception& e) {
         last_error = e.what();
         return MLGPU_ERR_INVALID_ARGUMENT;
+    }
+}
+
+// plenoscope::calibration::LixelStatisticsFiller on given per-photon results
+// (one block of n photons, in order): out[num_lixel][12] receives the
+// LixelStatistic fields.  sensor < 0: the photon reached no sensor.
+int ref_lixel_statistics(const int32_t* sensor, const float* cx, const float* cy, const float* x,
+                         const float* y, const float* t, uint64_t n, uint64_t num_lixel,
+                         uint64_t num_blocks, uint64_t photons_per_block, float* out) {
+    try {
+        std::vector<plenoscope::CalibrationPhotonResult> block(n);
+        for (uint64_t i = 0; i < n; i++) {
+            block[i].reached_sensor = sensor[i] >= 0;
+            block[i].lixel_id = sensor[i] >= 0 ? static_cast<uint32_t>(sensor[i]) : 0u;
+            block[i].x_tilt_vs_optical_axis = cx[i];
+            block[i].y_tilt_vs_optical_axis = cy[i];
+            block[i].x_pos_on_principal_aperture = x[i];
+            block[i].y_pos_on_principal_aperture = y[i];
+            block[i].time_of_flight = t[i];
+        }
+        plenoscope::calibration::LixelStatisticsFiller filler(num_lixel, num_blocks,
+                                                              photons_per_block);
+        filler.fill_in_block(block);
+        const std::vector<plenoscope::calibration::LixelStatistic> st =
+            filler.get_lixel_statistics();
+        for (uint64_t l = 0; l < num_lixel; l++) {
+            const plenoscope::calibration::LixelStatistic& a = st[l];
+            const float v[12] = {a.efficiency, a.efficiency_std, a.cx_mean, a.cx_std, a.cy_mean,
+                                 a.cy_std, a.x_mean, a.x_std, a.y_mean, a.y_std,
+                                 a.time_delay_mean, a.time_delay_std};
+            for (int k = 0; k < 12; k++) out[12*l + k] = v[k];
+        }
+        return 0;
+    } catch (const std::exception& e) {
+        last_error = e.what();
+        return MLGPU_ERR_RUNTIME;
     }
 }
 
