@@ -21,10 +21,11 @@ from __future__ import annotations
 import math
 from dataclasses import dataclass
 
-from .scenery import (ROT3_UNITY, UNIT_Z, Annulus, BiConvexLensHexBound, Cylinder, Disc,
-                      Frame, Func1, HexPlane, Plane, Rot3, Scenery, SphereCapWithHexagonalBound,
-                      SurfaceEntity, constant, deg2rad, hex_grid_annulus, hex_grid_flower, v_add,
-                      v_angle_in_between, v_cross, v_mul, v_norm, v_sub)
+from .scenery import (ROT3_UNITY, UNIT_X, UNIT_Y, UNIT_Z, Annulus, BiConvexLensHexBound,
+                      Cylinder, Disc, Frame, Func1, HexPlane, Plane, Rot3, Scenery, Sensor,
+                      SphereCapWithHexagonalBound, SurfaceEntity, constant, deg2rad,
+                      hex_grid_annulus, hex_grid_flower, hypot, v_add, v_angle_in_between,
+                      v_cross, v_div, v_dot, v_mul, v_norm, v_sub)
 
 
 # ---- segmented imaging reflector ---------------------------------------------
@@ -38,6 +39,28 @@ class ReflectorConfig:
     min_inner_aperture_radius: float = 0.2
     facet_inner_hex_radius: float = 0.30
     gap_between_facets: float = 0.01
+    outer_aperture_shape_hex: bool = False
+
+
+def hex_aperture_facets(outer: float, inner: float, spacing: float, max_outer_radius: float):
+    """Facet centres inside a hexagonal outer aperture and outside an inner
+    disc (Geometry.cpp:32-67)."""
+    unit_b = v_mul(UNIT_Y, spacing)
+    unit_a = v_mul(v_add(v_mul(UNIT_Y, 0.5), v_div(v_mul(UNIT_X, math.sqrt(3.0)), 2.0)), spacing)
+    unit_u = UNIT_X
+    unit_v = v_add(v_mul(UNIT_Y, math.sin(2.0 / 3.0 * math.pi)), v_mul(UNIT_X, math.cos(2.0 / 3.0 * math.pi)))
+    unit_w = v_add(v_mul(UNIT_Y, -math.sin(2.0 / 3.0 * math.pi)), v_mul(UNIT_X, math.cos(2.0 / 3.0 * math.pi)))
+    R = (math.sqrt(3.0) / 2.0) * outer
+    N = int(2.0 * math.ceil(max_outer_radius / spacing))
+    out = []
+    for a in range(-N, N + 1):
+        for b in range(-N, N + 1):
+            c = v_add(v_mul(unit_a, float(a)), v_mul(unit_b, float(b)))
+            u, v, w = v_dot(unit_u, c), v_dot(unit_v, c), v_dot(unit_w, c)
+            if (u < R and u > -R and v < R and v > -R and w < R and w > -R and
+                    hypot(c[0], c[1]) > inner):
+                out.append(c)
+    return out
 
 
 class ReflectorGeometry:
@@ -50,7 +73,10 @@ class ReflectorGeometry:
         spacing = self.facet_spacing
         outer = cfg.max_outer_aperture_radius - spacing / 2.0
         inner = cfg.min_inner_aperture_radius + spacing / 2.0
-        pos = hex_grid_annulus(outer, inner, spacing)
+        if cfg.outer_aperture_shape_hex:
+            pos = hex_aperture_facets(outer, inner, spacing, cfg.max_outer_aperture_radius)
+        else:
+            pos = hex_grid_annulus(outer, inner, spacing)
         pos = [(p[0], p[1], self.z_pos(math.sqrt(p[0] * p[0] + p[1] * p[1] + 0.0 * 0.0)))
                for p in pos]
         # move the dish until the mean facet distance to the focal point is f
@@ -190,55 +216,121 @@ class LightFieldSensorGeometry:
         return len(self.lixel_positions)
 
 
-def light_field_sensor(frame: Frame, scenery: Scenery, cfg: LightFieldSensorConfig):
-    """Factory::add_light_field_sensor_to_frame_in_scenery (Factory.cpp:235-249).
-    Adds the lixels as sensors 0..num_lixels-1 of `scenery`."""
-    g = LightFieldSensorGeometry(cfg)
-    front = frame.add(Frame("front", (0.0, 0.0, 0.0), ROT3_UNITY))
-    # lens array (Factory.cpp:16-37)
-    lens_array = front.add(Frame("lens_array", (0.0, 0.0, 0.0), ROT3_UNITY))
+# merlict's named colours the factory registers (merlict/Color.cpp); they
+# only matter for rendering, but their names take part in the scenery's
+# colour map and so in its duplicate-name errors.
+COLOR_WHITE, COLOR_GREEN, COLOR_GRAY, COLOR_RED = (255, 255, 255), (0, 255, 0), (128, 128, 128), (255, 0, 0)
+
+
+def _lens_array(frame: Frame, scenery: Scenery, g: "LightFieldSensorGeometry"):
+    """Factory::add_lens_array, Factory.cpp:16-37."""
+    scenery.colors.add("lens_white", COLOR_WHITE)
+    lens_array = frame.add(Frame("lens_array", (0.0, 0.0, 0.0), ROT3_UNITY))
     for i, pos in enumerate(g.pixel_grid):
         lens = lens_array.add(BiConvexLensHexBound(f"lens_{i}", pos, ROT3_UNITY))
-        lens.inner_refraction = cfg.lens_refraction
+        lens.inner_refraction = g.cfg.lens_refraction
         lens.set_curvature_radius_and_outer_hex_radius(
             g.pixel_lens_curvature_radius, g.pixel_lens_outer_aperture_radius)
-    # face plate (Factory.cpp:87-121)
+
+
+def _pixel_bin(frame: Frame, g: "LightFieldSensorGeometry", name: str, pos):
+    """Factory::add_pixel_bin_with_name_at_pos, Factory.cpp:58-85."""
+    b = frame.add(Frame(name, pos, ROT3_UNITY))
+    R = g.pixel_lens_inner_aperture_radius
+    h = g.bin_hight
+    for j in range(6):
+        phi = float(j) * 1.0 / 3.0 * math.pi
+        wall = b.add(Plane(f"{name}_{j}", (R * math.sin(phi), R * math.cos(phi), -0.5 * h),
+                           Rot3(-math.pi * 0.5, 0.0, phi)))
+        wall.set_x_y_width(g.pixel_lens_outer_aperture_radius, h)
+        wall.outer_reflection = g.cfg.bin_reflection
+
+
+def _pixel_bin_array(frame: Frame, scenery: Scenery, g: "LightFieldSensorGeometry"):
+    """Factory::add_pixel_bin_array, Factory.cpp:39-56."""
+    bins = frame.add(Frame("bin_array", (0.0, 0.0, g.pixel_plane_to_paxel_plane_distance),
+                           ROT3_UNITY))
+    scenery.colors.add("bin_wall_green", COLOR_GREEN)
+    for i, pos in enumerate(g.paxel_grid_centers):
+        _pixel_bin(bins, g, f"bin_{i}", pos)
+
+
+def _frontplate(frame: Frame, scenery: Scenery, g: "LightFieldSensorGeometry"):
+    """Factory::add_light_field_sensor_frontplate, Factory.cpp:87-124."""
+    scenery.colors.add("housing_gray", COLOR_GRAY)
     face_pos = hex_grid_annulus(g.max_outer_sensor_radius + g.pixel_spacing,
                                 g.max_outer_sensor_radius - g.pixel_lens_outer_aperture_radius,
                                 g.pixel_spacing)
-    face_plate = front.add(Frame("face_plate", (0.0, 0.0, 0.0), ROT3_UNITY))
+    face_plate = frame.add(Frame("face_plate", (0.0, 0.0, 0.0), ROT3_UNITY))
     for i, pos in enumerate(face_pos):
         face = face_plate.add(HexPlane(f"face_{i}", pos, ROT3_UNITY))
         face.set_outer_hex_radius(g.pixel_lens_outer_aperture_radius)
     ring = face_plate.add(Annulus("outer_front_ring", (0.0, 0.0, 0.0), ROT3_UNITY))
     ring.set_outer_inner_radius(g.outer_sensor_housing_radius, g.max_outer_sensor_radius)
-    # housing (Factory.cpp:153-189)
+
+
+def _lixel_sensor_plane(frame: Frame, scenery: Scenery, g: "LightFieldSensorGeometry", sensors):
+    """Factory::add_lixel_sensor_plane, Factory.cpp:126-151: lixel i is
+    sensor i."""
+    scenery.colors.add("cell_red", COLOR_RED)
+    lixels = frame.add(Frame("lixel_array", (0.0, 0.0, g.pixel_plane_to_paxel_plane_distance),
+                             ROT3_UNITY))
+    for i, pos in enumerate(g.lixel_positions):
+        lix = lixels.add(HexPlane(f"lixel_{i}", pos, Rot3(0.0, 0.0, g.lixel_z_orientation)))
+        lix.set_outer_hex_radius(g.lixel_outer_radius)
+        sensors.append(Sensor(i, lix))
+
+
+def _image_sensor_housing(frame: Frame, scenery: Scenery, g: "LightFieldSensorGeometry"):
+    """Factory::add_image_sensor_housing, Factory.cpp:153-189."""
+    scenery.colors.add("frontplate_gray", COLOR_GRAY)
     housing_height = .67 * g.outer_sensor_housing_radius
     housing = frame.add(Frame("sensor_housing", (0.0, 0.0, 0.0), ROT3_UNITY))
     top = housing.add(Disc("top", (0.0, 0.0, housing_height), ROT3_UNITY))
     top.set_radius(g.outer_sensor_housing_radius)
     cyl = housing.add(Cylinder("cylinder", (0.0, 0.0, 0.0), ROT3_UNITY))
     cyl.set_cylinder(g.outer_sensor_housing_radius, (0.0, 0.0, 0.0), (0.0, 0.0, housing_height))
-    # bins (Factory.cpp:39-85)
-    bins = frame.add(Frame("bin_array", (0.0, 0.0, g.pixel_plane_to_paxel_plane_distance), ROT3_UNITY))
-    R = g.pixel_lens_inner_aperture_radius
-    h = g.bin_hight
-    for i, pos in enumerate(g.paxel_grid_centers):
-        name = f"bin_{i}"
-        b = bins.add(Frame(name, pos, ROT3_UNITY))
-        for j in range(6):
-            phi = float(j) * 1.0 / 3.0 * math.pi
-            wall = b.add(Plane(f"{name}_{j}", (R * math.sin(phi), R * math.cos(phi), -0.5 * h),
-                               Rot3(-math.pi * 0.5, 0.0, phi)))
-            wall.set_x_y_width(g.pixel_lens_outer_aperture_radius, h)
-            wall.outer_reflection = cfg.bin_reflection
-    # lixels (Factory.cpp:123-151)
+
+
+def light_field_sensor(frame: Frame, scenery: Scenery, cfg: LightFieldSensorConfig,
+                       sensors: list | None = None):
+    """Factory::add_light_field_sensor_to_frame_in_scenery (Factory.cpp:191-207).
+    The lixels become sensors 0..num_lixels-1, appended to `sensors`
+    (default: the scenery's own sensors)."""
+    g = LightFieldSensorGeometry(cfg)
+    sensors = scenery.sensors if sensors is None else sensors
+    front = frame.add(Frame("front", (0.0, 0.0, 0.0), ROT3_UNITY))
+    _lens_array(front, scenery, g)
+    _frontplate(front, scenery, g)
+    _image_sensor_housing(frame, scenery, g)
+    _pixel_bin_array(frame, scenery, g)
+    _lixel_sensor_plane(frame, scenery, g, sensors)
+    return g
+
+
+def demonstration_light_field_sensor(frame: Frame, scenery: Scenery, cfg: LightFieldSensorConfig,
+                                     sensors: list | None = None):
+    """Factory::add_demonstration_light_field_sensor_to_frame_in_scenery
+    (Factory.cpp:209-266): one lens, one bin and the lixels of one pixel
+    (at 0.95 of their size)."""
+    g = LightFieldSensorGeometry(cfg)
+    sensors = scenery.sensors if sensors is None else sensors
+    scenery.colors.add("lens_white", COLOR_WHITE)
+    lens = frame.add(BiConvexLensHexBound("lens_0", (0.0, 0.0, 0.0), ROT3_UNITY))
+    lens.inner_refraction = cfg.lens_refraction
+    lens.set_curvature_radius_and_outer_hex_radius(
+        g.pixel_lens_curvature_radius, g.pixel_lens_outer_aperture_radius)
+    bins = frame.add(Frame("bin_array", (0.0, 0.0, g.pixel_plane_to_paxel_plane_distance),
+                           ROT3_UNITY))
+    scenery.colors.add("bin_wall_green", COLOR_GREEN)
+    _pixel_bin(bins, g, "bin_0", (0.0, 0.0, 0.0))
+    scenery.colors.add("light_field_sensor_cell_red", COLOR_RED)
     lixels = frame.add(Frame("lixel_array", (0.0, 0.0, g.pixel_plane_to_paxel_plane_distance),
                              ROT3_UNITY))
-    for i, pos in enumerate(g.lixel_positions):
+    for i, pos in enumerate(g.paxel_template):
         lix = lixels.add(HexPlane(f"lixel_{i}", pos, Rot3(0.0, 0.0, g.lixel_z_orientation)))
-        lix.set_outer_hex_radius(g.lixel_outer_radius)
-        scenery.add_sensor(i, lix)
+        lix.set_outer_hex_radius(0.95 * g.lixel_outer_radius)
+        sensors.append(Sensor(i, lix))
     return g
 
 

@@ -84,6 +84,165 @@ def isotropic_shell_source(n: int, seed: int, radius: float, aim_radius: float,
     return make_batch(sup, d, lam)
 
 
+# ---- merlict's own photon sources and photon tables -------------------------
+#
+# merlict::photon_source (merlict/Photons.cpp:83-127) and the raw photon
+# table (Photons.cpp:24-81, tsvio.cpp:80-132).  A merlict::Photon stores its
+# direction normalised (Ray.cpp:16-20); these sources store it the same way,
+# and the engine's own normalisation at intake then finds a unit vector.
+
+def _normalized(d: np.ndarray) -> np.ndarray:
+    """Vec3::normalize (Vec3.cpp:20-26): each component / sqrt(x x + y y + z z)."""
+    n = np.sqrt(d[:, 0] * d[:, 0] + d[:, 1] * d[:, 1] + d[:, 2] * d[:, 2])
+    return d / n[:, None]
+
+
+def point_like_towards_z_opening_angle_num_photons(opening_angle: float, num_photons: int,
+                                                   prng) -> dict:
+    """Photons from the origin into a cone of half angle `opening_angle`
+    around +z, uniform in solid angle, 433 nm, id = index (Photons.cpp:85-106,
+    SpherePointPicker.cpp:8-44).  Each photon draws the azimuth first, then
+    the zenith distance, from `prng` (a prng.Mt19937)."""
+    import math
+    n = int(num_photons)
+    u = prng.uniforms(2 * n).reshape(n, 2) if n else np.zeros((0, 2))
+    z_min = (math.cos(0.0) + 1.0) / 2.0
+    z_range = (math.cos(float(opening_angle)) + 1.0) / 2.0 - z_min
+    d = np.empty((n, 3))
+    two_pi = 2 * math.pi
+    for i in range(n):
+        az = two_pi * float(u[i, 0]) + 0.0
+        zd = math.acos(2.0 * (z_range * float(u[i, 1]) + z_min) - 1.0)
+        sin_zd = math.sin(zd)
+        d[i] = (sin_zd * math.cos(az), sin_zd * math.sin(az), math.cos(zd))
+    return make_batch(np.zeros((n, 3)), _normalized(d), np.full(n, 433e-9))
+
+
+def parallel_towards_z_from_xy_disc(disc_radius: float, num_photons: int, prng) -> dict:
+    """Photons along +z from points uniform on the xy disc of `disc_radius`,
+    433 nm, id = index (Photons.cpp:108-125).  Points come from rejection
+    sampling of pairs of draws (Generator.cpp:22-34)."""
+    n = int(num_photons)
+    r = float(disc_radius)
+    r_sq = r * r
+    xs, ys = [], []
+    have = 0
+    while have < n:
+        pairs = max(64, int((n - have) * 1.3) + 16)
+        saved = prng.getstate()
+        u = prng.uniforms(2 * pairs).reshape(pairs, 2)
+        x = r * (u[:, 0] * 2.0 - 1.0)
+        y = r * (u[:, 1] * 2.0 - 1.0)
+        ok = ~(x * x + y * y > r_sq)
+        idx = np.flatnonzero(ok)
+        if have + len(idx) > n:
+            # consume only the pairs up to the last photon's, as merlict does
+            idx = idx[:n - have]
+            prng.setstate(saved)
+            prng.uniforms(2 * (int(idx[-1]) + 1))
+        xs.append(x[idx])
+        ys.append(y[idx])
+        have += len(idx)
+    sx = np.concatenate(xs) if xs else np.zeros(0)
+    sy = np.concatenate(ys) if ys else np.zeros(0)
+    sup = np.stack([sx, sy, np.zeros(n)], axis=1)
+    d = np.zeros((n, 3))
+    d[:, 2] = 1.0
+    return make_batch(sup, _normalized(d), np.full(n, 433e-9))
+
+
+def transform_photons(batch: dict, T) -> dict:
+    """Ray::transform (Ray.cpp:40-43) with the 3x4 transformation T of
+    HomTra3::set_transformation: supports by HomTra3::position, directions
+    by HomTra3::orientation (HomTra3.cpp:154-200), in merlict's order of
+    operations."""
+    sx, sy, sz = batch["support_x"], batch["support_y"], batch["support_z"]
+    dx, dy, dz = batch["direction_x"], batch["direction_y"], batch["direction_z"]
+    out = dict(batch)
+    out["support_x"] = sx * T[0][0] + sy * T[0][1] + sz * T[0][2] + T[0][3]
+    out["support_y"] = sx * T[1][0] + sy * T[1][1] + sz * T[1][2] + T[1][3]
+    out["support_z"] = sx * T[2][0] + sy * T[2][1] + sz * T[2][2] + T[2][3]
+    out["direction_x"] = dx * T[0][0] + dy * T[0][1] + dz * T[0][2]
+    out["direction_y"] = dx * T[1][0] + dy * T[1][1] + dz * T[1][2]
+    out["direction_z"] = dx * T[2][0] + dy * T[2][1] + dz * T[2][2]
+    return out
+
+
+def raw_matrix2photons(rows) -> dict:
+    """Rows of [id, support x y z, direction x y z, wavelength] to photons
+    (Photons.cpp:24-81).  A row that does not have exactly 8 columns, or a
+    wavelength <= 0, raises ValueError.  The id column is a double in
+    merlict; here it is kept as int32 after a check that it is integral."""
+    m = [list(r) for r in rows]
+    for r in m:
+        if len(r) != 8:
+            raise ValueError("PhotonBunch, raw row of doubles to photon. Expected row to "
+                             f"have exactly 8 columns, but actual it has {len(r)} columns.")
+    a = np.asarray(m, dtype=np.float64).reshape(-1, 8)
+    ids = a[:, 0]
+    if np.any(ids != np.floor(ids)) or np.any(np.abs(ids) > 2**31 - 1):
+        raise ValueError("photon ids must be integers that fit in 32 bits")
+    return make_batch(a[:, 1:4], _normalized(a[:, 4:7]) if len(a) else a[:, 4:7], a[:, 7],
+                      ids.astype(np.int32))
+
+
+def photons2raw_matrix(batch: dict) -> np.ndarray:
+    """Photons to rows of [id, support, direction, wavelength] (Photons.cpp:33-59)."""
+    return np.stack([np.asarray(batch["id"], dtype=np.float64)] +
+                    [np.asarray(batch[k], dtype=np.float64) for k in PLANES], axis=1)
+
+
+def _to_double(token: str) -> float:
+    """txt::to_double (txt.cpp:108-125): the whole token must parse as a
+    number (strtod's syntax: decimal, hexadecimal, inf, nan)."""
+    t = token
+    low = t.lower().lstrip("+-")
+    try:
+        if "_" in t or not t:
+            raise ValueError
+        if low.startswith("0x"):
+            return float.fromhex(t)
+        return float(t)
+    except ValueError:
+        raise ValueError(f"txt::to_double: Can not parse '{token}' to double.") from None
+
+
+def gen_table_from_string(text: str) -> list:
+    """tsvio::TableReader (tsvio.cpp:80-132): one row per line, tokens split
+    at tabs and spaces, blank lines and lines starting with '#' skipped."""
+    table = []
+    for row_number, line in enumerate(text.split("\n"), start=1):
+        row = line.strip()
+        if not row or row[0] == "#":
+            continue
+        tokens = [t for t in row.replace("\t", " ").split(" ") if t]
+        numeric = []
+        for col, tok in enumerate(tokens, start=1):
+            try:
+                numeric.append(_to_double(tok))
+            except ValueError as e:
+                raise ValueError(f"TableReader: Can not convert item '{tok}' into a floating "
+                                 f"point number in row {row_number} and column {col}. {e}") from None
+        table.append(numeric)
+    return table
+
+
+def gen_table_from_file(path: str) -> list:
+    """tsvio::gen_table_from_file (tsvio.cpp:13-36)."""
+    try:
+        with open(path, "r") as f:
+            text = f.read()
+    except OSError:
+        raise RuntimeError(f"tsvio::gen_table_from_file Can not open file '{path}'.") from None
+    return gen_table_from_string(text)
+
+
+def load_photon_table(path: str) -> dict:
+    """A photon file of merlict's propagation program: raw_matrix2photons of
+    the table at `path` (merlict_tests/apps/propagate.cpp:63-64)."""
+    return raw_matrix2photons(gen_table_from_file(path))
+
+
 SPEED_OF_LIGHT = 299792458.0             # merlict/PhysicalConstants.h:7
 PRODUCTION_DISTANCE_OFFSET = 1e3         # merlict_corsika/PhotonFactory.cpp:51-57
 

@@ -63,10 +63,18 @@ def v_octant(a):
     return 4 * (a[0] >= 0.0) + 2 * (a[1] >= 0.0) + 1 * (a[2] >= 0.0)
 
 
+def c_acos(x: float) -> float:
+    """acos with C's domain behaviour: NaN outside [-1, 1]."""
+    return math.acos(x) if -1.0 <= x <= 1.0 else math.nan
+
+
 def v_angle_in_between(a, b):
     an = v_div(a, v_norm(a))
     bn = v_div(b, v_norm(b))
-    return math.acos(v_dot(an, bn))
+    return c_acos(v_dot(an, bn))
+
+
+MAX_DEVIATION_EQUAL_VEC3_SQUARE = 1e-14   # merlict/Vec3.h:45
 
 
 ORIGIN = (0.0, 0.0, 0.0)
@@ -577,10 +585,35 @@ class Triangle(SurfaceEntity):
     primitive = abi.PRIM_TRIANGLE
 
     def set_corners_in_xy_plane(self, ax, ay, bx, by, cx, cy):
-        self.A, self.B, self.C = (ax, ay), (bx, by), (cx, cy)
+        """Triangle.cpp:9-22: every edge longer than zero."""
+        self.A, self.B, self.C = ((float(ax), float(ay)), (float(bx), float(by)),
+                                  (float(cx), float(cy)))
+
+        def edge(p, q):
+            return math.sqrt((p[0] - q[0]) * (p[0] - q[0]) + (p[1] - q[1]) * (p[1] - q[1]))
+        for length, name in ((edge(self.A, self.B), "AB"), (edge(self.C, self.A), "AC"),
+                             (edge(self.C, self.B), "CB")):
+            if not length > 0.0:
+                raise ValueError(f"Triangle: expected edge length of {name} > 0.0, "
+                                 f"but actual {length}m")
         norms = [math.sqrt(p[0] * p[0] + p[1] * p[1]) for p in (self.A, self.B, self.C)]
         self.bounding_sphere_radius = max(norms)
         return self
+
+    def set_normal_and_3_vertecies(self, normal, a, b, c):
+        """Triangle.cpp:24-57: the frame at the centroid, rotated so that its
+        z axis is the facet normal; the corners in that frame's xy plane."""
+        pos = v_div(v_add(v_add(a, b), c), 3.0)
+        a, b, c = v_sub(a, pos), v_sub(b, pos), v_sub(c, pos)
+        d = v_sub(normal, UNIT_Z)
+        if v_dot(d, d) > MAX_DEVIATION_EQUAL_VEC3_SQUARE:
+            rot = Rot3(axis=v_cross(UNIT_Z, normal), angle=v_angle_in_between(UNIT_Z, normal))
+            inv = t_inverse(t_from_rot_pos(rot, ORIGIN))
+            a, b, c = t_orientation(inv, a), t_orientation(inv, b), t_orientation(inv, c)
+        else:
+            rot = ROT3_UNITY
+        self.set_name_pos_rot(self.name, pos, rot)
+        return self.set_corners_in_xy_plane(a[0], a[1], b[0], b[1], c[0], c[1])
 
     def params(self):
         return [self.A[0], self.A[1], self.B[0], self.B[1], self.C[0], self.C[1], 0.0, 0.0]
@@ -589,8 +622,26 @@ class Triangle(SurfaceEntity):
 class Cylinder(SurfaceEntity):
     primitive = abi.PRIM_CYLINDER
 
+    def set_radius_and_length(self, radius, length):
+        """Cylinder.cpp:68-72."""
+        self._set_radius(radius)
+        if not length > 0.0:
+            raise ValueError(f"The length of a cylinder must be larger than 0.0m, not {length}")
+        self.length = float(length)
+        self.bounding_sphere_radius = hypot(0.5 * self.length, self.radius)
+        return self
+
+    def _set_radius(self, radius):
+        if not radius > 0.0:
+            raise ValueError(f"The radius of a cylinder must be larger than 0.0m, not {radius}")
+        self.radius = float(radius)
+
     def set_cylinder(self, radius, start, end):
-        """Cylinder.cpp:21-67: position at the middle, z axis along end-start."""
+        """Cylinder.cpp:17-67: position at the middle, z axis along end-start."""
+        self._set_radius(radius)
+        d = v_sub(start, end)
+        if v_dot(d, d) <= MAX_DEVIATION_EQUAL_VEC3_SQUARE:
+            raise ValueError("The start and end point of a cylinder must not be the same")
         axis = v_sub(end, start)
         pos = v_add(start, v_div(axis, 2.0))
         if axis[0] == 0.0 and axis[1] == 0.0 and abs(axis[2]) > 0.0:
@@ -746,12 +797,46 @@ class Sensor:
         self.frame = frame
 
 
+class NoSuchKey(KeyError):
+    """ResourceMap::NoSuchKey (merlict/scenery/ResourceMap.h)."""
+
+
+class KeyAlreadyInUse(KeyError):
+    """ResourceMap::KeyAlreadyInUse (merlict/scenery/ResourceMap.h)."""
+
+
+class ResourceMap:
+    """A map of named resources that refuses unknown and reused names
+    (ColorMap.cpp:8-37, FunctionMap.cpp:8-35, SensorMap.cpp:8-47)."""
+
+    def __init__(self, kind: str):
+        self.kind = kind
+        self.items: dict = {}
+
+    def has(self, key) -> bool:
+        return key in self.items
+
+    def get(self, key):
+        if key not in self.items:
+            raise NoSuchKey(f"There is no {self.kind} called '{key}'.")
+        return self.items[key]
+
+    def add(self, key, value):
+        if key in self.items:
+            raise KeyAlreadyInUse(f"The {self.kind} key '{key}' is already in use.")
+        self.items[key] = value
+        return value
+
+
 class Scenery:
-    """A root frame plus the sensors of the scene (merlict/scenery/Scenery.h)."""
+    """A root frame plus the sensors, colors and functions of the scene
+    (merlict/scenery/Scenery.h)."""
 
     def __init__(self):
         self.root = Frame("root", ORIGIN, Rot3(0.0, 0.0, 0.0))
         self.sensors: list[Sensor] = []
+        self.colors = ResourceMap("color")
+        self.functions = ResourceMap("function")
 
     def add_sensor(self, id: int, frame: Frame) -> Sensor:
         s = Sensor(id, frame)

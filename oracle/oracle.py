@@ -152,6 +152,14 @@ def harness():
         lib.ref_scene_flat.argtypes = [C.c_void_p, C.POINTER(abi.mlgpu_flat_scene)]
         lib.ref_scene_num_sensors.argtypes = [C.c_void_p]
         lib.ref_last_error.restype = C.c_char_p
+        lib.ref_scene_from_json.restype = C.c_void_p
+        lib.ref_scene_from_json.argtypes = [C.c_char_p, C.c_int]
+        lib.ref_scene_sensor_ids.argtypes = [C.c_void_p, C.c_void_p, C.c_int]
+        for name in ("ref_json_photons", "ref_table_photons"):
+            getattr(lib, name).restype = C.c_int64
+            getattr(lib, name).argtypes = [C.c_char_p, C.c_void_p, C.c_uint64]
+        lib.ref_json_propagation_config.argtypes = [C.c_char_p, C.POINTER(C.c_uint64)]
+        lib.ref_mt19937_uniforms.argtypes = [C.c_uint64, C.c_uint64, C.c_void_p]
         lib.ref_propagate.restype = C.c_int
         lib.ref_propagate.argtypes = [
             C.c_void_p, C.POINTER(abi.mlgpu_photons), C.c_uint64, C.c_uint32,
@@ -179,6 +187,25 @@ class RefScene:
             raise RuntimeError(self.lib.ref_last_error().decode())
         self.kind = kind
         self.params = tuple(params)
+
+    @classmethod
+    def from_json(cls, path: str, plenoscope: bool = False) -> "RefScene":
+        """A scenery read by the reference's own JSON reader (merlict's, or
+        with `plenoscope` its plenoscope extension)."""
+        self = cls.__new__(cls)
+        self.lib = harness()
+        self.h = self.lib.ref_scene_from_json(os.fspath(path).encode(), int(plenoscope))
+        if not self.h:
+            raise RuntimeError(self.lib.ref_last_error().decode())
+        self.kind = "json"
+        self.params = (os.fspath(path), bool(plenoscope))
+        return self
+
+    def sensor_ids(self) -> np.ndarray:
+        n = self.lib.ref_scene_sensor_ids(self.h, None, 0)
+        ids = np.zeros(max(n, 1), dtype=np.uint64)
+        self.lib.ref_scene_sensor_ids(self.h, ids.ctypes.data, n)
+        return ids[:n]
 
     def __del__(self):
         if getattr(self, "h", None):
@@ -279,3 +306,39 @@ def lixel_statistics_reference(sensor, cx, cy, x, y, t, num_lixel: int, num_bloc
     if st != 0:
         raise RuntimeError("reference statistics failed")
     return out
+
+
+def _ref_rows(fn, path: str) -> np.ndarray:
+    L = harness()
+    n = getattr(L, fn)(os.fspath(path).encode(), None, 0)
+    if n < 0:
+        raise RuntimeError(L.ref_last_error().decode())
+    rows = np.zeros((max(n, 1), 8))
+    getattr(L, fn)(os.fspath(path).encode(), rows.ctypes.data, n)
+    return rows[:n]
+
+
+def json_photons_reference(path: str) -> np.ndarray:
+    """merlict's json::load_photons, as rows [id, support, direction, wavelength]."""
+    return _ref_rows("ref_json_photons", path)
+
+
+def table_photons_reference(path: str) -> np.ndarray:
+    """merlict's raw_matrix2photons(tsvio::gen_table_from_file), as rows."""
+    return _ref_rows("ref_table_photons", path)
+
+
+def json_propagation_config_reference(path: str) -> int:
+    """merlict's json::load_PropagationConfig: max_num_interactions_per_photon."""
+    L = harness()
+    v = C.c_uint64(0)
+    if L.ref_json_propagation_config(os.fspath(path).encode(), C.byref(v)) != 0:
+        raise RuntimeError(L.ref_last_error().decode())
+    return int(v.value)
+
+
+def mt19937_uniforms_reference(seed: int, n: int) -> np.ndarray:
+    """merlict's Mt19937(seed).uniform(), n times."""
+    out = np.zeros(max(int(n), 1))
+    harness().ref_mt19937_uniforms(int(seed), int(n), out.ctypes.data)
+    return out[:int(n)]

@@ -35,6 +35,9 @@
 #include "merlict_portal_plenoscope/calibration/LixelStatisticsFiller.h"
 #include "merlict_multi_thread/merlict_multi_thread.h"
 #include "merlict_portal_plenoscope/light_field_sensor/LightFieldSensor.h"
+#include "merlict_json/json.h"
+#include "merlict_portal_plenoscope/json_to_plenoscope.h"
+#include "merlict_portal_plenoscope/PlenoscopeScenery.h"
 #include "merlict_b200.h"
 #include "merlict_b200_philox.h"
 #include "merlict_b200_shim.h"
@@ -46,7 +49,7 @@ namespace {
 thread_local std::string last_error;
 
 struct Handle {
-    ml::Scenery scenery;
+    plenoscope::PlenoscopeScenery scenery;
     std::vector<ml::sensor::Sensor*> owned_sensors;
     ml::sensor::Sensors sensors;
     merlict_b200::FlatScene flat;
@@ -673,6 +676,93 @@ int ref_lixel_statistics(const int32_t* sensor, const float* cx, const float* cy
         last_error = e.what();
         return MLGPU_ERR_RUNTIME;
     }
+}
+
+// A scenery read by the reference's own JSON readers: merlict's
+// (json.cpp:270-288; its sensors are the frames with a sensor_id, in the
+// order read) or, with plenoscope != 0, the plenoscope extension
+// (json_to_plenoscope.h:122-138; its sensors are the lixels of the one
+// light-field sensor).
+void* ref_scene_from_json(const char* path, int plenoscope) {
+    try {
+        std::unique_ptr<Handle> h(new Handle);
+        if (plenoscope) {
+            plenoscope::json::append_to_frame_in_scenery(&h->scenery.root, &h->scenery, path);
+            if (h->scenery.plenoscopes.size() != 1)
+                throw std::invalid_argument("expected exactly one plenoscope in the scenery");
+            ml::sensor::Sensors* channels = h->scenery.plenoscopes.at(0).light_field_channels;
+            for (ml::sensor::Sensor* s : channels->by_occurence) h->owned_sensors.push_back(s);
+            delete channels;   // the Sensor objects are kept in owned_sensors
+            h->scenery.plenoscopes.at(0).light_field_channels = nullptr;
+            h->sensors.init(h->owned_sensors);
+        } else {
+            ml::json::append_to_frame_in_scenery(&h->scenery.root, &h->scenery, path);
+            h->sensors.init(h->scenery.sensors.sensors);
+        }
+        h->scenery.root.init_tree_based_on_mother_child_relations();
+        return h.release();
+    } catch (const std::exception& e) {
+        last_error = e.what();
+        return nullptr;
+    }
+}
+
+// The ids of the scene's sensors, by index.
+int ref_scene_sensor_ids(void* handle, uint64_t* ids, int capacity) {
+    Handle* h = static_cast<Handle*>(handle);
+    const int n = static_cast<int>(h->sensors.by_occurence.size());
+    for (int i = 0; i < n && i < capacity; i++) ids[i] = h->sensors.by_occurence[i]->id;
+    return n;
+}
+
+// json::load_photons (json.cpp:543-562) as rows of photons2raw_matrix
+// (id, support, direction, wavelength); returns the number of photons, or
+// -1 on error.  Writes at most `capacity` rows.
+int64_t ref_json_photons(const char* path, double* rows, uint64_t capacity) {
+    try {
+        std::vector<ml::Photon> photons = ml::json::load_photons(path);
+        const std::vector<std::vector<double>> m = ml::photons2raw_matrix(&photons);
+        for (uint64_t i = 0; i < m.size() && i < capacity; i++)
+            for (int k = 0; k < 8; k++) rows[8*i + k] = m[i][k];
+        return static_cast<int64_t>(m.size());
+    } catch (const std::exception& e) {
+        last_error = e.what();
+        return -1;
+    }
+}
+
+// raw_matrix2photons of tsvio::gen_table_from_file (merlict_tests/apps/
+// propagate.cpp:63-64), back as raw rows.
+int64_t ref_table_photons(const char* path, double* rows, uint64_t capacity) {
+    try {
+        std::vector<ml::Photon> photons =
+            ml::raw_matrix2photons(ml::tsvio::gen_table_from_file(path));
+        const std::vector<std::vector<double>> m = ml::photons2raw_matrix(&photons);
+        for (uint64_t i = 0; i < m.size() && i < capacity; i++)
+            for (int k = 0; k < 8; k++) rows[8*i + k] = m[i][k];
+        return static_cast<int64_t>(m.size());
+    } catch (const std::exception& e) {
+        last_error = e.what();
+        return -1;
+    }
+}
+
+// json::load_PropagationConfig (json.cpp:510-517).
+int ref_json_propagation_config(const char* path, uint64_t* max_num_interactions_per_photon) {
+    try {
+        const ml::PropagationConfig cfg = ml::json::load_PropagationConfig(path);
+        *max_num_interactions_per_photon = cfg.max_num_interactions_per_photon;
+        return 0;
+    } catch (const std::exception& e) {
+        last_error = e.what();
+        return 1;
+    }
+}
+
+// merlict's Mt19937(seed).uniform(), n times (Mt19937.cpp:8-20).
+void ref_mt19937_uniforms(uint64_t seed, uint64_t n, double* out) {
+    ml::random::Mt19937 prng(seed);
+    for (uint64_t i = 0; i < n; i++) out[i] = prng.uniform();
 }
 
 int ref_hardware_concurrency(void) {
