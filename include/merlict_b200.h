@@ -32,7 +32,7 @@
 extern "C" {
 #endif
 
-#define MLGPU_ABI_VERSION 3
+#define MLGPU_ABI_VERSION 4
 
 /* ---- status codes ------------------------------------------------------ */
 enum {
@@ -371,6 +371,80 @@ int mlgpu_lixel_statistics(
     uint64_t num_photons,
     double photons_emitted_per_lixel,
     float* statistics,
+    void* cuda_stream);
+
+/* ---- the signal chain after binning --------------------------------------- *
+ * Replaces, for one event, the steps plenoscope_propagation.cpp:201-247
+ * chains after Sensors::assign_photons: signal_processing::
+ * get_photon_pipelines (PipelinePhoton.cpp:25-65), plenoscope::
+ * night_sky_background::inject_nsb_into_photon_pipeline (Injector.cpp:
+ * 8-98), PhotoElectricConverter::Converter::get_pulse_pipeline_for_photon_
+ * pipeline (PhotoElectricConverter.cpp:31-90) and extract_pulses
+ * (pulse_extraction.cpp:9-52).
+ *
+ * Photon i (device arrays) reached sensor[i] (< 0: none) at arrival_time[i]
+ * with wavelength[i] and simulation_truth_id truth_id[i]; sensor s is lixel
+ * s with calibrated efficiency lixel_efficiency[s] (float, as
+ * calibration::read_efficiencies gives it).  Func1 tables are merlict's
+ * Func1 points (x, y, slope) sorted by x, n of them, host memory: the
+ * quantum efficiency and the background light's inverse wavelength CDF
+ * (night_sky_background::Light::wavelength_probability, with its
+ * total integral); nsb_rate is Light::rate and num_lixel the light-field
+ * sensor's lixel count (Light.cpp:8-24).
+ *
+ * The draws: PHILOX only; stage s (1 background, 2 conversion, 3
+ * extraction) of lixel i draws uniforms k = 0, 1, ... of stream
+ * ((0xF0 | s) << 56) | (photon_offset + i) in the order merlict's code asks
+ * for them; a normal deviate is mean + std sqrt(-2 ln(1 - u1)) cos(2 pi u2).
+ *
+ * Output: channel c's pulses are arrival_time_slice / simulation_truth_id
+ * [channel_offset[c], channel_offset[c + 1]) (device, channel_offset has
+ * num_sensors + 1 entries) in merlict's order; nsb_count (device, may be
+ * NULL) the background photons of each lixel; num_pulses and
+ * nsb_exposure_start_time (host) are set.  The call waits for
+ * `cuda_stream` once; if num_pulses exceeds `capacity` only the offsets are
+ * written and MLGPU_ERR_INVALID_ARGUMENT is returned (call again with
+ * larger buffers).  A wavelength outside the quantum efficiency's table is
+ * MLGPU_ERR_OUT_OF_RANGE (merlict throws std::out_of_range);
+ * probability_for_second_puls >= 1 is MLGPU_ERR_INVALID_ARGUMENT.        */
+typedef struct mlgpu_signal_chain_config {
+    const double* quantum_efficiency;       /* Func1 points, host             */
+    uint32_t num_quantum_efficiency;
+    uint32_t num_nsb_wavelength_cdf;
+    const double* nsb_wavelength_cdf;       /* Func1 points, host             */
+    double nsb_total_integral;
+    double nsb_rate;                        /* 1/s into the whole sensor      */
+    double dark_rate;                       /* 1/s per lixel                  */
+    double probability_for_second_puls;     /* crosstalk, < 1                 */
+    double nsb_exposure_time;               /* s                              */
+    double time_slice_duration;             /* s                              */
+    double arrival_time_std;                /* single_photon_arrival_time_resolution, s */
+    uint32_t num_lixel;
+    uint32_t reserved;
+} mlgpu_signal_chain_config;
+
+typedef struct mlgpu_photon_stream {
+    uint64_t* channel_offset;               /* [num_sensors + 1], device      */
+    uint8_t* arrival_time_slice;            /* [capacity], device             */
+    int32_t* simulation_truth_id;           /* [capacity], device             */
+    int32_t* nsb_count;                     /* [num_sensors], device, or NULL */
+    uint64_t capacity;
+    uint64_t num_pulses;                    /* out                            */
+    double nsb_exposure_start_time;         /* out, s                         */
+} mlgpu_photon_stream;
+
+int mlgpu_signal_chain(
+    mlgpu_scene* scene,
+    const mlgpu_signal_chain_config* config,
+    const int32_t* sensor,
+    const double* arrival_time,
+    const double* wavelength,
+    const int32_t* truth_id,
+    uint64_t num_photons,
+    const float* lixel_efficiency,
+    uint32_t num_sensors,
+    const mlgpu_rng* rng,
+    mlgpu_photon_stream* out,
     void* cuda_stream);
 
 /* ---- tuning ------------------------------------------------------------ *

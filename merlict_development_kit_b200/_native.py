@@ -70,6 +70,10 @@ def lib():
             C.POINTER(abi.mlgpu_photon_buffers), C.POINTER(C.c_uint64), C.c_void_p]
         L.mlgpu_lixel_statistics.argtypes = [C.c_void_p] + [C.c_void_p] * 6 + [
             C.c_uint64, C.c_double, C.c_void_p, C.c_void_p]
+        L.mlgpu_signal_chain.argtypes = [
+            C.c_void_p, C.POINTER(abi.mlgpu_signal_chain_config)] + [C.c_void_p] * 4 + [
+            C.c_uint64, C.c_void_p, C.c_uint32, C.POINTER(abi.mlgpu_rng),
+            C.POINTER(abi.mlgpu_photon_stream), C.c_void_p]
         L.mlgpu_scene_autotune.argtypes = [
             C.c_void_p, C.POINTER(abi.mlgpu_photons), C.c_uint64,
             C.POINTER(abi.mlgpu_settings), C.POINTER(abi.mlgpu_rng),
@@ -77,6 +81,7 @@ def lib():
         _declare_surrogate(L)
         for name in ("mlgpu_scene_create", "mlgpu_scene_destroy", "mlgpu_propagate",
                      "mlgpu_scene_autotune", "mlgpu_corsika_photons", "mlgpu_lixel_statistics",
+                     "mlgpu_signal_chain",
                      "mlgpu_propagate_host", "mlgpu_scene_sync_errors", "mlgpu_bin_arrivals",
                      "mlgpu_bin_arrivals_noalloc", "mlgpu_scene_kernel_launches"):
             getattr(L, name).restype = C.c_int
@@ -136,7 +141,7 @@ EXPORTED = (
     "mlgpu_propagate", "mlgpu_scene_sync_errors", "mlgpu_propagate_host",
     "mlgpu_bin_arrivals", "mlgpu_bin_arrivals_noalloc", "mlgpu_scene_kernel_launches",
     "mlgpu_scene_set_profiling", "mlgpu_scene_kernel_times", "mlgpu_scene_autotune",
-    "mlgpu_corsika_photons", "mlgpu_lixel_statistics",
+    "mlgpu_corsika_photons", "mlgpu_lixel_statistics", "mlgpu_signal_chain",
     # include/merlict_b200_surrogate.h
     "mlgpu_sg_image_offset", "mlgpu_sg_gemm_f32", "mlgpu_sg_param_count", "mlgpu_sg_image_bytes",
     "mlgpu_sg_pack_weights", "mlgpu_sg_workspace_bytes", "mlgpu_sg_forward",

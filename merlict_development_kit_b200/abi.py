@@ -11,7 +11,7 @@ from dataclasses import dataclass, field
 
 import numpy as np
 
-ABI_VERSION = 3
+ABI_VERSION = 4
 
 # status codes
 OK = 0
@@ -184,6 +184,36 @@ class mlgpu_photon_buffers(C.Structure):
     _fields_ = [(k, C.c_void_p) for k in (
         "support_x", "support_y", "support_z", "direction_x", "direction_y", "direction_z",
         "wavelength", "simulation_truth_id")] + [("capacity", C.c_uint64)]
+
+
+class mlgpu_signal_chain_config(C.Structure):
+    _fields_ = [
+        ("quantum_efficiency", C.c_void_p),
+        ("num_quantum_efficiency", C.c_uint32),
+        ("num_nsb_wavelength_cdf", C.c_uint32),
+        ("nsb_wavelength_cdf", C.c_void_p),
+        ("nsb_total_integral", C.c_double),
+        ("nsb_rate", C.c_double),
+        ("dark_rate", C.c_double),
+        ("probability_for_second_puls", C.c_double),
+        ("nsb_exposure_time", C.c_double),
+        ("time_slice_duration", C.c_double),
+        ("arrival_time_std", C.c_double),
+        ("num_lixel", C.c_uint32),
+        ("reserved", C.c_uint32),
+    ]
+
+
+class mlgpu_photon_stream(C.Structure):
+    _fields_ = [
+        ("channel_offset", C.c_void_p),
+        ("arrival_time_slice", C.c_void_p),
+        ("simulation_truth_id", C.c_void_p),
+        ("nsb_count", C.c_void_p),
+        ("capacity", C.c_uint64),
+        ("num_pulses", C.c_uint64),
+        ("nsb_exposure_start_time", C.c_double),
+    ]
 
 
 TRAVERSAL_BVH = 0

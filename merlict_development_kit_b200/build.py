@@ -29,6 +29,7 @@ EXTRA = {
     "wavefront_fp64.cu": ["--fmad=false"],
     "corsika.cu": ["--fmad=false"],
     "lixel_stats.cu": ["--fmad=false"],
+    "signal_chain.cu": ["--fmad=false"],
 }
 
 

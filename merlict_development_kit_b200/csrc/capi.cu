@@ -133,6 +133,7 @@ struct mlgpu_scene {
     DeviceBuffer order;                  // tracing order of a batch and its sort scratch
     DeviceBuffer corsika;                // bunch counts, offsets and the total
     DeviceBuffer stats;                  // sort buffers of the calibration statistics
+    DeviceBuffer signal, signal_tables;  // signal chain scratch; its Func1 tables
     // ray pools of the wavefront tracers
     DeviceBuffer wave;
     WaveCounters* wave_host = nullptr;   // pinned copy of the counters
@@ -840,6 +841,105 @@ int mlgpu_lixel_statistics(mlgpu_scene* scene, const int32_t* sensor, const floa
                                              static_cast<cudaStream_t>(cuda_stream));
     if (e != cudaSuccess) return cuda_fail(e, "calibration statistics");
     scene->launches += 3;
+    return MLGPU_OK;
+}
+
+int mlgpu_signal_chain(mlgpu_scene* scene, const mlgpu_signal_chain_config* cfg,
+                       const int32_t* sensor, const double* arrival_time,
+                       const double* wavelength, const int32_t* truth_id, uint64_t n,
+                       const float* lixel_efficiency, uint32_t num_sensors, const mlgpu_rng* rng,
+                       mlgpu_photon_stream* out, void* cuda_stream) {
+    if (!scene || !cfg || !rng || !out) return fail(MLGPU_ERR_INVALID_ARGUMENT, "NULL argument");
+    out->num_pulses = 0;
+    out->nsb_exposure_start_time = 0.0;
+    if (n > 0 && (!sensor || !arrival_time || !wavelength || !truth_id))
+        return fail(MLGPU_ERR_INVALID_ARGUMENT, "NULL photon array");
+    if (n >= (1ull << 31))
+        return fail(MLGPU_ERR_INVALID_ARGUMENT, "at most 2^31 - 1 photons per event");
+    if (num_sensors > 0 && !lixel_efficiency)
+        return fail(MLGPU_ERR_INVALID_ARGUMENT, "lixel_efficiency is NULL");
+    if (!out->channel_offset || (out->capacity > 0 && (!out->arrival_time_slice ||
+                                                        !out->simulation_truth_id)))
+        return fail(MLGPU_ERR_INVALID_ARGUMENT, "photon stream buffer is NULL");
+    if (rng->mode != MLGPU_RNG_PHILOX)
+        return fail(MLGPU_ERR_INVALID_ARGUMENT, "the signal chain draws from the Philox streams");
+    if (!(cfg->probability_for_second_puls < 1.0))
+        return fail(MLGPU_ERR_INVALID_ARGUMENT,
+                    "Expected config->probability_for_second_puls < 1.0, but actual it is: %g",
+                    cfg->probability_for_second_puls);
+    if (!cfg->quantum_efficiency || cfg->num_quantum_efficiency < 2 || !cfg->nsb_wavelength_cdf ||
+        cfg->num_nsb_wavelength_cdf < 2)
+        return fail(MLGPU_ERR_INVALID_ARGUMENT, "a Func1 table needs at least two points");
+    if (cfg->num_lixel == 0 || !(cfg->time_slice_duration != 0.0))
+        return fail(MLGPU_ERR_INVALID_ARGUMENT, "num_lixel and time_slice_duration must not be 0");
+    const cudaStream_t stream = static_cast<cudaStream_t>(cuda_stream);
+    // the two Func1 tables, on the device
+    const size_t nq = cfg->num_quantum_efficiency, nc = cfg->num_nsb_wavelength_cdf;
+    MLGPU_CUDA(scene->signal_tables.reserve(3*(nq + nc)*sizeof(double)));
+    double* tab = static_cast<double*>(scene->signal_tables.ptr);
+    MLGPU_CUDA(cudaMemcpyAsync(tab, cfg->quantum_efficiency, 3*nq*sizeof(double),
+                               cudaMemcpyHostToDevice, stream));
+    MLGPU_CUDA(cudaMemcpyAsync(tab + 3*nq, cfg->nsb_wavelength_cdf, 3*nc*sizeof(double),
+                               cudaMemcpyHostToDevice, stream));
+    const size_t bytes = signal_chain_scratch_bytes(n, num_sensors);
+    MLGPU_CUDA(scene->signal.reserve(bytes));
+    if (!scene->wave_host) MLGPU_CUDA(cudaMallocHost(&scene->wave_host, sizeof(WaveCounters)));
+    if (!scene->wave_grid) scene->wave_grid = wave_persistent_blocks();
+    SignalChainArgs a;
+    a.sensor = sensor; a.time = arrival_time; a.wavelength = wavelength; a.truth = truth_id;
+    a.num_photons = n; a.efficiency = lixel_efficiency; a.num_sensors = num_sensors;
+    a.seed = rng->seed; a.offset = rng->photon_offset;
+    a.params.qe = tab; a.params.num_qe = (int32_t)nq;
+    a.params.cdf = tab + 3*nq; a.params.num_cdf = (int32_t)nc;
+    a.params.dark_rate = cfg->dark_rate;
+    a.params.second_puls = cfg->probability_for_second_puls;
+    a.params.total_integral = cfg->nsb_total_integral;
+    a.params.nsb_rate = cfg->nsb_rate;
+    a.params.num_lixel = (double)cfg->num_lixel;
+    a.params.exposure_time = cfg->nsb_exposure_time;
+    a.params.time_slice_duration = cfg->time_slice_duration;
+    a.params.arrival_time_std = cfg->arrival_time_std;
+    a.channel_offset = out->channel_offset;
+    a.slice = out->arrival_time_slice;
+    a.slice_truth = out->simulation_truth_id;
+    a.nsb_count = out->nsb_count;
+    a.err = scene->error_word;
+    MLGPU_CUDA(cudaMemsetAsync(scene->error_word, 0, sizeof(unsigned int), stream));
+    const double* start_dev = nullptr;
+    cudaError_t e = launch_signal_chain_count(a, scene->signal.ptr, scene->signal.bytes,
+                                              scene->wave_grid, stream, &start_dev);
+    if (e != cudaSuccess) return cuda_fail(e, "signal chain kernels");
+    scene->launches += 7;
+    // the total, the window start and the error word, back on the host
+    uint64_t* host = reinterpret_cast<uint64_t*>(scene->wave_host);
+    MLGPU_CUDA(cudaMemcpyAsync(host, out->channel_offset + num_sensors, sizeof(uint64_t),
+                               cudaMemcpyDeviceToHost, stream));
+    MLGPU_CUDA(cudaMemcpyAsync(host + 1, start_dev, sizeof(double), cudaMemcpyDeviceToHost, stream));
+    MLGPU_CUDA(cudaMemcpyAsync(host + 2, scene->error_word, sizeof(unsigned int),
+                               cudaMemcpyDeviceToHost, stream));
+    MLGPU_CUDA(cudaStreamSynchronize(stream));
+    const uint64_t total = host[0];
+    double start = 0.0;
+    std::memcpy(&start, host + 1, sizeof(double));
+    const unsigned int err = static_cast<unsigned int>(host[2] & 0xffffffffu);
+    if (err) {
+        MLGPU_CUDA(cudaMemset(scene->error_word, 0, sizeof(unsigned int)));
+        return fail((int)err, "signal chain: %s",
+                    err == MLGPU_ERR_OUT_OF_RANGE
+                        ? "a wavelength is outside the quantum efficiency table or a draw outside "
+                          "the background's wavelength distribution (Func1 limits)"
+                    : err == MLGPU_ERR_INVALID_ARGUMENT
+                        ? "a photon's sensor index is not below num_sensors"
+                        : "a lixel needs more draws than one Philox stream holds");
+    }
+    out->num_pulses = total;
+    out->nsb_exposure_start_time = start;
+    if (total > out->capacity)
+        return fail(MLGPU_ERR_INVALID_ARGUMENT, "the event gives %llu pulses, the buffers hold %llu",
+                    (unsigned long long)total, (unsigned long long)out->capacity);
+    e = launch_signal_chain_write(a, scene->signal.ptr, scene->signal.bytes, stream);
+    if (e != cudaSuccess) return cuda_fail(e, "signal chain write kernel");
+    scene->launches += 1;
     return MLGPU_OK;
 }
 

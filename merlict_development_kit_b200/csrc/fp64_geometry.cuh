@@ -101,13 +101,10 @@ __device__ double func_eval(const DevScene& sc, int32_t f, double x, int* err) {
     return slope*x + __ldg(p0 + 1) - slope*__ldg(p0);
 }
 
-// func_eval on tables at `pts` / `off` (a shared-memory copy, say); the
-// same arithmetic, so the same bits.
-__device__ double func_eval_tab(const double* pts, const int32_t* off, int32_t f, double x,
-                                int* err) {
-    const int32_t b = off[f];
-    const int32_t n = off[f + 1] - b;
-    const double* p = pts + 3*(size_t)b;
+// func_eval on one table of n (x, y, slope) points at `p`; the same
+// arithmetic, so the same bits.
+__device__ __forceinline__ double func_eval_points(const double* p, int32_t n, double x,
+                                                   int* err) {
     if (x < p[0] || x >= p[3*(n - 1)]) {
         if (!*err) *err = MLGPU_ERR_OUT_OF_RANGE;
         return 0.0;
@@ -126,6 +123,13 @@ __device__ double func_eval_tab(const double* pts, const int32_t* off, int32_t f
     const double* p0 = p + 3*(first - 1);
     const double slope = p0[2];
     return slope*x + p0[1] - slope*p0[0];
+}
+
+// func_eval on tables at `pts` / `off` (a shared-memory copy, say).
+__device__ double func_eval_tab(const double* pts, const int32_t* off, int32_t f, double x,
+                                int* err) {
+    const int32_t b = off[f];
+    return func_eval_points(pts + 3*(size_t)b, off[f + 1] - b, x, err);
 }
 
 // HexagonalPrismZ::is_inside, HexagonalPrismZ.cpp:14-30

@@ -226,6 +226,36 @@ size_t lixel_stats_scratch_bytes(uint64_t n);
 cudaError_t launch_lixel_stats(const int32_t* sensor, const float* const* values, uint64_t n,
                                uint32_t num_sensors, double emitted, float* out, void* scratch,
                                size_t scratch_bytes, int grid, cudaStream_t s);
+// The signal chain after binning for one event (signal_chain.cu).
+struct SignalChainParams {
+    const double* qe;                // Func1 points (x, y, slope) on the device
+    int32_t num_qe;
+    const double* cdf;               // the background's inverse wavelength CDF
+    int32_t num_cdf;
+    double dark_rate, second_puls, total_integral, nsb_rate, num_lixel, exposure_time;
+    double time_slice_duration, arrival_time_std;
+};
+struct SignalChainArgs {
+    const int32_t* sensor;
+    const double* time;
+    const double* wavelength;
+    const int32_t* truth;
+    uint64_t num_photons;
+    const float* efficiency;
+    uint32_t num_sensors;
+    uint64_t seed, offset;
+    SignalChainParams params;
+    uint64_t* channel_offset;        // [num_sensors + 1]
+    uint8_t* slice;
+    int32_t* slice_truth;
+    int32_t* nsb_count;              // may be null
+    unsigned int* err;
+};
+size_t signal_chain_scratch_bytes(uint64_t n, uint32_t num_sensors);
+cudaError_t launch_signal_chain_count(const SignalChainArgs& a, void* scratch, size_t scratch_bytes,
+                                      int grid, cudaStream_t s, const double** start_dev);
+cudaError_t launch_signal_chain_write(const SignalChainArgs& a, void* scratch, size_t scratch_bytes,
+                                      cudaStream_t s);
 // A coherent tracing order of a photon batch (photon_order.cu): `order`
 // receives n photon indices; `scratch` holds photon_order_scratch_bytes(n).
 size_t photon_order_scratch_bytes(uint64_t n);

@@ -225,6 +225,47 @@ class Func1:
         return total / num_samples
 
 
+def _func1_max(self) -> float:
+    """Func1::max (Func1.cpp:149-153): the largest value in the table."""
+    m = self.points[0][1]
+    for p in self.points:
+        if p[1] > m:
+            m = p[1]
+    return m
+
+
+Func1.max = _func1_max
+
+FUNCTION_DEFAULT_STEPS = 4096   # merlict/function/tools.h:12
+
+
+def function_integral(f: Func1, steps: int = FUNCTION_DEFAULT_STEPS) -> Func1:
+    """merlict::function::integral (merlict/function/tools.cpp:38-58): the
+    running sum of f(x) step on `steps` points, the last one evaluated just
+    inside the upper limit."""
+    lo, hi = f.limits
+    step = (hi - lo) / float(steps)
+    F = [[lo, 0.0]]
+    for i in range(1, steps):
+        x = lo + i * step
+        F.append([x, f.evaluate(x) * step + F[-1][1]])
+    F.append([hi, f.evaluate(math.nextafter(hi, lo)) * step + F[-1][1]])
+    return Func1(F)
+
+
+def function_inverse(f: Func1, steps: int = FUNCTION_DEFAULT_STEPS) -> Func1:
+    """merlict::function::inverse (merlict/function/tools.cpp:60-79): the
+    table of (f(x), x) on `steps` points."""
+    lo, hi = f.limits
+    step = (hi - lo) / float(steps)
+    inv = [[f.evaluate(lo), lo]]
+    for i in range(1, steps):
+        x = lo + i * step
+        inv.append([f.evaluate(x), x])
+    inv.append([f.evaluate(math.nextafter(hi, lo)), hi])
+    return Func1(inv)
+
+
 DEFAULT_REFLECTION = Func1([[200e-9, 0.0], [1200e-9, 0.0]])
 DEFAULT_REFRACTION = Func1([[200e-9, 1.0], [1200e-9, 1.0]])
 DEFAULT_ABSORPTION = Func1([[200e-9, math.inf], [1200e-9, math.inf]])

@@ -342,3 +342,79 @@ def mt19937_uniforms_reference(seed: int, n: int) -> np.ndarray:
     out = np.zeros(max(int(n), 1))
     harness().ref_mt19937_uniforms(int(seed), int(n), out.ctypes.data)
     return out[:int(n)]
+
+
+def signal_chain_reference(mode: int, seed: int, offset: int, sensor, time, wavelength, truth,
+                           num_sensors: int, lixel_efficiency, qe_xy, dark_rate: float,
+                           probability_for_second_puls: float, flux_xy, lfs, exposure_time: float,
+                           time_slice_duration: float, arrival_time_std: float, nsb_count=None):
+    """merlict's own signal chain for one event (see ref_signal_chain):
+    mode 0 replays the engine's per-lixel Philox draws (nsb_count gives the
+    background photons per lixel), mode 1 runs merlict's Mt19937(seed).
+    Returns a dict of numpy arrays plus the start time and the seconds the
+    chain took."""
+    L = harness()
+    if not hasattr(L, "_signal_declared"):
+        L.ref_signal_chain.restype = C.c_void_p
+        L.ref_signal_chain.argtypes = [C.c_int, C.c_uint64, C.c_uint64] + [C.c_void_p] * 4 + [
+            C.c_uint64, C.c_uint32, C.c_void_p, C.c_void_p, C.c_uint32, C.c_double, C.c_double,
+            C.c_void_p, C.c_uint32, C.c_void_p, C.c_void_p, C.c_void_p]
+        L.ref_signal_result.restype = C.c_uint64
+        L.ref_signal_result.argtypes = [C.c_void_p, C.c_int, C.c_void_p]
+        L.ref_signal_start_time.restype = C.c_double
+        L.ref_signal_start_time.argtypes = [C.c_void_p]
+        L.ref_signal_seconds.restype = C.c_double
+        L.ref_signal_seconds.argtypes = [C.c_void_p]
+        L.ref_signal_free.argtypes = [C.c_void_p]
+        L._signal_declared = True
+    keep = []
+
+    def arr(a, dt):
+        a = np.ascontiguousarray(a, dtype=dt)
+        keep.append(a)
+        return a.ctypes.data
+
+    n = len(sensor)
+    qe = np.ascontiguousarray(qe_xy, dtype=np.float64).reshape(-1, 2)
+    flux = np.ascontiguousarray(flux_xy, dtype=np.float64).reshape(-1, 2)
+    nc = None if nsb_count is None else arr(nsb_count, np.uint32)
+    h = L.ref_signal_chain(int(mode), int(seed), int(offset), arr(sensor, np.int32),
+                           arr(time, np.float64), arr(wavelength, np.float64), arr(truth, np.int32),
+                           n, int(num_sensors), arr(lixel_efficiency, np.float32), arr(qe, np.float64),
+                           qe.shape[0], float(dark_rate), float(probability_for_second_puls),
+                           arr(flux, np.float64), flux.shape[0], arr(lfs, np.float64),
+                           arr([exposure_time, time_slice_duration, arrival_time_std], np.float64), nc)
+    if not h:
+        raise RuntimeError(L.ref_last_error().decode())
+    try:
+        types = [np.uint64] * 3 + [np.float64, np.float64, np.int32, np.float64, np.int32, np.uint8,
+                                   np.int32]
+        names = ["pipeline_offset", "pulse_offset", "channel_offset", "pipeline_time",
+                 "pipeline_wavelength", "pipeline_truth", "pulse_time", "pulse_truth",
+                 "channel_slice", "channel_truth"]
+        out = {}
+        for which, (name, dt) in enumerate(zip(names, types)):
+            m = L.ref_signal_result(h, which, None)
+            a = np.zeros(max(int(m), 1), dtype=dt)
+            L.ref_signal_result(h, which, a.ctypes.data)
+            out[name] = a[:int(m)]
+        out["nsb_exposure_start_time"] = L.ref_signal_start_time(h)
+        out["seconds"] = L.ref_signal_seconds(h)
+        return out
+    finally:
+        L.ref_signal_free(h)
+
+
+def photon_stream_write_reference(path: str, truth_path: str, offsets, slices, truth,
+                                  time_slice_duration: float) -> None:
+    """merlict's PhotonStream::write and write_simulation_truth."""
+    L = harness()
+    L.ref_photon_stream_write.argtypes = [C.c_char_p, C.c_char_p] + [C.c_void_p] * 3 + [
+        C.c_uint32, C.c_float]
+    o = np.ascontiguousarray(offsets, dtype=np.uint64)
+    sl = np.ascontiguousarray(slices, dtype=np.uint8)
+    tr = np.ascontiguousarray(truth, dtype=np.int32)
+    if L.ref_photon_stream_write(os.fspath(path).encode(), os.fspath(truth_path).encode(),
+                                 o.ctypes.data, sl.ctypes.data, tr.ctypes.data, len(o) - 1,
+                                 float(time_slice_duration)) != 0:
+        raise RuntimeError(L.ref_last_error().decode())

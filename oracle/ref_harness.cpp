@@ -38,6 +38,11 @@
 #include "merlict_json/json.h"
 #include "merlict_portal_plenoscope/json_to_plenoscope.h"
 #include "merlict_portal_plenoscope/PlenoscopeScenery.h"
+#include "merlict_portal_plenoscope/night_sky_background/NightSkyBackground.h"
+#include "merlict_signal_processing/PhotoElectricConverter.h"
+#include "merlict_signal_processing/PhotonStream.h"
+#include "merlict_signal_processing/PipelinePhoton.h"
+#include "merlict_signal_processing/pulse_extraction.h"
 #include "merlict_b200.h"
 #include "merlict_b200_philox.h"
 #include "merlict_b200_shim.h"
@@ -763,6 +768,241 @@ int ref_json_propagation_config(const char* path, uint64_t* max_num_interactions
 void ref_mt19937_uniforms(uint64_t seed, uint64_t n, double* out) {
     ml::random::Mt19937 prng(seed);
     for (uint64_t i = 0; i < n; i++) out[i] = prng.uniform();
+}
+
+// ---- the signal chain after binning --------------------------------------
+//
+// ref_signal_chain runs merlict's own steps for one event, as
+// plenoscope_propagation.cpp:201-247 chains them: get_photon_pipelines,
+// night_sky_background::inject_nsb_into_photon_pipeline,
+// PhotoElectricConverter::Converter per lixel and extract_pulses per lixel.
+// mode 0 replays the engine's draw schedule (stage s of lixel i draws from
+// Philox stream ((0xF0 | s) << 56) | (offset + i); the background stage
+// moves on to the next lixel after 2 nsb_count[i] + 1 draws); mode 1 uses
+// merlict's Mt19937(seed) for everything, in merlict's order.
+
+namespace {
+
+class SignalReplay : public ml::random::Generator {
+ public:
+    uint64_t key = 0, stream = 0, offset = 0;
+    uint32_t k = 0;
+    const uint32_t* budget_of = nullptr;   // background stage: draws per lixel
+    uint64_t next_lixel = 0, left = 0;
+    uint64_t stage = 0;
+
+    static uint64_t stream_of(uint64_t stage, uint64_t offset, uint64_t lixel) {
+        return ((0xF0ull | stage) << 56) | ((offset + lixel) & ((1ull << 56) - 1));
+    }
+    void select(uint64_t st, uint64_t lixel) {
+        stage = st;
+        stream = stream_of(st, offset, lixel);
+        k = 0;
+    }
+    double uniform() override {
+        if (budget_of) {
+            while (left == 0) {
+                select(stage, next_lixel);
+                left = 2ull*budget_of[next_lixel] + 1ull;
+                next_lixel++;
+            }
+            left--;
+        }
+        return mlgpu_philox_uniform(key, stream, k++);
+    }
+    uint64_t create_seed() override { return 0; }
+    double normal(const double mean, const double std_dev) override {
+        const double u1 = uniform();
+        const double u2 = uniform();
+        return mean + std_dev*(sqrt(-2.0*log(1.0 - u1))*cos(2.0*M_PI*u2));
+    }
+};
+
+struct SignalResult {
+    std::vector<uint64_t> offsets[3];        // photon pipelines, pulses, channels
+    std::vector<double> pipe_time, pipe_wavelength, pulse_time;
+    std::vector<int32_t> pipe_truth, pulse_truth, channel_truth;
+    std::vector<uint8_t> channel_slice;
+    double nsb_exposure_start_time = 0.0;
+    double seconds = 0.0;
+};
+
+std::vector<std::vector<double>> xy_table(const double* xy, uint32_t n) {
+    std::vector<std::vector<double>> t;
+    for (uint32_t i = 0; i < n; i++) t.push_back({xy[2*i], xy[2*i + 1]});
+    return t;
+}
+
+}  // namespace
+
+// lfs: expected focal length, expected aperture radius, max FoV diameter
+// [deg], pixel FoV flat2flat [deg], paxels on the pixel diagonal, housing
+// overhead -- the light-field sensor whose geometry the background light
+// uses (Light.cpp:8-24).  times: exposure, time slice, arrival time std.
+void* ref_signal_chain(int mode, uint64_t seed, uint64_t offset, const int32_t* sensor,
+                       const double* time, const double* wavelength, const int32_t* truth,
+                       uint64_t n, uint32_t num_sensors, const float* lixel_efficiency,
+                       const double* qe_xy, uint32_t num_qe, double dark_rate,
+                       double probability_for_second_puls, const double* flux_xy,
+                       uint32_t num_flux, const double* lfs, const double* times,
+                       const uint32_t* nsb_count) {
+    try {
+        namespace sp = signal_processing;
+        namespace nsb = plenoscope::night_sky_background;
+        std::unique_ptr<SignalResult> r(new SignalResult);
+        // the light-field sensor's geometry, for the background light
+        ml::function::Func1 lens_n({{200e-9, 1.5}, {1200e-9, 1.5}});
+        plenoscope::light_field_sensor::Config lc;
+        lc.expected_imaging_system_focal_length = lfs[0];
+        lc.expected_imaging_system_max_aperture_radius = lfs[1];
+        lc.max_FoV_diameter = ml::deg2rad(lfs[2]);
+        lc.pixel_FoV_hex_flat2flat = ml::deg2rad(lfs[3]);
+        lc.num_paxel_on_pixel_diagonal = static_cast<unsigned int>(lfs[4]);
+        lc.housing_overhead = lfs[5];
+        lc.lens_refraction = &lens_n;
+        lc.bin_reflection = &lens_n;
+        plenoscope::light_field_sensor::Geometry geometry(lc);
+        if (geometry.num_lixel() != num_sensors)
+            throw std::invalid_argument("the light-field sensor's lixels differ from the sensors");
+        const ml::function::Func1 flux(xy_table(flux_xy, num_flux));
+        const nsb::Light light(&geometry, &flux);
+        const ml::function::Func1 qe(xy_table(qe_xy, num_qe));
+        sp::PhotoElectricConverter::Config pc;
+        pc.quantum_efficiency_vs_wavelength = &qe;
+        pc.dark_rate = dark_rate;
+        pc.probability_for_second_puls = probability_for_second_puls;
+        sp::PhotoElectricConverter::Converter converter(&pc);
+        const std::vector<float> efficiency(lixel_efficiency, lixel_efficiency + num_sensors);
+        const double exposure = times[0], slice = times[1], time_std = times[2];
+
+        // the arrivals as merlict's sensors hold them (Sensor::assign_photon)
+        std::unique_ptr<ml::Frame[]> frames(new ml::Frame[num_sensors]);
+        std::vector<ml::sensor::Sensor> sensors;
+        sensors.reserve(num_sensors);
+        for (uint32_t i = 0; i < num_sensors; i++) sensors.emplace_back(i, &frames[i]);
+        for (uint64_t i = 0; i < n; i++) {
+            if (sensor[i] < 0) continue;
+            ml::sensor::PhotonArrival a;
+            a.simulation_truth_id = truth[i];
+            a.wavelength = wavelength[i];
+            a.arrival_time = time[i];
+            sensors.at(sensor[i]).photon_arrival_history.push_back(a);
+        }
+        std::vector<ml::sensor::Sensor*> ptrs;
+        for (ml::sensor::Sensor& s : sensors) ptrs.push_back(&s);
+        ml::sensor::Sensors channels(ptrs);
+
+        SignalReplay replay;
+        replay.key = seed;
+        replay.offset = offset;
+        ml::random::Mt19937 mt(seed);
+        const auto t0 = std::chrono::steady_clock::now();
+        std::vector<std::vector<sp::PipelinePhoton>> pipes = sp::get_photon_pipelines(&channels);
+        if (mode == 0) {
+            replay.budget_of = nsb_count;
+            replay.stage = 1;
+        }
+        nsb::inject_nsb_into_photon_pipeline(&pipes, exposure, &efficiency, &light,
+                                             &r->nsb_exposure_start_time,
+                                             mode == 0 ? static_cast<ml::random::Generator*>(&replay)
+                                                       : &mt);
+        replay.budget_of = nullptr;
+        std::vector<std::vector<sp::ElectricPulse>> electric;
+        electric.reserve(pipes.size());
+        for (uint64_t i = 0; i < pipes.size(); i++) {
+            replay.select(2, i);
+            electric.push_back(converter.get_pulse_pipeline_for_photon_pipeline(
+                pipes[i], exposure, mode == 0 ? static_cast<ml::random::Generator*>(&replay) : &mt));
+        }
+        std::vector<std::vector<sp::ExtractedPulse>> extracted;
+        if (mode == 0) {
+            for (uint64_t i = 0; i < electric.size(); i++) {
+                replay.select(3, i);
+                extracted.push_back(sp::extract_pulses(electric[i], slice, time_std, &replay));
+            }
+        } else {
+            extracted = sp::extract_pulses(electric, slice, time_std, &mt);
+        }
+        r->seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+
+        for (int j = 0; j < 3; j++) r->offsets[j].push_back(0);
+        for (const auto& p : pipes) {
+            for (const sp::PipelinePhoton& ph : p) {
+                r->pipe_time.push_back(ph.arrival_time);
+                r->pipe_wavelength.push_back(ph.wavelength);
+                r->pipe_truth.push_back(ph.simulation_truth_id);
+            }
+            r->offsets[0].push_back(r->pipe_time.size());
+        }
+        for (const auto& p : electric) {
+            for (const sp::ElectricPulse& e : p) {
+                r->pulse_time.push_back(e.arrival_time);
+                r->pulse_truth.push_back(e.simulation_truth_id);
+            }
+            r->offsets[1].push_back(r->pulse_time.size());
+        }
+        for (const auto& p : extracted) {
+            for (const sp::ExtractedPulse& e : p) {
+                r->channel_slice.push_back(e.arrival_time_slice);
+                r->channel_truth.push_back(e.simulation_truth_id);
+            }
+            r->offsets[2].push_back(r->channel_slice.size());
+        }
+        return r.release();
+    } catch (const std::exception& e) {
+        last_error = e.what();
+        return nullptr;
+    }
+}
+
+// The result's arrays: 0-2 offsets (pipelines, pulses, channels), 3 pipeline
+// times, 4 pipeline wavelengths, 5 pipeline truth ids, 6 pulse times, 7 pulse
+// truth ids, 8 channel slices, 9 channel truth ids.  Returns the element
+// count; copies when `out` is not NULL.
+uint64_t ref_signal_result(void* handle, int which, void* out) {
+    SignalResult* r = static_cast<SignalResult*>(handle);
+    auto put = [out](const auto& v) {
+        if (out) std::memcpy(out, v.data(), v.size()*sizeof(v[0]));
+        return static_cast<uint64_t>(v.size());
+    };
+    switch (which) {
+        case 0: case 1: case 2: return put(r->offsets[which]);
+        case 3: return put(r->pipe_time);
+        case 4: return put(r->pipe_wavelength);
+        case 5: return put(r->pipe_truth);
+        case 6: return put(r->pulse_time);
+        case 7: return put(r->pulse_truth);
+        case 8: return put(r->channel_slice);
+        case 9: return put(r->channel_truth);
+        default: return 0;
+    }
+}
+
+double ref_signal_start_time(void* handle) {
+    return static_cast<SignalResult*>(handle)->nsb_exposure_start_time;
+}
+
+double ref_signal_seconds(void* handle) { return static_cast<SignalResult*>(handle)->seconds; }
+
+void ref_signal_free(void* handle) { delete static_cast<SignalResult*>(handle); }
+
+// PhotonStream::write and write_simulation_truth (PhotonStream.cpp:15-78)
+// of channels given as offsets [num_channels + 1], slices and truth ids.
+int ref_photon_stream_write(const char* path, const char* truth_path, const uint64_t* offsets,
+                            const uint8_t* slices, const int32_t* truth, uint32_t num_channels,
+                            float time_slice_duration) {
+    try {
+        std::vector<std::vector<signal_processing::ExtractedPulse>> channels(num_channels);
+        for (uint32_t c = 0; c < num_channels; c++)
+            for (uint64_t k = offsets[c]; k < offsets[c + 1]; k++)
+                channels[c].emplace_back(slices[k], truth[k]);
+        signal_processing::PhotonStream::write(channels, time_slice_duration, path);
+        signal_processing::PhotonStream::write_simulation_truth(channels, truth_path);
+        return 0;
+    } catch (const std::exception& e) {
+        last_error = e.what();
+        return 1;
+    }
 }
 
 int ref_hardware_concurrency(void) {

@@ -37,11 +37,13 @@ def test_struct_layouts_match_header(tmp_path):
     src.write_text(
         '#include <stdio.h>\n#include <stddef.h>\n#include "merlict_b200.h"\n'
         '#include "merlict_b200_surrogate.h"\n'
-        "int main(void){printf(\"%zu %zu %zu %zu %zu %zu %zu %zu %zu %zu\\n\","
+        "int main(void){printf(\"%zu %zu %zu %zu %zu %zu %zu %zu %zu %zu %zu %zu %zu %zu\\n\","
         "sizeof(mlgpu_flat_scene), sizeof(mlgpu_photons), sizeof(mlgpu_history_entry),"
         "sizeof(mlgpu_results), sizeof(mlgpu_rng), sizeof(mlgpu_settings),"
         "offsetof(mlgpu_flat_scene, hex_unit_u), offsetof(mlgpu_flat_scene, num_sensors),"
-        "sizeof(mlgpu_sg_sensor_grid), offsetof(mlgpu_sg_sensor_grid, hex_u));"
+        "sizeof(mlgpu_sg_sensor_grid), offsetof(mlgpu_sg_sensor_grid, hex_u),"
+        "sizeof(mlgpu_signal_chain_config), offsetof(mlgpu_signal_chain_config, num_lixel),"
+        "sizeof(mlgpu_photon_stream), offsetof(mlgpu_photon_stream, nsb_exposure_start_time));"
         "return 0;}\n")
     exe = tmp_path / "sizes"
     subprocess.run(["gcc", "-I" + os.path.join(REPO, "include"), str(src), "-o", str(exe)], check=True)
@@ -50,7 +52,10 @@ def test_struct_layouts_match_header(tmp_path):
                 C.sizeof(abi.mlgpu_history_entry), C.sizeof(abi.mlgpu_results),
                 C.sizeof(abi.mlgpu_rng), C.sizeof(abi.mlgpu_settings),
                 abi.mlgpu_flat_scene.hex_unit_u.offset, abi.mlgpu_flat_scene.num_sensors.offset,
-                C.sizeof(_native.mlgpu_sg_sensor_grid), _native.mlgpu_sg_sensor_grid.hex_u.offset]
+                C.sizeof(_native.mlgpu_sg_sensor_grid), _native.mlgpu_sg_sensor_grid.hex_u.offset,
+                C.sizeof(abi.mlgpu_signal_chain_config), abi.mlgpu_signal_chain_config.num_lixel.offset,
+                C.sizeof(abi.mlgpu_photon_stream),
+                abi.mlgpu_photon_stream.nsb_exposure_start_time.offset]
     assert [int(x) for x in out] == expected
 
 
