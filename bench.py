@@ -50,6 +50,12 @@ FLOP_STAGE = {"nodes": "walk", "leaves": "intersect", "caps": "intersect",
 FP64_PEAK_TFLOPS_NOMINAL = 37.0   # B200 vector FP64, nominal (no measured figure)
 FP32_PEAK_TFLOPS_NOMINAL = 75.0   # B200 vector FP32 (non-tensor), nominal
 WORKLOAD = "light-field telescope, 1039 lenses x 61 lixels (config 1)"
+# the signal chain after binning (workload "signal"): quantum efficiency,
+# dark rate [1/s], crosstalk, night-sky background flux [1/(s sr m^2 m)],
+# exposure, time slice and single-photon time resolution [s]
+SIGNAL = dict(qe=[[200e-9, 0.0], [450e-9, 0.6], [1200e-9, 0.0]], dark_rate=5e6, crosstalk=0.1,
+              nsb_flux=[[250e-9, 1e17], [400e-9, 3e17], [700e-9, 2e17]], exposure=50e-9,
+              time_slice=0.5e-9, time_std=0.4e-9)
 
 
 def scene_config_name():
@@ -529,6 +535,122 @@ def run_bunches(args, world, rank, local):
     scene.close()
 
 
+def run_signal(args, world, rank, local):
+    """The signal chain after binning, one event per step: the photons of a
+    config-1 batch that reached lixels (propagated once, untimed) go through
+    the night-sky background, photo-electric conversion and pulse
+    extraction of all 63,379 lixels (mlgpu_signal_chain), each step with
+    its own Philox key.  The CPU baseline is merlict's own chain (one core,
+    its Mt19937) on the same photons."""
+    import torch
+    from merlict_development_kit_b200 import engine, factories as F, signal_chain as SC
+    from merlict_development_kit_b200.scenery import Func1
+
+    torch.cuda.set_device(local)
+    dev = torch.device(f"cuda:{local}")
+    scene_py = F.light_field_telescope(**SCENE)
+    scene = engine.Scene(scene_py.flatten())
+    n_in = args.event_photons
+    ph = engine.photons_to_device(make_photons(n_in, 17 + rank))
+    out = scene.propagate(ph, engine.PropagationConfig(MAX_INTERACTIONS), engine.Philox(5 + rank),
+                          outputs=("sensor", "time"))
+    sensor = out["sensor"].contiguous()
+    time_ = out["time"].to(torch.float64).contiguous()
+    wavelength = ph["wavelength"].to(torch.float64).contiguous()
+    truth = ph["id"].to(torch.int32).contiguous()
+    g = F.LightFieldSensorGeometry(F.LightFieldSensorConfig(
+        expected_imaging_system_focal_length=SCENE["focal_length"],
+        expected_imaging_system_max_aperture_radius=SCENE["aperture_radius"],
+        max_FoV_diameter=np.deg2rad(SCENE["fov_deg"]),
+        pixel_FoV_hex_flat2flat=np.deg2rad(SCENE["pixel_fov_deg"]),
+        num_paxel_on_pixel_diagonal=SCENE["paxels_on_diagonal"],
+        housing_overhead=SCENE["housing_overhead"],
+        lens_refraction=Func1([[200e-9, 1.5], [1200e-9, 1.5]]),
+        bin_reflection=Func1([[200e-9, 0.9], [1200e-9, 0.9]])))
+    nl = g.num_lixels
+    eff = torch.as_tensor(np.random.default_rng(3).uniform(0.3, 0.7, nl).astype(np.float32),
+                          device=dev)
+    light = SC.NightSkyBackgroundLight(g, Func1(SIGNAL["nsb_flux"]))
+    cfg = SC.SignalChainConfig(
+        SC.PhotoElectricConverterConfig(Func1(SIGNAL["qe"]), SIGNAL["dark_rate"],
+                                        SIGNAL["crosstalk"]),
+        light, SIGNAL["exposure"], SIGNAL["time_slice"], SIGNAL["time_std"])
+    n = int(sensor.numel())
+    on_lixels = int((sensor >= 0).sum())
+    stream = torch.cuda.current_stream()
+    for w in range(args.warmup):
+        SC.run(scene, cfg, sensor, time_, wavelength, truth, eff, engine.Philox(1000 + w))
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
+    clocks = ClockSampler(local)
+    clocks.start()
+    barrier(world)
+    torch.cuda.synchronize()
+    ev[0].record(stream)
+    pulses = 0
+    for k in range(args.steps):
+        ps = SC.run(scene, cfg, sensor, time_, wavelength, truth, eff, engine.Philox(k))
+        pulses += len(ps.arrival_time_slice)
+    ev[1].record(stream)
+    torch.cuda.synchronize()
+    # end to end: host photon arrays in, the photon stream out, every event
+    host = [t.cpu().pin_memory() for t in (sensor, time_, wavelength, truth)]
+    dev_bufs = [torch.empty_like(t, device=dev) for t in host]
+    barrier(world)
+    torch.cuda.synchronize()
+    ev[2].record(stream)
+    d2h = 0
+    for k in range(args.steps):
+        for d, h in zip(dev_bufs, host):
+            d.copy_(h, non_blocking=True)
+        ps = SC.run(scene, cfg, *dev_bufs, eff, engine.Philox(k))
+        res = [ps.channel_offset.cpu(), ps.arrival_time_slice.cpu(), ps.simulation_truth_id.cpu()]
+        d2h = sum(r.numel() * r.element_size() for r in res)
+    ev[3].record(stream)
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    ms = max_over_ranks(ev[0].elapsed_time(ev[1]) / args.steps, world)
+    ms_e2e = max_over_ranks(ev[2].elapsed_time(ev[3]) / args.steps, world)
+    h2d = sum(h.numel() * h.element_size() for h in host)
+    line = {
+        "metric": "photons/s", "value": n * world / (ms * 1e-3), "unit": "photons/s",
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic",
+        "config": {"workload": "signal chain after binning of one config-1 event: night-sky "
+                               "background, photo-electric conversion and pulse extraction of "
+                               f"{nl} lixels", "photons_per_event": n,
+                   "photons_on_lixels": on_lixels, "pulses_per_event": pulses / args.steps,
+                   "signal": SIGNAL, "inputs_larger_than_l2": n * 24 > 126e6},
+        "events_per_s": world / (ms * 1e-3),
+        "e2e": {"value": n * world / (ms_e2e * 1e-3), "unit": "photons/s",
+                "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+        "gpu_launches": 8 * args.steps,
+        "clocks": clk,
+    }
+    if rank == 0 and not args.no_cpu_baseline:
+        from oracle import oracle as O
+        if O.harness_available():
+            idx = torch.nonzero(sensor >= 0).flatten()
+            take = idx[:min(len(idx), args.ref_photons)]
+            r = O.signal_chain_reference(
+                1, 1, 0, sensor[take].cpu().numpy(), time_[take].cpu().numpy(),
+                wavelength[take].cpu().numpy(), truth[take].cpu().numpy(), nl, eff.cpu().numpy(),
+                SIGNAL["qe"], SIGNAL["dark_rate"], SIGNAL["crosstalk"], SIGNAL["nsb_flux"],
+                [SCENE["focal_length"], SCENE["aperture_radius"], SCENE["fov_deg"],
+                 SCENE["pixel_fov_deg"], SCENE["paxels_on_diagonal"], SCENE["housing_overhead"]],
+                SIGNAL["exposure"], SIGNAL["time_slice"], SIGNAL["time_std"])
+            # per input photon of the event: the sample holds the lixel photons
+            per_photon = r["seconds"] / max(len(take), 1) * (on_lixels / max(n, 1))
+            line["cpu_baseline"] = {
+                "value": 1.0 / per_photon, "unit": "photons/s", "cores": 1, "kind": "reference",
+                "sample": f"merlict's chain (get_photon_pipelines, inject_nsb_into_photon_pipeline,"
+                          f" Converter, extract_pulses; Mt19937) on {len(take)} of the event's "
+                          f"lixel photons and all {nl} lixels: {r['seconds']:.3f} s"}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    scene.close()
+
+
 def run_precision(args, world, rank, local):
     """Precision study (config 3): the large parabolic reflector (0.9 m facets
     of curvature radius 213 m on a 35.5 m aperture) with 8,443 flat pixels at
@@ -725,12 +847,16 @@ def main():
                     help="skip the FP32 form's line items in the default workload")
     ap.add_argument("--no-autotune", dest="autotune", action="store_false",
                     help="default wavefront knobs instead of mlgpu_scene_autotune's")
-    ap.add_argument("--workload", choices=["telescope", "bunches", "precision", "surrogate"],
+    ap.add_argument("--workload", choices=["telescope", "bunches", "precision", "surrogate",
+                                           "signal"],
                     default="telescope",
                     help="telescope: the light-field telescope batch; bunches: 4096 "
                          "air-shower-like events of uneven sizes, batched vs one call per event; "
-                         "precision: the FP32 forms against FP64 on the large reflector")
+                         "precision: the FP32 forms against FP64 on the large reflector; "
+                         "signal: the signal chain after binning of one config-1 event")
     ap.add_argument("--events", type=int, default=4096)
+    ap.add_argument("--event-photons", type=int, default=1_000_000,
+                    help="photons of the event the signal workload propagates once")
     ap.add_argument("--train-photons", type=int, default=200_000_000)
     ap.add_argument("--epochs", type=int, default=8)
     ap.add_argument("--js-target", type=float, default=1e-3)
@@ -749,6 +875,8 @@ def main():
             run_precision(args, world, rank, local)
         elif args.workload == "surrogate":
             run_surrogate(args, world, rank, local)
+        elif args.workload == "signal":
+            run_signal(args, world, rank, local)
         else:
             run_ours(args, world, rank, local)
     finally:

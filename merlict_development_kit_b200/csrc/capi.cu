@@ -133,7 +133,7 @@ struct mlgpu_scene {
     DeviceBuffer order;                  // tracing order of a batch and its sort scratch
     DeviceBuffer corsika;                // bunch counts, offsets and the total
     DeviceBuffer stats;                  // sort buffers of the calibration statistics
-    DeviceBuffer signal, signal_tables;  // signal chain scratch; its Func1 tables
+    DeviceBuffer signal, signal_pulses, signal_tables;   // signal chain scratch, Func1 tables
     // ray pools of the wavefront tracers
     DeviceBuffer wave;
     WaveCounters* wave_host = nullptr;   // pinned copy of the counters
@@ -881,8 +881,7 @@ int mlgpu_signal_chain(mlgpu_scene* scene, const mlgpu_signal_chain_config* cfg,
                                cudaMemcpyHostToDevice, stream));
     MLGPU_CUDA(cudaMemcpyAsync(tab + 3*nq, cfg->nsb_wavelength_cdf, 3*nc*sizeof(double),
                                cudaMemcpyHostToDevice, stream));
-    const size_t bytes = signal_chain_scratch_bytes(n, num_sensors);
-    MLGPU_CUDA(scene->signal.reserve(bytes));
+    MLGPU_CUDA(scene->signal.reserve(signal_chain_photon_scratch_bytes(n, num_sensors)));
     if (!scene->wave_host) MLGPU_CUDA(cudaMallocHost(&scene->wave_host, sizeof(WaveCounters)));
     if (!scene->wave_grid) scene->wave_grid = wave_persistent_blocks();
     SignalChainArgs a;
@@ -905,24 +904,24 @@ int mlgpu_signal_chain(mlgpu_scene* scene, const mlgpu_signal_chain_config* cfg,
     a.nsb_count = out->nsb_count;
     a.err = scene->error_word;
     MLGPU_CUDA(cudaMemsetAsync(scene->error_word, 0, sizeof(unsigned int), stream));
+    const uint64_t* total_dev = nullptr;
     const double* start_dev = nullptr;
     cudaError_t e = launch_signal_chain_count(a, scene->signal.ptr, scene->signal.bytes,
-                                              scene->wave_grid, stream, &start_dev);
+                                              scene->wave_grid, stream, &total_dev, &start_dev);
     if (e != cudaSuccess) return cuda_fail(e, "signal chain kernels");
-    scene->launches += 7;
-    // the total, the window start and the error word, back on the host
+    scene->launches += 10;
+    // the electric pulses, the window start and the error word, on the host
     uint64_t* host = reinterpret_cast<uint64_t*>(scene->wave_host);
-    MLGPU_CUDA(cudaMemcpyAsync(host, out->channel_offset + num_sensors, sizeof(uint64_t),
-                               cudaMemcpyDeviceToHost, stream));
-    MLGPU_CUDA(cudaMemcpyAsync(host + 1, start_dev, sizeof(double), cudaMemcpyDeviceToHost, stream));
-    MLGPU_CUDA(cudaMemcpyAsync(host + 2, scene->error_word, sizeof(unsigned int),
-                               cudaMemcpyDeviceToHost, stream));
-    MLGPU_CUDA(cudaStreamSynchronize(stream));
-    const uint64_t total = host[0];
-    double start = 0.0;
-    std::memcpy(&start, host + 1, sizeof(double));
-    const unsigned int err = static_cast<unsigned int>(host[2] & 0xffffffffu);
-    if (err) {
+    auto read_back = [&](const uint64_t* count_dev) -> int {
+        MLGPU_CUDA(cudaMemcpyAsync(host, count_dev, sizeof(uint64_t), cudaMemcpyDeviceToHost,
+                                   stream));
+        MLGPU_CUDA(cudaMemcpyAsync(host + 1, start_dev, sizeof(double), cudaMemcpyDeviceToHost,
+                                   stream));
+        MLGPU_CUDA(cudaMemcpyAsync(host + 2, scene->error_word, sizeof(unsigned int),
+                                   cudaMemcpyDeviceToHost, stream));
+        MLGPU_CUDA(cudaStreamSynchronize(stream));
+        const unsigned int err = static_cast<unsigned int>(host[2] & 0xffffffffu);
+        if (!err) return MLGPU_OK;
         MLGPU_CUDA(cudaMemset(scene->error_word, 0, sizeof(unsigned int)));
         return fail((int)err, "signal chain: %s",
                     err == MLGPU_ERR_OUT_OF_RANGE
@@ -931,15 +930,47 @@ int mlgpu_signal_chain(mlgpu_scene* scene, const mlgpu_signal_chain_config* cfg,
                     : err == MLGPU_ERR_INVALID_ARGUMENT
                         ? "a photon's sensor index is not below num_sensors"
                         : "a lixel needs more draws than one Philox stream holds");
-    }
-    out->num_pulses = total;
+    };
+    int st = read_back(total_dev);
+    if (st) return st;
+    const uint64_t electric = host[0];
+    double start = 0.0;
+    std::memcpy(&start, host + 1, sizeof(double));
     out->nsb_exposure_start_time = start;
-    if (total > out->capacity)
-        return fail(MLGPU_ERR_INVALID_ARGUMENT, "the event gives %llu pulses, the buffers hold %llu",
-                    (unsigned long long)total, (unsigned long long)out->capacity);
-    e = launch_signal_chain_write(a, scene->signal.ptr, scene->signal.bytes, stream);
-    if (e != cudaSuccess) return cuda_fail(e, "signal chain write kernel");
+    if (electric >= (1ull << 31))
+        return fail(MLGPU_ERR_RUNTIME, "more than 2^31 - 1 electric pulses in one event");
+    const size_t pulse_bytes = signal_chain_pulse_scratch_bytes(electric);
+    MLGPU_CUDA(scene->signal_pulses.reserve(pulse_bytes));
+    const uint64_t* kept_dev = nullptr;
+    e = launch_signal_chain_extract(a, scene->signal.ptr, scene->signal.bytes,
+                                    scene->signal_pulses.ptr, scene->signal_pulses.bytes, electric,
+                                    scene->wave_grid, stream, &kept_dev);
+    if (e != cudaSuccess) return cuda_fail(e, "signal chain extraction kernels");
+    scene->launches += 6;
+    // the kept pulses fit when the electric ones do; otherwise look first
+    uint64_t kept = electric;
+    const bool look_first = electric > out->capacity;
+    if (look_first) {
+        st = read_back(kept_dev);
+        if (st) return st;
+        kept = host[0];
+        if (kept > out->capacity) {
+            out->num_pulses = kept;
+            return fail(MLGPU_ERR_INVALID_ARGUMENT,
+                        "the event gives %llu pulses, the buffers hold %llu",
+                        (unsigned long long)kept, (unsigned long long)out->capacity);
+        }
+    }
+    e = launch_signal_chain_scatter(a, scene->signal_pulses.ptr, scene->signal_pulses.bytes,
+                                    electric, scene->wave_grid, stream);
+    if (e != cudaSuccess) return cuda_fail(e, "signal chain scatter kernel");
     scene->launches += 1;
+    if (!look_first) {
+        st = read_back(kept_dev);
+        if (st) return st;
+        kept = host[0];
+    }
+    out->num_pulses = kept;
     return MLGPU_OK;
 }
 

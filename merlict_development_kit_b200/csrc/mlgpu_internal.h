@@ -251,11 +251,21 @@ struct SignalChainArgs {
     int32_t* nsb_count;              // may be null
     unsigned int* err;
 };
-size_t signal_chain_scratch_bytes(uint64_t n, uint32_t num_sensors);
-cudaError_t launch_signal_chain_count(const SignalChainArgs& a, void* scratch, size_t scratch_bytes,
-                                      int grid, cudaStream_t s, const double** start_dev);
-cudaError_t launch_signal_chain_write(const SignalChainArgs& a, void* scratch, size_t scratch_bytes,
-                                      cudaStream_t s);
+// Three launches with two host reads between them: count (the electric
+// pulses of the event -> *total_dev), extract (-> *kept_dev, the channel
+// offsets), scatter (the kept pulses into the caller's buffers).
+size_t signal_chain_photon_scratch_bytes(uint64_t n, uint32_t num_sensors);
+size_t signal_chain_pulse_scratch_bytes(uint64_t num_pulses);
+cudaError_t launch_signal_chain_count(const SignalChainArgs& a, void* scratch, size_t bytes,
+                                      int grid, cudaStream_t s, const uint64_t** total_dev,
+                                      const double** start_dev);
+cudaError_t launch_signal_chain_extract(const SignalChainArgs& a, void* scratch, size_t bytes,
+                                        void* pulse_scratch, size_t pulse_bytes,
+                                        uint64_t num_pulses, int grid, cudaStream_t s,
+                                        const uint64_t** kept_dev);
+cudaError_t launch_signal_chain_scatter(const SignalChainArgs& a, void* pulse_scratch,
+                                        size_t pulse_bytes, uint64_t num_pulses, int grid,
+                                        cudaStream_t s);
 // A coherent tracing order of a photon batch (photon_order.cu): `order`
 // receives n photon indices; `scratch` holds photon_order_scratch_bytes(n).
 size_t photon_order_scratch_bytes(uint64_t n);

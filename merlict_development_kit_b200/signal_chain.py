@@ -242,7 +242,11 @@ def _points(f: Func1) -> np.ndarray:
 
 
 def device_config(cfg: SignalChainConfig):
-    """The mlgpu_signal_chain_config of `cfg` and the arrays it points to."""
+    """The mlgpu_signal_chain_config of `cfg` and the arrays it points to
+    (built once per configuration object and kept on it)."""
+    cached = getattr(cfg, "_device_config", None)
+    if cached is not None and cached[0] == _config_key(cfg):
+        return cached[1], cached[2]
     cfg.converter.check()
     qe = _points(cfg.converter.quantum_efficiency_vs_wavelength)
     cdf = _points(cfg.light.wavelength_probability.cumulative_distribution_function)
@@ -259,7 +263,16 @@ def device_config(cfg: SignalChainConfig):
     c.nsb_exposure_time = cfg.nsb_exposure_time
     c.time_slice_duration = cfg.time_slice_duration
     c.arrival_time_std = cfg.single_photon_arrival_time_resolution
+    cfg._device_config = (_config_key(cfg), c, [qe, cdf])
     return c, [qe, cdf]
+
+
+def _config_key(cfg: SignalChainConfig):
+    conv = cfg.converter
+    return (id(conv.quantum_efficiency_vs_wavelength), conv.dark_rate,
+            conv.probability_for_second_puls, id(cfg.light), cfg.light.rate,
+            cfg.nsb_exposure_time, cfg.time_slice_duration,
+            cfg.single_photon_arrival_time_resolution)
 
 
 def run(scene, cfg: SignalChainConfig, sensor, arrival_time, wavelength, truth_id,

@@ -33,7 +33,7 @@ def scene(eng):
     s.close()
 
 
-def config(g, flux=FLUX, dark=5e6, p2=0.1, qe=QE, T=500e-9, dt=0.5e-9, sigma=0.4e-9):
+def config(g, flux=FLUX, dark=5e6, p2=0.1, qe=QE, T=50e-9, dt=0.5e-9, sigma=0.4e-9):
     light = SC.NightSkyBackgroundLight(g, Func1(flux))
     return SC.SignalChainConfig(SC.PhotoElectricConverterConfig(Func1(qe), dark, p2), light, T, dt,
                                 sigma), light
@@ -79,7 +79,7 @@ def test_gpu_matches_oracle_and_merlict(eng, scene, case):
     assert np.array_equal(trg, o_tr)
     if O.harness_available():
         r = O.signal_chain_reference(0, 99, 7, sensor, t, w, tr, nl, eff, QE, kw.get("dark", 5e6),
-                                     kw.get("p2", 0.1), FLUX, LFS, 500e-9, 0.5e-9, 0.4e-9,
+                                     kw.get("p2", 0.1), FLUX, LFS, 50e-9, 0.5e-9, 0.4e-9,
                                      nsb_count=nsb)
         assert r["nsb_exposure_start_time"] == start
         assert np.array_equal(off, r["channel_offset"])
@@ -131,15 +131,15 @@ def test_full_light_field_sensor_event(eng, scene):
     off, sl, trg, start, nsb = gpu_chain(eng, scene, cfg, sensor, t, w, tr, eff, 5, 0)
     kw = chain_kwargs(light, nl, seed=5, offset=0)
     pipes = SO.photon_pipelines(sensor, t, w, tr, nl)
-    S = SO.nsb_exposure_start_time(pipes, 500e-9)
+    S = SO.nsb_exposure_start_time(pipes, 50e-9)
     assert start == S
     assert np.all(np.diff(off.astype(np.int64)) >= 0) and int(off[-1]) == len(sl)
     assert sl.max() < 100
     for lix in random.Random(0).sample(range(nl), 150):
-        p, k = SO.inject_nsb_lixel(pipes[lix], S, 500e-9, eff[lix], light.rate, nl, kw["nsb_cdf"],
+        p, k = SO.inject_nsb_lixel(pipes[lix], S, 50e-9, eff[lix], light.rate, nl, kw["nsb_cdf"],
                                    kw["nsb_total_integral"], SO.Draws(5, SO.STAGE_NSB, 0, lix))
         assert k == nsb[lix]
-        e = SO.photo_electric(p, kw["qe"], 5e6, 0.1, 500e-9, SO.Draws(5, SO.STAGE_PEC, 0, lix))
+        e = SO.photo_electric(p, kw["qe"], 5e6, 0.1, 50e-9, SO.Draws(5, SO.STAGE_PEC, 0, lix))
         x = SO.extract(e, 0.5e-9, 0.4e-9, SO.Draws(5, SO.STAGE_EXTRACT, 0, lix))
         a, b = int(off[lix]), int(off[lix + 1])
         assert [s for s, _ in x] == list(sl[a:b])

@@ -39,7 +39,7 @@ def event(seed, n, num_lixel, spread=3e-9, one_lixel=None):
     return sensor, t, w, tr, eff
 
 
-def chain_kwargs(light, num_lixel, dark=5e6, p2=0.1, T=500e-9, dt=0.5e-9, sigma=0.4e-9, seed=99,
+def chain_kwargs(light, num_lixel, dark=5e6, p2=0.1, T=50e-9, dt=0.5e-9, sigma=0.4e-9, seed=99,
                  offset=7, qe=QE):
     return dict(qe=Func1(qe), dark_rate=dark, probability_for_second_puls=p2,
                 nsb_cdf=light.wavelength_probability.cumulative_distribution_function,
@@ -122,7 +122,7 @@ def test_quantum_efficiency_out_of_range_fails_in_both():
         run_both(sensor, t, w, tr, eff, g)
     with pytest.raises(RuntimeError):
         O.signal_chain_reference(1, 1, 0, sensor, t, w, tr, g.num_lixels, eff, QE, 0.0, 0.0, FLUX,
-                                 LFS, 500e-9, 0.5e-9, 0.4e-9)
+                                 LFS, 50e-9, 0.5e-9, 0.4e-9)
 
 
 @needs_ref
@@ -131,7 +131,7 @@ def test_crosstalk_probability_one_is_refused():
     sensor, t, w, tr, eff = event(4, 10, g.num_lixels)
     with pytest.raises(RuntimeError):
         O.signal_chain_reference(1, 1, 0, sensor, t, w, tr, g.num_lixels, eff, QE, 0.0, 1.0, FLUX,
-                                 LFS, 500e-9, 0.5e-9, 0.4e-9)
+                                 LFS, 50e-9, 0.5e-9, 0.4e-9)
     with pytest.raises(ValueError):
         SC.PhotoElectricConverterConfig(Func1(QE), 0.0, 1.0).check()
 
@@ -152,7 +152,7 @@ def test_production_mode_agrees_in_distribution():
         o = SO.signal_chain(sensor, t, w, tr, g.num_lixels, eff, **k)
         _, sl, *_ = flat(o)
         r = O.signal_chain_reference(1, 100 + s, 0, sensor, t, w, tr, g.num_lixels, eff, QE, 2e7,
-                                     0.1, FLUX, LFS, 500e-9, 0.5e-9, 0.4e-9)
+                                     0.1, FLUX, LFS, 50e-9, 0.5e-9, 0.4e-9)
         counts_o.append(len(sl))
         counts_r.append(len(r["channel_slice"]))
         hist_o += np.bincount(sl, minlength=100)
