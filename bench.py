@@ -630,8 +630,9 @@ def run_signal(args, world, rank, local):
     if rank == 0 and not args.no_cpu_baseline:
         from oracle import oracle as O
         if O.harness_available():
-            idx = torch.nonzero(sensor >= 0).flatten()
-            take = idx[:min(len(idx), args.ref_photons)]
+            # the whole event: the chain's per-lixel work (background, dark
+            # pulses of all lixels) does not shrink with a photon sample
+            take = torch.nonzero(sensor >= 0).flatten()
             r = O.signal_chain_reference(
                 1, 1, 0, sensor[take].cpu().numpy(), time_[take].cpu().numpy(),
                 wavelength[take].cpu().numpy(), truth[take].cpu().numpy(), nl, eff.cpu().numpy(),
@@ -639,13 +640,11 @@ def run_signal(args, world, rank, local):
                 [SCENE["focal_length"], SCENE["aperture_radius"], SCENE["fov_deg"],
                  SCENE["pixel_fov_deg"], SCENE["paxels_on_diagonal"], SCENE["housing_overhead"]],
                 SIGNAL["exposure"], SIGNAL["time_slice"], SIGNAL["time_std"])
-            # per input photon of the event: the sample holds the lixel photons
-            per_photon = r["seconds"] / max(len(take), 1) * (on_lixels / max(n, 1))
             line["cpu_baseline"] = {
-                "value": 1.0 / per_photon, "unit": "photons/s", "cores": 1, "kind": "reference",
+                "value": n / r["seconds"], "unit": "photons/s", "cores": 1, "kind": "reference",
                 "sample": f"merlict's chain (get_photon_pipelines, inject_nsb_into_photon_pipeline,"
-                          f" Converter, extract_pulses; Mt19937) on {len(take)} of the event's "
-                          f"lixel photons and all {nl} lixels: {r['seconds']:.3f} s"}
+                          f" Converter, extract_pulses; Mt19937) on the same event ({len(take)} "
+                          f"lixel photons of {n}, all {nl} lixels): {r['seconds']:.3f} s"}
     if rank == 0:
         print(json.dumps(line), flush=True)
     scene.close()

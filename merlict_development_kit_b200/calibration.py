@@ -92,3 +92,35 @@ def calibrate(scene: engine.Scene, aperture_radius: float, max_fov_radius: float
     cat = lambda xs: torch.cat(xs) if len(xs) > 1 else xs[0]
     return lixel_statistics(scene, cat(sensors), *[cat(v) for v in vals],
                             num_photons / scene.num_sensors)
+
+
+# ---- the lixel statistics file, LixelStatistics.cpp:19-83 -------------------------------
+# A file of LixelStatistic records, twelve float32 each (FIELDS order),
+# written back to back; a trailing partial record is ignored.
+
+def write(statistics: dict, path: str) -> None:
+    """calibration::write: `statistics` as lixel_statistics returns it."""
+    rows = np.stack([np.asarray(statistics[f], dtype="<f4") for f in FIELDS], axis=1)
+    try:
+        with open(path, "wb") as f:
+            f.write(np.ascontiguousarray(rows).tobytes())
+    except OSError:
+        raise RuntimeError(f"LixelStatistics: Unable to write file: '{path}'") from None
+
+
+def read(path: str) -> dict:
+    """calibration::read."""
+    try:
+        with open(path, "rb") as f:
+            data = f.read()
+    except OSError:
+        raise RuntimeError(f"LixelStatistics: Unable to read file: '{path}'") from None
+    n = len(data) // (4 * len(FIELDS))
+    rows = np.frombuffer(data, dtype="<f4", count=n * len(FIELDS)).reshape(n, len(FIELDS))
+    return {f: rows[:, k].copy() for k, f in enumerate(FIELDS)}
+
+
+def read_efficiencies(path: str) -> np.ndarray:
+    """calibration::read_efficiencies: the efficiency of every lixel, the
+    per-lixel input of the night-sky background injection."""
+    return read(path)["efficiency"].astype(np.float32)

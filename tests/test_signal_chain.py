@@ -250,3 +250,18 @@ def test_photon_stream_round_trip_and_rules(tmp_path):
     with pytest.raises(RuntimeError):
         SC.read(str(tmp_path / "missing.phs"))
     assert os.path.getsize(p) == 16
+
+
+def test_lixel_statistics_file_round_trip(tmp_path):
+    from merlict_development_kit_b200 import calibration as CAL
+    rng = np.random.default_rng(2)
+    st = {f: rng.normal(size=7).astype(np.float32) for f in CAL.FIELDS}
+    p = str(tmp_path / "lixel_statistics.bin")
+    CAL.write(st, p)
+    assert os.path.getsize(p) == 7 * 48
+    with open(p, "ab") as f:
+        f.write(b"\0" * 20)                       # a partial record is not read
+    back = CAL.read(p)
+    for f in CAL.FIELDS:
+        assert np.array_equal(back[f], st[f])
+    assert np.array_equal(CAL.read_efficiencies(p), st["efficiency"])
