@@ -418,3 +418,31 @@ def photon_stream_write_reference(path: str, truth_path: str, offsets, slices, t
                                  o.ctypes.data, sl.ctypes.data, tr.ctypes.data, len(o) - 1,
                                  float(time_slice_duration)) != 0:
         raise RuntimeError(L.ref_last_error().decode())
+
+
+def corsika_file_reference(path: str, kind: str) -> dict:
+    """A CORSIKA file through merlict's own reader: kind 'eventio'
+    (eventio::Run) or 'event_tape' (event_tape::Run)."""
+    L = harness()
+    L.ref_corsika_file_read.restype = C.c_void_p
+    L.ref_corsika_file_read.argtypes = [C.c_char_p, C.c_int]
+    L.ref_corsika_file_result.restype = C.c_uint64
+    L.ref_corsika_file_result.argtypes = [C.c_void_p, C.c_int, C.c_void_p]
+    L.ref_corsika_file_free.argtypes = [C.c_void_p]
+    h = L.ref_corsika_file_read(os.fspath(path).encode(), 0 if kind == "eventio" else 1)
+    if not h:
+        raise RuntimeError(L.ref_last_error().decode())
+    try:
+        names = ["run_header", "telescope_positions", "event_headers", "telescope_offsets",
+                 "offset_start", "bunches", "bunch_start", "input_card"]
+        types = [np.float32] * 4 + [np.uint64, np.float32, np.uint64, np.uint8]
+        out = {}
+        for which, (name, dt) in enumerate(zip(names, types)):
+            m = int(L.ref_corsika_file_result(h, which, None))
+            a = np.zeros(max(m, 1), dtype=dt)
+            L.ref_corsika_file_result(h, which, a.ctypes.data)
+            out[name] = a[:m]
+        out["input_card"] = out["input_card"].tobytes().decode("latin-1")
+        return out
+    finally:
+        L.ref_corsika_file_free(h)

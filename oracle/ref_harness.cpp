@@ -32,6 +32,8 @@
 #include "merlict/merlict.h"
 #include "merlict/scenery/segmented_imaging_reflector/segmented_imaging_reflector.h"
 #include "merlict_corsika/PhotonFactory.h"
+#include "merlict_corsika/event_tape.h"
+#include "merlict_corsika/eventio.h"
 #include "merlict_portal_plenoscope/calibration/LixelStatisticsFiller.h"
 #include "merlict_multi_thread/merlict_multi_thread.h"
 #include "merlict_portal_plenoscope/light_field_sensor/LightFieldSensor.h"
@@ -1004,6 +1006,81 @@ int ref_photon_stream_write(const char* path, const char* truth_path, const uint
         return 1;
     }
 }
+
+// ---- CORSIKA files ----------------------------------------------------------
+// A whole file through merlict's readers: eventio::Run (kind 0) or
+// event_tape::Run (kind 1), every event's header, telescope offsets (EventIO)
+// and bunches kept for ref_corsika_file_result.
+
+namespace {
+struct CorsikaFile {
+    std::vector<float> run_header, tel_pos, event_headers, offsets, bunches;
+    std::vector<uint64_t> offset_start{0}, bunch_start{0};
+    std::string input_card;
+};
+}  // namespace
+
+void* ref_corsika_file_read(const char* path, int kind) {
+    try {
+        std::unique_ptr<CorsikaFile> r(new CorsikaFile);
+        auto add_bunches = [&](const std::vector<std::array<float, 8>>& b) {
+            for (const auto& row : b) r->bunches.insert(r->bunches.end(), row.begin(), row.end());
+            r->bunch_start.push_back(r->bunches.size()/8);
+        };
+        if (kind == 0) {
+            eventio::Run run(path);
+            r->run_header.assign(run.header.raw.begin(), run.header.raw.end());
+            r->input_card = run.header.input_card;
+            for (const eventio::TelPos& t : run.header.tel_pos)
+                r->tel_pos.insert(r->tel_pos.end(), {t.x, t.y, t.z, t.r});
+            while (run.has_still_events_left()) {
+                eventio::Event e = run.next_event();
+                r->event_headers.insert(r->event_headers.end(), e.header.raw.begin(),
+                                        e.header.raw.end());
+                for (const eventio::TelOffset& o : e.header.telescope_offsets)
+                    r->offsets.insert(r->offsets.end(), {o.toff, o.xoff, o.yoff, o.weight});
+                r->offset_start.push_back(r->offsets.size()/4);
+                add_bunches(e.photons);
+            }
+        } else {
+            event_tape::Run run(path);
+            r->run_header.assign(run.header.begin(), run.header.end());
+            while (run.has_still_events_left()) {
+                event_tape::Event e = run.next_event();
+                r->event_headers.insert(r->event_headers.end(), e.header.begin(), e.header.end());
+                add_bunches(e.photons);
+            }
+        }
+        return r.release();
+    } catch (const std::exception& e) {
+        last_error = e.what();
+        return nullptr;
+    }
+}
+
+// 0 run header, 1 telescope positions, 2 event headers, 3 telescope offsets,
+// 4 offsets per event (uint64 starts), 5 bunches, 6 bunch starts (uint64),
+// 7 input card (bytes).  Returns the element count; copies when out != NULL.
+uint64_t ref_corsika_file_result(void* handle, int which, void* out) {
+    CorsikaFile* r = static_cast<CorsikaFile*>(handle);
+    auto put = [out](const auto& v) {
+        if (out && !v.empty()) std::memcpy(out, v.data(), v.size()*sizeof(v[0]));
+        return static_cast<uint64_t>(v.size());
+    };
+    switch (which) {
+        case 0: return put(r->run_header);
+        case 1: return put(r->tel_pos);
+        case 2: return put(r->event_headers);
+        case 3: return put(r->offsets);
+        case 4: return put(r->offset_start);
+        case 5: return put(r->bunches);
+        case 6: return put(r->bunch_start);
+        case 7: return put(r->input_card);
+        default: return 0;
+    }
+}
+
+void ref_corsika_file_free(void* handle) { delete static_cast<CorsikaFile*>(handle); }
 
 int ref_hardware_concurrency(void) {
     return static_cast<int>(std::thread::hardware_concurrency());

@@ -83,3 +83,32 @@ def test_device_bunches_match_the_reference_factory():
         bad[2, 6] = -1.0
         scene.corsika_photons(torch.as_tensor(bad, device="cuda"), engine.Philox(5))
     scene.close()
+
+
+@pytest.mark.gpu
+def test_event_tape_bunches_through_the_device_factory(tmp_path):
+    """An event tape written and read back by corsika_io, its events'
+    bunches expanded on the device: the reference factory's photons."""
+    import torch
+    from merlict_development_kit_b200 import corsika_io as CI, engine
+    from conftest import load_golden
+    p = str(tmp_path / "run.tar")
+    w = CI.EventTapeWriter(p, buffer_size=1000)
+    w.write_runh(CI.header_block("RUNH", {1: 9}))
+    sizes = [3000, 1, 2500]
+    for e, n in enumerate(sizes, start=1):
+        w.write_evth(CI.header_block("EVTH", {1: e, 43: 9}))
+        w.write_bunches(random_bunches(n, 10 + e)[0])
+    w.close()
+    scene = engine.Scene(load_golden("sphere")[0])
+    for e, ev in enumerate(CI.EventTapeRun(p), start=1):
+        b = ev.photons
+        assert len(b) == sizes[e - 1]
+        u = np.random.default_rng(e).random(len(b))
+        ref = (O.corsika_photons_reference(b, u) if O.harness_available()
+               else O.corsika_photons_numpy(b, u))
+        got = scene.corsika_photons(torch.as_tensor(b, device="cuda"),
+                                    engine.Replay(torch.as_tensor(u[:, None], device="cuda")))
+        for k in ("support_x", "support_y", "support_z", "wavelength", "id"):
+            assert np.array_equal(got[k].cpu().numpy(), ref[k]), k
+    scene.close()
