@@ -32,7 +32,7 @@
 extern "C" {
 #endif
 
-#define MLGPU_ABI_VERSION 4
+#define MLGPU_ABI_VERSION 5
 
 /* ---- status codes ------------------------------------------------------ */
 enum {
@@ -233,7 +233,15 @@ typedef struct mlgpu_settings {
     int32_t grid_blocks;    /* blocks of the grid-stride kernels (8 per SM)   */
     int32_t staged_levels;  /* top BVH levels read from shared memory (0)     */
     int32_t photon_order;   /* MLGPU_ORDER_*: the order photons enter the pool */
+    int32_t walk;           /* MLGPU_WALK_*: how rays walk the BVH             */
 } mlgpu_settings;
+
+/* walk: LEVELS runs one kernel per BVH level over queued (ray, node) pairs
+ * and one over the hit leaf ranges; STACK walks each ray's whole BVH in one
+ * thread with a stack.  Both test the same boxes and bounding spheres and
+ * find the same candidate leaves, so the results are the same.  DEFAULT is
+ * LEVELS.                                                                  */
+enum { MLGPU_WALK_DEFAULT = 0, MLGPU_WALK_LEVELS = 1, MLGPU_WALK_STACK = 2 };
 
 /* photon_order: COHERENT sorts the batch by a 4-D cell key of support and
  * direction before tracing, so that neighbouring ray slots follow nearly

@@ -11,7 +11,7 @@ from dataclasses import dataclass, field
 
 import numpy as np
 
-ABI_VERSION = 4
+ABI_VERSION = 5
 
 # status codes
 OK = 0
@@ -223,6 +223,10 @@ ORDER_DEFAULT = 0
 ORDER_INPUT = 1
 ORDER_COHERENT = 2
 
+WALK_DEFAULT = 0
+WALK_LEVELS = 1
+WALK_STACK = 2
+
 
 class mlgpu_settings(C.Structure):
     _fields_ = [
@@ -237,10 +241,11 @@ class mlgpu_settings(C.Structure):
         ("grid_blocks", C.c_int32),
         ("staged_levels", C.c_int32),
         ("photon_order", C.c_int32),
+        ("walk", C.c_int32),
     ]
 
     TUNING = ("pool_size", "check_period", "use_graph", "grid_blocks", "staged_levels",
-              "photon_order")
+              "photon_order", "walk")
 
     def tuning(self) -> dict:
         return {k: int(getattr(self, k)) for k in self.TUNING}

@@ -370,6 +370,8 @@ int check_propagate_args(const mlgpu_scene* scene, const mlgpu_photons* ph,
         return fail(MLGPU_ERR_INVALID_ARGUMENT, "use_graph must be 0 or 1");
     if (st->photon_order < MLGPU_ORDER_DEFAULT || st->photon_order > MLGPU_ORDER_COHERENT)
         return fail(MLGPU_ERR_INVALID_ARGUMENT, "unknown photon_order %d", st->photon_order);
+    if (st->walk < MLGPU_WALK_DEFAULT || st->walk > MLGPU_WALK_STACK)
+        return fail(MLGPU_ERR_INVALID_ARGUMENT, "unknown walk %d", st->walk);
     return MLGPU_OK;
 }
 
@@ -519,6 +521,7 @@ int run_wavefront(mlgpu_scene* scene, TraceArgs a, const mlgpu_settings* st,
     const int rc = wave_buffers(scene, pool, st->grid_blocks, st->staged_levels, &w,
                                 &pools[0], &pools[1]);
     if (rc) return rc;
+    w.walk = st->walk == MLGPU_WALK_STACK ? MLGPU_WALK_STACK : MLGPU_WALK_LEVELS;
     // per-kernel events cannot be taken inside a graph: profiling runs launch by launch
     const bool graph = st->use_graph != 0 && !scene->prof.on;
     int period = st->check_period > 0 ? st->check_period : 4;
@@ -722,6 +725,7 @@ int mlgpu_scene_autotune(mlgpu_scene* scene, const mlgpu_photons* sample, uint64
     cur.pool_size = 0; cur.check_period = 0; cur.use_graph = 1; cur.grid_blocks = 0;
     cur.staged_levels = 0;
     cur.photon_order = MLGPU_ORDER_DEFAULT;
+    cur.walk = MLGPU_WALK_DEFAULT;
     double cur_ms = 0.0;
     st = time_of(cur, &cur_ms);
     // candidate values of each knob, tried one knob at a time
@@ -731,9 +735,10 @@ int mlgpu_scene_autotune(mlgpu_scene* scene, const mlgpu_photons* sample, uint64
     const int stages[] = {0, 3, 5};
     const int graphs[] = {0, 1};
     const int orders[] = {MLGPU_ORDER_INPUT, MLGPU_ORDER_COHERENT};
+    const int walks[] = {MLGPU_WALK_LEVELS, MLGPU_WALK_STACK};
     for (int pass = 0; pass < 2 && st == MLGPU_OK; pass++) {
         const double start_ms = cur_ms;
-        for (int knob = 0; knob < 6 && st == MLGPU_OK; knob++) {
+        for (int knob = 0; knob < 7 && st == MLGPU_OK; knob++) {
             const int count = knob <= 1 ? 4 : knob <= 3 ? 3 : 2;
             for (int c = 0; c < count && st == MLGPU_OK; c++) {
                 mlgpu_settings cand = cur;
@@ -746,7 +751,8 @@ int mlgpu_scene_autotune(mlgpu_scene* scene, const mlgpu_photons* sample, uint64
                 case 2: cand.grid_blocks = grids[c]; break;
                 case 3: cand.staged_levels = stages[c]; break;
                 case 4: cand.use_graph = graphs[c]; break;
-                default: cand.photon_order = orders[c]; break;
+                case 5: cand.photon_order = orders[c]; break;
+                default: cand.walk = walks[c]; break;
                 }
                 if (std::memcmp(&cand, &cur, sizeof(cand)) == 0) continue;
                 double ms = 0.0;

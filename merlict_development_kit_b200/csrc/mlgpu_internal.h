@@ -180,6 +180,7 @@ struct WaveBuffers {
     uint32_t pool;
     int grid;                // blocks of the persistent (grid-stride) kernels
     int staged_levels;       // BVH levels whose nodes each block stages in shared memory
+    int walk;                // MLGPU_WALK_LEVELS or MLGPU_WALK_STACK
     int fn_smem_bytes;       // property tables staged in shared memory (0: read from global)
     int32_t* step;           // [pool] 0, or kNoStep: the photon takes no step
     float4* ray_o;           // [pool] single-precision origin, box inflation

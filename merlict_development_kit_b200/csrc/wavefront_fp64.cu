@@ -14,6 +14,8 @@
 //   spheres    one thread per (ray, leaf range): merlict's own bounding-sphere
 //              test of each leaf (RayAndFrame.cpp:16-107); the leaves that
 //              pass are the ray's candidates;
+//   (or walk   one thread per ray: levels and spheres in one depth-first
+//              walk with a stack, the same tests, the same candidates;)
 //   intersect, ties, overflow, resolve: wave_resolve.cuh.
 // The arithmetic is the shared FP64 code, compiled with --fmad=false.
 #include <cstdint>
@@ -138,8 +140,29 @@ wave_intake_kernel(const TraceArgs a, const WaveBuffers w, const RayPool cur) {
     }
 }
 
-// One BVH level: the four child boxes of each queued (ray, node) pair, slab
-// tests in single precision on boxes widened by the ray's rounding.  With
+// The four child boxes of a BVH node: slab tests in single precision on
+// boxes widened by the ray's rounding (o.w).  Bit k of the result: child k
+// is hit.
+__device__ __forceinline__ uint32_t node_box_hits(float4 lx, float4 ly, float4 lz, float4 hx,
+                                                  float4 hy, float4 hz, const int32_t* child,
+                                                  float4 o, float4 iv) {
+    const float lox[4] = {lx.x, lx.y, lx.z, lx.w}, loy[4] = {ly.x, ly.y, ly.z, ly.w};
+    const float loz[4] = {lz.x, lz.y, lz.z, lz.w}, hix[4] = {hx.x, hx.y, hx.z, hx.w};
+    const float hiy[4] = {hy.x, hy.y, hy.z, hy.w}, hiz[4] = {hz.x, hz.y, hz.z, hz.w};
+    uint32_t hit = 0;
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+        const float ax = (lox[k] - o.w - o.x)*iv.x, bx = (hix[k] + o.w - o.x)*iv.x;
+        const float ay = (loy[k] - o.w - o.y)*iv.y, by = (hiy[k] + o.w - o.y)*iv.y;
+        const float az = (loz[k] - o.w - o.z)*iv.z, bz = (hiz[k] + o.w - o.z)*iv.z;
+        const float tmin = fmaxf(fmaxf(fminf(ax, bx), fminf(ay, by)), fmaxf(fminf(az, bz), 0.0f));
+        const float tmax = fminf(fminf(fmaxf(ax, bx), fmaxf(ay, by)), fmaxf(az, bz));
+        if (tmin <= tmax && child[k] != kBvhEmpty) hit |= 1u << k;
+    }
+    return hit;
+}
+
+// One BVH level: the four child boxes of each queued (ray, node) pair.  With
 // `staged` > 0 the block first copies the level's `staged` nodes (a
 // contiguous range, the tree being numbered breadth first) into shared
 // memory and reads them from there.
@@ -182,19 +205,8 @@ wave_level_kernel(const TraceArgs a, const WaveBuffers w, int level, int staged)
                 hx = __ldg(nq + 3); hy = __ldg(nq + 4); hz = __ldg(nq + 5);
                 ch = __ldg(reinterpret_cast<const int4*>(nq + 6));
             }
-            const float lox[4] = {lx.x, lx.y, lx.z, lx.w}, loy[4] = {ly.x, ly.y, ly.z, ly.w};
-            const float loz[4] = {lz.x, lz.y, lz.z, lz.w}, hix[4] = {hx.x, hx.y, hx.z, hx.w};
-            const float hiy[4] = {hy.x, hy.y, hy.z, hy.w}, hiz[4] = {hz.x, hz.y, hz.z, hz.w};
             child[0] = ch.x; child[1] = ch.y; child[2] = ch.z; child[3] = ch.w;
-#pragma unroll
-            for (int k = 0; k < 4; k++) {
-                const float ax = (lox[k] - o.w - o.x)*iv.x, bx = (hix[k] + o.w - o.x)*iv.x;
-                const float ay = (loy[k] - o.w - o.y)*iv.y, by = (hiy[k] + o.w - o.y)*iv.y;
-                const float az = (loz[k] - o.w - o.z)*iv.z, bz = (hiz[k] + o.w - o.z)*iv.z;
-                const float tmin = fmaxf(fmaxf(fminf(ax, bx), fminf(ay, by)), fmaxf(fminf(az, bz), 0.0f));
-                const float tmax = fminf(fminf(fmaxf(ax, bx), fmaxf(ay, by)), fmaxf(az, bz));
-                if (tmin <= tmax && child[k] != kBvhEmpty) hit |= 1u << k;
-            }
+            hit = node_box_hits(lx, ly, lz, hx, hy, hz, child, o, iv);
         }
         uint32_t nn = 0, nr = 0;
 #pragma unroll
@@ -282,6 +294,92 @@ wave_sphere_kernel(const TraceArgs a, const WaveBuffers w, const RayPool cur) {
     }
 }
 
+// The whole walk of a ray in one thread: a depth-first walk of the BVH with
+// a stack, the same box tests as wave_level_kernel and the same sphere tests
+// as wave_sphere_kernel, so the same candidate leaves; they are queued once
+// per warp after the walk.  A ray whose stack or candidate list fills up
+// goes to merlict's own walk (the overflow kernel).  One thread per ray of
+// the root queue; the ray's FP64 state is read when its first leaf range
+// is hit.
+constexpr int kWalkStack = 3*kMaxBvhLevels + 4;
+constexpr int kWalkCands = 32;
+
+template <bool kF32>
+__global__ void __launch_bounds__(256)
+wave_walk_kernel(const TraceArgs a, const WaveBuffers w, const RayPool cur) {
+    const DevScene& sc = a.scene;
+    const uint32_t len = w.counters->level_len[0];
+    const uint32_t n = len < w.level_cap ? len : w.level_cap;
+    const int lane = threadIdx.x & 31;
+    for (uint32_t first = warp_first(); first < n; first += gridDim.x*blockDim.x) {
+        const uint32_t e = first + (uint32_t)lane;
+        uint32_t slot = 0;
+        int32_t cand[kWalkCands];
+        uint32_t nc = 0;
+        bool over = false;
+        if (e < n) {
+            const uint2 q = w.level_q[0][e];
+            slot = q.x;
+            const float4 o = w.ray_o[slot], iv = w.ray_i[slot];
+            const float3 dv = make_float3(1.0f/iv.x, 1.0f/iv.y, 1.0f/iv.z);
+            v3 s = mk(0, 0, 0), d = mk(0, 0, 0);
+            double sd = 0.0;
+            bool have_ray = false;
+            int32_t stack[kWalkStack];
+            int sp = 0;
+            stack[sp++] = (int32_t)q.y;
+            while (sp > 0 && !over) {
+                const float4* nq = reinterpret_cast<const float4*>(sc.bvh + stack[--sp]);
+                const float4 lx = __ldg(nq), ly = __ldg(nq + 1), lz = __ldg(nq + 2);
+                const float4 hx = __ldg(nq + 3), hy = __ldg(nq + 4), hz = __ldg(nq + 5);
+                const int4 ch = __ldg(reinterpret_cast<const int4*>(nq + 6));
+                const int32_t child[4] = {ch.x, ch.y, ch.z, ch.w};
+                const uint32_t hit = node_box_hits(lx, ly, lz, hx, hy, hz, child, o, iv);
+                for (int k = 3; k >= 0; k--) {
+                    if (!(hit & (1u << k))) continue;
+                    if (child[k] >= 0) {
+                        if (sp < kWalkStack) stack[sp++] = child[k];
+                        else over = true;
+                        continue;
+                    }
+                    const int32_t ref = child[k];
+                    const int32_t start = (ref & 0x7fffffff) >> 3;
+                    const int32_t count = (ref & 7) + 1;
+                    if (!kF32 && !have_ray) {
+                        s = mk(cur.sx[slot], cur.sy[slot], cur.sz[slot]);
+                        d = mk(cur.dx[slot], cur.dy[slot], cur.dz[slot]);
+                        sd = dot(s, d);
+                        have_ray = true;
+                    }
+                    for (int32_t j = start; j < start + count; j++) {
+                        bool pass;
+                        if (kF32) {
+                            pass = sphere_cull32(__ldg(sc.bvh_sphere_f + j), o, dv);
+                        } else {
+                            const double2* c = reinterpret_cast<const double2*>(sc.bvh_sphere + j);
+                            const double2 c01 = __ldg(c), c23 = __ldg(c + 1);
+                            pass = sphere_cull(make_double4(c01.x, c01.y, c23.x, c23.y), s, d, sd);
+                        }
+                        if (pass) {
+                            if (nc < (uint32_t)kWalkCands) cand[nc++] = __ldg(sc.bvh_leaf + j);
+                            else over = true;
+                        }
+                    }
+                }
+            }
+        }
+        if (over) {
+            mark_overflow(w, slot);
+            nc = 0;
+        }
+        const uint32_t cb = warp_reserve(&w.counters->isect_len, nc);
+        for (uint32_t k = 0; k < nc; k++) {
+            if (cb + k < w.isect_cap) w.isect_q[cb + k] = make_uint2(slot, (uint32_t)cand[k]);
+            else mark_overflow(w, slot);
+        }
+    }
+}
+
 // counters between the kernels of an iteration
 __global__ void wave_after_intake_kernel(WaveCounters* c, uint32_t pool, uint64_t num_photons) {
     const unsigned long long remaining = num_photons - c->next_input;
@@ -314,13 +412,19 @@ cudaError_t launch_wave_iteration(const TraceArgs& a, const WaveBuffers& w, cons
         wave_intake_kernel<float><<<slot_blocks, 256, 0, s>>>(a, w, cur);
     wave_after_intake_kernel<<<1, 1, 0, s>>>(w.counters, w.pool, a.num_photons);
     if (ev) cudaEventRecord(ev[1], s);
-    for (int k = 0; k < a.scene.bvh_levels; k++) {
-        const int count = a.scene.bvh_level_start[k + 1] - a.scene.bvh_level_start[k];
-        const int staged = k < w.staged_levels && count <= kMaxStagedNodes ? count : 0;
-        wave_level_kernel<<<w.grid, 256, (size_t)staged*sizeof(BvhNode4), s>>>(a, w, k, staged);
+    if (w.walk == MLGPU_WALK_STACK) {
+        if (form == MLGPU_TRACER_FP64) wave_walk_kernel<false><<<w.grid, 256, 0, s>>>(a, w, cur);
+        else wave_walk_kernel<true><<<w.grid, 256, 0, s>>>(a, w, cur);
+    } else {
+        for (int k = 0; k < a.scene.bvh_levels; k++) {
+            const int count = a.scene.bvh_level_start[k + 1] - a.scene.bvh_level_start[k];
+            const int staged = k < w.staged_levels && count <= kMaxStagedNodes ? count : 0;
+            wave_level_kernel<<<w.grid, 256, (size_t)staged*sizeof(BvhNode4), s>>>(a, w, k,
+                                                                                   staged);
+        }
+        if (form == MLGPU_TRACER_FP64) wave_sphere_kernel<false><<<w.grid, 256, 0, s>>>(a, w, cur);
+        else wave_sphere_kernel<true><<<w.grid, 256, 0, s>>>(a, w, cur);
     }
-    if (form == MLGPU_TRACER_FP64) wave_sphere_kernel<false><<<w.grid, 256, 0, s>>>(a, w, cur);
-    else wave_sphere_kernel<true><<<w.grid, 256, 0, s>>>(a, w, cur);
     if (ev) cudaEventRecord(ev[2], s);
     if (form == MLGPU_TRACER_FP64) {
         wave_isect_kernel<kIsectFp64><<<w.grid, 256, 0, s>>>(a, w, cur);

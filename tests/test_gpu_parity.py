@@ -184,3 +184,35 @@ def test_production_mode_histograms_match_the_reference(eng):
     assert chi2 < dof + 5 * np.sqrt(2 * dof), (chi2, dof)
     ks = stats.ks_2samp(ref["time"][ref["sensor"] >= 0], got["time"][got["sensor"] >= 0])
     assert ks.pvalue > 1e-3, ks
+
+
+@pytest.mark.parametrize("name,n", [("reflector_camera", 200_000), ("light_field_small", 100_000),
+                                    ("primitive_zoo", 200_000)])
+def test_stack_walk_finds_the_same_hits(eng, oracle, name, n):
+    """walk=STACK (one thread walks a ray's whole BVH) against the oracle,
+    and against walk=LEVELS for the FP32 forms: the same candidates, so
+    the same results."""
+    flat, _, _, meta = load_golden(name)
+    if name == "primitive_zoo":
+        ph = P.isotropic_shell_source(n, 321, 4.0, 2.5)
+    elif name == "light_field_small":
+        ph = P.downward_disc_source(n, 321, 5.55, 21.4, 0.5)
+    else:
+        ph = P.downward_disc_source(n, 321, 2.0, 10.0, 1.5)
+    status, ref, _ = oracle.propagate(flat, ph, meta["max_interactions"], seed=78)
+    assert status == 0
+    scene = eng.Scene(flat)
+    dev = eng.photons_to_device(ph)
+    outs = ("sensor", "x", "y", "time", "final_leaf")
+    for tracer in ("fp64", "fp32"):
+        got = {}
+        for walk in (1, 2):
+            o = scene.propagate(dev, eng.PropagationConfig(meta["max_interactions"]),
+                                eng.Philox(78), tracer=tracer, outputs=outs,
+                                tuning={"walk": walk})
+            got[walk] = {k: v.cpu().numpy() for k, v in o.items()}
+        for k in outs:
+            assert np.array_equal(got[1][k], got[2][k]), (tracer, k)
+        if tracer == "fp64":
+            assert mismatches(ref, got[2]) == {}
+    scene.close()
