@@ -6,6 +6,7 @@
 #ifndef MLGPU_FP64_GEOMETRY_CUH_
 #define MLGPU_FP64_GEOMETRY_CUH_
 
+#include <cstddef>
 #include <cstdint>
 
 #include "mlgpu_internal.h"
@@ -366,18 +367,38 @@ __device__ __forceinline__ void test_candidate(const DevScene& sc, int32_t leaf,
 }
 
 // merlict's intersection of one leaf with a world ray; leaf < 0 if none.
+// The first 200 bytes of a leaf record (T, tinv, params, r2, primitive) in
+// 16-byte loads: a warp whose lanes hold different leaves issues half as
+// many load requests as with 8-byte loads.
+static_assert(offsetof(LeafRec, tinv) == 96 && offsetof(LeafRec, params) == 120 &&
+              offsetof(LeafRec, r2) == 184 && offsetof(LeafRec, primitive) == 192,
+              "load_leaf reads the leaf record in 16-byte pieces");
+__device__ __forceinline__ void load_leaf(const LeafRec* L, double* T, double* ti, double* pr,
+                                          double* r2, int32_t* prim) {
+    const double2* q = reinterpret_cast<const double2*>(L);
+    double v[24];
+#pragma unroll
+    for (int k = 0; k < 12; k++) {
+        const double2 x = __ldg(q + k);
+        v[2*k] = x.x;
+        v[2*k + 1] = x.y;
+    }
+#pragma unroll
+    for (int k = 0; k < 12; k++) T[k] = v[k];
+    ti[0] = v[12]; ti[1] = v[13]; ti[2] = v[14];
+#pragma unroll
+    for (int k = 0; k < MLGPU_LEAF_PARAMS; k++) pr[k] = v[15 + k];
+    *r2 = v[23];
+    *prim = __ldg(&L->primitive);
+}
+
 __device__ __forceinline__ Isec leaf_hit(const DevScene& sc, int32_t leaf, v3 s, v3 d) {
-    const LeafRec* L = sc.leaf + leaf;
-    double T[12], ti[3], pr[MLGPU_LEAF_PARAMS];
-#pragma unroll
-    for (int k = 0; k < 12; k++) T[k] = __ldg(&L->T[k]);
-#pragma unroll
-    for (int k = 0; k < 3; k++) ti[k] = __ldg(&L->tinv[k]);
-#pragma unroll
-    for (int k = 0; k < MLGPU_LEAF_PARAMS; k++) pr[k] = __ldg(&L->params[k]);
+    double T[12], ti[3], pr[MLGPU_LEAF_PARAMS], r2;
+    int32_t prim;
+    load_leaf(sc.leaf + leaf, T, ti, pr, &r2, &prim);
     Isec h;
-    intersect_leaf(sc, leaf, __ldg(&L->primitive), pr, __ldg(&L->r2), position_inverse(T, ti, s),
-                   orientation_inverse(T, d), &h);
+    intersect_leaf(sc, leaf, prim, pr, r2, position_inverse(T, ti, s), orientation_inverse(T, d),
+                   &h);
     return h;
 }
 

@@ -230,8 +230,13 @@ wave_resolve_kernel(const TraceArgs a, const WaveBuffers w, const RayPool cur, c
             const bool hit = is.leaf >= 0;
             const LeafRec* L = hit ? sc.leaf + is.leaf : nullptr;
             if (hit) {
+                const double2* q = reinterpret_cast<const double2*>(L->T);
 #pragma unroll
-                for (int k = 0; k < 12; k++) T[k] = __ldg(&L->T[k]);
+                for (int k = 0; k < 6; k++) {
+                    const double2 x = __ldg(q + k);
+                    T[2*k] = x.x;
+                    T[2*k + 1] = x.y;
+                }
             } else {
 #pragma unroll
                 for (int k = 0; k < 12; k++) T[k] = IDENTITY[k];
@@ -239,10 +244,16 @@ wave_resolve_kernel(const TraceArgs a, const WaveBuffers w, const RayPool cur, c
             int32_t fn[6] = {0, 0, 0, 0, 0, 0};
             int32_t flags = 0, allowed = -1;
             if (hit) {
-#pragma unroll
-                for (int k = 0; k < 6; k++) fn[k] = __ldg(&L->fn[k]);
-                flags = __ldg(&L->flags);
-                allowed = __ldg(&L->allowed_node);
+                static_assert(offsetof(LeafRec, allowed_node) == 200 &&
+                              offsetof(LeafRec, flags) == 204 && offsetof(LeafRec, fn) == 208,
+                              "the resolve step reads these fields in 8- and 16-byte pieces");
+                const int2 af = __ldg(reinterpret_cast<const int2*>(&L->allowed_node));
+                const int4 f03 = __ldg(reinterpret_cast<const int4*>(L->fn));
+                const int2 f45 = __ldg(reinterpret_cast<const int2*>(L->fn + 4));
+                allowed = af.x;
+                flags = af.y;
+                fn[0] = f03.x; fn[1] = f03.y; fn[2] = f03.z; fn[3] = f03.w;
+                fn[4] = f45.x; fn[5] = f45.y;
             }
             auto draw = [&]() -> double {
                 const uint32_t k = (uint32_t)k_draw++;
