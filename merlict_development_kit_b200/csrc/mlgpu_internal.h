@@ -185,6 +185,8 @@ struct WaveBuffers {
     int32_t* step;           // [pool] 0, or kNoStep: the photon takes no step
     float4* ray_o;           // [pool] single-precision origin, box inflation
     float4* ray_i;           // [pool] reciprocal direction
+    double2* ray_sd;         // [pool][3] the FP64 support and direction, one 48-byte
+                             // record per slot for the kernels that read rays by queue
     uint2* level_q[2];       // (slot, node) pairs, ping-pong between BVH levels
     uint32_t level_cap;
     uint2* range_q;          // (slot, BVH leaf-range reference)

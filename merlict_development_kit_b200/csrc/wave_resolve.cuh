@@ -89,6 +89,13 @@ __device__ __forceinline__ uint32_t warp_first() {
     return blockIdx.x*blockDim.x + (threadIdx.x & ~31u);
 }
 
+// The FP64 ray of a slot from its 48-byte record (written by the intake).
+__device__ __forceinline__ void load_ray(const WaveBuffers& w, uint32_t slot, v3* s, v3* d) {
+    const double2 a = w.ray_sd[3*slot], b = w.ray_sd[3*slot + 1], c = w.ray_sd[3*slot + 2];
+    *s = mk(a.x, a.y, b.x);
+    *d = mk(b.y, c.x, c.y);
+}
+
 template <int kIsect>
 __global__ void __launch_bounds__(256)
 wave_isect_kernel(const TraceArgs a, const WaveBuffers w, const RayPool cur) {
@@ -98,8 +105,8 @@ wave_isect_kernel(const TraceArgs a, const WaveBuffers w, const RayPool cur) {
         const uint2 q = w.isect_q[e];
         const uint32_t slot = q.x;
         const int32_t leaf = (int32_t)q.y;
-        const v3 s = mk(cur.sx[slot], cur.sy[slot], cur.sz[slot]);
-        const v3 d = mk(cur.dx[slot], cur.dy[slot], cur.dz[slot]);
+        v3 s, d;
+        load_ray(w, slot, &s, &d);
         double dist = -1.0;
         if (kIsect == kIsectFp64) {
             const Isec h = leaf_hit(sc, leaf, s, d);

@@ -77,6 +77,9 @@ wave_intake_kernel(const TraceArgs a, const WaveBuffers w, const RayPool cur) {
             root = cur.root[slot];
             n_int = (uint32_t)cur.n_int[slot];
         }
+        w.ray_sd[3*slot] = make_double2(s.x, s.y);
+        w.ray_sd[3*slot + 1] = make_double2(s.z, d.x);
+        w.ray_sd[3*slot + 2] = make_double2(d.y, d.z);
         w.best_key[slot] = kNoKey;
         w.best_leaf[slot] = kNoLeaf;
         w.overflow_flag[slot] = 0u;
@@ -275,8 +278,8 @@ wave_sphere_kernel(const TraceArgs a, const WaveBuffers w, const RayPool cur) {
                     if (sphere_cull32(__ldg(sc.bvh_sphere_f + j), o, dv))
                         pass[np++] = __ldg(sc.bvh_leaf + j);
             } else {
-                const v3 s = mk(cur.sx[slot], cur.sy[slot], cur.sz[slot]);
-                const v3 d = mk(cur.dx[slot], cur.dy[slot], cur.dz[slot]);
+                v3 s, d;
+                load_ray(w, slot, &s, &d);
                 const double sd = dot(s, d);
                 for (int32_t j = start; j < start + count; j++) {
                     const double2* c = reinterpret_cast<const double2*>(sc.bvh_sphere + j);
@@ -346,8 +349,7 @@ wave_walk_kernel(const TraceArgs a, const WaveBuffers w, const RayPool cur) {
                     const int32_t start = (ref & 0x7fffffff) >> 3;
                     const int32_t count = (ref & 7) + 1;
                     if (!kF32 && !have_ray) {
-                        s = mk(cur.sx[slot], cur.sy[slot], cur.sz[slot]);
-                        d = mk(cur.dx[slot], cur.dy[slot], cur.dz[slot]);
+                        load_ray(w, slot, &s, &d);
                         sd = dot(s, d);
                         have_ray = true;
                     }
