@@ -20,6 +20,7 @@
 #ifndef MLGPU_FP32_GEOMETRY_CUH_
 #define MLGPU_FP32_GEOMETRY_CUH_
 
+#include <cstddef>
 #include <cstdint>
 
 #include "mlgpu_internal.h"
@@ -108,8 +109,17 @@ template <bool kNeedHit>
 __device__ Hit32 intersect32(const DevScene& sc, int32_t leaf, d3 s, d3 d, bool pure) {
     Hit32 h;
     h.leaf = -1;
-    const LeafRecF* L = sc.leaf_f + leaf;
-    const int32_t prim = __ldg(&L->primitive);
+    // R, params, r2 and primitive: the record's first 80 bytes in 16-byte loads
+    static_assert(offsetof(LeafRecF, params) == 36 && offsetof(LeafRecF, r2) == 68 &&
+                  offsetof(LeafRecF, primitive) == 72, "intersect32 reads LeafRecF in pieces");
+    const float4* Lq = reinterpret_cast<const float4*>(sc.leaf_f + leaf);
+    float v[20];
+#pragma unroll
+    for (int k = 0; k < 5; k++) {
+        const float4 x = __ldg(Lq + k);
+        v[4*k] = x.x; v[4*k + 1] = x.y; v[4*k + 2] = x.z; v[4*k + 3] = x.w;
+    }
+    const int32_t prim = __float_as_int(v[18]);
     if (prim == MLGPU_PRIM_NONE) return h;
     const LeafAnchor* A = sc.leaf_anchor + leaf;
     const double2 o01 = __ldg(reinterpret_cast<const double2*>(A) + 0);   // origin x, y
@@ -117,8 +127,8 @@ __device__ Hit32 intersect32(const DevScene& sc, int32_t leaf, d3 s, d3 d, bool 
     const d3 c = dmk(o01.x, o01.y, o2R.x);
     float R[9];
 #pragma unroll
-    for (int k = 0; k < 9; k++) R[k] = __ldg(&L->R[k]);
-    const float r2 = __ldg(&L->r2);
+    for (int k = 0; k < 9; k++) R[k] = v[k];
+    const float r2 = v[17];
     // rebase the ray (FP64) to where it enters the leaf's bounding sphere,
     // then go to the leaf frame (FP32).  A ray that starts inside the sphere
     // -- on the surface it just left, say -- is not moved, so its
@@ -134,7 +144,7 @@ __device__ Hit32 intersect32(const DevScene& sc, int32_t leaf, d3 s, d3 d, bool 
     const f3 dl = to_local(R, fmk((float)d.x, (float)d.y, (float)d.z));
     float pr[MLGPU_LEAF_PARAMS];
 #pragma unroll
-    for (int k = 0; k < MLGPU_LEAF_PARAMS; k++) pr[k] = __ldg(&L->params[k]);
+    for (int k = 0; k < MLGPU_LEAF_PARAMS; k++) pr[k] = v[9 + k];
     const double v_min = 1e-7;   // merlict's self-intersection guard, |hit - support|^2 > 1e-14
 
     switch (prim) {
