@@ -421,7 +421,9 @@ def run_ours(args, world, rank, local):
     achieved_gbs = bpp * n / (kernel_ms * 1e-3) / 1e9
     hbm = {"bound": "hbm", "achieved": achieved_gbs, "peak": hbm_peak, "unit": "GB/s",
            "frac": achieved_gbs / hbm_peak,
-           "peak_source": f"{peak_kind} MEASURED_PEAKS.json hbm_gbs",
+           "peak_source": ("measured: MEASURED_PEAKS.json hbm_gbs" if peak_kind == "measured"
+                           else "fallback: 6,650 GB/s of the profiling recipe (no "
+                                "MEASURED_PEAKS.json)"),
            "bytes_per_photon": bpp, "scope": "whole propagate call"}
     cpu = None
     if world == 1 and not args.no_cpu_baseline:
