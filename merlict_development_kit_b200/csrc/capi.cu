@@ -123,6 +123,9 @@ struct Profiler {
 
 }  // namespace
 
+// Pieces of an mlgpu_propagate_host batch at most.
+constexpr int kHostChunks = 4;
+
 struct mlgpu_scene {
     int device = 0;
     DevScene dev;
@@ -137,12 +140,17 @@ struct mlgpu_scene {
     // ray pools of the wavefront tracers
     DeviceBuffer wave;
     WaveCounters* wave_host = nullptr;   // pinned copy of the counters
+    WaveCounters* wave_host_dev = nullptr;   // its device address
     int wave_grid = 0;                   // default blocks of the persistent kernels
     // one check period of wavefront iterations as a CUDA graph, recorded on
     // a private stream and replayed on the caller's
     cudaGraphExec_t wave_graph = nullptr;
     cudaStream_t capture_stream = nullptr;
     uint64_t launches = 0;               // kernels launched for this scene
+    // mlgpu_propagate_host's pipeline: trace, upload and download streams;
+    // events: the caller's default stream, inputs of each piece, results of each piece
+    cudaStream_t host_stream[3] = {nullptr, nullptr, nullptr};
+    cudaEvent_t host_event[1 + 2*kHostChunks] = {};
     Profiler prof;
 };
 
@@ -415,6 +423,9 @@ int wave_buffers(mlgpu_scene* scene, uint32_t pool, int grid, int staged, WaveBu
         up(isect_cap*8) + up(isect_cap*8) + up(P*8) + 3*up(P*4);
     MLGPU_CUDA(scene->wave.reserve(256 + 2*per_pool + rest));
     if (!scene->wave_host) MLGPU_CUDA(cudaMallocHost(&scene->wave_host, sizeof(WaveCounters)));
+    if (!scene->wave_host_dev)
+        MLGPU_CUDA(cudaHostGetDevicePointer(reinterpret_cast<void**>(&scene->wave_host_dev),
+                                            scene->wave_host, 0));
     if (!scene->wave_grid) scene->wave_grid = wave_persistent_blocks();
     char* b = static_cast<char*>(scene->wave.ptr);
     w->counters = reinterpret_cast<WaveCounters*>(b);
@@ -465,9 +476,7 @@ int record_wave_graph(mlgpu_scene* scene, const TraceArgs& a, const WaveBuffers&
     cudaError_t e = cudaSuccess;
     for (int g = 0; g < period && e == cudaSuccess; g++)
         e = launch_wave_iteration(a, w, pools[g & 1], pools[(g + 1) & 1], form, cs, nullptr);
-    if (e == cudaSuccess)
-        e = cudaMemcpyAsync(scene->wave_host, w.counters, sizeof(WaveCounters),
-                            cudaMemcpyDeviceToHost, cs);
+    if (e == cudaSuccess) e = launch_wave_counters_to_host(w.counters, scene->wave_host_dev, cs);
     cudaGraph_t graph = nullptr;
     const cudaError_t e2 = cudaStreamEndCapture(cs, &graph);
     if (e != cudaSuccess || e2 != cudaSuccess) {
@@ -541,7 +550,7 @@ int run_wavefront(mlgpu_scene* scene, TraceArgs a, const mlgpu_settings* st,
         if (graph) {
             MLGPU_CUDA(cudaGraphLaunch(scene->wave_graph, stream));
             iteration += (uint64_t)period;
-            scene->launches += (uint64_t)period*((uint64_t)levels + 8);
+            scene->launches += (uint64_t)period*((uint64_t)levels + 8) + 1;
         } else {
             for (int g = 0; g < period; g++, iteration++) {
                 const RayPool& cur = pools[iteration & 1];
@@ -561,8 +570,10 @@ int run_wavefront(mlgpu_scene* scene, TraceArgs a, const mlgpu_settings* st,
                     scene->prof.add(ch);
                 }
             }
-            MLGPU_CUDA(cudaMemcpyAsync(scene->wave_host, w.counters, sizeof(WaveCounters),
-                                       cudaMemcpyDeviceToHost, stream));
+            const cudaError_t e = launch_wave_counters_to_host(w.counters, scene->wave_host_dev,
+                                                               stream);
+            if (e != cudaSuccess) return cuda_fail(e, "wavefront counters");
+            scene->launches++;
         }
         MLGPU_CUDA(cudaStreamSynchronize(stream));
         if (scene->wave_host->active == 0 && scene->wave_host->next_input >= a.num_photons) break;
@@ -665,6 +676,10 @@ int mlgpu_scene_destroy(mlgpu_scene* scene) {
     if (scene->wave_host) cudaFreeHost(scene->wave_host);
     if (scene->wave_graph) cudaGraphExecDestroy(scene->wave_graph);
     if (scene->capture_stream) cudaStreamDestroy(scene->capture_stream);
+    for (cudaStream_t hs : scene->host_stream)
+        if (hs) cudaStreamDestroy(hs);
+    for (cudaEvent_t he : scene->host_event)
+        if (he) cudaEventDestroy(he);
     scene->prof.release();
     delete scene;
     return MLGPU_OK;
@@ -1003,76 +1018,141 @@ int mlgpu_propagate_host(mlgpu_scene* scene, const mlgpu_photons* photons, uint6
     const size_t ein = photons->dtype == MLGPU_F64 ? 8 : 4;
     const size_t eout = results->dtype == MLGPU_F64 ? 8 : 4;
     const size_t hist_len = settings->max_num_interactions_per_photon + 1;
-    // input planes, then output planes laid out one after another
-    MLGPU_CUDA(scene->staging_in.reserve(7*ein*n));
-    const size_t out_bytes = n*(4 + 2*eout + 8 + 2*eout + 4 + 4 + 3*8 + 3*8);
-    MLGPU_CUDA(scene->staging_out.reserve(out_bytes));
-    if (results->history)
-        MLGPU_CUDA(scene->staging_hist.reserve(n*hist_len*sizeof(mlgpu_history_entry)));
-    char* din = static_cast<char*>(scene->staging_in.ptr);
+    const size_t hist_row = hist_len*sizeof(mlgpu_history_entry);
+    const size_t stride = rng->mode == MLGPU_RNG_REPLAY ? rng->stride : 0;
     const void* planes[7] = {photons->support_x, photons->support_y, photons->support_z,
                              photons->direction_x, photons->direction_y, photons->direction_z,
                              photons->wavelength};
-    mlgpu_photons dph = *photons;
-    const void** dplanes[7] = {&dph.support_x, &dph.support_y, &dph.support_z,
-                               &dph.direction_x, &dph.direction_y, &dph.direction_z,
-                               &dph.wavelength};
-    cudaStream_t stream = 0;
-    for (int k = 0; k < 7; k++) {
-        MLGPU_CUDA(cudaMemcpyAsync(din + k*ein*n, planes[k], ein*n, cudaMemcpyHostToDevice, stream));
-        *dplanes[k] = din + k*ein*n;
+    // result planes: host pointer and bytes per photon
+    struct Plane { void* host; size_t bytes; };
+    const Plane back[] = {
+        {results->sensor, 4}, {results->x, eout}, {results->y, eout}, {results->time, 8},
+        {results->theta_x, eout}, {results->theta_y, eout}, {results->final_leaf, 4},
+        {results->info, 4}, {results->final_position, 24}, {results->final_direction, 24},
+        {results->history, hist_row},
+    };
+    constexpr int kPlanes = sizeof(back)/sizeof(back[0]);
+
+    // device staging: the input planes one after another, the result planes
+    // each on a 256-byte boundary
+    MLGPU_CUDA(scene->staging_in.reserve(7*ein*n));
+    size_t out_bytes = 0;
+    size_t out_off[kPlanes];
+    for (int k = 0; k < kPlanes - 1; k++) {
+        out_off[k] = out_bytes;
+        if (back[k].host) out_bytes += (back[k].bytes*n + 255) & ~size_t(255);
     }
-    dph.simulation_truth_id = nullptr;
-    mlgpu_rng drng = *rng;
-    if (rng->mode == MLGPU_RNG_REPLAY) {
-        const size_t ub = n*(size_t)rng->stride*sizeof(double);
-        MLGPU_CUDA(scene->staging_rng.reserve(ub));
-        MLGPU_CUDA(cudaMemcpyAsync(scene->staging_rng.ptr, rng->uniforms, ub,
-                                   cudaMemcpyHostToDevice, stream));
-        drng.uniforms = static_cast<const double*>(scene->staging_rng.ptr);
-    }
+    MLGPU_CUDA(scene->staging_out.reserve(out_bytes + 256));
+    if (results->history) MLGPU_CUDA(scene->staging_hist.reserve(n*hist_row));
+    if (stride) MLGPU_CUDA(scene->staging_rng.reserve(n*stride*sizeof(double)));
+    char* din = static_cast<char*>(scene->staging_in.ptr);
     char* dout = static_cast<char*>(scene->staging_out.ptr);
-    mlgpu_results dres;
-    std::memset(&dres, 0, sizeof(dres));
-    dres.dtype = results->dtype;
-    size_t off = 0;
-    auto take = [&](const void* host, size_t bytes) -> void* {
-        if (!host) return nullptr;
-        void* p = dout + off;
-        off += (bytes + 255) & ~size_t(255);
-        return p;
+    void* dev_plane[kPlanes];
+    for (int k = 0; k < kPlanes - 1; k++) dev_plane[k] = back[k].host ? dout + out_off[k] : nullptr;
+    dev_plane[kPlanes - 1] = results->history ? scene->staging_hist.ptr : nullptr;
+
+    // Pieces of at least one ray pool each, when every host buffer is pinned
+    // (copies from pageable memory would not overlap anything)
+    auto pinned = [](const void* p) {
+        if (!p) return true;
+        cudaPointerAttributes at;
+        if (cudaPointerGetAttributes(&at, p) != cudaSuccess) {
+            cudaGetLastError();
+            return false;
+        }
+        return at.type == cudaMemoryTypeHost;
     };
-    // (re-laid out with 256-byte alignment; reserve enough)
-    MLGPU_CUDA(scene->staging_out.reserve(out_bytes + 16*256));
-    dout = static_cast<char*>(scene->staging_out.ptr);
-    dres.sensor = static_cast<int32_t*>(take(results->sensor, 4*n));
-    dres.x = take(results->x, eout*n);
-    dres.y = take(results->y, eout*n);
-    dres.time = static_cast<double*>(take(results->time, 8*n));
-    dres.theta_x = take(results->theta_x, eout*n);
-    dres.theta_y = take(results->theta_y, eout*n);
-    dres.final_leaf = static_cast<int32_t*>(take(results->final_leaf, 4*n));
-    dres.info = static_cast<uint32_t*>(take(results->info, 4*n));
-    dres.final_position = static_cast<double*>(take(results->final_position, 24*n));
-    dres.final_direction = static_cast<double*>(take(results->final_direction, 24*n));
-    dres.history = results->history
-        ? static_cast<mlgpu_history_entry*>(scene->staging_hist.ptr) : nullptr;
-    const TraceArgs a = make_args(scene, &dph, n, settings, &drng, &dres);
-    st = launch(scene, a, settings, stream);
-    if (st) return st;
-    struct Back { void* host; const void* dev; size_t bytes; };
-    const Back back[] = {
-        {results->sensor, dres.sensor, 4*n}, {results->x, dres.x, eout*n},
-        {results->y, dres.y, eout*n}, {results->time, dres.time, 8*n},
-        {results->theta_x, dres.theta_x, eout*n}, {results->theta_y, dres.theta_y, eout*n},
-        {results->final_leaf, dres.final_leaf, 4*n}, {results->info, dres.info, 4*n},
-        {results->final_position, dres.final_position, 24*n},
-        {results->final_direction, dres.final_direction, 24*n},
-        {results->history, dres.history, n*hist_len*sizeof(mlgpu_history_entry)},
+    bool all_pinned = !stride || pinned(rng->uniforms);
+    for (const void* p : planes) all_pinned = all_pinned && pinned(p);
+    for (const Plane& b : back) all_pinned = all_pinned && pinned(b.host);
+    const uint64_t pool = settings->tracer == MLGPU_TRACER_FP64_PLAIN || !settings->pool_size
+        ? kWavePool : settings->pool_size;
+    const int chunks = all_pinned
+        ? (int)std::max<uint64_t>(1, std::min<uint64_t>(kHostChunks, n/pool)) : 1;
+
+    if (!scene->host_stream[0]) {
+        for (cudaStream_t& hs : scene->host_stream)
+            MLGPU_CUDA(cudaStreamCreateWithFlags(&hs, cudaStreamNonBlocking));
+        for (cudaEvent_t& he : scene->host_event)
+            MLGPU_CUDA(cudaEventCreateWithFlags(&he, cudaEventDisableTiming));
+    }
+    cudaStream_t trace = scene->host_stream[0], upload = scene->host_stream[1],
+                 download = scene->host_stream[2];
+    cudaEvent_t* in_ready = scene->host_event + 1;
+    cudaEvent_t* out_ready = scene->host_event + 1 + kHostChunks;
+    // after the caller's work on the legacy default stream, as a call on it would be
+    MLGPU_CUDA(cudaEventRecord(scene->host_event[0], 0));
+    MLGPU_CUDA(cudaStreamWaitEvent(upload, scene->host_event[0], 0));
+    MLGPU_CUDA(cudaStreamWaitEvent(trace, scene->host_event[0], 0));
+    auto first = [&](int c) { return n*(uint64_t)c/(uint64_t)chunks; };
+    // every piece's inputs are queued at once; each piece records its arrival
+    for (int c = 0; c < chunks; c++) {
+        const uint64_t a0 = first(c), len = first(c + 1) - a0;
+        for (int k = 0; k < 7; k++)
+            MLGPU_CUDA(cudaMemcpyAsync(din + (k*n + a0)*ein,
+                                       static_cast<const char*>(planes[k]) + a0*ein, len*ein,
+                                       cudaMemcpyHostToDevice, upload));
+        if (stride)
+            MLGPU_CUDA(cudaMemcpyAsync(static_cast<double*>(scene->staging_rng.ptr) + a0*stride,
+                                       rng->uniforms + a0*stride, len*stride*sizeof(double),
+                                       cudaMemcpyHostToDevice, upload));
+        MLGPU_CUDA(cudaEventRecord(in_ready[c], upload));
+    }
+    // a failed piece leaves no copy in flight behind it
+    auto drain = [&](int code) {
+        cudaStreamSynchronize(upload);
+        cudaStreamSynchronize(trace);
+        cudaStreamSynchronize(download);
+        return code;
     };
-    for (const Back& b : back)
-        if (b.host) MLGPU_CUDA(cudaMemcpyAsync(b.host, b.dev, b.bytes, cudaMemcpyDeviceToHost, stream));
-    return mlgpu_scene_sync_errors(scene, stream);
+    for (int c = 0; c < chunks; c++) {
+        const uint64_t a0 = first(c), len = first(c + 1) - a0;
+        if (cudaStreamWaitEvent(trace, in_ready[c], 0) != cudaSuccess)
+            return drain(cuda_fail(cudaGetLastError(), "pipeline event"));
+        // photon i of the piece is photon a0 + i of the batch
+        mlgpu_photons dph = *photons;
+        const void** dp[7] = {&dph.support_x, &dph.support_y, &dph.support_z, &dph.direction_x,
+                              &dph.direction_y, &dph.direction_z, &dph.wavelength};
+        for (int k = 0; k < 7; k++) *dp[k] = din + (k*n + a0)*ein;
+        dph.simulation_truth_id = nullptr;
+        mlgpu_rng drng = *rng;
+        drng.photon_offset = rng->photon_offset + a0;
+        if (stride) drng.uniforms = static_cast<const double*>(scene->staging_rng.ptr) + a0*stride;
+        mlgpu_results dres;
+        std::memset(&dres, 0, sizeof(dres));
+        dres.dtype = results->dtype;
+        void* piece[kPlanes];
+        for (int k = 0; k < kPlanes; k++)
+            piece[k] = dev_plane[k] ? static_cast<char*>(dev_plane[k]) + a0*back[k].bytes : nullptr;
+        dres.sensor = static_cast<int32_t*>(piece[0]);
+        dres.x = piece[1];
+        dres.y = piece[2];
+        dres.time = static_cast<double*>(piece[3]);
+        dres.theta_x = piece[4];
+        dres.theta_y = piece[5];
+        dres.final_leaf = static_cast<int32_t*>(piece[6]);
+        dres.info = static_cast<uint32_t*>(piece[7]);
+        dres.final_position = static_cast<double*>(piece[8]);
+        dres.final_direction = static_cast<double*>(piece[9]);
+        dres.history = static_cast<mlgpu_history_entry*>(piece[10]);
+        const TraceArgs a = make_args(scene, &dph, len, settings, &drng, &dres);
+        st = launch(scene, a, settings, trace);
+        if (st) return drain(st);
+        // the piece's results go back while the next piece is traced
+        if (cudaEventRecord(out_ready[c], trace) != cudaSuccess ||
+            cudaStreamWaitEvent(download, out_ready[c], 0) != cudaSuccess)
+            return drain(cuda_fail(cudaGetLastError(), "pipeline event"));
+        for (int k = 0; k < kPlanes; k++) {
+            if (!back[k].host) continue;
+            const cudaError_t e = cudaMemcpyAsync(static_cast<char*>(back[k].host) + a0*back[k].bytes,
+                                                  piece[k], len*back[k].bytes,
+                                                  cudaMemcpyDeviceToHost, download);
+            if (e != cudaSuccess) return drain(cuda_fail(e, "copying results to the host"));
+        }
+    }
+    const cudaError_t e = cudaStreamSynchronize(download);
+    if (e != cudaSuccess) return drain(cuda_fail(e, "copying results to the host"));
+    return mlgpu_scene_sync_errors(scene, trace);
 }
 
 int mlgpu_bin_arrivals(mlgpu_scene* scene, const int32_t* sensor, const double* time,

@@ -207,6 +207,9 @@ struct WaveBuffers {
 // it, after the BVH walk, after the intersections and after the resolve step.
 cudaError_t launch_wave_iteration(const TraceArgs& a, const WaveBuffers& w, const RayPool& cur,
                                   const RayPool& nxt, int form, cudaStream_t s, cudaEvent_t* ev);
+// The counters to `host`: the device address of pinned host memory.
+cudaError_t launch_wave_counters_to_host(const WaveCounters* c, WaveCounters* host,
+                                         cudaStream_t s);
 // the FP32 forms' intersection and resolve kernels; `mid` (may be null) is
 // recorded between them
 cudaError_t launch_wave32_isect_resolve(const TraceArgs& a, const WaveBuffers& w,

@@ -402,7 +402,22 @@ __global__ void wave_after_resolve_kernel(WaveCounters* c) {
     for (int k = threadIdx.x; k < kMaxBvhLevels; k += blockDim.x) c->level_len[k] = 0;
 }
 
+// The counters into pinned host memory, stored by the SM rather than moved
+// by a copy engine, so that the host's check after a period never queues
+// behind bulk copies of results on another stream.
+__global__ void wave_counters_to_host_kernel(const WaveCounters* c, WaveCounters* host) {
+    const uint32_t* src = reinterpret_cast<const uint32_t*>(c);
+    uint32_t* dst = reinterpret_cast<uint32_t*>(host);
+    for (int k = threadIdx.x; k < (int)(sizeof(WaveCounters)/4); k += blockDim.x) dst[k] = src[k];
+}
+
 }  // namespace
+
+cudaError_t launch_wave_counters_to_host(const WaveCounters* c, WaveCounters* host,
+                                         cudaStream_t s) {
+    wave_counters_to_host_kernel<<<1, 64, 0, s>>>(c, host);
+    return cudaGetLastError();
+}
 
 cudaError_t launch_wave_iteration(const TraceArgs& a, const WaveBuffers& w, const RayPool& cur,
                                   const RayPool& nxt, int form, cudaStream_t s, cudaEvent_t* ev) {

@@ -101,6 +101,81 @@ def test_propagate_host_entry_point(eng):
     assert history_mismatches(ref["history"], out["history"]) == {}
 
 
+def host_call_pinned(scene, photons, max_int, tracer, pool, seed=0, uniforms=None):
+    """mlgpu_propagate_host on page-locked buffers (so that it pipelines the
+    batch in pieces of at least `pool` photons)."""
+    import torch
+    from merlict_development_kit_b200 import _native, abi
+    n = len(photons["wavelength"])
+    keep = []
+
+    def pinned(shape, dtype):
+        dt = np.dtype(dtype)
+        t = torch.empty(int(np.prod(shape)) * dt.itemsize, dtype=torch.uint8).pin_memory()
+        keep.append(t)
+        return t.numpy().view(dt).reshape(shape)
+
+    ps = abi.mlgpu_photons()
+    ps.dtype = abi.F64
+    for name in ("support_x", "support_y", "support_z", "direction_x", "direction_y",
+                 "direction_z", "wavelength"):
+        a = pinned((n,), np.float64)
+        a[:] = photons[name]
+        setattr(ps, name, a.ctypes.data)
+    out = {"sensor": pinned((n,), np.int32), "x": pinned((n,), np.float64),
+           "y": pinned((n,), np.float64), "time": pinned((n,), np.float64),
+           "theta_x": pinned((n,), np.float64), "theta_y": pinned((n,), np.float64),
+           "final_leaf": pinned((n,), np.int32), "info": pinned((n,), np.uint32),
+           "final_position": pinned((n, 3), np.float64),
+           "final_direction": pinned((n, 3), np.float64),
+           "history": pinned((n, max_int + 1), abi.HISTORY_DTYPE)}
+    rs = abi.mlgpu_results()
+    rs.dtype = abi.F64
+    for k, a in out.items():
+        setattr(rs, k, a.ctypes.data)
+    tracers = {"fp64": abi.TRACER_FP64, "fp32": abi.TRACER_FP32, "fp64_plain": abi.TRACER_FP64_PLAIN}
+    st = abi.mlgpu_settings(max_int, 0, tracers[tracer], 0, abi.TRAVERSAL_BVH)
+    st.pool_size = pool
+    rng = abi.mlgpu_rng()
+    if uniforms is None:
+        rng.mode = abi.RNG_PHILOX
+        rng.seed = seed
+    else:
+        u = pinned(uniforms.shape, np.float64)
+        u[:] = uniforms
+        rng.mode = abi.RNG_REPLAY
+        rng.stride = uniforms.shape[1]
+        rng.uniforms = u.ctypes.data
+    _native.check(_native.lib().mlgpu_propagate_host(scene.handle, C.byref(ps), n, C.byref(st),
+                                                     C.byref(rng), C.byref(rs)))
+    return {k: v.copy() for k, v in out.items()}
+
+
+@pytest.mark.parametrize("tracer", ["fp64", "fp32"])
+@pytest.mark.parametrize("rng_mode", ["philox", "replay"])
+def test_propagate_host_in_pieces(eng, tracer, rng_mode):
+    """Pinned host buffers and a 1024-slot pool: mlgpu_propagate_host traces
+    the 4000 photons in three pieces whose copies overlap the tracing.
+    Photon i of a piece keeps its own random stream, so every result and
+    history entry equals one call on device buffers (and, for the FP64
+    tracer with Philox draws, merlict's own)."""
+    flat, photons, ref, meta = load_golden("light_field_small")
+    uniforms = None
+    if rng_mode == "replay":
+        uniforms = np.random.default_rng(5).random((len(photons["wavelength"]), 64))
+    scene = eng.Scene(flat)
+    got = host_call_pinned(scene, photons, meta["max_interactions"], tracer, 1024,
+                           seed=meta["seed"], uniforms=uniforms)
+    scene.close()
+    want = run_gpu(eng, flat, photons, meta["max_interactions"], seed=meta["seed"],
+                   uniforms=uniforms, history=True, tracer=tracer)
+    assert mismatches(want, got) == {}
+    assert history_mismatches(want["history"], got["history"]) == {}
+    if tracer == "fp64" and rng_mode == "philox":
+        assert mismatches(ref, got) == {}
+        assert history_mismatches(ref["history"], got["history"]) == {}
+
+
 def test_wavelength_outside_property_table_raises(eng):
     flat, photons, ref, meta = load_golden("mirror_absorber")
     ph = {k: v.copy() for k, v in photons.items()}
