@@ -1,11 +1,11 @@
-// bvh_build.cu -- host-side construction of the 4-wide bounding-volume
+// bvh_build.cu -- host-side construction of the 8-wide bounding-volume
 // hierarchy the tracers use to find candidate leaves in the world tree.
 //
 // merlict finds candidates by walking its own frame tree, whose octant
 // clustering (merlict/Frame.cpp:190-255) gives heavily overlapping bounding
 // spheres: ~400 sphere tests per photon in the light-field telescope.  The
 // tracers instead walk a BVH built here by binned surface-area-heuristic
-// splits over the leaves' bounding spheres, collapsed to four children per
+// splits over the leaves' bounding spheres, collapsed to eight children per
 // node.  The BVH only proposes candidates; every candidate is then put
 // through merlict's own bounding-sphere test of that leaf and merlict's
 // intersection, and ties are broken in merlict's visiting order, so the
@@ -167,7 +167,7 @@ void build_bvh4(const mlgpu_flat_scene* f, double inflate, BvhHost* out) {
     for (int32_t i = 0; i < n; i++) ids[i] = out->leaf_ids[b.order[i]];
     out->leaf_ids.swap(ids);
 
-    // collapse to 4-wide nodes, breadth first from the root
+    // collapse to kBvhWidth-wide nodes, breadth first from the root
     std::vector<int32_t> queue = {0};
     std::vector<int32_t> wide_of(b.nodes.size(), -1);
     std::vector<int32_t> level = {0};   // per wide node
@@ -183,7 +183,7 @@ void build_bvh4(const mlgpu_flat_scene* f, double inflate, BvhHost* out) {
         } else {
             kids.push_back(b.nodes[bn].left);
             kids.push_back(b.nodes[bn].right);
-            while (kids.size() < 4) {
+            while (kids.size() < (size_t)kBvhWidth) {
                 int best = -1;
                 double area = -1.0;
                 for (size_t k = 0; k < kids.size(); k++) {
@@ -196,9 +196,9 @@ void build_bvh4(const mlgpu_flat_scene* f, double inflate, BvhHost* out) {
                 kids.push_back(c.right);
             }
         }
-        BvhNode4 node;
+        BvhNode node;
         std::memset(&node, 0, sizeof(node));
-        for (int k = 0; k < 4; k++) {
+        for (int k = 0; k < kBvhWidth; k++) {
             node.lo[0][k] = 1.0f; node.hi[0][k] = -1.0f;   // empty slot never hits
             node.lo[1][k] = 1.0f; node.hi[1][k] = -1.0f;
             node.lo[2][k] = 1.0f; node.hi[2][k] = -1.0f;

@@ -489,27 +489,31 @@ __device__ bool first_intersection_bvh(const DevScene& sc, v3 s, v3 d, Isec* out
             continue;
         }
         const float4* nq = reinterpret_cast<const float4*>(sc.bvh + ref);
-        const float4 lx = __ldg(nq), ly = __ldg(nq + 1), lz = __ldg(nq + 2);
-        const float4 hx = __ldg(nq + 3), hy = __ldg(nq + 4), hz = __ldg(nq + 5);
-        const int4 ch = __ldg(reinterpret_cast<const int4*>(nq + 6));
-        const float lox[4] = {lx.x, lx.y, lx.z, lx.w}, loy[4] = {ly.x, ly.y, ly.z, ly.w};
-        const float loz[4] = {lz.x, lz.y, lz.z, lz.w}, hix[4] = {hx.x, hx.y, hx.z, hx.w};
-        const float hiy[4] = {hy.x, hy.y, hy.z, hy.w}, hiz[4] = {hz.x, hz.y, hz.z, hz.w};
-        const int32_t child[4] = {ch.x, ch.y, ch.z, ch.w};
-        float tnear[4];
-        int32_t cref[4];
+        float tnear[kBvhWidth];
+        int32_t cref[kBvhWidth];
         int nhit = 0;
 #pragma unroll
-        for (int k = 0; k < 4; k++) {
-            const float ax = (lox[k] - eps - ox)*idx, bx = (hix[k] + eps - ox)*idx;
-            const float ay = (loy[k] - eps - oy)*idy, by = (hiy[k] + eps - oy)*idy;
-            const float az = (loz[k] - eps - oz)*idz, bz = (hiz[k] + eps - oz)*idz;
-            const float tmin = fmaxf(fmaxf(fminf(ax, bx), fminf(ay, by)), fmaxf(fminf(az, bz), 0.0f));
-            const float tmax = fminf(fminf(fmaxf(ax, bx), fmaxf(ay, by)), fminf(fmaxf(az, bz), tbest));
-            if (tmin <= tmax && child[k] != kBvhEmpty) {
-                tnear[nhit] = tmin;
-                cref[nhit] = child[k];
-                nhit++;
+        for (int g = 0; g < kBvhGroups; g++) {
+            const float4 lx = __ldg(nq + g), ly = __ldg(nq + kBvhGroups + g);
+            const float4 lz = __ldg(nq + 2*kBvhGroups + g), hx = __ldg(nq + 3*kBvhGroups + g);
+            const float4 hy = __ldg(nq + 4*kBvhGroups + g), hz = __ldg(nq + 5*kBvhGroups + g);
+            const int4 ch = __ldg(reinterpret_cast<const int4*>(nq + 6*kBvhGroups + g));
+            const float lox[4] = {lx.x, lx.y, lx.z, lx.w}, loy[4] = {ly.x, ly.y, ly.z, ly.w};
+            const float loz[4] = {lz.x, lz.y, lz.z, lz.w}, hix[4] = {hx.x, hx.y, hx.z, hx.w};
+            const float hiy[4] = {hy.x, hy.y, hy.z, hy.w}, hiz[4] = {hz.x, hz.y, hz.z, hz.w};
+            const int32_t child[4] = {ch.x, ch.y, ch.z, ch.w};
+#pragma unroll
+            for (int k = 0; k < 4; k++) {
+                const float ax = (lox[k] - eps - ox)*idx, bx = (hix[k] + eps - ox)*idx;
+                const float ay = (loy[k] - eps - oy)*idy, by = (hiy[k] + eps - oy)*idy;
+                const float az = (loz[k] - eps - oz)*idz, bz = (hiz[k] + eps - oz)*idz;
+                const float tmin = fmaxf(fmaxf(fminf(ax, bx), fminf(ay, by)), fmaxf(fminf(az, bz), 0.0f));
+                const float tmax = fminf(fminf(fmaxf(ax, bx), fmaxf(ay, by)), fminf(fmaxf(az, bz), tbest));
+                if (tmin <= tmax && child[k] != kBvhEmpty) {
+                    tnear[nhit] = tmin;
+                    cref[nhit] = child[k];
+                    nhit++;
+                }
             }
         }
         if (sp + nhit > kBvhStack) return false;

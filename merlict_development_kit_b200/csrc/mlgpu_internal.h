@@ -60,19 +60,27 @@ static_assert(sizeof(LeafAnchor) == 64, "LeafAnchor must be 64 bytes");
 static_assert(offsetof(LeafAnchor, R) == 24 && offsetof(LeafAnchor, center) == 32,
               "LeafAnchor fields must sit where the 16-byte loads expect them");
 
-// 4-wide BVH node: child boxes as [axis][child] (float, rounded outwards)
-// and child references: a node index, a leaf range (kBvhLeafFlag | start << 3
-// | count - 1, into DevScene::bvh_leaf) or kBvhEmpty.
-struct __align__(128) BvhNode4 {
-    float lo[3][4];
-    float hi[3][4];
-    int32_t child[4];
-    int32_t pad[4];
+// BVH node of kBvhWidth children: child boxes as [axis][child] (float,
+// rounded outwards) and child references: a node index, a leaf range
+// (kBvhLeafFlag | start << 3 | count - 1, into DevScene::bvh_leaf) or
+// kBvhEmpty.  The kernels read it as 16-byte words, four children at a
+// time: word a*G + g holds the low bounds on axis a of children 4g..4g+3,
+// word (3 + a)*G + g the high bounds, word 6*G + g their references
+// (G = kBvhWidth/4).
+constexpr int kBvhWidth = 8;
+constexpr int kBvhGroups = kBvhWidth/4;
+struct __align__(128) BvhNode {
+    float lo[3][kBvhWidth];
+    float hi[3][kBvhWidth];
+    int32_t child[kBvhWidth];
+    int32_t pad[kBvhWidth == 4 ? 4 : 8];
 };
-static_assert(sizeof(BvhNode4) == 128, "BvhNode4 must be 128 bytes");
+static_assert(sizeof(BvhNode) == 32*kBvhWidth, "BvhNode must be 32 bytes per child");
+static_assert(offsetof(BvhNode, child) == 6*kBvhGroups*16,
+              "BvhNode references must follow the boxes");
 constexpr int32_t kBvhLeafFlag = (int32_t)0x80000000u;
 constexpr int32_t kBvhEmpty = 0x7fffffff;
-constexpr int kBvhStack = 48;
+constexpr int kBvhStack = 64;
 constexpr int kMaxBvhLevels = 48;
 
 struct DevScene {
@@ -93,7 +101,7 @@ struct DevScene {
     double hex_u[3], hex_v[3], hex_w[3];
     unsigned int* error_word;   // first device-side error code
     // BVH over the leaves with geometry (empty: walk the frame tree)
-    const BvhNode4* bvh;
+    const BvhNode* bvh;
     const int32_t* bvh_leaf;
     const double4* bvh_sphere;  // per BVH leaf slot: world centre and radius^2 of that leaf
     const float4* bvh_sphere_f; // the same in FP32: centre (rounded) and radius (rounded up)
@@ -144,10 +152,10 @@ struct TraceArgs {
 };
 
 struct BvhHost {
-    std::vector<BvhNode4> nodes;         // breadth first: each level is an index range
+    std::vector<BvhNode> nodes;         // breadth first: each level is an index range
     std::vector<int32_t> leaf_ids;
     std::vector<int32_t> level_start;    // levels + 1 entries
-    int levels = 0;              // depth of the 4-wide tree (root alone: 1)
+    int levels = 0;              // depth of the tree (root alone: 1)
 };
 void build_bvh4(const mlgpu_flat_scene* f, double inflate, BvhHost* out);
 

@@ -26,7 +26,7 @@ namespace mlgpu {
 namespace {
 
 constexpr int kTreeCands = 16;   // candidates of a frame-tree walk before it overflows
-constexpr int kMaxStagedNodes = 256;   // 32 KB of shared memory per block
+constexpr int kMaxStagedNodes = 32768/(int)sizeof(BvhNode);   // 32 KB of shared memory per block
 
 template <typename In>
 __global__ void __launch_bounds__(256)
@@ -143,9 +143,8 @@ wave_intake_kernel(const TraceArgs a, const WaveBuffers w, const RayPool cur) {
     }
 }
 
-// The four child boxes of a BVH node: slab tests in single precision on
-// boxes widened by the ray's rounding (o.w).  Bit k of the result: child k
-// is hit.
+// Four child boxes of a BVH node: slab tests in single precision on boxes
+// widened by the ray's rounding (o.w).  Bit k of the result: child k is hit.
 __device__ __forceinline__ uint32_t node_box_hits(float4 lx, float4 ly, float4 lz, float4 hx,
                                                   float4 hy, float4 hz, const int32_t* child,
                                                   float4 o, float4 iv) {
@@ -165,7 +164,27 @@ __device__ __forceinline__ uint32_t node_box_hits(float4 lx, float4 ly, float4 l
     return hit;
 }
 
-// One BVH level: the four child boxes of each queued (ray, node) pair.  With
+// All children of the node at `nq` (global memory through the read-only
+// path, or shared memory), four at a time; their references into `child`.
+template <bool kShared>
+__device__ __forceinline__ uint32_t node_hits(const float4* nq, float4 o, float4 iv,
+                                              int32_t* child) {
+    auto ld = [nq](int k) { return kShared ? nq[k] : __ldg(nq + k); };
+    uint32_t hit = 0;
+#pragma unroll
+    for (int g = 0; g < kBvhGroups; g++) {
+        const float4 c = ld(6*kBvhGroups + g);
+        int32_t* cg = child + 4*g;
+        cg[0] = __float_as_int(c.x); cg[1] = __float_as_int(c.y);
+        cg[2] = __float_as_int(c.z); cg[3] = __float_as_int(c.w);
+        hit |= node_box_hits(ld(g), ld(kBvhGroups + g), ld(2*kBvhGroups + g),
+                             ld(3*kBvhGroups + g), ld(4*kBvhGroups + g), ld(5*kBvhGroups + g),
+                             cg, o, iv) << (4*g);
+    }
+    return hit;
+}
+
+// One BVH level: the child boxes of each queued (ray, node) pair.  With
 // `staged` > 0 the block first copies the level's `staged` nodes (a
 // contiguous range, the tree being numbered breadth first) into shared
 // memory and reads them from there.
@@ -182,43 +201,34 @@ wave_level_kernel(const TraceArgs a, const WaveBuffers w, int level, int staged)
     const int32_t base = sc.bvh_level_start[level];
     if (staged > 0) {
         const float4* src = reinterpret_cast<const float4*>(sc.bvh + base);
-        for (int k = threadIdx.x; k < staged*8; k += blockDim.x) stage[k] = __ldg(src + k);
+        const int words = staged*(int)(sizeof(BvhNode)/16);
+        for (int k = threadIdx.x; k < words; k += blockDim.x) stage[k] = __ldg(src + k);
         __syncthreads();
     }
     for (uint32_t first = warp_first(); first < n; first += gridDim.x*blockDim.x) {
         const uint32_t e = first + (uint32_t)lane;
         uint32_t slot = 0;
-        int32_t child[4] = {kBvhEmpty, kBvhEmpty, kBvhEmpty, kBvhEmpty};
+        int32_t child[kBvhWidth];
         uint32_t hit = 0;   // bit k: child k hit
         if (e < n) {
             const uint2 q = in[e];
             slot = q.x;
             const float4 o = w.ray_o[slot], iv = w.ray_i[slot];
-            float4 lx, ly, lz, hx, hy, hz;
-            int4 ch;
-            if ((uint32_t)((int32_t)q.y - base) < (uint32_t)staged) {
-                const float4* nq = stage + 8*((int32_t)q.y - base);
-                lx = nq[0]; ly = nq[1]; lz = nq[2]; hx = nq[3]; hy = nq[4]; hz = nq[5];
-                const float4 c = nq[6];
-                ch = make_int4(__float_as_int(c.x), __float_as_int(c.y), __float_as_int(c.z),
-                               __float_as_int(c.w));
-            } else {
-                const float4* nq = reinterpret_cast<const float4*>(sc.bvh + q.y);
-                lx = __ldg(nq); ly = __ldg(nq + 1); lz = __ldg(nq + 2);
-                hx = __ldg(nq + 3); hy = __ldg(nq + 4); hz = __ldg(nq + 5);
-                ch = __ldg(reinterpret_cast<const int4*>(nq + 6));
-            }
-            child[0] = ch.x; child[1] = ch.y; child[2] = ch.z; child[3] = ch.w;
-            hit = node_box_hits(lx, ly, lz, hx, hy, hz, child, o, iv);
+            if ((uint32_t)((int32_t)q.y - base) < (uint32_t)staged)
+                hit = node_hits<true>(stage + (sizeof(BvhNode)/16)*((int32_t)q.y - base), o, iv,
+                                      child);
+            else
+                hit = node_hits<false>(reinterpret_cast<const float4*>(sc.bvh + q.y), o, iv,
+                                       child);
         }
         uint32_t nn = 0, nr = 0;
 #pragma unroll
-        for (int k = 0; k < 4; k++)
+        for (int k = 0; k < kBvhWidth; k++)
             if (hit & (1u << k)) { if (child[k] < 0) nr++; else nn++; }
         uint32_t nb = warp_reserve(&w.counters->level_len[last ? level : level + 1], last ? 0u : nn);
         uint32_t rb = warp_reserve(&w.counters->range_len, nr);
 #pragma unroll
-        for (int k = 0; k < 4; k++) {
+        for (int k = 0; k < kBvhWidth; k++) {
             if (!(hit & (1u << k))) continue;
             if (child[k] < 0) {
                 if (rb < w.range_cap) w.range_q[rb] = make_uint2(slot, (uint32_t)child[k]);
@@ -332,13 +342,10 @@ wave_walk_kernel(const TraceArgs a, const WaveBuffers w, const RayPool cur) {
             int sp = 0;
             stack[sp++] = (int32_t)q.y;
             while (sp > 0 && !over) {
-                const float4* nq = reinterpret_cast<const float4*>(sc.bvh + stack[--sp]);
-                const float4 lx = __ldg(nq), ly = __ldg(nq + 1), lz = __ldg(nq + 2);
-                const float4 hx = __ldg(nq + 3), hy = __ldg(nq + 4), hz = __ldg(nq + 5);
-                const int4 ch = __ldg(reinterpret_cast<const int4*>(nq + 6));
-                const int32_t child[4] = {ch.x, ch.y, ch.z, ch.w};
-                const uint32_t hit = node_box_hits(lx, ly, lz, hx, hy, hz, child, o, iv);
-                for (int k = 3; k >= 0; k--) {
+                int32_t child[kBvhWidth];
+                const uint32_t hit = node_hits<false>(
+                    reinterpret_cast<const float4*>(sc.bvh + stack[--sp]), o, iv, child);
+                for (int k = kBvhWidth - 1; k >= 0; k--) {
                     if (!(hit & (1u << k))) continue;
                     if (child[k] >= 0) {
                         if (sp < kWalkStack) stack[sp++] = child[k];
@@ -436,7 +443,7 @@ cudaError_t launch_wave_iteration(const TraceArgs& a, const WaveBuffers& w, cons
         for (int k = 0; k < a.scene.bvh_levels; k++) {
             const int count = a.scene.bvh_level_start[k + 1] - a.scene.bvh_level_start[k];
             const int staged = k < w.staged_levels && count <= kMaxStagedNodes ? count : 0;
-            wave_level_kernel<<<w.grid, 256, (size_t)staged*sizeof(BvhNode4), s>>>(a, w, k,
+            wave_level_kernel<<<w.grid, 256, (size_t)staged*sizeof(BvhNode), s>>>(a, w, k,
                                                                                    staged);
         }
         if (form == MLGPU_TRACER_FP64) wave_sphere_kernel<false><<<w.grid, 256, 0, s>>>(a, w, cur);
