@@ -314,8 +314,9 @@ int mlgpu_scene_sync_errors(mlgpu_scene* scene, void* cuda_stream);
  * traces, copies the results out and synchronises.  This is the call the
  * reference-side C++ shim makes.  When every buffer is page-locked
  * (cudaHostAlloc, cudaHostRegister, torch pin_memory) the batch moves in
- * up to four pieces of at least one ray pool each, whose copies overlap
- * the tracing of their neighbours; the results are those of one call.
+ * pieces (up to four of at least one ray pool each, the first and the last
+ * cut in half) whose copies overlap the tracing of their neighbours; the
+ * results are those of one call.
  * Ordered after earlier work on the legacy default stream.               */
 int mlgpu_propagate_host(
     mlgpu_scene* scene,

@@ -123,8 +123,10 @@ struct Profiler {
 
 }  // namespace
 
-// Pieces of an mlgpu_propagate_host batch at most.
+// Whole pieces of an mlgpu_propagate_host batch at most (plus one: the
+// first and the last piece are halves).
 constexpr int kHostChunks = 4;
+constexpr int kHostPieces = kHostChunks + 1;
 
 struct mlgpu_scene {
     int device = 0;
@@ -150,7 +152,7 @@ struct mlgpu_scene {
     // mlgpu_propagate_host's pipeline: trace, upload and download streams;
     // events: the caller's default stream, inputs of each piece, results of each piece
     cudaStream_t host_stream[3] = {nullptr, nullptr, nullptr};
-    cudaEvent_t host_event[1 + 2*kHostChunks] = {};
+    cudaEvent_t host_event[1 + 2*kHostPieces] = {};
     Profiler prof;
 };
 
@@ -1069,6 +1071,9 @@ int mlgpu_propagate_host(mlgpu_scene* scene, const mlgpu_photons* photons, uint6
         ? kWavePool : settings->pool_size;
     const int chunks = all_pinned
         ? (int)std::max<uint64_t>(1, std::min<uint64_t>(kHostChunks, n/pool)) : 1;
+    // With two or more whole pieces the first and the last are halves: only
+    // the first piece's inputs and the last piece's results wait uncovered.
+    const int pieces = chunks > 1 ? chunks + 1 : 1;
 
     if (!scene->host_stream[0]) {
         for (cudaStream_t& hs : scene->host_stream)
@@ -1079,14 +1084,19 @@ int mlgpu_propagate_host(mlgpu_scene* scene, const mlgpu_photons* photons, uint6
     cudaStream_t trace = scene->host_stream[0], upload = scene->host_stream[1],
                  download = scene->host_stream[2];
     cudaEvent_t* in_ready = scene->host_event + 1;
-    cudaEvent_t* out_ready = scene->host_event + 1 + kHostChunks;
+    cudaEvent_t* out_ready = scene->host_event + 1 + kHostPieces;
     // after the caller's work on the legacy default stream, as a call on it would be
     MLGPU_CUDA(cudaEventRecord(scene->host_event[0], 0));
     MLGPU_CUDA(cudaStreamWaitEvent(upload, scene->host_event[0], 0));
     MLGPU_CUDA(cudaStreamWaitEvent(trace, scene->host_event[0], 0));
-    auto first = [&](int c) { return n*(uint64_t)c/(uint64_t)chunks; };
+    // piece c starts at n * (2c - 1) / (2 chunks), clamped to [0, n]
+    auto first = [&](int c) -> uint64_t {
+        if (c <= 0) return 0;
+        if (c >= pieces) return n;
+        return pieces == 1 ? 0 : n*(2*(uint64_t)c - 1)/(2*(uint64_t)chunks);
+    };
     // every piece's inputs are queued at once; each piece records its arrival
-    for (int c = 0; c < chunks; c++) {
+    for (int c = 0; c < pieces; c++) {
         const uint64_t a0 = first(c), len = first(c + 1) - a0;
         for (int k = 0; k < 7; k++)
             MLGPU_CUDA(cudaMemcpyAsync(din + (k*n + a0)*ein,
@@ -1105,7 +1115,7 @@ int mlgpu_propagate_host(mlgpu_scene* scene, const mlgpu_photons* photons, uint6
         cudaStreamSynchronize(download);
         return code;
     };
-    for (int c = 0; c < chunks; c++) {
+    for (int c = 0; c < pieces; c++) {
         const uint64_t a0 = first(c), len = first(c + 1) - a0;
         if (cudaStreamWaitEvent(trace, in_ready[c], 0) != cudaSuccess)
             return drain(cuda_fail(cudaGetLastError(), "pipeline event"));

@@ -155,7 +155,9 @@ def host_call_pinned(scene, photons, max_int, tracer, pool, seed=0, uniforms=Non
 @pytest.mark.parametrize("rng_mode", ["philox", "replay"])
 def test_propagate_host_in_pieces(eng, tracer, rng_mode):
     """Pinned host buffers and a 1024-slot pool: mlgpu_propagate_host traces
-    the 4000 photons in three pieces whose copies overlap the tracing.
+    the 4000 photons in four pieces (666, 1334, 1333 and 667 photons: three
+    whole pieces, the first and the last cut in half) whose copies overlap
+    the tracing.
     Photon i of a piece keeps its own random stream, so every result and
     history entry equals one call on device buffers (and, for the FP64
     tracer with Philox draws, merlict's own)."""
