@@ -139,7 +139,7 @@ float round_up(double x) {
 // Builds the BVH of all leaves with geometry.  `inflate` widens every leaf
 // box (absolute, metres) so that single-precision slab tests stay
 // conservative.
-void build_bvh4(const mlgpu_flat_scene* f, double inflate, BvhHost* out) {
+void build_bvh(const mlgpu_flat_scene* f, double inflate, BvhHost* out) {
     out->nodes.clear();
     out->leaf_ids.clear();
     out->levels = 0;

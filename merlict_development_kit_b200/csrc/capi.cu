@@ -297,7 +297,7 @@ int build_device_scene(mlgpu_scene* s, const mlgpu_flat_scene* f) {
         const double extent = std::fabs(root[0]) + std::fabs(root[1]) + std::fabs(root[2]) +
             2.0*root[3];
         BvhHost bvh;
-        build_bvh4(f, 0.0, &bvh);
+        build_bvh(f, 0.0, &bvh);
         if (!bvh.nodes.empty()) {
             if ((st = upload(s, bvh.nodes.data(), bvh.nodes.size(), &s->dev.bvh))) return st;
             if ((st = upload(s, bvh.leaf_ids.data(), bvh.leaf_ids.size(), &s->dev.bvh_leaf))) return st;

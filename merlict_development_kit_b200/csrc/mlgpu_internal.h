@@ -157,7 +157,7 @@ struct BvhHost {
     std::vector<int32_t> level_start;    // levels + 1 entries
     int levels = 0;              // depth of the tree (root alone: 1)
 };
-void build_bvh4(const mlgpu_flat_scene* f, double inflate, BvhHost* out);
+void build_bvh(const mlgpu_flat_scene* f, double inflate, BvhHost* out);
 
 // wavefront tracers: a pool of ray slots, two of them (current, next)
 struct WaveCounters {
