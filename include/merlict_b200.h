@@ -32,7 +32,7 @@
 extern "C" {
 #endif
 
-#define MLGPU_ABI_VERSION 5
+#define MLGPU_ABI_VERSION 6
 
 /* ---- status codes ------------------------------------------------------ */
 enum {
@@ -210,7 +210,7 @@ enum {
 };
 
 /* How candidate surfaces are found for a ray in the whole tree.
- * BVH: a 4-wide bounding-volume hierarchy built at scene creation proposes
+ * BVH: an 8-wide bounding-volume hierarchy built at scene creation proposes
  * candidates; each still passes merlict's own bounding-sphere test of the
  * leaf and merlict's intersection, ties broken in merlict's visiting order.
  * FRAME_TREE: merlict's own walk over the frame tree's bounding spheres
@@ -234,6 +234,14 @@ typedef struct mlgpu_settings {
     int32_t staged_levels;  /* top BVH levels read from shared memory (0)     */
     int32_t photon_order;   /* MLGPU_ORDER_*: the order photons enter the pool */
     int32_t walk;           /* MLGPU_WALK_*: how rays walk the BVH             */
+    uint32_t queue_capacity; /* entries of each wavefront work queue: the
+                               (ray, BVH node) queues, the (ray, leaf range)
+                               queue and the (ray, candidate) queue; 0 = 8, 16
+                               and 16 entries per ray slot.  A ray whose
+                               entries do not fit takes merlict's own frame
+                               walk instead (same results); a small capacity
+                               only makes that fallback common.  0 or at
+                               least 32.                                     */
 } mlgpu_settings;
 
 /* walk: LEVELS runs one kernel per BVH level over queued (ray, node) pairs
@@ -289,6 +297,20 @@ int mlgpu_scene_set_profiling(mlgpu_scene* scene, int enable);
  * last turned on; waits for the outstanding timed launches.  `ms` and
  * `launches` hold MLGPU_KERNEL_CLASSES entries each (either may be NULL). */
 int mlgpu_scene_kernel_times(mlgpu_scene* scene, double* ms, uint64_t* launches);
+
+/* Counters of the wavefront tracers since the scene was created (or since
+ * the last call with reset != 0): propagations, iterations (each advances
+ * every live ray by one interaction) and rays that did not fit a work
+ * queue and were resolved by merlict's own walk of the frame tree
+ * (RayAndFrame.cpp:126-173), counted once per ray and iteration.  No
+ * counterpart in the reference.  Reads host-side totals only.            */
+typedef struct mlgpu_wavefront_stats {
+    uint64_t calls;
+    uint64_t iterations;
+    uint64_t overflow_rays;
+} mlgpu_wavefront_stats;
+
+int mlgpu_scene_wavefront_stats(mlgpu_scene* scene, mlgpu_wavefront_stats* stats, int reset);
 
 /* ---- propagation ------------------------------------------------------ *
  * Replaces propagate_photons_in_frame_with_config (merlict/Photons.cpp:9-22)

@@ -59,6 +59,8 @@ def lib():
             C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint64, C.c_void_p, C.c_void_p,
             C.c_uint32, C.c_double, C.c_double, C.c_void_p]
         L.mlgpu_scene_kernel_launches.argtypes = [C.c_void_p, C.POINTER(C.c_uint64)]
+        L.mlgpu_scene_wavefront_stats.argtypes = [C.c_void_p,
+                                                  C.POINTER(abi.mlgpu_wavefront_stats), C.c_int]
         L.mlgpu_scene_set_profiling.argtypes = [C.c_void_p, C.c_int]
         L.mlgpu_scene_kernel_times.argtypes = [C.c_void_p, C.POINTER(C.c_double),
                                                C.POINTER(C.c_uint64)]
@@ -83,7 +85,8 @@ def lib():
                      "mlgpu_scene_autotune", "mlgpu_corsika_photons", "mlgpu_lixel_statistics",
                      "mlgpu_signal_chain",
                      "mlgpu_propagate_host", "mlgpu_scene_sync_errors", "mlgpu_bin_arrivals",
-                     "mlgpu_bin_arrivals_noalloc", "mlgpu_scene_kernel_launches"):
+                     "mlgpu_bin_arrivals_noalloc", "mlgpu_scene_kernel_launches",
+                     "mlgpu_scene_wavefront_stats"):
             getattr(L, name).restype = C.c_int
         if L.mlgpu_abi_version() != abi.ABI_VERSION:
             raise ImportError("libmerlict_b200.so ABI version mismatch")
@@ -140,6 +143,7 @@ EXPORTED = (
     "mlgpu_abi_version", "mlgpu_last_error", "mlgpu_scene_create", "mlgpu_scene_destroy",
     "mlgpu_propagate", "mlgpu_scene_sync_errors", "mlgpu_propagate_host",
     "mlgpu_bin_arrivals", "mlgpu_bin_arrivals_noalloc", "mlgpu_scene_kernel_launches",
+    "mlgpu_scene_wavefront_stats",
     "mlgpu_scene_set_profiling", "mlgpu_scene_kernel_times", "mlgpu_scene_autotune",
     "mlgpu_corsika_photons", "mlgpu_lixel_statistics", "mlgpu_signal_chain",
     # include/merlict_b200_surrogate.h

@@ -11,7 +11,7 @@ from dataclasses import dataclass, field
 
 import numpy as np
 
-ABI_VERSION = 5
+ABI_VERSION = 6
 
 # status codes
 OK = 0
@@ -242,13 +242,18 @@ class mlgpu_settings(C.Structure):
         ("staged_levels", C.c_int32),
         ("photon_order", C.c_int32),
         ("walk", C.c_int32),
+        ("queue_capacity", C.c_uint32),
     ]
 
     TUNING = ("pool_size", "check_period", "use_graph", "grid_blocks", "staged_levels",
-              "photon_order", "walk")
+              "photon_order", "walk", "queue_capacity")
 
     def tuning(self) -> dict:
         return {k: int(getattr(self, k)) for k in self.TUNING}
+
+
+class mlgpu_wavefront_stats(C.Structure):
+    _fields_ = [("calls", C.c_uint64), ("iterations", C.c_uint64), ("overflow_rays", C.c_uint64)]
 
 
 def _ptr(a: np.ndarray, ctype):

@@ -149,6 +149,7 @@ struct mlgpu_scene {
     cudaGraphExec_t wave_graph = nullptr;
     cudaStream_t capture_stream = nullptr;
     uint64_t launches = 0;               // kernels launched for this scene
+    mlgpu_wavefront_stats wave_stats = {0, 0, 0};
     // mlgpu_propagate_host's pipeline: trace, upload and download streams;
     // events: the caller's default stream, inputs of each piece, results of each piece
     cudaStream_t host_stream[3] = {nullptr, nullptr, nullptr};
@@ -382,6 +383,8 @@ int check_propagate_args(const mlgpu_scene* scene, const mlgpu_photons* ph,
         return fail(MLGPU_ERR_INVALID_ARGUMENT, "unknown photon_order %d", st->photon_order);
     if (st->walk < MLGPU_WALK_DEFAULT || st->walk > MLGPU_WALK_STACK)
         return fail(MLGPU_ERR_INVALID_ARGUMENT, "unknown walk %d", st->walk);
+    if (st->queue_capacity != 0 && (st->queue_capacity < 32 || st->queue_capacity > (1u << 28)))
+        return fail(MLGPU_ERR_INVALID_ARGUMENT, "queue_capacity must be 0 or in [32, 2^28]");
     return MLGPU_OK;
 }
 
@@ -415,11 +418,13 @@ constexpr uint32_t kWavePool = 1u << 21;   // ray slots of the wavefront tracers
 
 // Carves the two ray pools, the candidate lists and the counters out of
 // one device buffer.
-int wave_buffers(mlgpu_scene* scene, uint32_t pool, int grid, int staged, WaveBuffers* w,
-                 RayPool* p0, RayPool* p1) {
+int wave_buffers(mlgpu_scene* scene, uint32_t pool, int grid, int staged, uint32_t queue_cap,
+                 WaveBuffers* w, RayPool* p0, RayPool* p1) {
     auto up = [](size_t x) { return (x + 255) & ~size_t(255); };
     const size_t P = pool;
-    const size_t level_cap = 8*P, range_cap = 16*P, isect_cap = 16*P;
+    const size_t level_cap = queue_cap ? queue_cap : 8*P;
+    const size_t range_cap = queue_cap ? queue_cap : 16*P;
+    const size_t isect_cap = queue_cap ? queue_cap : 16*P;
     const size_t per_pool = 8*up(P*8) + 5*up(P*4);
     const size_t rest = up(P*4) + 2*up(P*16) + up(P*48) + 2*up(level_cap*8) + up(range_cap*8) +
         up(isect_cap*8) + up(isect_cap*8) + up(P*8) + 3*up(P*4);
@@ -530,8 +535,8 @@ int run_wavefront(mlgpu_scene* scene, TraceArgs a, const mlgpu_settings* st,
     const uint32_t pool = (uint32_t)std::min<uint64_t>(a.num_photons, want);
     WaveBuffers w;
     RayPool pools[2];
-    const int rc = wave_buffers(scene, pool, st->grid_blocks, st->staged_levels, &w,
-                                &pools[0], &pools[1]);
+    const int rc = wave_buffers(scene, pool, st->grid_blocks, st->staged_levels,
+                                st->queue_capacity, &w, &pools[0], &pools[1]);
     if (rc) return rc;
     w.walk = st->walk == MLGPU_WALK_STACK ? MLGPU_WALK_STACK : MLGPU_WALK_LEVELS;
     // per-kernel events cannot be taken inside a graph: profiling runs launch by launch
@@ -582,6 +587,9 @@ int run_wavefront(mlgpu_scene* scene, TraceArgs a, const mlgpu_settings* st,
         if (iteration > bound)
             return fail(MLGPU_ERR_RUNTIME, "wavefront tracer did not drain its pool");
     }
+    scene->wave_stats.calls++;
+    scene->wave_stats.iterations += iteration;
+    scene->wave_stats.overflow_rays += scene->wave_host->overflow_total;
     return MLGPU_OK;
 }
 
@@ -1194,6 +1202,13 @@ int mlgpu_bin_arrivals(mlgpu_scene* scene, const int32_t* sensor, const double* 
     }
     if (e != cudaSuccess) return cuda_fail(e, "binning kernels");
     scene->launches += 2;
+    return MLGPU_OK;
+}
+
+int mlgpu_scene_wavefront_stats(mlgpu_scene* scene, mlgpu_wavefront_stats* stats, int reset) {
+    if (!scene) return fail(MLGPU_ERR_INVALID_ARGUMENT, "scene is NULL");
+    if (stats) *stats = scene->wave_stats;
+    if (reset) scene->wave_stats = mlgpu_wavefront_stats{0, 0, 0};
     return MLGPU_OK;
 }
 

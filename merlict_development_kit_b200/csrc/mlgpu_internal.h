@@ -169,7 +169,9 @@ struct WaveCounters {
     unsigned int isect_len;          // (slot, leaf) candidates to intersect
     unsigned int overflow_len;       // slots sent to merlict's own walk
     unsigned int level_len[kMaxBvhLevels];   // (slot, node) pairs of each BVH level
+    unsigned long long overflow_total;       // overflow_len summed over the iterations
 };
+static_assert(sizeof(WaveCounters) <= 256, "the counters sit in the first 256 bytes of the pool");
 
 struct RayPool {
     int32_t* photon;

@@ -401,6 +401,7 @@ __global__ void wave_after_intake_kernel(WaveCounters* c, uint32_t pool, uint64_
 
 __global__ void wave_after_resolve_kernel(WaveCounters* c) {
     if (threadIdx.x == 0) {
+        c->overflow_total += c->overflow_len;
         c->active = c->next;
         c->range_len = 0;
         c->isect_len = 0;

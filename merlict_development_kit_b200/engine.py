@@ -252,6 +252,15 @@ class Scene:
         check(lib().mlgpu_scene_kernel_launches(self._h, C.byref(v)))
         return int(v.value)
 
+    def wavefront_stats(self, reset: bool = False) -> dict:
+        """Wavefront propagations, iterations and rays resolved by merlict's
+        own frame walk after a work queue overflowed, since the scene was
+        created or the last reset."""
+        s = abi.mlgpu_wavefront_stats()
+        check(lib().mlgpu_scene_wavefront_stats(self._h, C.byref(s), int(bool(reset))))
+        return {"calls": int(s.calls), "iterations": int(s.iterations),
+                "overflow_rays": int(s.overflow_rays)}
+
     KERNEL_CLASSES = ("walk", "intake", "intersect", "resolve", "plain", "bin")
 
     def set_profiling(self, enable: bool) -> None:

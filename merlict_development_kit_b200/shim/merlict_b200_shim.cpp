@@ -1,6 +1,7 @@
 // merlict_b200_shim.cpp -- the drop-in propagation entry points declared
 // in merlict_b200_shim.h: they flatten and upload a scene once per world
-// frame (merlict_b200_flatten.cpp) and call the engine's C ABI.
+// frame (merlict_b200_flatten.cpp), call the engine's C ABI and rebuild the
+// photons' histories (merlict_b200_history.cpp).
 #include "merlict_b200_shim.h"
 
 #include <cstring>
@@ -9,26 +10,7 @@
 #include <stdexcept>
 
 namespace merlict_b200 {
-namespace {
-
 namespace ml = merlict;
-
-template <typename Tag, typename Tag::type Member>
-struct Accessor {
-    friend typename Tag::type member_of(Tag) { return Member; }
-};
-
-#define MLGPU_MEMBER(TAG, CLASS, TYPE, NAME)                        \
-    struct TAG {                                                    \
-        typedef TYPE CLASS::*type;                                  \
-        friend type member_of(TAG);                                 \
-    };                                                              \
-    template struct Accessor<TAG, &CLASS::NAME>
-
-MLGPU_MEMBER(RaySupport, ml::Ray, ml::Vec3, support_);
-MLGPU_MEMBER(RayDirection, ml::Ray, ml::Vec3, direction_);
-
-}  // namespace
 
 void throw_on_error(int status) {
     if (status == MLGPU_OK) return;
@@ -142,43 +124,8 @@ void propagate_photons_in_frame_with_config(
     res.history = history.data();
     throw_on_error(mlgpu_propagate_host(ds->scene, &planes.view, n, &st, &rng, &res));
 
-    // Rebuild each photon's history with merlict's own types, so that the
-    // photons look as if merlict's Propagator had run (PhotonAndFrame.cpp).
-    for (size_t i = 0; i < n; i++) {
-        ml::Photon& photon = (*photons)[i];
-        const uint32_t n_int = (info[i] >> 8) & 0xff;
-        const mlgpu_history_entry* h = &history[i*len];
-        const ml::Intersection* previous = nullptr;
-        std::vector<ml::Intersection> rebuilt;
-        rebuilt.reserve(n_int);
-        for (uint32_t k = 1; k < n_int; k++) {
-            const ml::SurfaceEntity* object = h[k].leaf >= 0
-                ? ds->flat.leaf_entity[h[k].leaf] : &ml::VOID_SURFACE_ENTITY;
-            const ml::Vec3 normal(h[k].normal[0], h[k].normal[1], h[k].normal[2]);
-            const ml::Vec3 incident = normal*(h[k].from_outside_to_inside ? -1.0 : 1.0);
-            rebuilt.emplace_back(
-                object,
-                ml::Vec3(h[k].position[0], h[k].position[1], h[k].position[2]),
-                normal, h[k].distance, incident);
-        }
-        for (uint32_t k = 1; k < n_int; k++)
-            photon.push_back_intersection_and_interaction(
-                rebuilt[k - 1], static_cast<ml::Interaction>(h[k].interaction));
-        // The ray ends where its last step started, or at the final
-        // intersection when that step reflected or refracted.
-        if (n_int > 1) {
-            const uint8_t last = h[n_int - 1].interaction;
-            const bool moved = last == MLGPU_REFLECTION_ON_SURFACE ||
-                last == MLGPU_FRESNEL_REFLECTION_ON_SURFACE ||
-                last == MLGPU_REFRACTION_TO_INSIDE || last == MLGPU_REFRACTION_TO_OUTSIDE;
-            if (moved) previous = &rebuilt[n_int - 2];
-            else if (n_int > 2) previous = &rebuilt[n_int - 3];
-            ml::Ray& ray = photon;
-            if (previous) ray.*member_of(RaySupport()) = previous->position_in_root_frame();
-            ray.*member_of(RayDirection()) = ml::Vec3(
-                final_direction[3*i], final_direction[3*i + 1], final_direction[3*i + 2]);
-        }
-    }
+    rebuild_histories(photons, ds->flat, history.data(), info.data(), final_direction.data(),
+                      st.max_num_interactions_per_photon);
 }
 
 void propagate_photons_in_frame_with_config_multi_thread(
@@ -187,7 +134,8 @@ void propagate_photons_in_frame_with_config_multi_thread(
     const ml::PropagationConfig* settings,
     ml::random::Generator* prng
 ) {
-    propagate_photons_in_frame_with_config(photons, world, settings, prng);
+    // qualified: argument-dependent lookup would also find merlict's own
+    merlict_b200::propagate_photons_in_frame_with_config(photons, world, settings, prng);
 }
 
 void propagate_and_assign_photons(

@@ -95,6 +95,23 @@ void propagate_and_assign_photons(
 // Throws the exception the reference raises for an engine status.
 void throw_on_error(int status);
 
+// Appends to each fresh photon (only its production interaction) the
+// intersections and interactions the engine recorded for it --
+// history[i*(max_interactions + 1) + k], k < info[i] >> 8 & 0xff -- through
+// merlict's public RayForPropagation::push_back_intersection_and_interaction
+// (RayForPropagation.h:49-51) and Intersection's constructor
+// (Intersection.h:24-29), objects mapped back through flat.leaf_entity; and
+// sets the photon's ray to the support and direction merlict's Propagator
+// would have left (final_direction[3 i .. 3 i + 2]).  Throws
+// std::runtime_error on a history that names no known leaf.
+void rebuild_histories(
+    std::vector<merlict::Photon>* photons,
+    const FlatScene& flat,
+    const mlgpu_history_entry* history,
+    const uint32_t* info,
+    const double* final_direction,
+    uint32_t max_interactions);
+
 }  // namespace merlict_b200
 
 #endif  // MERLICT_B200_SHIM_H_

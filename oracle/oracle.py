@@ -20,9 +20,16 @@ import numpy as np
 from merlict_development_kit_b200 import abi
 
 HERE = os.path.dirname(os.path.abspath(__file__))
+REPO = os.path.dirname(HERE)
 ORACLE_SO = os.path.join(HERE, "_build", "libmerlict_oracle.so")
 HARNESS_SO = os.path.join(HERE, "_ref", "libmerlict_ref_harness.so")
-REFERENCE_DIR = os.environ.get("MERLICT_REFERENCE_DIR", "/root/reference")
+SHIM_HARNESS_SO = os.path.join(HERE, "_ref", "libmerlict_shim_harness.so")
+SANITIZE_EXE = os.path.join(HERE, "_ref", "sanitize_shim")
+ENGINE_SO = os.path.join(REPO, "merlict_development_kit_b200", "_build", "libmerlict_b200.so")
+# the reference source tree: $MERLICT_REFERENCE_DIR, else `reference` beside
+# the repository; without it the reference-built checkers are not rebuilt
+REFERENCE_DIR = os.environ.get("MERLICT_REFERENCE_DIR",
+                               os.path.join(os.path.dirname(REPO), "reference"))
 
 
 class OracleCounters(C.Structure):
@@ -38,17 +45,24 @@ class OracleCounters(C.Structure):
 
 
 def build(reference: bool = True) -> None:
-    """Builds the oracle, and the reference harness when the reference
-    sources are present."""
+    """Builds the oracle, and -- when the reference sources are present --
+    the reference harness, the sanitizer check of the drop-in's host code
+    and (once the engine library is built) the drop-in's test harness."""
     targets = ["oracle"]
     if reference and os.path.isdir(REFERENCE_DIR):
-        targets.append("ref")
+        targets += ["ref", "sanitize"]
+        if os.path.exists(ENGINE_SO):
+            targets.append("shim")
     subprocess.run(["make", "-s", "-C", HERE, f"-j{os.cpu_count() or 4}",
                     f"REF={REFERENCE_DIR}"] + targets, check=True)
 
 
 def harness_available() -> bool:
     return os.path.exists(HARNESS_SO)
+
+
+def shim_harness_available() -> bool:
+    return os.path.exists(SHIM_HARNESS_SO)
 
 
 def _photon_struct(ph: dict) -> tuple[abi.mlgpu_photons, list]:
@@ -137,15 +151,16 @@ class Oracle:
         return counts, (hist if num_bins else None)
 
 
-_harness = None
+_harness = {}
 
 
-def harness():
-    global _harness
-    if _harness is None:
-        if not os.path.exists(HARNESS_SO):
-            raise RuntimeError("reference harness not built (oracle/Makefile target ref)")
-        lib = C.CDLL(HARNESS_SO)
+def harness(path: str = HARNESS_SO):
+    """The reference harness library (or, with SHIM_HARNESS_SO, the same
+    harness with the C++ drop-in linked in), its functions declared."""
+    if path not in _harness:
+        if not os.path.exists(path):
+            raise RuntimeError(f"{os.path.basename(path)} not built (oracle/Makefile)")
+        lib = C.CDLL(path)
         lib.ref_scene_build.restype = C.c_void_p
         lib.ref_scene_build.argtypes = [C.c_char_p, C.POINTER(C.c_double), C.c_int]
         lib.ref_scene_free.argtypes = [C.c_void_p]
@@ -165,8 +180,19 @@ def harness():
             C.c_void_p, C.POINTER(abi.mlgpu_photons), C.c_uint64, C.c_uint32,
             C.c_int, C.c_uint64, C.c_void_p, C.c_uint32, C.c_int,
             C.POINTER(abi.mlgpu_results), C.POINTER(C.c_double)]
-        _harness = lib
-    return _harness
+        lib.ref_last_supports.restype = C.c_uint64
+        lib.ref_last_supports.argtypes = [C.c_void_p, C.c_void_p]
+        lib.ref_rebuild_photons.restype = C.c_int
+        lib.ref_rebuild_photons.argtypes = [
+            C.c_void_p, C.POINTER(abi.mlgpu_photons), C.c_uint64, C.c_uint32, C.c_void_p,
+            C.c_void_p, C.c_void_p, C.POINTER(abi.mlgpu_results)]
+        if hasattr(lib, "shim_propagate"):
+            lib.shim_propagate.restype = C.c_int
+            lib.shim_propagate.argtypes = [
+                C.c_void_p, C.POINTER(abi.mlgpu_photons), C.c_uint64, C.c_uint32, C.c_int,
+                C.c_uint64, C.POINTER(C.c_uint64), C.POINTER(abi.mlgpu_results)]
+        _harness[path] = lib
+    return _harness[path]
 
 
 # propagation modes of ref_propagate
@@ -179,8 +205,8 @@ REFERENCE_MULTI_THREAD = 3
 class RefScene:
     """A scene built and propagated by the reference library."""
 
-    def __init__(self, kind: str, params=()):
-        self.lib = harness()
+    def __init__(self, kind: str, params=(), lib_path: str = HARNESS_SO):
+        self.lib = harness(lib_path)
         p = (C.c_double * max(len(params), 1))(*params)
         self.h = self.lib.ref_scene_build(kind.encode(), p, len(params))
         if not self.h:
@@ -241,6 +267,44 @@ class RefScene:
         if status != 0 and out is None:
             raise RuntimeError(self.lib.ref_last_error().decode())
         return status, out, sec.value
+
+    def last_supports(self) -> np.ndarray:
+        """[n][3]: the ray support of each photon after the last propagation."""
+        n = int(self.lib.ref_last_supports(self.h, None))
+        out = np.zeros((max(n, 1), 3))
+        self.lib.ref_last_supports(self.h, out.ctypes.data)
+        return out[:n]
+
+    def rebuild(self, photons: dict, max_interactions: int, results: dict):
+        """merlict_b200::rebuild_histories on fresh photons from the exported
+        `results` (history, info, final_direction), then merlict's
+        Sensors::assign_photons; returns (status, results dict)."""
+        n = len(photons["wavelength"])
+        ps, keep = _photon_struct(photons)
+        hist = np.ascontiguousarray(results["history"])
+        info = np.ascontiguousarray(results["info"], dtype=np.uint32)
+        fd = np.ascontiguousarray(results["final_direction"], dtype=np.float64)
+        rs, out = alloc_results(n, max_interactions, True)
+        status = self.lib.ref_rebuild_photons(self.h, C.byref(ps), n, max_interactions,
+                                              hist.ctypes.data, info.ctypes.data,
+                                              fd.ctypes.data, C.byref(rs))
+        return status, out
+
+    def shim_propagate(self, photons: dict, max_interactions: int, mode: int, mt_seed: int):
+        """The C++ drop-in on this scene (needs SHIM_HARNESS_SO): mode 0
+        propagate_photons_in_frame_with_config + merlict's assign_photons, 1
+        the _multi_thread twin, 2 propagate_and_assign_photons.  Returns
+        (status, results dict, the Philox seed the drop-in drew)."""
+        n = len(photons["wavelength"])
+        ps, keep = _photon_struct(photons)
+        rs, out = alloc_results(n, max_interactions, True)
+        seed = C.c_uint64(0)
+        status = self.lib.shim_propagate(self.h, C.byref(ps), n, max_interactions, mode,
+                                         mt_seed, C.byref(seed), C.byref(rs))
+        return status, out, int(seed.value)
+
+    def last_error(self) -> str:
+        return self.lib.ref_last_error().decode()
 
 
 def corsika_photons_reference(bunches: np.ndarray, uniforms: np.ndarray) -> dict:

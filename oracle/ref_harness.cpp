@@ -61,6 +61,8 @@ struct Handle {
     ml::sensor::Sensors sensors;
     merlict_b200::FlatScene flat;
     bool flattened = false;
+    std::vector<double> last_support;   // ray supports after the last propagation
+    std::vector<std::unique_ptr<plenoscope::light_field_sensor::Geometry>> geometries;
     std::vector<std::unique_ptr<ml::function::Func1>> functions;
     const ml::function::Func1* fn(std::vector<std::vector<double>> xy) {
         functions.emplace_back(new ml::function::Func1(xy));
@@ -317,6 +319,46 @@ void build_reflector_camera(Handle* h, const double* p, int n) {
     }
 }
 
+// A large parabolic segmented reflector with a flat camera of hexagonal
+// pixels in its focal plane; the pixel grid is the one
+// light_field_sensor/Geometry.cpp:13-77 lays out for its lens array
+// (spacing 2 f tan(pixel FoV / 2) out to f tan(FoV / 2)).
+// p: f, max aperture radius, DC mixing, facet inner hex radius, gap, FoV
+//    diameter [deg], pixel FoV [deg], reflectivity
+void build_large_reflector(Handle* h, const double* p, int n) {
+    const double f = param(p, n, 0, 106.5);
+    ml::segmented_imaging_reflector::Config c;
+    c.focal_length = f;
+    c.DaviesCotton_over_parabolic_mixing_factor = param(p, n, 2, 0.0);
+    c.max_outer_aperture_radius = param(p, n, 1, 35.5);
+    c.min_inner_aperture_radius = 0.0;
+    c.facet_inner_hex_radius = param(p, n, 3, 0.45);
+    c.gap_between_facets = param(p, n, 4, 0.01);
+    const double fov = ml::deg2rad(param(p, n, 5, 6.5));
+    const double pixel_fov = ml::deg2rad(param(p, n, 6, 0.06667));
+    const double reflectivity = param(p, n, 7, 0.9);
+
+    ml::SurfaceEntity* reflector = h->scenery.root.add<ml::SurfaceEntity>();
+    reflector->set_name_pos_rot("reflector", ml::VEC3_ORIGIN, ml::ROT3_UNITY);
+    reflector->outer_reflection = h->fn({{200e-9, reflectivity}, {1200e-9, reflectivity}});
+    ml::segmented_imaging_reflector::Factory fab(c);
+    fab.add_to_SurfaceEntity(reflector);
+
+    const double inner = f*std::tan(pixel_fov/2.0);
+    const double outer = inner*2.0/std::sqrt(3.0);
+    const double max_radius = f*std::tan(fov/2.0);
+    ml::HexGridAnnulus grid(max_radius - outer, 0.0, 2.0*inner);
+    const std::vector<ml::Vec3> cells = grid.get_grid();
+    ml::Frame* cam = h->scenery.root.add<ml::Frame>();
+    cam->set_name_pos_rot("camera", ml::Vec3(0.0, 0.0, f), ml::ROT3_UNITY);
+    for (size_t i = 0; i < cells.size(); i++) {
+        ml::HexPlane* pix = cam->add<ml::HexPlane>();
+        pix->set_name_pos_rot("pixel_" + std::to_string(i), cells[i], ml::ROT3_UNITY);
+        pix->set_outer_hex_radius(outer);
+        h->owned_sensors.push_back(new ml::sensor::Sensor(static_cast<unsigned>(i), pix));
+    }
+}
+
 // Segmented reflector plus the light-field sensor of
 // merlict_portal_plenoscope/light_field_sensor/Factory.cpp:235-249 at the
 // focal plane.
@@ -353,7 +395,8 @@ void build_light_field_sensor(Handle* h, const double* p, int n) {
     lc.housing_overhead = param(p, n, 5, 1.1);
     lc.lens_refraction = n_lens;
     lc.bin_reflection = refl;
-    auto* geometry = new plenoscope::light_field_sensor::Geometry(lc);
+    h->geometries.emplace_back(new plenoscope::light_field_sensor::Geometry(lc));
+    plenoscope::light_field_sensor::Geometry* geometry = h->geometries.back().get();
     ml::Frame* lfs = h->scenery.root.add<ml::Frame>();
     lfs->set_name_pos_rot("light_field_sensor", ml::Vec3(0, 0, f), ml::ROT3_UNITY);
     plenoscope::light_field_sensor::Factory factory(geometry);
@@ -394,6 +437,132 @@ struct InteractionHistory {
 };
 template struct Accessor<InteractionHistory, &ml::RayForPropagation::interaction_history>;
 
+// The reference's photons for a batch of host planes (FP64), photon i with
+// simulation_truth_id i.
+std::vector<ml::Photon> make_photons(const mlgpu_photons* ph, uint64_t n) {
+    std::vector<ml::Photon> photons;
+    photons.reserve(n);
+    for (uint64_t i = 0; i < n; i++) {
+        const ml::Vec3 s(((const double*)ph->support_x)[i], ((const double*)ph->support_y)[i],
+                         ((const double*)ph->support_z)[i]);
+        const ml::Vec3 d(((const double*)ph->direction_x)[i], ((const double*)ph->direction_y)[i],
+                         ((const double*)ph->direction_z)[i]);
+        ml::Photon p(s, d, ((const double*)ph->wavelength)[i]);
+        p.simulation_truth_id = static_cast<int32_t>(i);
+        photons.push_back(p);
+    }
+    return photons;
+}
+
+// The ray support each photon holds after propagation (ref_last_supports).
+void keep_supports(Handle* h, const std::vector<ml::Photon>& photons) {
+    h->last_support.resize(3*photons.size());
+    for (size_t i = 0; i < photons.size(); i++) {
+        const ml::Vec3 s = photons[i].support();
+        h->last_support[3*i] = s.x;
+        h->last_support[3*i + 1] = s.y;
+        h->last_support[3*i + 2] = s.z;
+    }
+}
+
+// Per-photon results of propagated photons whose arrivals the scene's
+// sensors hold (after Sensors::assign_photons), read through merlict's
+// public accessors; used[i] = uniforms photon i drew (0 when unknown).
+void write_results(Handle* h, const std::vector<ml::Photon>& photons,
+                   const std::vector<uint32_t>& used, uint32_t max_interactions,
+                   mlgpu_results* out) {
+    const uint64_t n = photons.size();
+    const merlict_b200::FlatScene* flat = nullptr;
+    if (!h->flattened) {
+        h->flat = merlict_b200::flatten(&h->scenery.root, &h->sensors);
+        h->flattened = true;
+    }
+    flat = &h->flat;
+    std::map<const ml::Frame*, int32_t> leaf_of;
+    for (size_t l = 0; l < flat->leaf_node.size(); l++)
+        leaf_of[flat->node_frame[flat->leaf_node[l]]] = static_cast<int32_t>(l);
+    auto leaf_id = [&](const ml::SurfaceEntity* o) -> int32_t {
+        if (o == &ml::VOID_SURFACE_ENTITY) return MLGPU_LEAF_VOID;
+        auto it = leaf_of.find(o);
+        return it == leaf_of.end() ? MLGPU_LEAF_PHOTON_SOURCE : it->second;
+    };
+    // arrivals by photon id (simulation_truth_id == photon index)
+    std::vector<int32_t> sensor_of(n, -1);
+    std::vector<const ml::sensor::PhotonArrival*> arrival_of(n, nullptr);
+    for (size_t s = 0; s < h->sensors.by_occurence.size(); s++)
+        for (const ml::sensor::PhotonArrival& a : h->sensors.by_occurence[s]->photon_arrival_history) {
+            sensor_of[a.simulation_truth_id] = static_cast<int32_t>(s);
+            arrival_of[a.simulation_truth_id] = &a;
+        }
+    const uint32_t len = max_interactions + 1;
+    for (uint64_t i = 0; i < n; i++) {
+        const ml::Photon& p = photons[i];
+        const ml::Intersection& fin = p.final_intersection();
+        const int32_t leaf = p.num_interactions() > 1 ? leaf_id(fin.object())
+                                                      : MLGPU_LEAF_PHOTON_SOURCE;
+        out->sensor[i] = sensor_of[i];
+        double x = fin.position_in_object_frame().x;
+        double y = fin.position_in_object_frame().y;
+        double t, tx, ty;
+        if (arrival_of[i]) {
+            t = arrival_of[i]->arrival_time;
+            tx = arrival_of[i]->theta_x;
+            ty = arrival_of[i]->theta_y;
+            x = arrival_of[i]->x_intersect;
+            y = arrival_of[i]->y_intersect;
+        } else {
+            // merlict evaluates the time of flight only for photons given
+            // to a sensor (Sensor.cpp:14-30).  For a photon that ended in
+            // the void it would dereference the refraction table of
+            // VOID_SURFACE_ENTITY, which is built before the default
+            // tables in SurfaceEntity.cpp:9-27 and holds null pointers.
+            t = NAN;
+            const ml::Vec3 inc = p.final_intersection_incident_direction_wrt_frame();
+            tx = -1.0*inc.x; ty = -1.0*inc.y;
+        }
+        if (out->x) ((double*)out->x)[i] = x;
+        if (out->y) ((double*)out->y)[i] = y;
+        if (out->time) out->time[i] = t;
+        if (out->theta_x) ((double*)out->theta_x)[i] = tx;
+        if (out->theta_y) ((double*)out->theta_y)[i] = ty;
+        if (out->final_leaf) out->final_leaf[i] = leaf;
+        if (out->info) {
+            const uint32_t u = used[i] > 255 ? 255 : used[i];
+            out->info[i] = static_cast<uint32_t>(p.final_interaction()) |
+                (p.num_interactions() << 8) | (u << 16);
+        }
+        if (out->final_position) {
+            const ml::Vec3 w = fin.position_in_root_frame();
+            out->final_position[3*i] = w.x;
+            out->final_position[3*i + 1] = w.y;
+            out->final_position[3*i + 2] = w.z;
+        }
+        if (out->final_direction) {
+            out->final_direction[3*i] = p.direction().x;
+            out->final_direction[3*i + 1] = p.direction().y;
+            out->final_direction[3*i + 2] = p.direction().z;
+        }
+        if (out->history) {
+            const std::vector<ml::Interaction>& kinds = p.*member_of(InteractionHistory());
+            for (uint32_t k = 0; k < len; k++) {
+                mlgpu_history_entry* e = &out->history[i*len + k];
+                std::memset(e, 0, sizeof(*e));
+                e->leaf = MLGPU_LEAF_PHOTON_SOURCE;
+                if (k >= p.num_interactions()) continue;
+                const ml::Intersection& is = p.intersection_at(k);
+                const ml::Vec3 pos = is.position_in_object_frame();
+                const ml::Vec3 nrm = is.surface_normal_in_object_frame();
+                e->position[0] = pos.x; e->position[1] = pos.y; e->position[2] = pos.z;
+                e->normal[0] = nrm.x; e->normal[1] = nrm.y; e->normal[2] = nrm.z;
+                e->distance = is.distance_to_ray_support();
+                e->leaf = k == 0 ? MLGPU_LEAF_PHOTON_SOURCE : leaf_id(is.object());
+                e->interaction = static_cast<uint8_t>(kinds[k]);
+                e->from_outside_to_inside = is.from_outside_to_inside() ? 1 : 0;
+            }
+        }
+    }
+}
+
 }  // namespace
 
 extern "C" {
@@ -413,6 +582,7 @@ void* ref_scene_build(const char* kind, const double* params, int num_params) {
         else if (k == "primitive_zoo") build_primitive_zoo(h.get());
         else if (k == "reflector_camera") build_reflector_camera(h.get(), params, num_params);
         else if (k == "light_field_sensor") build_light_field_sensor(h.get(), params, num_params);
+        else if (k == "large_reflector") build_large_reflector(h.get(), params, num_params);
         else throw std::invalid_argument("unknown scene kind '" + k + "'");
         h->sensors.init(h->owned_sensors);
         h->scenery.root.init_tree_based_on_mother_child_relations();
@@ -456,17 +626,7 @@ int ref_propagate(void* handle, const mlgpu_photons* ph, uint64_t n,
                   mlgpu_results* out, double* seconds) {
     Handle* h = static_cast<Handle*>(handle);
     try {
-        std::vector<ml::Photon> photons;
-        photons.reserve(n);
-        for (uint64_t i = 0; i < n; i++) {
-            const ml::Vec3 s(((const double*)ph->support_x)[i], ((const double*)ph->support_y)[i],
-                             ((const double*)ph->support_z)[i]);
-            const ml::Vec3 d(((const double*)ph->direction_x)[i], ((const double*)ph->direction_y)[i],
-                             ((const double*)ph->direction_z)[i]);
-            ml::Photon p(s, d, ((const double*)ph->wavelength)[i]);
-            p.simulation_truth_id = static_cast<int32_t>(i);
-            photons.push_back(p);
-        }
+        std::vector<ml::Photon> photons = make_photons(ph, n);
         ml::PropagationConfig cfg;
         cfg.max_num_interactions_per_photon = max_interactions;
         std::vector<uint32_t> used(n, 0);
@@ -506,96 +666,8 @@ int ref_propagate(void* handle, const mlgpu_photons* ph, uint64_t n,
         const auto t1 = std::chrono::steady_clock::now();
         if (seconds) *seconds = std::chrono::duration<double>(t1 - t0).count();
 
-        if (!out) return 0;
-        const merlict_b200::FlatScene* flat = nullptr;
-        if (!h->flattened) {
-            h->flat = merlict_b200::flatten(&h->scenery.root, &h->sensors);
-            h->flattened = true;
-        }
-        flat = &h->flat;
-        std::map<const ml::Frame*, int32_t> leaf_of;
-        for (size_t l = 0; l < flat->leaf_node.size(); l++)
-            leaf_of[flat->node_frame[flat->leaf_node[l]]] = static_cast<int32_t>(l);
-        auto leaf_id = [&](const ml::SurfaceEntity* o) -> int32_t {
-            if (o == &ml::VOID_SURFACE_ENTITY) return MLGPU_LEAF_VOID;
-            auto it = leaf_of.find(o);
-            return it == leaf_of.end() ? MLGPU_LEAF_PHOTON_SOURCE : it->second;
-        };
-        // arrivals by photon id (simulation_truth_id == photon index)
-        std::vector<int32_t> sensor_of(n, -1);
-        std::vector<const ml::sensor::PhotonArrival*> arrival_of(n, nullptr);
-        for (size_t s = 0; s < h->sensors.by_occurence.size(); s++)
-            for (const ml::sensor::PhotonArrival& a : h->sensors.by_occurence[s]->photon_arrival_history) {
-                sensor_of[a.simulation_truth_id] = static_cast<int32_t>(s);
-                arrival_of[a.simulation_truth_id] = &a;
-            }
-        const uint32_t len = max_interactions + 1;
-        for (uint64_t i = 0; i < n; i++) {
-            const ml::Photon& p = photons[i];
-            const ml::Intersection& fin = p.final_intersection();
-            const int32_t leaf = p.num_interactions() > 1 ? leaf_id(fin.object())
-                                                          : MLGPU_LEAF_PHOTON_SOURCE;
-            out->sensor[i] = sensor_of[i];
-            double x = fin.position_in_object_frame().x;
-            double y = fin.position_in_object_frame().y;
-            double t, tx, ty;
-            if (arrival_of[i]) {
-                t = arrival_of[i]->arrival_time;
-                tx = arrival_of[i]->theta_x;
-                ty = arrival_of[i]->theta_y;
-                x = arrival_of[i]->x_intersect;
-                y = arrival_of[i]->y_intersect;
-            } else {
-                // merlict evaluates the time of flight only for photons given
-                // to a sensor (Sensor.cpp:14-30).  For a photon that ended in
-                // the void it would dereference the refraction table of
-                // VOID_SURFACE_ENTITY, which is built before the default
-                // tables in SurfaceEntity.cpp:9-27 and holds null pointers.
-                t = NAN;
-                const ml::Vec3 inc = p.final_intersection_incident_direction_wrt_frame();
-                tx = -1.0*inc.x; ty = -1.0*inc.y;
-            }
-            if (out->x) ((double*)out->x)[i] = x;
-            if (out->y) ((double*)out->y)[i] = y;
-            if (out->time) out->time[i] = t;
-            if (out->theta_x) ((double*)out->theta_x)[i] = tx;
-            if (out->theta_y) ((double*)out->theta_y)[i] = ty;
-            if (out->final_leaf) out->final_leaf[i] = leaf;
-            if (out->info) {
-                const uint32_t u = used[i] > 255 ? 255 : used[i];
-                out->info[i] = static_cast<uint32_t>(p.final_interaction()) |
-                    (p.num_interactions() << 8) | (u << 16);
-            }
-            if (out->final_position) {
-                const ml::Vec3 w = fin.position_in_root_frame();
-                out->final_position[3*i] = w.x;
-                out->final_position[3*i + 1] = w.y;
-                out->final_position[3*i + 2] = w.z;
-            }
-            if (out->final_direction) {
-                out->final_direction[3*i] = p.direction().x;
-                out->final_direction[3*i + 1] = p.direction().y;
-                out->final_direction[3*i + 2] = p.direction().z;
-            }
-            if (out->history) {
-                const std::vector<ml::Interaction>& kinds = p.*member_of(InteractionHistory());
-                for (uint32_t k = 0; k < len; k++) {
-                    mlgpu_history_entry* e = &out->history[i*len + k];
-                    std::memset(e, 0, sizeof(*e));
-                    e->leaf = MLGPU_LEAF_PHOTON_SOURCE;
-                    if (k >= p.num_interactions()) continue;
-                    const ml::Intersection& is = p.intersection_at(k);
-                    const ml::Vec3 pos = is.position_in_object_frame();
-                    const ml::Vec3 nrm = is.surface_normal_in_object_frame();
-                    e->position[0] = pos.x; e->position[1] = pos.y; e->position[2] = pos.z;
-                    e->normal[0] = nrm.x; e->normal[1] = nrm.y; e->normal[2] = nrm.z;
-                    e->distance = is.distance_to_ray_support();
-                    e->leaf = k == 0 ? MLGPU_LEAF_PHOTON_SOURCE : leaf_id(is.object());
-                    e->interaction = static_cast<uint8_t>(kinds[k]);
-                    e->from_outside_to_inside = is.from_outside_to_inside() ? 1 : 0;
-                }
-            }
-        }
+        keep_supports(h, photons);
+        if (out) write_results(h, photons, used, max_interactions, out);
         return 0;
     } catch (const std::out_of_range& e) {
         last_error = e.what();
@@ -1085,5 +1157,111 @@ void ref_corsika_file_free(void* handle) { delete static_cast<CorsikaFile*>(hand
 int ref_hardware_concurrency(void) {
     return static_cast<int>(std::thread::hardware_concurrency());
 }
+
+// The ray supports (x, y, z per photon) the photons held after the last
+// ref_propagate (or shim_propagate) on this scene; returns the photon count,
+// copies when out != NULL.
+uint64_t ref_last_supports(void* handle, double* out) {
+    const Handle* h = static_cast<const Handle*>(handle);
+    if (out && !h->last_support.empty())
+        std::memcpy(out, h->last_support.data(), h->last_support.size()*sizeof(double));
+    return h->last_support.size()/3;
+}
+
+// The drop-in's history rebuild (merlict_b200::rebuild_histories) without
+// the engine: fresh photons from the planes get the given histories (rows
+// of max_interactions + 1 entries, as mlgpu_results.history holds them),
+// infos and final directions, then merlict's own Sensors::assign_photons
+// runs on them; their results (and supports) are written as ref_propagate
+// writes them.  Fed with ref_propagate's own export of the same photons,
+// the results must come back unchanged.
+int ref_rebuild_photons(void* handle, const mlgpu_photons* ph, uint64_t n,
+                        uint32_t max_interactions, const mlgpu_history_entry* history,
+                        const uint32_t* info, const double* final_direction,
+                        mlgpu_results* out) {
+    Handle* h = static_cast<Handle*>(handle);
+    try {
+        std::vector<ml::Photon> photons = make_photons(ph, n);
+        if (!h->flattened) {
+            h->flat = merlict_b200::flatten(&h->scenery.root, &h->sensors);
+            h->flattened = true;
+        }
+        merlict_b200::rebuild_histories(&photons, h->flat, history, info, final_direction,
+                                        max_interactions);
+        h->sensors.clear_history();
+        h->sensors.assign_photons(&photons);
+        keep_supports(h, photons);
+        if (out) write_results(h, photons, std::vector<uint32_t>(n, 0), max_interactions, out);
+        return 0;
+    } catch (const std::exception& e) {
+        last_error = e.what();
+        return MLGPU_ERR_RUNTIME;
+    }
+}
+
+#ifdef MLGPU_WITH_SHIM
+// The product's C++ drop-in (merlict_b200_shim.h) on a scene built here, the
+// way a merlict application would call it in place of the reference's own
+// functions:
+//   mode 0  merlict_b200::propagate_photons_in_frame_with_config, then
+//           merlict's own Sensors::assign_photons on the rebuilt photons;
+//   mode 1  merlict_b200::propagate_photons_in_frame_with_config_multi_thread,
+//           then Sensors::assign_photons;
+//   mode 2  merlict_b200::propagate_and_assign_photons (arrivals written
+//           straight into the sensors; the photons keep no history).
+// The generator is merlict's Mt19937(mt_seed); *philox_seed receives the
+// seed the drop-in drew from it (Generator::create_seed), with which
+// ref_propagate's mode 0 replays the same streams.  Results as for
+// ref_propagate (info without the uniform count); in mode 2 only the
+// arrival fields (sensor, x, y, time, theta_x, theta_y) are meaningful.
+// A std:: exception from the drop-in returns the status of its type.
+int shim_propagate(void* handle, const mlgpu_photons* ph, uint64_t n,
+                   uint32_t max_interactions, int mode, uint64_t mt_seed,
+                   uint64_t* philox_seed, mlgpu_results* out) {
+    Handle* h = static_cast<Handle*>(handle);
+    struct Recording : ml::random::Mt19937 {
+        explicit Recording(uint64_t seed) : ml::random::Mt19937(seed) {}
+        uint64_t drawn = 0;
+        uint64_t create_seed() override {
+            drawn = ml::random::Mt19937::create_seed();
+            return drawn;
+        }
+    };
+    try {
+        std::vector<ml::Photon> photons = make_photons(ph, n);
+        ml::PropagationConfig cfg;
+        cfg.max_num_interactions_per_photon = max_interactions;
+        Recording prng(mt_seed);
+        h->sensors.clear_history();
+        if (mode == 0) {
+            merlict_b200::propagate_photons_in_frame_with_config(
+                &photons, &h->scenery.root, &cfg, &prng);
+            h->sensors.assign_photons(&photons);
+        } else if (mode == 1) {
+            merlict_b200::propagate_photons_in_frame_with_config_multi_thread(
+                &photons, &h->scenery.root, &cfg, &prng);
+            h->sensors.assign_photons(&photons);
+        } else if (mode == 2) {
+            merlict_b200::propagate_and_assign_photons(
+                &photons, &h->scenery.root, &cfg, &prng, &h->sensors);
+        } else {
+            throw std::invalid_argument("unknown mode");
+        }
+        if (philox_seed) *philox_seed = prng.drawn;
+        keep_supports(h, photons);
+        if (out) write_results(h, photons, std::vector<uint32_t>(n, 0), max_interactions, out);
+        return 0;
+    } catch (const std::out_of_range& e) {
+        last_error = e.what();
+        return MLGPU_ERR_OUT_OF_RANGE;
+    } catch (const std::invalid_argument& e) {
+        last_error = e.what();
+        return MLGPU_ERR_INVALID_ARGUMENT;
+    } catch (const std::exception& e) {
+        last_error = e.what();
+        return MLGPU_ERR_RUNTIME;
+    }
+}
+#endif
 
 }  // extern "C"
