@@ -192,8 +192,10 @@ def cpu_reference_run(photons_per_step: int, steps: int, warmup: int, threads_mo
             if k >= warmup:
                 secs.append(sec)
         total = float(sum(secs))
+        what = ("merlict_multi_thread" if threads_mode == "multi"
+                else "propagate_photons_in_frame_with_config (one thread)")
         return photons_per_step * steps / total, total, cores, "reference", \
-            f"{steps} x {photons_per_step} photons, reference merlict_multi_thread + assign_photons"
+            f"{steps} x {photons_per_step} photons, reference {what} + assign_photons"
     # the C restatement when the reference library is not built here
     from merlict_development_kit_b200 import factories as F
     flat = F.light_field_telescope(**SCENE).flatten()
@@ -283,10 +285,14 @@ def run_ours(args, world, rank, local):
     t_start = torch.cuda.Event(enable_timing=True)
     t_stop = torch.cuda.Event(enable_timing=True)
     launches0 = scene.kernel_launches()
+    # the timed steps as one NVTX range, so that a profiler can capture
+    # exactly their launches (ncu --nvtx --nvtx-include "bench_timed/")
+    torch.cuda.nvtx.range_push("bench_timed")
     t_start.record(stream)
     for k in range(args.steps):
         step(kernel_events[k])
     t_stop.record(stream)
+    torch.cuda.nvtx.range_pop()
     launches = scene.kernel_launches() - launches0
     torch.cuda.synchronize()
     barrier(world)
@@ -342,8 +348,11 @@ def run_ours(args, world, rank, local):
                           "tuning": tune32}}
         del dev32, dev64r, ref, res32
 
-    # e2e: the C-ABI host-buffer call (H2D of the batch, trace, D2H of the
-    # results, synchronise), pinned host memory, same batch size
+    # e2e: the C-ABI host-buffer call that does a step's whole work --
+    # H2D of the batch, trace, per-lixel binning, D2H of the per-photon
+    # results and the lixel counts, synchronise -- pinned host memory, same
+    # batch size (mlgpu_propagate_and_bin_host: merlict's propagate +
+    # Sensors::assign_photons pair)
     pin = {k: torch.from_numpy(np.ascontiguousarray(host[k])).to(in_dtype).pin_memory()
            for k in ("support_x", "support_y", "support_z", "direction_x", "direction_y",
                      "direction_z", "wavelength")}
@@ -355,6 +364,7 @@ def run_ours(args, world, rank, local):
     h_x = torch.empty(n, dtype=out_dtype).pin_memory()
     h_y = torch.empty(n, dtype=out_dtype).pin_memory()
     h_t = torch.empty(n, dtype=torch.float64).pin_memory()
+    h_counts = torch.empty(flat.num_sensors, dtype=torch.int32).pin_memory()
     res = abi.mlgpu_results()
     res.dtype = abi.F64 if out_dtype == torch.float64 else abi.F32
     res.sensor, res.x, res.y, res.time = (h_sensor.data_ptr(), h_x.data_ptr(), h_y.data_ptr(),
@@ -365,20 +375,33 @@ def run_ours(args, world, rank, local):
     r.seed = 99 + rank
     L = _native.lib()
     e2e_steps = max(1, min(args.steps, 5))
+
+    def host_step():
+        _native.check(L.mlgpu_propagate_and_bin_host(
+            scene.handle, C.byref(ph), n, C.byref(st), C.byref(r), C.byref(res),
+            C.c_void_p(h_counts.data_ptr()), None, 0, 0.0, 0.0))
     for _ in range(1):
-        _native.check(L.mlgpu_propagate_host(scene.handle, C.byref(ph), n, C.byref(st),
-                                             C.byref(r), C.byref(res)))
+        host_step()
     barrier(world)
     t0 = time.perf_counter()
     for _ in range(e2e_steps):
-        _native.check(L.mlgpu_propagate_host(scene.handle, C.byref(ph), n, C.byref(st),
-                                             C.byref(r), C.byref(res)))
+        host_step()
     e2e_s = max_over_ranks(time.perf_counter() - t0, world)
     e2e_value = n * world * e2e_steps / e2e_s
     elt = 8 if in_dtype == torch.float64 else 4
     eout = 8 if out_dtype == torch.float64 else 4
     h2d = 7 * elt * n
-    d2h = (4 + 2 * eout + 8) * n
+    d2h = (4 + 2 * eout + 8) * n + 4 * flat.num_sensors
+    del pin, h_sensor, h_x, h_y, h_t, dev
+    torch.cuda.empty_cache()
+    # the other configurations' forms, each on its own scene and photons
+    if tracer == "fp64" and not args.no_forms:
+        clk_forms = ClockSampler(local)
+        clk_forms.start()
+        forms = forms or {}
+        forms["batched_events"] = bunches_form(flat, args.events, 2, 1, world, rank, local)
+        forms["precision"] = precision_form(args.precision_photons, 2, 1, world, rank, local)
+        forms["clocks"] = clk_forms.stop()
 
     if rank != 0:
         return
@@ -429,6 +452,11 @@ def run_ours(args, world, rank, local):
     if world == 1 and not args.no_cpu_baseline:
         v, secs, cores, kind, sample = cpu_reference_run(args.ref_photons, 2, 1)
         cpu = {"value": v, "unit": "photons/s", "cores": cores, "kind": kind, "sample": sample}
+        # merlict's single-thread loop (Photons.cpp:9-22), which beats its
+        # thread pool on cheap scenes
+        v1, _, c1, k1, s1 = cpu_reference_run(args.ref_photons // 5, 2, 1, threads_mode="single")
+        cpu["single_thread"] = {"value": v1, "unit": "photons/s", "cores": c1, "kind": k1,
+                                "sample": s1}
     line = {
         "metric": "photons/s", "value": value, "unit": "photons/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": elapsed_ms / args.steps,
@@ -456,21 +484,20 @@ def run_ours(args, world, rank, local):
     scene.close()
 
 
-def run_bunches(args, world, rank, local):
-    """Batched uneven events: `args.events` air-shower-like events with
+def bunches_form(flat, events: int, steps: int, warmup: int, world: int, rank: int, local: int,
+                 seed: int = 0):
+    """Batched uneven events (config 2): `events` air-shower-like events with
     log-uniform sizes in [1e2, 1e6] photons on the light-field telescope,
     traced (a) as one photon stream with autotuned knobs and CUDA-graph
     launches and (b) with one propagate call per event (the reference's
     per-event loop, plenoscope_propagation.cpp:206-210), same Philox streams,
-    so the two give identical results."""
+    so the two give identical results.  Returns the form's line items."""
     import torch
-    from merlict_development_kit_b200 import engine, factories as F, photons as P
+    from merlict_development_kit_b200 import engine, photons as P
 
-    torch.cuda.set_device(local)
-    flat = F.light_field_telescope(**SCENE).flatten()
     scene = engine.Scene(flat)
-    sizes = P.cherenkov_event_sizes(args.events, 2024 + rank)
-    dev, off = P.cherenkov_events(sizes, 4048 + rank, device=f"cuda:{local}")
+    sizes = P.cherenkov_event_sizes(events, 2024 + rank + seed)
+    dev, off = P.cherenkov_events(sizes, 4048 + rank + seed, device=f"cuda:{local}")
     n = int(off[-1])
     cfg = engine.PropagationConfig(MAX_INTERACTIONS)
     stream = torch.cuda.current_stream()
@@ -492,18 +519,16 @@ def run_bunches(args, world, rank, local):
             scene.propagate(part, cfg, engine.Philox(11, photon_offset=a), outputs=outs,
                             sync=False, results=r)
 
-    for _ in range(args.warmup):
+    for _ in range(warmup):
         batched()
     scene.sync_errors()
     for k, v in res_batched.items():
         res_events[k] = torch.empty_like(v)
     ev = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
-    clocks = ClockSampler(local)
-    clocks.start()
     barrier(world)
     torch.cuda.synchronize()
     ev[0].record(stream)
-    for _ in range(args.steps):
+    for _ in range(steps):
         batched()
     ev[1].record(stream)
     torch.cuda.synchronize()
@@ -511,30 +536,69 @@ def run_bunches(args, world, rank, local):
     per_event()
     ev[3].record(stream)
     torch.cuda.synchronize()
-    clk = clocks.stop()
     scene.sync_errors()
-    identical = all(bool(torch.equal(res_batched[k], res_events[k])) for k in ("sensor", "x", "y"))
-    ms_b = max_over_ranks(ev[0].elapsed_time(ev[1]) / args.steps, world)
+    identical = all(bool(torch.equal(res_batched[k], res_events[k])) for k in outs)
+    ms_b = max_over_ranks(ev[0].elapsed_time(ev[1]) / steps, world)
     ms_e = max_over_ranks(ev[2].elapsed_time(ev[3]), world)
-    if rank == 0:
-        hit = float((res_batched["sensor"] >= 0).float().mean())
-        print(json.dumps({
-            "metric": "photons/s", "value": n * world / (ms_b * 1e-3), "unit": "photons/s",
-            "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_b,
-            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-            "data": "synthetic",
-            "config": {"workload": f"{args.events} air-shower-like events, log-uniform 1e2-1e6 "
-                                   "photons, on the light-field telescope (config 2)",
-                       "photons_per_step_per_gpu": n, "events": int(len(sizes)),
-                       "max_interactions": MAX_INTERACTIONS, "tuning": tuning,
-                       "fraction_on_lixels": hit},
+    # (c) one persistent launch whose warps pull photon tiles from a device
+    # work queue (tracer fp64_queue), same streams
+    res_queue = {}
+
+    def queued():
+        return scene.propagate(dev, cfg, engine.Philox(11), outputs=outs, sync=False,
+                               results=res_queue, tracer="fp64_queue")
+    queued()
+    torch.cuda.synchronize()
+    ev[0].record(stream)
+    for _ in range(steps):
+        queued()
+    ev[1].record(stream)
+    torch.cuda.synchronize()
+    scene.sync_errors()
+    ms_q = max_over_ranks(ev[0].elapsed_time(ev[1]) / steps, world)
+    identical_q = all(bool(torch.equal(res_batched[k], res_queue[k])) for k in outs)
+    hit = float((res_batched["sensor"] >= 0).float().mean())
+    scene.close()
+    del dev, res_batched, res_events, res_queue
+    torch.cuda.empty_cache()
+    return {"value": n * world / (ms_b * 1e-3), "unit": "photons/s", "ms_per_step": ms_b,
+            "photons_per_step_per_gpu": n, "events": int(len(sizes)), "steps": steps,
+            "tuning": tuning, "fraction_on_lixels": hit,
             "one_call_per_event": {"value": n * world / (ms_e * 1e-3), "unit": "photons/s",
                                    "ms": ms_e, "calls": int(len(sizes))},
-            "batched_over_per_event": ms_e / ms_b,
-            "identical_results": identical,
+            "persistent_work_queue": {"value": n * world / (ms_q * 1e-3), "unit": "photons/s",
+                                      "ms": ms_q, "identical_results": identical_q},
+            "batched_over_per_event": ms_e / ms_b, "identical_results": identical}
+
+
+def run_bunches(args, world, rank, local):
+    import torch
+    from merlict_development_kit_b200 import factories as F
+
+    torch.cuda.set_device(local)
+    flat = F.light_field_telescope(**SCENE).flatten()
+    clocks = ClockSampler(local)
+    clocks.start()
+    form = bunches_form(flat, args.events, args.steps, args.warmup, world, rank, local)
+    clk = clocks.stop()
+    if rank == 0:
+        print(json.dumps({
+            "metric": "photons/s", "value": form["value"], "unit": "photons/s",
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": form["ms_per_step"], "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": f"{args.events} air-shower-like events, log-uniform 1e2-1e6 "
+                                   "photons, on the light-field telescope (config 2)",
+                       "photons_per_step_per_gpu": form["photons_per_step_per_gpu"],
+                       "events": form["events"], "max_interactions": MAX_INTERACTIONS,
+                       "tuning": form["tuning"],
+                       "fraction_on_lixels": form["fraction_on_lixels"]},
+            "one_call_per_event": form["one_call_per_event"],
+            "persistent_work_queue": form["persistent_work_queue"],
+            "batched_over_per_event": form["batched_over_per_event"],
+            "identical_results": form["identical_results"],
             "clocks": clk,
         }), flush=True)
-    scene.close()
 
 
 def run_signal(args, world, rank, local):
@@ -652,7 +716,7 @@ def run_signal(args, world, rank, local):
     scene.close()
 
 
-def run_precision(args, world, rank, local):
+def precision_form(n: int, steps: int, warmup: int, world: int, rank: int, local: int):
     """Precision study (config 3): the large parabolic reflector (0.9 m facets
     of curvature radius 213 m on a 35.5 m aperture) with 8,443 flat pixels at
     106.5 m; photons within 3.5 degrees of the axis.  Photons/s of each form
@@ -660,9 +724,7 @@ def run_precision(args, world, rank, local):
     import torch
     from merlict_development_kit_b200 import engine, factories as F, photons as P, precision
 
-    torch.cuda.set_device(local)
     flat = F.large_reflector_camera().flatten()
-    n = args.photons
     ph = P.downward_disc_source_device(n, 303 + rank, 40.0, 110.0, 3.5, device=f"cuda:{local}",
                                        dtype=torch.float32)
     scene = engine.Scene(flat)
@@ -672,30 +734,44 @@ def run_precision(args, world, rank, local):
         dt = torch.float32 if form.startswith("fp32") else torch.float64
         planes = {k: v.to(dt) for k, v in ph.items()}
         res = {}
-        for _ in range(args.warmup):
+        for _ in range(warmup):
             scene.propagate(planes, cfg, engine.Philox(5), tracer=form, sync=False, results=res,
                             outputs=("sensor", "x", "y", "time"), out_dtype=dt)
+        barrier(world)
         torch.cuda.synchronize()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record()
-        for _ in range(args.steps):
+        for _ in range(steps):
             scene.propagate(planes, cfg, engine.Philox(5), tracer=form, sync=False, results=res,
                             outputs=("sensor", "x", "y", "time"), out_dtype=dt)
         e1.record()
         torch.cuda.synchronize()
-        rates[form] = n * args.steps / (e0.elapsed_time(e1) * 1e-3)
+        ms = max_over_ranks(e0.elapsed_time(e1) / steps, world)
+        rates[form] = n * world / (ms * 1e-3)
         del planes, res
     scene.close()
     errors = precision.study(flat, ph, seed=9, max_interactions=5)
+    del ph
+    torch.cuda.empty_cache()
+    return {"value": rates["fp32"], "unit": "photons/s", "photons_per_s": rates,
+            "photons_per_step_per_gpu": n, "steps": steps,
+            "fp32_over_fp64": rates["fp32"] / rates["fp64"],
+            "errors_vs_fp64": errors}
+
+
+def run_precision(args, world, rank, local):
+    import torch
+    torch.cuda.set_device(local)
+    form = precision_form(args.photons, args.steps, args.warmup, world, rank, local)
     if rank == 0:
         print(json.dumps({
-            "metric": "photons/s", "value": rates["fp32"], "unit": "photons/s", "n_gpus": world,
+            "metric": "photons/s", "value": form["value"], "unit": "photons/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
             "config": {"workload": "precision study: 5,388-facet parabolic reflector, R = 213 m, "
                                    "8,443 pixels at 106.5 m (config 3)",
-                       "photons": n, "max_interactions": 5},
-            "photons_per_s": rates, "errors_vs_fp64": errors,
+                       "photons": args.photons, "max_interactions": 5},
+            "photons_per_s": form["photons_per_s"], "errors_vs_fp64": form["errors_vs_fp64"],
         }), flush=True)
 
 
@@ -856,6 +932,8 @@ def main():
                          "precision: the FP32 forms against FP64 on the large reflector; "
                          "signal: the signal chain after binning of one config-1 event")
     ap.add_argument("--events", type=int, default=4096)
+    ap.add_argument("--precision-photons", type=int, default=100_000_000,
+                    help="photons of the precision study (config 3) in the default line's forms")
     ap.add_argument("--event-photons", type=int, default=1_000_000,
                     help="photons of the event the signal workload propagates once")
     ap.add_argument("--train-photons", type=int, default=200_000_000)

@@ -206,7 +206,11 @@ enum {
     MLGPU_TRACER_FP64 = 0,        /* wavefront, FP64                                  */
     MLGPU_TRACER_FP32 = 1,        /* wavefront, FP32 bulk math, FP64 where needed     */
     MLGPU_TRACER_FP32_PURE = 2,   /* FP32 everywhere (precision study only)           */
-    MLGPU_TRACER_FP64_PLAIN = 3   /* one thread per photon, FP64                      */
+    MLGPU_TRACER_FP64_PLAIN = 3,  /* one thread per photon, FP64                      */
+    MLGPU_TRACER_FP64_QUEUE = 4   /* FP64 in one persistent launch: warps take tiles
+                                     of photons from a device work queue and advance
+                                     them one interaction per round, refilling the
+                                     lanes whose photons have ended                  */
 };
 
 /* How candidate surfaces are found for a ray in the whole tree.
@@ -347,6 +351,28 @@ int mlgpu_propagate_host(
     const mlgpu_settings* settings,
     const mlgpu_rng* rng,
     mlgpu_results* results);
+
+/* Propagation and arrival binning in one host-buffer call: the pair a
+ * merlict application runs per event, propagate_photons_in_frame_with_config
+ * then Sensors::assign_photons (merlict/Photons.cpp:9-22,
+ * merlict/sensor/Sensors.cpp:79-81), for callers that want per-sensor
+ * statistics beside the per-photon results.  As mlgpu_propagate_host; then,
+ * on the device, mlgpu_bin_arrivals' counts and time histograms of the whole
+ * batch, copied to counts[num_sensors] and time_hist[num_sensors]
+ * [num_time_bins] (host; time_hist and results->time are needed only when
+ * num_time_bins > 0).                                                      */
+int mlgpu_propagate_and_bin_host(
+    mlgpu_scene* scene,
+    const mlgpu_photons* photons,
+    uint64_t num_photons,
+    const mlgpu_settings* settings,
+    const mlgpu_rng* rng,
+    mlgpu_results* results,
+    uint32_t* counts,
+    uint32_t* time_hist,
+    uint32_t num_time_bins,
+    double t_min,
+    double t_max);
 
 /* ---- CORSIKA photon bunches --------------------------------------------- *
  * Replaces merlict::EventIoPhotonFactory (merlict_corsika/PhotonFactory.cpp:
@@ -539,7 +565,10 @@ int mlgpu_bin_arrivals(
  * Limit: num_sensors x (num_time_bins + 1) must not exceed
  * MLGPU_NOALLOC_BIN_SCRATCH_WORDS; larger requests return
  * MLGPU_ERR_INVALID_ARGUMENT and do nothing.  The inputs and outputs are
- * the caller's device buffers, as for mlgpu_bin_arrivals.
+ * the caller's device buffers, as for mlgpu_bin_arrivals.  The scene's
+ * device must be the current device (else MLGPU_ERR_INVALID_ARGUMENT).
+ * Its two kernel launches count in mlgpu_scene_kernel_launches and, while
+ * profiling is on, in the MLGPU_KERNEL_BIN times.
  *
  * The first call on a device looks up the array's device address (this
  * may load the library's device code into the context); make that first

@@ -54,6 +54,11 @@ def lib():
             C.c_void_p, C.POINTER(abi.mlgpu_photons), C.c_uint64,
             C.POINTER(abi.mlgpu_settings), C.POINTER(abi.mlgpu_rng),
             C.POINTER(abi.mlgpu_results)]
+        L.mlgpu_propagate_and_bin_host.argtypes = [
+            C.c_void_p, C.POINTER(abi.mlgpu_photons), C.c_uint64,
+            C.POINTER(abi.mlgpu_settings), C.POINTER(abi.mlgpu_rng),
+            C.POINTER(abi.mlgpu_results), C.c_void_p, C.c_void_p, C.c_uint32, C.c_double,
+            C.c_double]
         L.mlgpu_scene_sync_errors.argtypes = [C.c_void_p, C.c_void_p]
         L.mlgpu_bin_arrivals.argtypes = [
             C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint64, C.c_void_p, C.c_void_p,
@@ -84,7 +89,8 @@ def lib():
         for name in ("mlgpu_scene_create", "mlgpu_scene_destroy", "mlgpu_propagate",
                      "mlgpu_scene_autotune", "mlgpu_corsika_photons", "mlgpu_lixel_statistics",
                      "mlgpu_signal_chain",
-                     "mlgpu_propagate_host", "mlgpu_scene_sync_errors", "mlgpu_bin_arrivals",
+                     "mlgpu_propagate_host", "mlgpu_propagate_and_bin_host",
+                     "mlgpu_scene_sync_errors", "mlgpu_bin_arrivals",
                      "mlgpu_bin_arrivals_noalloc", "mlgpu_scene_kernel_launches",
                      "mlgpu_scene_wavefront_stats"):
             getattr(L, name).restype = C.c_int
@@ -142,6 +148,7 @@ def check(status: int) -> None:
 EXPORTED = (
     "mlgpu_abi_version", "mlgpu_last_error", "mlgpu_scene_create", "mlgpu_scene_destroy",
     "mlgpu_propagate", "mlgpu_scene_sync_errors", "mlgpu_propagate_host",
+    "mlgpu_propagate_and_bin_host",
     "mlgpu_bin_arrivals", "mlgpu_bin_arrivals_noalloc", "mlgpu_scene_kernel_launches",
     "mlgpu_scene_wavefront_stats",
     "mlgpu_scene_set_profiling", "mlgpu_scene_kernel_times", "mlgpu_scene_autotune",

@@ -86,6 +86,7 @@ TRACER_FP64 = 0
 TRACER_FP32 = 1
 TRACER_FP32_PURE = 2
 TRACER_FP64_PLAIN = 3
+TRACER_FP64_QUEUE = 4
 
 _dp = C.POINTER(C.c_double)
 _ip = C.POINTER(C.c_int32)
@@ -408,6 +409,11 @@ class FlatScene:
             raise ValueError("allowed node out of range")
         if np.any((self.leaf_sensor < -1) | (self.leaf_sensor >= self.num_sensors)):
             raise ValueError("sensor index out of range")
+        sensed = self.leaf_sensor[self.leaf_sensor >= 0]
+        if len(np.unique(sensed)) != len(sensed):
+            # one sensor per frame and no two sensors on one frame
+            # (Sensors::assert_no_two_sensors_have_same_frame)
+            raise ValueError("a sensor index is on two leaves")
         off = self.function_offset
         if off[0] != 0 or np.any(np.diff(off) < 1) or off[-1] != self.function_points.shape[0]:
             raise ValueError("function offsets malformed")

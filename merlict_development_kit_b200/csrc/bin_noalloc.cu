@@ -66,15 +66,29 @@ extern "C" int mlgpu_bin_arrivals_noalloc(
                       (unsigned long long)keys, (unsigned)MLGPU_NOALLOC_BIN_SCRATCH_WORDS);
         return mlgpu::report_error(MLGPU_ERR_INVALID_ARGUMENT, msg);
     }
+    // the array used is the current device's: it must be the scene's
+    int device = -1;
+    cudaError_t e = cudaGetDevice(&device);
+    if (e != cudaSuccess) return mlgpu::report_error(MLGPU_ERR_CUDA, cudaGetErrorString(e));
+    if (device != mlgpu::scene_device(scene)) {
+        char msg[160];
+        std::snprintf(msg, sizeof(msg),
+                      "the current device (%d) is not the scene's device (%d)", device,
+                      mlgpu::scene_device(scene));
+        return mlgpu::report_error(MLGPU_ERR_INVALID_ARGUMENT, msg);
+    }
     uint32_t* scratch = nullptr;
     const int st = scratch_of_current_device(&scratch);
     if (st != MLGPU_OK) return st;
+    const cudaStream_t stream = static_cast<cudaStream_t>(cuda_stream);
+    mlgpu::ProfileMark mark;
+    mlgpu::profile_mark_begin(scene, stream, &mark);
     // The tile kernel stores every word of the partial histograms before
     // the reduction reads it, so the scratch needs no clearing.
-    const cudaError_t e = mlgpu::launch_bin_arrivals(
+    e = mlgpu::launch_bin_arrivals(
         *dev, sensor, time, n, counts, num_time_bins ? time_hist : nullptr, num_time_bins,
-        t_min, t_max, scratch, MLGPU_NOALLOC_BIN_SCRATCH_WORDS,
-        static_cast<cudaStream_t>(cuda_stream));
+        t_min, t_max, scratch, MLGPU_NOALLOC_BIN_SCRATCH_WORDS, stream);
+    mlgpu::profile_mark_end(scene, stream, &mark, MLGPU_KERNEL_BIN, 2);
     if (e != cudaSuccess) return mlgpu::report_error(MLGPU_ERR_CUDA, cudaGetErrorString(e));
     return MLGPU_OK;
 }

@@ -135,7 +135,10 @@ struct mlgpu_scene {
     unsigned int* error_word = nullptr;
     // staging for mlgpu_propagate_host and scratch for binning
     DeviceBuffer staging_in, staging_out, staging_hist, staging_rng, bin_scratch, tune_out;
+    DeviceBuffer staging_bins;           // counts and time histograms of a host call
     DeviceBuffer order;                  // tracing order of a batch and its sort scratch
+    DeviceBuffer queue;                  // the work-queue tracer's counter
+    int queue_blocks = 0;                // its resident blocks per SM
     DeviceBuffer corsika;                // bunch counts, offsets and the total
     DeviceBuffer stats;                  // sort buffers of the calibration statistics
     DeviceBuffer signal, signal_pulses, signal_tables;   // signal chain scratch, Func1 tables
@@ -195,8 +198,33 @@ int validate(const mlgpu_flat_scene* f) {
             return fail(MLGPU_ERR_INVALID_ARGUMENT, "node %d: leaf/subtree mismatch", i);
         if (leaf >= 0 && f->leaf_node[leaf] != i)
             return fail(MLGPU_ERR_INVALID_ARGUMENT, "node %d: leaf_node disagrees", i);
+        // a frame's bounding sphere is centred on its position
+        // (RayAndFrame.cpp:16-24, Frame::position_in_world = the frame-to-
+        // world translation); the kernels take a leaf's centre from its
+        // transform
+        if (leaf >= 0 && f->leaf_frame2world) {
+            const double* t = f->leaf_frame2world + 12*(size_t)leaf;
+            const double* c = f->node_sphere + 4*(size_t)i;
+            if (!(c[0] == t[3] && c[1] == t[7] && c[2] == t[11]))
+                return fail(MLGPU_ERR_INVALID_ARGUMENT,
+                            "leaf %d: bounding sphere not centred on the frame's position", leaf);
+        }
         if (!(f->node_sphere[4*i + 3] >= 0.0))
             return fail(MLGPU_ERR_INVALID_ARGUMENT, "node %d: negative bounding radius", i);
+    }
+    // merlict binds each sensor to one frame and no two sensors to the same
+    // frame (Sensors::assert_no_two_sensors_have_same_frame,
+    // Sensors.cpp:84-100); in the flat layout a sensor index on two leaves
+    // is the same inconsistency
+    if (f->num_sensors < 0) return fail(MLGPU_ERR_INVALID_ARGUMENT, "negative sensor count");
+    std::vector<int32_t> leaf_of_sensor((size_t)f->num_sensors, -1);
+    for (int32_t l = 0; l < nl; l++) {
+        const int32_t sen = f->leaf_sensor[l];
+        if (sen < 0 || sen >= f->num_sensors) continue;
+        if (leaf_of_sensor[sen] >= 0)
+            return fail(MLGPU_ERR_INVALID_ARGUMENT, "sensor %d is on leaves %d and %d", sen,
+                        leaf_of_sensor[sen], l);
+        leaf_of_sensor[sen] = l;
     }
     for (int32_t l = 0; l < nl; l++) {
         const int32_t prim = f->leaf_primitive[l];
@@ -365,7 +393,8 @@ int check_propagate_args(const mlgpu_scene* scene, const mlgpu_photons* ph,
     if (rng->mode == MLGPU_RNG_REPLAY && !rng->uniforms)
         return fail(MLGPU_ERR_INVALID_ARGUMENT, "replay rng without uniforms");
     if (st->tracer != MLGPU_TRACER_FP64 && st->tracer != MLGPU_TRACER_FP32 &&
-        st->tracer != MLGPU_TRACER_FP32_PURE && st->tracer != MLGPU_TRACER_FP64_PLAIN)
+        st->tracer != MLGPU_TRACER_FP32_PURE && st->tracer != MLGPU_TRACER_FP64_PLAIN &&
+        st->tracer != MLGPU_TRACER_FP64_QUEUE)
         return fail(MLGPU_ERR_INVALID_ARGUMENT, "unknown tracer %d", st->tracer);
     if (st->traversal != MLGPU_TRAVERSAL_BVH && st->traversal != MLGPU_TRAVERSAL_FRAME_TREE)
         return fail(MLGPU_ERR_INVALID_ARGUMENT, "unknown traversal %d", st->traversal);
@@ -423,10 +452,9 @@ int wave_buffers(mlgpu_scene* scene, uint32_t pool, int grid, int staged, uint32
     auto up = [](size_t x) { return (x + 255) & ~size_t(255); };
     const size_t P = pool;
     const size_t level_cap = queue_cap ? queue_cap : 8*P;
-    const size_t range_cap = queue_cap ? queue_cap : 16*P;
     const size_t isect_cap = queue_cap ? queue_cap : 16*P;
     const size_t per_pool = 8*up(P*8) + 5*up(P*4);
-    const size_t rest = up(P*4) + 2*up(P*16) + up(P*48) + 2*up(level_cap*8) + up(range_cap*8) +
+    const size_t rest = up(P*4) + up(P*48) + 2*up(level_cap*32) +
         up(isect_cap*8) + up(isect_cap*8) + up(P*8) + 3*up(P*4);
     MLGPU_CUDA(scene->wave.reserve(256 + 2*per_pool + rest));
     if (!scene->wave_host) MLGPU_CUDA(cudaMallocHost(&scene->wave_host, sizeof(WaveCounters)));
@@ -449,14 +477,10 @@ int wave_buffers(mlgpu_scene* scene, uint32_t pool, int grid, int staged, uint32
     w->grid = grid > 0 ? grid : scene->wave_grid;
     w->staged_levels = staged;
     w->step = reinterpret_cast<int32_t*>(take(P*4));
-    w->ray_o = reinterpret_cast<float4*>(take(P*16));
-    w->ray_i = reinterpret_cast<float4*>(take(P*16));
     w->ray_sd = reinterpret_cast<double2*>(take(P*48));
-    w->level_q[0] = reinterpret_cast<uint2*>(take(level_cap*8));
-    w->level_q[1] = reinterpret_cast<uint2*>(take(level_cap*8));
+    w->level_q[0] = reinterpret_cast<uint4*>(take(level_cap*32));
+    w->level_q[1] = reinterpret_cast<uint4*>(take(level_cap*32));
     w->level_cap = (uint32_t)level_cap;
-    w->range_q = reinterpret_cast<uint2*>(take(range_cap*8));
-    w->range_cap = (uint32_t)range_cap;
     w->isect_q = reinterpret_cast<uint2*>(take(isect_cap*8));
     w->isect_dist = reinterpret_cast<double*>(take(isect_cap*8));
     w->isect_cap = (uint32_t)isect_cap;
@@ -513,24 +537,33 @@ int record_wave_graph(mlgpu_scene* scene, const TraceArgs& a, const WaveBuffers&
 // checking the counters on the host after every `check_period` iterations
 // (one CUDA-graph launch per period with use_graph).  `form` selects the
 // intersection arithmetic (FP64 or one of the FP32 forms).
+// The order in which a batch's photons enter the tracers: coherent (a sort
+// by support and direction, photon_order.cu) or the input order (a.order
+// stays null).
+int tracing_order(mlgpu_scene* scene, TraceArgs* a, const mlgpu_settings* st,
+                  cudaStream_t stream) {
+    const bool coherent = a->num_photons < (1ull << 32) &&
+        (st->photon_order == MLGPU_ORDER_COHERENT ||
+         (st->photon_order == MLGPU_ORDER_DEFAULT && a->num_photons >= 65536));
+    if (!coherent) return MLGPU_OK;
+    const size_t obytes = (size_t)a->num_photons*sizeof(uint32_t);
+    MLGPU_CUDA(scene->order.reserve(obytes + 256 + photon_order_scratch_bytes(a->num_photons)));
+    uint32_t* order = static_cast<uint32_t*>(scene->order.ptr);
+    char* scratch = static_cast<char*>(scene->order.ptr) + ((obytes + 255) & ~size_t(255));
+    if (!scene->wave_grid) scene->wave_grid = wave_persistent_blocks();
+    const cudaError_t e = launch_photon_order(a->photons, a->in_dtype, a->num_photons, order,
+                                              scratch, scene->wave_grid, stream);
+    if (e != cudaSuccess) return cuda_fail(e, "photon order kernels");
+    scene->launches += 7;
+    a->order = order;
+    return MLGPU_OK;
+}
+
 int run_wavefront(mlgpu_scene* scene, TraceArgs a, const mlgpu_settings* st,
                   cudaStream_t stream) {
     const int form = st->tracer;
-    const bool coherent = a.num_photons < (1ull << 32) &&
-        (st->photon_order == MLGPU_ORDER_COHERENT ||
-         (st->photon_order == MLGPU_ORDER_DEFAULT && a.num_photons >= 65536));
-    if (coherent) {
-        const size_t obytes = (size_t)a.num_photons*sizeof(uint32_t);
-        MLGPU_CUDA(scene->order.reserve(obytes + 256 + photon_order_scratch_bytes(a.num_photons)));
-        uint32_t* order = static_cast<uint32_t*>(scene->order.ptr);
-        char* scratch = static_cast<char*>(scene->order.ptr) + ((obytes + 255) & ~size_t(255));
-        if (!scene->wave_grid) scene->wave_grid = wave_persistent_blocks();
-        const cudaError_t e = launch_photon_order(a.photons, a.in_dtype, a.num_photons, order,
-                                                  scratch, scene->wave_grid, stream);
-        if (e != cudaSuccess) return cuda_fail(e, "photon order kernels");
-        scene->launches += 7;
-        a.order = order;
-    }
+    const int ro = tracing_order(scene, &a, st, stream);
+    if (ro) return ro;
     const uint32_t want = st->pool_size ? st->pool_size : kWavePool;
     const uint32_t pool = (uint32_t)std::min<uint64_t>(a.num_photons, want);
     WaveBuffers w;
@@ -551,13 +584,15 @@ int run_wavefront(mlgpu_scene* scene, TraceArgs a, const mlgpu_settings* st,
     // every iteration advances each live photon by one step
     const uint64_t bound = (a.num_photons*(uint64_t)(a.max_interactions + 1))/pool +
         a.max_interactions + 16 + (uint64_t)period;
-    const int levels = scene->dev.bvh_levels;
+    // launches per iteration: intake and its counters, the walk, intersections
+    // and ties, the overflow walk, resolve and its counters
+    const int walk_launches = w.walk == MLGPU_WALK_STACK ? 1 : scene->dev.bvh_levels;
     uint64_t iteration = 0;
     while (true) {
         if (graph) {
             MLGPU_CUDA(cudaGraphLaunch(scene->wave_graph, stream));
             iteration += (uint64_t)period;
-            scene->launches += (uint64_t)period*((uint64_t)levels + 8) + 1;
+            scene->launches += (uint64_t)period*((uint64_t)walk_launches + 7) + 1;
         } else {
             for (int g = 0; g < period; g++, iteration++) {
                 const RayPool& cur = pools[iteration & 1];
@@ -567,12 +602,12 @@ int run_wavefront(mlgpu_scene* scene, TraceArgs a, const mlgpu_settings* st,
                 const cudaError_t e = launch_wave_iteration(a, w, cur, nxt, form, stream,
                                                             timed ? ch.ev : nullptr);
                 if (e != cudaSuccess) return cuda_fail(e, "wavefront kernels");
-                scene->launches += (uint64_t)levels + 8;
+                scene->launches += (uint64_t)walk_launches + 7;
                 if (timed) {
                     ch.n = 5;
                     const int cls[4] = {MLGPU_KERNEL_INTAKE, MLGPU_KERNEL_WALK,
                                         MLGPU_KERNEL_INTERSECT, MLGPU_KERNEL_RESOLVE};
-                    const int launches[4] = {2, levels + 1, 2, 3};
+                    const int launches[4] = {2, walk_launches, 2, 3};
                     for (int k = 0; k < 4; k++) { ch.cls[k] = cls[k]; ch.launches[k] = launches[k]; }
                     scene->prof.add(ch);
                 }
@@ -600,6 +635,29 @@ int launch(mlgpu_scene* scene, const TraceArgs& a, const mlgpu_settings* st,
     case MLGPU_TRACER_FP64:
     case MLGPU_TRACER_FP32:
     case MLGPU_TRACER_FP32_PURE: return run_wavefront(scene, a, st, stream);
+    case MLGPU_TRACER_FP64_QUEUE: {
+        TraceArgs q = a;
+        const int ro = tracing_order(scene, &q, st, stream);
+        if (ro) return ro;
+        MLGPU_CUDA(scene->queue.reserve(256));
+        int sms = 0, dev = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        if (!scene->queue_blocks) scene->queue_blocks = queue_trace_blocks_per_sm();
+        const int grid = st->grid_blocks > 0 ? st->grid_blocks : sms*scene->queue_blocks;
+        Profiler::Chain ch;
+        const bool timed = scene->prof.on && scene->prof.take(2, ch.ev);
+        if (timed) cudaEventRecord(ch.ev[0], stream);
+        e = launch_queue_trace(q, static_cast<unsigned long long*>(scene->queue.ptr), grid,
+                               stream);
+        scene->launches++;
+        if (timed) {
+            cudaEventRecord(ch.ev[1], stream);
+            ch.n = 2; ch.cls[0] = MLGPU_KERNEL_PLAIN; ch.launches[0] = 1;
+            scene->prof.add(ch);
+        }
+        break;
+    }
     default: {
         Profiler::Chain ch;
         const bool timed = scene->prof.on && scene->prof.take(2, ch.ev);
@@ -620,6 +678,9 @@ int launch(mlgpu_scene* scene, const TraceArgs& a, const mlgpu_settings* st,
 
 const char* device_error_text(unsigned int code) {
     switch (code) {
+    case MLGPU_ERR_INVALID_ARGUMENT:
+        return "Expected photon wavelength lambda > 0.0nm (Photon.cpp:20-28), but a "
+               "photon's wavelength is <= 0";
     case MLGPU_ERR_OUT_OF_RANGE:
         return "a photon's wavelength is outside the argument range of a surface "
                "property table (Func1 limits [x_first, x_last))";
@@ -637,6 +698,28 @@ namespace mlgpu {
 int report_error(int code, const char* message) { return fail(code, "%s", message); }
 
 const DevScene* device_scene(const mlgpu_scene* scene) { return &scene->dev; }
+
+int scene_device(const mlgpu_scene* scene) { return scene->device; }
+
+void profile_mark_begin(mlgpu_scene* scene, cudaStream_t s, ProfileMark* mark) {
+    mark->timed = scene->prof.on && scene->prof.take(2, mark->ev);
+    if (mark->timed) cudaEventRecord(mark->ev[0], s);
+}
+
+void profile_mark_end(mlgpu_scene* scene, cudaStream_t s, ProfileMark* mark, int cls,
+                      int launches) {
+    if (mark->timed) {
+        cudaEventRecord(mark->ev[1], s);
+        Profiler::Chain ch;
+        ch.n = 2;
+        ch.ev[0] = mark->ev[0];
+        ch.ev[1] = mark->ev[1];
+        ch.cls[0] = cls;
+        ch.launches[0] = launches;
+        scene->prof.add(ch);
+    }
+    scene->launches += (uint64_t)launches;
+}
 
 }  // namespace mlgpu
 
@@ -678,8 +761,10 @@ int mlgpu_scene_destroy(mlgpu_scene* scene) {
     scene->staging_hist.release();
     scene->staging_rng.release();
     scene->bin_scratch.release();
+    scene->staging_bins.release();
     scene->tune_out.release();
     scene->order.release();
+    scene->queue.release();
     scene->corsika.release();
     scene->stats.release();
     scene->wave.release();
@@ -1019,12 +1104,41 @@ int mlgpu_scene_sync_errors(mlgpu_scene* scene, void* cuda_stream) {
     return MLGPU_OK;
 }
 
-int mlgpu_propagate_host(mlgpu_scene* scene, const mlgpu_photons* photons, uint64_t n,
-                         const mlgpu_settings* settings, const mlgpu_rng* rng,
-                         mlgpu_results* results) {
+}  // extern "C"
+
+namespace {
+
+// Per-sensor binning requested with a host-buffer propagation.
+struct HostBinning {
+    uint32_t* counts;        // host [num_sensors]
+    uint32_t* time_hist;     // host [num_sensors][num_bins] or null
+    uint32_t num_bins;
+    double t_min, t_max;
+};
+
+int propagate_host(mlgpu_scene* scene, const mlgpu_photons* photons, uint64_t n,
+                   const mlgpu_settings* settings, const mlgpu_rng* rng,
+                   mlgpu_results* results, const HostBinning* bin) {
     int st = check_propagate_args(scene, photons, settings, rng, results);
     if (st) return st;
-    if (n == 0) return MLGPU_OK;
+    if (bin) {
+        if (!bin->counts) return fail(MLGPU_ERR_INVALID_ARGUMENT, "counts is NULL");
+        if (bin->num_bins > 0 && (!bin->time_hist || !results->time || !(bin->t_max > bin->t_min)))
+            return fail(MLGPU_ERR_INVALID_ARGUMENT,
+                        "time histograms need results.time, an output and t_max > t_min");
+        const uint64_t keys = (uint64_t)scene->dev.num_sensors*(bin->num_bins + 1ull);
+        if (keys >= (1ull << 31))
+            return fail(MLGPU_ERR_INVALID_ARGUMENT, "too many sensor x time bins");
+    }
+    if (n == 0) {
+        if (bin) {
+            std::memset(bin->counts, 0, sizeof(uint32_t)*(size_t)scene->dev.num_sensors);
+            if (bin->num_bins)
+                std::memset(bin->time_hist, 0,
+                            sizeof(uint32_t)*(size_t)scene->dev.num_sensors*bin->num_bins);
+        }
+        return MLGPU_OK;
+    }
     const size_t ein = photons->dtype == MLGPU_F64 ? 8 : 4;
     const size_t eout = results->dtype == MLGPU_F64 ? 8 : 4;
     const size_t hist_len = settings->max_num_interactions_per_photon + 1;
@@ -1168,9 +1282,52 @@ int mlgpu_propagate_host(mlgpu_scene* scene, const mlgpu_photons* photons, uint6
             if (e != cudaSuccess) return drain(cuda_fail(e, "copying results to the host"));
         }
     }
+    if (bin) {
+        // the whole batch's sensors (and times) are on the device once the
+        // last piece is traced: bin them there, copy the bins back
+        const size_t ns = (size_t)scene->dev.num_sensors;
+        const size_t keys = ns*(bin->num_bins + 1ull);
+        const size_t slices = 32;
+        if (scene->bin_scratch.reserve(slices*keys*sizeof(uint32_t) + 256) != cudaSuccess ||
+            scene->staging_bins.reserve(keys*sizeof(uint32_t)) != cudaSuccess)
+            return drain(cuda_fail(cudaGetLastError(), "binning buffers"));
+        uint32_t* dcounts = static_cast<uint32_t*>(scene->staging_bins.ptr);
+        uint32_t* dhist = bin->num_bins ? dcounts + ns : nullptr;
+        cudaError_t e = launch_bin_arrivals(
+            scene->dev, static_cast<const int32_t*>(dev_plane[0]),
+            static_cast<const double*>(dev_plane[3]), n, dcounts, dhist, bin->num_bins,
+            bin->t_min, bin->t_max, static_cast<uint32_t*>(scene->bin_scratch.ptr),
+            scene->bin_scratch.bytes/sizeof(uint32_t), trace);
+        if (e != cudaSuccess) return drain(cuda_fail(e, "binning kernels"));
+        scene->launches += 2;
+        e = cudaMemcpyAsync(bin->counts, dcounts, ns*sizeof(uint32_t), cudaMemcpyDeviceToHost,
+                            trace);
+        if (e == cudaSuccess && dhist)
+            e = cudaMemcpyAsync(bin->time_hist, dhist, ns*bin->num_bins*sizeof(uint32_t),
+                                cudaMemcpyDeviceToHost, trace);
+        if (e != cudaSuccess) return drain(cuda_fail(e, "copying bins to the host"));
+    }
     const cudaError_t e = cudaStreamSynchronize(download);
     if (e != cudaSuccess) return drain(cuda_fail(e, "copying results to the host"));
     return mlgpu_scene_sync_errors(scene, trace);
+}
+
+}  // namespace
+
+extern "C" {
+
+int mlgpu_propagate_host(mlgpu_scene* scene, const mlgpu_photons* photons, uint64_t n,
+                         const mlgpu_settings* settings, const mlgpu_rng* rng,
+                         mlgpu_results* results) {
+    return propagate_host(scene, photons, n, settings, rng, results, nullptr);
+}
+
+int mlgpu_propagate_and_bin_host(mlgpu_scene* scene, const mlgpu_photons* photons, uint64_t n,
+                                 const mlgpu_settings* settings, const mlgpu_rng* rng,
+                                 mlgpu_results* results, uint32_t* counts, uint32_t* time_hist,
+                                 uint32_t num_time_bins, double t_min, double t_max) {
+    const HostBinning bin = {counts, time_hist, num_time_bins, t_min, t_max};
+    return propagate_host(scene, photons, n, settings, rng, results, &bin);
 }
 
 int mlgpu_bin_arrivals(mlgpu_scene* scene, const int32_t* sensor, const double* time,

@@ -17,6 +17,20 @@ namespace {   // one copy per translation unit
 
 struct v3 { double x, y, z; };
 
+// Records a device-side error of a call in the scene's error word: the
+// lowest non-zero status wins, so that a malformed photon
+// (MLGPU_ERR_INVALID_ARGUMENT, which merlict throws from Photon's
+// constructor before anything is propagated, Photon.cpp:20-28) is reported
+// over the errors of photons traced beside it.
+__device__ __forceinline__ void raise_error(unsigned int* word, unsigned int code) {
+    unsigned int old = *reinterpret_cast<volatile unsigned int*>(word);
+    while (old == 0u || old > code) {
+        const unsigned int seen = atomicCAS(word, old, code);
+        if (seen == old) break;
+        old = seen;
+    }
+}
+
 __device__ __forceinline__ v3 mk(double x, double y, double z) { v3 r; r.x = x; r.y = y; r.z = z; return r; }
 // Vec3::operator*(Vec3), merlict/Vec3.cpp:35-37
 __device__ __forceinline__ double dot(v3 self, v3 v) { return v.x*self.x + v.y*self.y + v.z*self.z; }

@@ -165,7 +165,6 @@ struct WaveCounters {
     unsigned int active;             // rays carried over into the current pool
     unsigned int total;              // active + new photons of this iteration
     unsigned int next;               // survivors written to the next pool
-    unsigned int range_len;          // (slot, BVH leaf range) pairs for the sphere tests
     unsigned int isect_len;          // (slot, leaf) candidates to intersect
     unsigned int overflow_len;       // slots sent to merlict's own walk
     unsigned int level_len[kMaxBvhLevels];   // (slot, node) pairs of each BVH level
@@ -193,14 +192,12 @@ struct WaveBuffers {
     int walk;                // MLGPU_WALK_LEVELS or MLGPU_WALK_STACK
     int fn_smem_bytes;       // property tables staged in shared memory (0: read from global)
     int32_t* step;           // [pool] 0, or kNoStep: the photon takes no step
-    float4* ray_o;           // [pool] single-precision origin, box inflation
-    float4* ray_i;           // [pool] reciprocal direction
     double2* ray_sd;         // [pool][3] the FP64 support and direction, one 48-byte
                              // record per slot for the kernels that read rays by queue
-    uint2* level_q[2];       // (slot, node) pairs, ping-pong between BVH levels
+    uint4* level_q[2];       // (ray, node) entries of two uint4 each, ping-pong between
+                             // BVH levels: {slot, node, origin x, y}, {origin z, 1/dir x,
+                             // y, z} (floats as bits): each entry carries its ray
     uint32_t level_cap;
-    uint2* range_q;          // (slot, BVH leaf-range reference)
-    uint32_t range_cap;
     uint2* isect_q;          // (slot, leaf) candidates
     double* isect_dist;      // distance to each candidate's hit, -1: none
     uint32_t isect_cap;
@@ -227,6 +224,11 @@ cudaError_t launch_wave32_isect_resolve(const TraceArgs& a, const WaveBuffers& w
                                         cudaStream_t s, cudaEvent_t mid);
 
 cudaError_t launch_trace_fp64(const TraceArgs& a, int block, cudaStream_t s);
+// The persistent work-queue tracer (trace_fp64.cu): `grid` blocks of 128
+// threads drain the batch through the counter `queue` (zeroed here).
+cudaError_t launch_queue_trace(const TraceArgs& a, unsigned long long* queue, int grid,
+                               cudaStream_t s);
+int queue_trace_blocks_per_sm();
 // CORSIKA bunches to photons (corsika.cu): counts and offsets into
 // `scratch` (corsika_scratch_bytes), the total to *total_dev; then the
 // expansion into the seven FP64 planes.
@@ -298,6 +300,20 @@ cudaError_t launch_bin_arrivals(const DevScene& sc, const int32_t* sensor,
 int report_error(int code, const char* message);
 // The device scene of a handle (capi.cu).
 const DevScene* device_scene(const mlgpu_scene* scene);
+// The CUDA device the scene was created on (capi.cu).
+int scene_device(const mlgpu_scene* scene);
+// Launch accounting for entry points outside capi.cu: profile_mark_begin
+// records the first event of a timed chain on `s` when the scene's profiling
+// is on (with events the profiler already holds or creates, never device
+// memory); profile_mark_end closes it with `launches` kernels of class `cls`
+// and adds the launches to the scene's count (mlgpu_scene_kernel_launches).
+struct ProfileMark {
+    cudaEvent_t ev[2];
+    bool timed;
+};
+void profile_mark_begin(mlgpu_scene* scene, cudaStream_t s, ProfileMark* mark);
+void profile_mark_end(mlgpu_scene* scene, cudaStream_t s, ProfileMark* mark, int cls,
+                      int launches);
 
 }  // namespace mlgpu
 

@@ -217,6 +217,7 @@ umma_gemm_kernel(const GemmArgs g) {
     uint64_t* done = empty + kStages;
     uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(done + 1);
     __shared__ int s_failed;
+    __shared__ uint32_t s_issued, s_consumed;   // K chunks copied in / taken by the MMAs
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const uint32_t m0 = blockIdx.x*128u, n0 = blockIdx.y*(uint32_t)kN;
     const uint32_t kc0 = blockIdx.z*g.k_chunks;
@@ -225,6 +226,8 @@ umma_gemm_kernel(const GemmArgs g) {
         for (int s = 0; s < kStages; s++) { mbar_init(&full[s], 1); mbar_init(&empty[s], 1); }
         mbar_init(done, 1);
         s_failed = 0;
+        s_issued = 0;
+        s_consumed = 0;
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     if (warp == 1) {
@@ -251,6 +254,7 @@ umma_gemm_kernel(const GemmArgs g) {
                 bulk_g2s(dst, g.a + (kk*(g.a_rows >> 3) + (m0 >> 3))*1024u, kBytesA, &full[s]);
                 bulk_g2s(dst + kBytesA, g.b + (kk*(g.b_rows >> 3) + (n0 >> 3))*1024u, kBytesB,
                          &full[s]);
+                s_issued = kc + 1;
             }
         }
     } else if (warp == 1) {
@@ -260,6 +264,7 @@ umma_gemm_kernel(const GemmArgs g) {
             for (uint32_t kc = 0; kc < g.k_chunks; kc++) {
                 const uint32_t s = kc % kStages;
                 if (!mbar_wait(&full[s], (kc/kStages) & 1)) { s_failed = 1; break; }
+                s_consumed = kc + 1;
                 tc_fence_after();
                 const uint32_t a_addr = smem_u32(smem + s*kStage);
                 const uint32_t b_addr = a_addr + kBytesA;
@@ -344,7 +349,16 @@ umma_gemm_kernel(const GemmArgs g) {
     }
     tc_fence_before();
     __syncthreads();
-    if (threadIdx.x == 0 && s_failed) atomicCAS(&g_error, 0u, (unsigned)MLGPU_ERR_RUNTIME);
+    if (threadIdx.x == 0 && s_failed) {
+        atomicCAS(&g_error, 0u, (unsigned)MLGPU_ERR_RUNTIME);
+        // A CTA must not exit, nor free its tensor memory, with its own bulk
+        // copies or MMAs still in flight: wait (again bounded) for the
+        // copies no MMA consumed and for the MMAs' final commit.
+        for (uint32_t kc = s_consumed; kc < s_issued; kc++)
+            mbar_wait(&full[kc % kStages], (kc/kStages) & 1);
+        mbar_wait(done, 0);
+    }
+    __syncthreads();
     if (warp == 1) {
         tc_fence_after();
         asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;"
@@ -448,15 +462,20 @@ umma_persistent_kernel(const GemmArgs g, uint32_t num_tiles) {
     uint64_t* a_empty = a_full + kARing;
     uint64_t* acc_full = a_empty + kARing;
     uint64_t* acc_empty = acc_full + 2;
-    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(acc_empty + 2);
+    uint64_t* drained = acc_empty + 2;             // the MMA thread's last commit
+    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(drained + 1);
     __shared__ int s_failed;
+    __shared__ uint32_t s_issued, s_consumed;   // A chunks copied in / taken by the MMAs
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
 
     if (threadIdx.x == 0) {
         mbar_init(b_full, 1);
         for (int s = 0; s < kARing; s++) { mbar_init(&a_full[s], 1); mbar_init(&a_empty[s], 1); }
         for (int s = 0; s < 2; s++) { mbar_init(&acc_full[s], 1); mbar_init(&acc_empty[s], 8); }
+        mbar_init(drained, 1);
         s_failed = 0;
+        s_issued = 0;
+        s_consumed = 0;
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     if (warp == 1) {
@@ -487,6 +506,7 @@ umma_persistent_kernel(const GemmArgs g, uint32_t num_tiles) {
                     bulk_g2s(sA + s*16384u,
                              g.a + ((uint64_t)kc*(g.a_rows >> 3) + (uint64_t)tile*16u)*1024u,
                              16384u, &a_full[s]);
+                    s_issued = it + 1;
                 }
             }
             if (!ok) s_failed = 1;
@@ -504,6 +524,7 @@ umma_persistent_kernel(const GemmArgs g, uint32_t num_tiles) {
                 for (uint32_t kc = 0; kc < (uint32_t)kKChunks; kc++, it++) {
                     const uint32_t s = it % kARing;
                     if (!mbar_wait(&a_full[s], (it/kARing) & 1)) { ok = false; break; }
+                    s_consumed = it + 1;
                     tc_fence_after();
                     const uint32_t a_addr = smem_u32(sA + s*16384u);
                     const uint32_t b_addr = smem_u32(sB + kc*kBChunk);
@@ -517,6 +538,8 @@ umma_persistent_kernel(const GemmArgs g, uint32_t num_tiles) {
                 umma_commit(&acc_full[acc]);
             }
             if (!ok) s_failed = 1;
+            // arrives when every MMA issued above has completed
+            umma_commit(drained);
         }
     } else {
         // warp w reads tensor-memory lanes 32 (w % 4) .. + 31; warps 2..5
@@ -543,7 +566,17 @@ umma_persistent_kernel(const GemmArgs g, uint32_t num_tiles) {
     }
     tc_fence_before();
     __syncthreads();
-    if (threadIdx.x == 0 && s_failed) atomicCAS(&g_error, 0u, (unsigned)MLGPU_ERR_RUNTIME);
+    if (threadIdx.x == 0 && s_failed) {
+        atomicCAS(&g_error, 0u, (unsigned)MLGPU_ERR_RUNTIME);
+        // no exit, and no freeing of tensor memory, with this CTA's bulk
+        // copies or MMAs in flight: wait (again bounded) for the weight
+        // copies, the A chunks no MMA consumed and the MMAs' final commit
+        mbar_wait(b_full, 0);
+        for (uint32_t it = s_consumed; it < s_issued; it++)
+            mbar_wait(&a_full[it % kARing], (it/kARing) & 1);
+        mbar_wait(drained, 0);
+    }
+    __syncthreads();
     if (warp == 1) {
         tc_fence_after();
         asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;"

@@ -109,8 +109,19 @@ wave_isect_kernel(const TraceArgs a, const WaveBuffers w, const RayPool cur) {
         load_ray(w, slot, &s, &d);
         double dist = -1.0;
         if (kIsect == kIsectFp64) {
-            const Isec h = leaf_hit(sc, leaf, s, d);
-            if (h.leaf >= 0) dist = h.dist;
+            double T[12], ti[3], pr[MLGPU_LEAF_PARAMS], r2;
+            int32_t prim;
+            load_leaf(sc.leaf + leaf, T, ti, pr, &r2, &prim);
+            // merlict's bounding-sphere test of the leaf (RayAndFrame.cpp:
+            // 16-107; the sphere is centred on the frame's position,
+            // Frame::position_in_world): the walk proposed the leaf with a
+            // conservative single-precision version of it
+            if (sphere_cull(make_double4(T[3], T[7], T[11], r2), s, d, dot(s, d))) {
+                Isec h;
+                intersect_leaf(sc, leaf, prim, pr, r2, position_inverse(T, ti, s),
+                               orientation_inverse(T, d), &h);
+                if (h.leaf >= 0) dist = h.dist;
+            }
         } else {
             const fp32::Hit32 h = fp32::intersect32<false>(sc, leaf, fp32::dmk(s.x, s.y, s.z),
                                                     fp32::dmk(d.x, d.y, d.z),
@@ -384,7 +395,7 @@ wave_resolve_kernel(const TraceArgs a, const WaveBuffers w, const RayPool cur, c
             if (hist)
                 for (uint32_t k = (uint32_t)n_next; k < hist_len; k++)
                     store_hist(&hist[k], mk(0, 0, 0), mk(0, 0, 0), 0.0, MLGPU_LEAF_PHOTON_SOURCE, 0, false);
-            if (err) atomicCAS(sc.error_word, 0u, (unsigned int)err);
+            if (err) raise_error(sc.error_word, (unsigned int)err);
         }
     }
     // warp-ballot compaction of the surviving rays into the next pool

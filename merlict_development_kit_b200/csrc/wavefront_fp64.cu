@@ -9,13 +9,12 @@
 //              (RayAndFrame.cpp:137-149), every other ray queues the root
 //              of the BVH;
 //   levels     one pass per BVH level, one thread per (ray, node) pair: the
-//              four child boxes; hit children go to the next level's queue,
-//              hit leaf ranges to the sphere queue;
-//   spheres    one thread per (ray, leaf range): merlict's own bounding-sphere
-//              test of each leaf (RayAndFrame.cpp:16-107); the leaves that
-//              pass are the ray's candidates;
-//   (or walk   one thread per ray: levels and spheres in one depth-first
-//              walk with a stack, the same tests, the same candidates;)
+//              eight child boxes; hit children go to the next level's queue;
+//              the leaves of hit leaf ranges that pass a conservative FP32
+//              version of merlict's bounding-sphere test become candidates
+//              (merlict's exact test follows in the intersection step);
+//   (or walk   one thread per ray: levels and sphere tests in one
+//              depth-first walk with a stack, the same candidates;)
 //   intersect, ties, overflow, resolve: wave_resolve.cuh.
 // The arithmetic is the shared FP64 code, compiled with --fmad=false.
 #include <cstdint>
@@ -27,6 +26,34 @@ namespace {
 
 constexpr int kTreeCands = 16;   // candidates of a frame-tree walk before it overflows
 constexpr int kMaxStagedNodes = 32768/(int)sizeof(BvhNode);   // 32 KB of shared memory per block
+
+// A (ray, BVH node) work item with the ray's FP32 origin and reciprocal
+// direction, so that the level kernels read their rays with the queue.
+struct WalkRay {
+    float4 o;    // origin, box inflation
+    float4 iv;   // reciprocal direction
+};
+
+__device__ __forceinline__ float box_inflation(const DevScene& sc, float ox, float oy, float oz) {
+    return sc.bvh_eps + 4e-7f*(fabsf(ox) + fabsf(oy) + fabsf(oz));
+}
+
+__device__ __forceinline__ void put_entry(uint4* q, uint32_t e, uint32_t slot, uint32_t node,
+                                          const WalkRay& r) {
+    q[2*e] = make_uint4(slot, node, __float_as_uint(r.o.x), __float_as_uint(r.o.y));
+    q[2*e + 1] = make_uint4(__float_as_uint(r.o.z), __float_as_uint(r.iv.x),
+                            __float_as_uint(r.iv.y), __float_as_uint(r.iv.z));
+}
+
+__device__ __forceinline__ void get_entry(const DevScene& sc, const uint4* q, uint32_t e,
+                                          uint32_t* slot, uint32_t* node, WalkRay* r) {
+    const uint4 a = q[2*e], b = q[2*e + 1];
+    *slot = a.x;
+    *node = a.y;
+    const float ox = __uint_as_float(a.z), oy = __uint_as_float(a.w), oz = __uint_as_float(b.x);
+    r->o = make_float4(ox, oy, oz, box_inflation(sc, ox, oy, oz));
+    r->iv = make_float4(__uint_as_float(b.y), __uint_as_float(b.z), __uint_as_float(b.w), 0.0f);
+}
 
 template <typename In>
 __global__ void __launch_bounds__(256)
@@ -42,6 +69,7 @@ wave_intake_kernel(const TraceArgs a, const WaveBuffers w, const RayPool cur) {
     const uint32_t max_int = a.max_interactions;
     const uint32_t hist_len = max_int + 1;
     bool bvh = false;          // queue the BVH root for this ray
+    WalkRay wr;                // its FP32 walk ray
     int nc = 0;                // candidates of a frame-tree walk
     int32_t cand[kTreeCands];
     if (slot < total) {
@@ -62,7 +90,11 @@ wave_intake_kernel(const TraceArgs a, const WaveBuffers w, const RayPool cur) {
             cur.photon[slot] = (int32_t)p;
             cur.sx[slot] = s.x; cur.sy[slot] = s.y; cur.sz[slot] = s.z;
             cur.dx[slot] = d.x; cur.dy[slot] = d.y; cur.dz[slot] = d.z;
-            cur.lambda[slot] = load_in<In>(a.photons.wavelength, p);
+            const double lambda = load_in<In>(a.photons.wavelength, p);
+            // Photon::assert_wavelength_is_positive (Photon.cpp:20-28):
+            // merlict throws std::invalid_argument before propagating
+            if (lambda <= 0.0) raise_error(sc.error_word, MLGPU_ERR_INVALID_ARGUMENT);
+            cur.lambda[slot] = lambda;
             cur.tof[slot] = 0.0;
             cur.root[slot] = root;
             cur.n_int[slot] = 1;
@@ -123,9 +155,8 @@ wave_intake_kernel(const TraceArgs a, const WaveBuffers w, const RayPool cur) {
                     if (fabsf(fdx) < 1e-30f) fdx = copysignf(1e-30f, fdx);
                     if (fabsf(fdy) < 1e-30f) fdy = copysignf(1e-30f, fdy);
                     if (fabsf(fdz) < 1e-30f) fdz = copysignf(1e-30f, fdz);
-                    const float eps = sc.bvh_eps + 4e-7f*(fabsf(ox) + fabsf(oy) + fabsf(oz));
-                    w.ray_o[slot] = make_float4(ox, oy, oz, eps);
-                    w.ray_i[slot] = make_float4(1.0f/fdx, 1.0f/fdy, 1.0f/fdz, 0.0f);
+                    wr.o = make_float4(ox, oy, oz, box_inflation(sc, ox, oy, oz));
+                    wr.iv = make_float4(1.0f/fdx, 1.0f/fdy, 1.0f/fdz, 0.0f);
                 }
             }
         }
@@ -133,7 +164,7 @@ wave_intake_kernel(const TraceArgs a, const WaveBuffers w, const RayPool cur) {
     // queue the BVH root and the frame-tree candidates (all lanes take part)
     const uint32_t qb = warp_reserve(&w.counters->level_len[0], bvh ? 1u : 0u);
     if (bvh) {
-        if (qb < w.level_cap) w.level_q[0][qb] = make_uint2(slot, 0u);
+        if (qb < w.level_cap) put_entry(w.level_q[0], qb, slot, 0u, wr);
         else mark_overflow(w, slot);
     }
     const uint32_t cb = warp_reserve(&w.counters->isect_len, (uint32_t)nc);
@@ -184,6 +215,25 @@ __device__ __forceinline__ uint32_t node_hits(const float4* nq, float4 o, float4
     return hit;
 }
 
+// merlict's bounding-sphere test of a leaf (RayAndFrame.cpp:16-107) in
+// single precision on the walk's FP32 ray, with the radius widened by the
+// rounding of the ray, the centre and the distance along the ray, so that
+// every leaf the exact test passes also passes this one.  The FP64 tracer
+// then repeats merlict's exact test on each candidate (wave_isect_kernel);
+// the FP32 forms keep the candidates this test passes (their extra
+// candidates are rejected by the intersection, whose hits lie inside the
+// sphere).
+__device__ __forceinline__ bool sphere_cull32(float4 c, float4 o, float3 dv) {
+    const float wx = c.x - o.x, wy = c.y - o.y, wz = c.z - o.z;
+    const float alpha = dv.x*wx + dv.y*wy + dv.z*wz;
+    const float m = o.w + 4e-7f*(fabsf(c.x) + fabsf(c.y) + fabsf(c.z) + fabsf(alpha)) + 1e-6f*c.w;
+    const float rr = (c.w + m)*(c.w + m);
+    const float sx = wx - dv.x*alpha, sy = wy - dv.y*alpha, sz = wz - dv.z*alpha;
+    if (sx*sx + sy*sy + sz*sz > rr) return false;
+    if (alpha < -m) return wx*wx + wy*wy + wz*wz <= rr;
+    return true;
+}
+
 // One BVH level: the child boxes of each queued (ray, node) pair.  With
 // `staged` > 0 the block first copies the level's `staged` nodes (a
 // contiguous range, the tree being numbered breadth first) into shared
@@ -192,8 +242,8 @@ __global__ void __launch_bounds__(256)
 wave_level_kernel(const TraceArgs a, const WaveBuffers w, int level, int staged) {
     extern __shared__ float4 stage[];
     const DevScene& sc = a.scene;
-    const uint2* in = w.level_q[level & 1];
-    uint2* out = w.level_q[(level + 1) & 1];
+    const uint4* in = w.level_q[level & 1];
+    uint4* out = w.level_q[(level + 1) & 1];
     const uint32_t len = w.counters->level_len[level];
     const uint32_t n = len < w.level_cap ? len : w.level_cap;
     const bool last = level + 1 >= kMaxBvhLevels;
@@ -207,102 +257,58 @@ wave_level_kernel(const TraceArgs a, const WaveBuffers w, int level, int staged)
     }
     for (uint32_t first = warp_first(); first < n; first += gridDim.x*blockDim.x) {
         const uint32_t e = first + (uint32_t)lane;
-        uint32_t slot = 0;
+        uint32_t slot = 0, node = 0;
         int32_t child[kBvhWidth];
         uint32_t hit = 0;   // bit k: child k hit
+        WalkRay r;
+        r.o = make_float4(0.f, 0.f, 0.f, 0.f);
+        r.iv = make_float4(1.f, 1.f, 1.f, 0.f);
         if (e < n) {
-            const uint2 q = in[e];
-            slot = q.x;
-            const float4 o = w.ray_o[slot], iv = w.ray_i[slot];
-            if ((uint32_t)((int32_t)q.y - base) < (uint32_t)staged)
-                hit = node_hits<true>(stage + (sizeof(BvhNode)/16)*((int32_t)q.y - base), o, iv,
-                                      child);
+            get_entry(sc, in, e, &slot, &node, &r);
+            if ((uint32_t)((int32_t)node - base) < (uint32_t)staged)
+                hit = node_hits<true>(stage + (sizeof(BvhNode)/16)*((int32_t)node - base), r.o,
+                                      r.iv, child);
             else
-                hit = node_hits<false>(reinterpret_cast<const float4*>(sc.bvh + q.y), o, iv,
+                hit = node_hits<false>(reinterpret_cast<const float4*>(sc.bvh + node), r.o, r.iv,
                                        child);
         }
-        uint32_t nn = 0, nr = 0;
+        uint32_t nn = 0, ranges = 0;   // bit k of ranges: child k is a hit leaf range
 #pragma unroll
         for (int k = 0; k < kBvhWidth; k++)
-            if (hit & (1u << k)) { if (child[k] < 0) nr++; else nn++; }
+            if (hit & (1u << k)) { if (child[k] < 0) ranges |= 1u << k; else nn++; }
         uint32_t nb = warp_reserve(&w.counters->level_len[last ? level : level + 1], last ? 0u : nn);
-        uint32_t rb = warp_reserve(&w.counters->range_len, nr);
 #pragma unroll
         for (int k = 0; k < kBvhWidth; k++) {
-            if (!(hit & (1u << k))) continue;
-            if (child[k] < 0) {
-                if (rb < w.range_cap) w.range_q[rb] = make_uint2(slot, (uint32_t)child[k]);
-                else mark_overflow(w, slot);
-                rb++;
-            } else {
-                if (!last && nb < w.level_cap) out[nb] = make_uint2(slot, (uint32_t)child[k]);
-                else mark_overflow(w, slot);
-                nb++;
-            }
-        }
-    }
-}
-
-// The FP32 forms' version of merlict's bounding-sphere test: the same
-// geometry in single precision on the walk's FP32 ray, with the radius
-// widened by the rounding of the ray, the centre and the distance along the
-// ray, so that every leaf the exact test passes also passes this one (the
-// extra candidates are then rejected by their intersection, whose hits lie
-// inside the sphere).
-__device__ __forceinline__ bool sphere_cull32(float4 c, float4 o, float3 dv) {
-    const float wx = c.x - o.x, wy = c.y - o.y, wz = c.z - o.z;
-    const float alpha = dv.x*wx + dv.y*wy + dv.z*wz;
-    const float m = o.w + 4e-7f*(fabsf(c.x) + fabsf(c.y) + fabsf(c.z) + fabsf(alpha)) + 1e-6f*c.w;
-    const float rr = (c.w + m)*(c.w + m);
-    const float sx = wx - dv.x*alpha, sy = wy - dv.y*alpha, sz = wz - dv.z*alpha;
-    if (sx*sx + sy*sy + sz*sz > rr) return false;
-    if (alpha < -m) return wx*wx + wy*wy + wz*wz <= rr;
-    return true;
-}
-
-// merlict's bounding-sphere test (RayAndFrame.cpp:16-107) of every leaf in
-// the queued leaf ranges; the leaves that pass become candidates.
-// kF32: the FP32 forms' conservative test (sphere_cull32).
-template <bool kF32>
-__global__ void __launch_bounds__(256)
-wave_sphere_kernel(const TraceArgs a, const WaveBuffers w, const RayPool cur) {
-    const DevScene& sc = a.scene;
-    const uint32_t len = w.counters->range_len;
-    const uint32_t n = len < w.range_cap ? len : w.range_cap;
-    const int lane = threadIdx.x & 31;
-    for (uint32_t first = warp_first(); first < n; first += gridDim.x*blockDim.x) {
-        const uint32_t e = first + (uint32_t)lane;
-        uint32_t slot = 0;
-        int32_t pass[8];
-        uint32_t np = 0;
-        if (e < n) {
-            const uint2 q = w.range_q[e];
-            slot = q.x;
-            const int32_t ref = (int32_t)q.y;
-            const int32_t start = (ref & 0x7fffffff) >> 3;
-            const int32_t count = (ref & 7) + 1;
-            if (kF32) {
-                const float4 o = w.ray_o[slot], iv = w.ray_i[slot];
-                const float3 dv = make_float3(1.0f/iv.x, 1.0f/iv.y, 1.0f/iv.z);
-                for (int32_t j = start; j < start + count; j++)
-                    if (sphere_cull32(__ldg(sc.bvh_sphere_f + j), o, dv))
-                        pass[np++] = __ldg(sc.bvh_leaf + j);
-            } else {
-                v3 s, d;
-                load_ray(w, slot, &s, &d);
-                const double sd = dot(s, d);
-                for (int32_t j = start; j < start + count; j++) {
-                    const double2* c = reinterpret_cast<const double2*>(sc.bvh_sphere + j);
-                    const double2 c01 = __ldg(c), c23 = __ldg(c + 1);
-                    if (sphere_cull(make_double4(c01.x, c01.y, c23.x, c23.y), s, d, sd))
-                        pass[np++] = __ldg(sc.bvh_leaf + j);
-                }
-            }
-        }
-        const uint32_t cb = warp_reserve(&w.counters->isect_len, np);
-        for (uint32_t k = 0; k < np; k++) {
-            if (cb + k < w.isect_cap) w.isect_q[cb + k] = make_uint2(slot, (uint32_t)pass[k]);
+            if (!(hit & (1u << k)) || child[k] < 0) continue;
+            if (!last && nb < w.level_cap) put_entry(out, nb, slot, (uint32_t)child[k], r);
             else mark_overflow(w, slot);
+            nb++;
+        }
+        // the leaves of the hit leaf ranges whose bounding spheres the ray
+        // may pass become candidates, one leaf range of the warp at a time
+        const float3 dv = make_float3(1.0f/r.iv.x, 1.0f/r.iv.y, 1.0f/r.iv.z);
+#pragma unroll
+        for (int k = 0; k < kBvhWidth; k++) {
+            const bool is_range = (ranges >> k) & 1u;
+            if (!__any_sync(kFull, is_range)) continue;
+            uint32_t pass = 0;   // bit j: leaf j of the range
+            int32_t start = 0;
+            if (is_range) {
+                start = (child[k] & 0x7fffffff) >> 3;
+                const int32_t count = (child[k] & 7) + 1;
+                for (int32_t j = 0; j < count; j++)
+                    if (sphere_cull32(__ldg(sc.bvh_sphere_f + start + j), r.o, dv))
+                        pass |= 1u << j;
+            }
+            uint32_t cb = warp_reserve(&w.counters->isect_len, (uint32_t)__popc(pass));
+            while (pass) {
+                const int j = __ffs(pass) - 1;
+                pass &= pass - 1u;
+                if (cb < w.isect_cap)
+                    w.isect_q[cb] = make_uint2(slot, (uint32_t)__ldg(sc.bvh_leaf + start + j));
+                else mark_overflow(w, slot);
+                cb++;
+            }
         }
     }
 }
@@ -331,16 +337,17 @@ wave_walk_kernel(const TraceArgs a, const WaveBuffers w, const RayPool cur) {
         uint32_t nc = 0;
         bool over = false;
         if (e < n) {
-            const uint2 q = w.level_q[0][e];
-            slot = q.x;
-            const float4 o = w.ray_o[slot], iv = w.ray_i[slot];
+            uint32_t root = 0;
+            WalkRay r;
+            get_entry(sc, w.level_q[0], e, &slot, &root, &r);
+            const float4 o = r.o, iv = r.iv;
             const float3 dv = make_float3(1.0f/iv.x, 1.0f/iv.y, 1.0f/iv.z);
             v3 s = mk(0, 0, 0), d = mk(0, 0, 0);
             double sd = 0.0;
             bool have_ray = false;
             int32_t stack[kWalkStack];
             int sp = 0;
-            stack[sp++] = (int32_t)q.y;
+            stack[sp++] = (int32_t)root;
             while (sp > 0 && !over) {
                 int32_t child[kBvhWidth];
                 const uint32_t hit = node_hits<false>(
@@ -403,7 +410,6 @@ __global__ void wave_after_resolve_kernel(WaveCounters* c) {
     if (threadIdx.x == 0) {
         c->overflow_total += c->overflow_len;
         c->active = c->next;
-        c->range_len = 0;
         c->isect_len = 0;
         c->overflow_len = 0;
     }
@@ -447,8 +453,6 @@ cudaError_t launch_wave_iteration(const TraceArgs& a, const WaveBuffers& w, cons
             wave_level_kernel<<<w.grid, 256, (size_t)staged*sizeof(BvhNode), s>>>(a, w, k,
                                                                                    staged);
         }
-        if (form == MLGPU_TRACER_FP64) wave_sphere_kernel<false><<<w.grid, 256, 0, s>>>(a, w, cur);
-        else wave_sphere_kernel<true><<<w.grid, 256, 0, s>>>(a, w, cur);
     }
     if (ev) cudaEventRecord(ev[2], s);
     if (form == MLGPU_TRACER_FP64) {

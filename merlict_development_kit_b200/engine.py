@@ -16,7 +16,7 @@ from ._native import check, lib
 from .photons import PLANES
 
 TRACERS = {"fp64": abi.TRACER_FP64, "fp32": abi.TRACER_FP32, "fp32_pure": abi.TRACER_FP32_PURE,
-           "fp64_plain": abi.TRACER_FP64_PLAIN}
+           "fp64_plain": abi.TRACER_FP64_PLAIN, "fp64_queue": abi.TRACER_FP64_QUEUE}
 TRAVERSALS = {"bvh": abi.TRAVERSAL_BVH, "frame_tree": abi.TRAVERSAL_FRAME_TREE}
 
 

@@ -636,6 +636,11 @@ int oracle_propagate(const mlgpu_flat_scene* scene,
                      const mlgpu_settings* settings, const mlgpu_rng* rng,
                      const mlgpu_results* results, oracle_counters* counters) {
     int first_error = 0;
+    /* Photon::assert_wavelength_is_positive (merlict/Photon.cpp:20-28): the
+     * caller builds every Photon before propagating, so a non-positive
+     * wavelength fails the call before anything is traced. */
+    for (uint64_t i = 0; i < num_photons; i++)
+        if (((const double*)photons->wavelength)[i] <= 0.0) return MLGPU_ERR_INVALID_ARGUMENT;
     for (uint64_t i = 0; i < num_photons; i++) {
         ctx c;
         c.s = scene; c.error = 0; c.cnt = counters;

@@ -112,3 +112,26 @@ def test_invalid_tuning_is_rejected(eng, events):
         with pytest.raises(ValueError):
             scene.propagate(batch, eng.PropagationConfig(10), eng.Philox(1), tuning=bad)
     scene.close()
+
+
+@pytest.mark.parametrize("grid_blocks", [0, 3, 1000])
+def test_persistent_work_queue_equals_per_event_calls(eng, events, grid_blocks):
+    """The whole batch of uneven events in one persistent launch whose warps
+    pull photon tiles from a device work queue (tracer fp64_queue), with the
+    default grid, a grid far smaller than the GPU (3 blocks drain the whole
+    queue) and a larger one: bit-identical to per-event wavefront calls."""
+    batch, off = events
+    flat = load_golden("light_field_small")[0]
+    scene = eng.Scene(flat)
+    cfg = eng.PropagationConfig(10)
+    launches0 = scene.kernel_launches()
+    queued = host(scene.propagate(batch, cfg, eng.Philox(9), outputs=OUTPUTS, tracer="fp64_queue",
+                                  tuning=dict(grid_blocks=grid_blocks)))
+    # one launch for the queue (plus the tracing order's kernels)
+    assert scene.kernel_launches() - launches0 <= 8
+    for e in range(len(off) - 1):
+        a, b = int(off[e]), int(off[e + 1])
+        part = {k: v[a:b].contiguous() for k, v in batch.items()}
+        got = host(scene.propagate(part, cfg, eng.Philox(9, photon_offset=a), outputs=OUTPUTS))
+        assert_same(got, {k: v[a:b] for k, v in queued.items()})
+    scene.close()

@@ -39,7 +39,7 @@ def run_gpu(eng, flat, photons, max_int, seed=0, uniforms=None, history=False,
     return got
 
 
-FP64_TRACERS = ("fp64", "fp64_plain")
+FP64_TRACERS = ("fp64", "fp64_plain", "fp64_queue")
 
 
 @pytest.mark.parametrize("tracer", FP64_TRACERS)
@@ -99,6 +99,48 @@ def test_propagate_host_entry_point(eng):
                                                      C.byref(rng), C.byref(rs)))
     assert mismatches(ref, out) == {}
     assert history_mismatches(ref["history"], out["history"]) == {}
+
+
+def test_propagate_and_bin_host_entry_point(eng, oracle):
+    """mlgpu_propagate_and_bin_host: the per-photon results of
+    mlgpu_propagate_host plus per-sensor counts and time histograms of the
+    whole batch, equal to the oracle's binning of those results."""
+    from merlict_development_kit_b200 import _native, abi
+    from oracle.oracle import _photon_struct, alloc_results
+    flat, _, _, meta = load_golden("light_field_small")
+    photons = P.downward_disc_source(300_000, 4, 5.55, 21.4, 0.5)
+    scene = eng.Scene(flat)
+    ps, keep = _photon_struct(photons)
+    n = len(photons["wavelength"])
+    st = abi.mlgpu_settings(meta["max_interactions"], 0, abi.TRACER_FP64, 0, abi.TRAVERSAL_BVH)
+    st.pool_size = 65536   # several pieces when the buffers are pinned; pageable here
+    rng = abi.mlgpu_rng()
+    rng.mode = abi.RNG_PHILOX
+    rng.seed = 12
+    L = _native.lib()
+    rs0, want = alloc_results(n, meta["max_interactions"], history=False)
+    _native.check(L.mlgpu_propagate_host(scene.handle, C.byref(ps), n, C.byref(st), C.byref(rng),
+                                         C.byref(rs0)))
+    t = want["time"][want["sensor"] >= 0]
+    t0, t1, nb = float(t.min()) - 1e-12, float(t.max()) + 1e-12, 24
+    rs1, got = alloc_results(n, meta["max_interactions"], history=False)
+    counts = np.full(flat.num_sensors, 7, np.uint32)
+    hist = np.full((flat.num_sensors, nb), 7, np.uint32)
+    _native.check(L.mlgpu_propagate_and_bin_host(
+        scene.handle, C.byref(ps), n, C.byref(st), C.byref(rng), C.byref(rs1),
+        counts.ctypes.data, hist.ctypes.data, nb, t0, t1))
+    assert mismatches(want, got) == {}
+    ref_counts, ref_hist = oracle.bin_arrivals(want["sensor"], want["time"], flat.num_sensors,
+                                               nb, t0, t1)
+    assert np.array_equal(counts, ref_counts)
+    assert np.array_equal(hist, ref_hist)
+    # counts only
+    counts[:] = 7
+    _native.check(L.mlgpu_propagate_and_bin_host(
+        scene.handle, C.byref(ps), n, C.byref(st), C.byref(rng), C.byref(rs1),
+        counts.ctypes.data, None, 0, 0.0, 0.0))
+    assert np.array_equal(counts, ref_counts)
+    scene.close()
 
 
 def host_call_pinned(scene, photons, max_int, tracer, pool, seed=0, uniforms=None):

@@ -46,23 +46,36 @@ def test_noalloc_binning_matches_the_allocating_entry_point_on_two_calls():
     t = time[sensor >= 0]
     t0, t1 = float(t.min()) - 1e-12, float(t.max()) + 1e-12
     n_s = flat.num_sensors
-
-    # first call: counts and a 16-bin time histogram of all photons
-    ref_counts, ref_hist = scene.bin_arrivals(sensor, time, 16, t0, t1)
+    half = sensor[: sensor.shape[0] // 2].contiguous()
     counts = torch.full((n_s,), -1, dtype=torch.int32, device="cuda")
     hist = torch.full((n_s, 16), -1, dtype=torch.int32, device="cuda")
+    counts2 = torch.full((n_s,), -1, dtype=torch.int32, device="cuda")
+    launches0 = scene.kernel_launches()
+
+    # The scene has not binned anything yet, so it owns no binning scratch.
+    # A first call may load the library's device code into the context;
+    # after it, calls must not change the device's free memory.
+    _native.check(call_noalloc(scene, half, None, counts2, None, 0, 0.0, 1.0))
+    torch.cuda.synchronize()
+    free_before = torch.cuda.mem_get_info()[0]
+
+    # first call: counts and a 16-bin time histogram of all photons
     _native.check(call_noalloc(scene, sensor, time, counts, hist, 16, t0, t1))
+    torch.cuda.synchronize()
+    # second call, right after: counts only, of a different (half) batch, so
+    # anything left over in the shared scratch from the first call would show
+    counts2.fill_(-1)
+    _native.check(call_noalloc(scene, half, None, counts2, None, 0, 0.0, 1.0))
+    torch.cuda.synchronize()
+    assert torch.cuda.mem_get_info()[0] == free_before
+    assert scene.kernel_launches() - launches0 == 6
+
+    # the allocating entry point on the same inputs
+    ref_counts, ref_hist = scene.bin_arrivals(sensor, time, 16, t0, t1)
+    ref_counts2, _ = scene.bin_arrivals(half)
     torch.cuda.synchronize()
     assert torch.equal(counts, ref_counts)
     assert torch.equal(hist, ref_hist)
-
-    # second call, right after: counts only, of a different (half) batch, so
-    # anything left over in the shared scratch from the first call would show
-    half = sensor[: sensor.shape[0] // 2].contiguous()
-    ref_counts2, _ = scene.bin_arrivals(half)
-    counts2 = torch.full((n_s,), -1, dtype=torch.int32, device="cuda")
-    _native.check(call_noalloc(scene, half, None, counts2, None, 0, 0.0, 1.0))
-    torch.cuda.synchronize()
     assert torch.equal(counts2, ref_counts2)
     assert int(counts2.sum()) == int((half >= 0).sum())
     assert not torch.equal(counts2, counts)
