@@ -47,7 +47,12 @@ FLOP_STAGE = {"nodes": "walk", "leaves": "intersect", "caps": "intersect",
               "cap_bounds": "intersect", "planes": "intersect", "others": "intersect",
               "reflections": "resolve", "fresnels": "resolve", "segments": "resolve",
               "funcs": "resolve"}
-FP64_PEAK_TFLOPS_NOMINAL = 37.0   # B200 vector FP64, nominal (no measured figure)
+FP64_PEAK_TFLOPS_NOMINAL = 37.0   # B200 vector FP64 with FMAs, nominal
+# DRAM bytes per photon of each kernel class on the light-field telescope,
+# from an ncu capture of the timed step (dram__bytes_read.sum +
+# dram__bytes_write.sum summed over the class's launches, divided by the
+# photons of the step; profiles/wavefront_fp64_light_field_telescope.md)
+STAGE_DRAM_BYTES_PER_PHOTON = {}
 FP32_PEAK_TFLOPS_NOMINAL = 75.0   # B200 vector FP32 (non-tensor), nominal
 WORKLOAD = "light-field telescope, 1039 lenses x 61 lixels (config 1)"
 # the signal chain after binning (workload "signal"): quantum efficiency,
@@ -430,16 +435,30 @@ def run_ours(args, world, rank, local):
     # reference's operation counts for that stage, per photon, times the
     # photons of a step, over the stage's device time per step
     achieved = dk["flops_per_photon"] * n / (dk["ms_per_step"] * 1e-3) / 1e12
+    # the denominator, measured on this GPU: separate FP64 adds and
+    # multiplies (the reference's operations, which the bit-exact tracer may
+    # not contract into FMAs), with the FMA rate beside it
+    rate_addmul, rate_fma = C.c_double(0.0), C.c_double(0.0)
+    _native.check(L.mlgpu_probe_fp64_rate(0, C.byref(rate_addmul), None))
+    _native.check(L.mlgpu_probe_fp64_rate(1, C.byref(rate_fma), None))
+    peak = rate_addmul.value / 1e12 if not fp32 else vec_peak
+    traffic = STAGE_DRAM_BYTES_PER_PHOTON.get(dominant)
     roofline = {"bound": "fp32" if fp32 else "fp64", "kernel": dominant,
-                "achieved": achieved, "peak": vec_peak, "unit": "TFLOP/s",
-                "frac": achieved / vec_peak, "traffic": None,
-                "peak_source": "nominal B200 vector %s peak (no measured figure)" %
-                               ("FP32" if fp32 else "FP64"),
+                "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+                "frac": achieved / peak,
+                "traffic": traffic * n / dk["launches"] * args.steps if traffic else None,
+                "traffic_unit": "DRAM bytes per launch of the stage (ncu, scaled by photons)",
+                "peak_source": ("measured on this GPU: FP64 adds and multiplies "
+                                "(mlgpu_probe_fp64_rate, no FMA)" if not fp32 else
+                                "nominal B200 vector FP32 peak (no measured figure)"),
+                "peak_fp64_fma_measured": rate_fma.value / 1e12,
+                "frac_of_fma_peak": achieved / (rate_fma.value / 1e12),
+                "peak_fp64_nominal": FP64_PEAK_TFLOPS_NOMINAL,
                 "flops_per_photon": dk["flops_per_photon"]}
     flops = sum(stage_flops.values())
     whole = flops * n / (kernel_ms * 1e-3) / 1e12
     compute = {"bound": roofline["bound"], "flops_per_photon": flops, "achieved": whole,
-               "peak": vec_peak, "unit": "TFLOP/s", "frac": whole / vec_peak,
+               "peak": peak, "unit": "TFLOP/s", "frac": whole / peak,
                "scope": "whole propagate call"}
     achieved_gbs = bpp * n / (kernel_ms * 1e-3) / 1e9
     hbm = {"bound": "hbm", "achieved": achieved_gbs, "peak": hbm_peak, "unit": "GB/s",

@@ -316,6 +316,15 @@ typedef struct mlgpu_wavefront_stats {
 
 int mlgpu_scene_wavefront_stats(mlgpu_scene* scene, mlgpu_wavefront_stats* stats, int reset);
 
+/* The current GPU's FP64 arithmetic rate in FLOP/s, measured by a short
+ * kernel of independent FP64 operation chains on every SM (about a tenth
+ * of a second; synchronises `cuda_stream`).  fma != 0: fused multiply-adds
+ * (2 FLOP each); fma == 0: separate adds and multiplies (1 FLOP each), the
+ * only forms the bit-exact FP64 tracers use.  No counterpart in the
+ * reference: it is the measured denominator of the tracers' compute
+ * roofline, whose numerators are the reference's own operation counts.   */
+int mlgpu_probe_fp64_rate(int fma, double* flops_per_second, void* cuda_stream);
+
 /* ---- propagation ------------------------------------------------------ *
  * Replaces propagate_photons_in_frame_with_config (merlict/Photons.cpp:9-22)
  * and its thread-pool twin (merlict_multi_thread.cpp:28-55).

@@ -60,6 +60,7 @@ def lib():
             C.POINTER(abi.mlgpu_results), C.c_void_p, C.c_void_p, C.c_uint32, C.c_double,
             C.c_double]
         L.mlgpu_scene_sync_errors.argtypes = [C.c_void_p, C.c_void_p]
+        L.mlgpu_probe_fp64_rate.argtypes = [C.c_int, C.POINTER(C.c_double), C.c_void_p]
         L.mlgpu_bin_arrivals.argtypes = [
             C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint64, C.c_void_p, C.c_void_p,
             C.c_uint32, C.c_double, C.c_double, C.c_void_p]
@@ -92,7 +93,7 @@ def lib():
                      "mlgpu_propagate_host", "mlgpu_propagate_and_bin_host",
                      "mlgpu_scene_sync_errors", "mlgpu_bin_arrivals",
                      "mlgpu_bin_arrivals_noalloc", "mlgpu_scene_kernel_launches",
-                     "mlgpu_scene_wavefront_stats"):
+                     "mlgpu_scene_wavefront_stats", "mlgpu_probe_fp64_rate"):
             getattr(L, name).restype = C.c_int
         if L.mlgpu_abi_version() != abi.ABI_VERSION:
             raise ImportError("libmerlict_b200.so ABI version mismatch")
@@ -150,7 +151,7 @@ EXPORTED = (
     "mlgpu_propagate", "mlgpu_scene_sync_errors", "mlgpu_propagate_host",
     "mlgpu_propagate_and_bin_host",
     "mlgpu_bin_arrivals", "mlgpu_bin_arrivals_noalloc", "mlgpu_scene_kernel_launches",
-    "mlgpu_scene_wavefront_stats",
+    "mlgpu_scene_wavefront_stats", "mlgpu_probe_fp64_rate",
     "mlgpu_scene_set_profiling", "mlgpu_scene_kernel_times", "mlgpu_scene_autotune",
     "mlgpu_corsika_photons", "mlgpu_lixel_statistics", "mlgpu_signal_chain",
     # include/merlict_b200_surrogate.h

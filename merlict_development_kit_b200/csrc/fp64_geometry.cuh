@@ -381,29 +381,51 @@ __device__ __forceinline__ void test_candidate(const DevScene& sc, int32_t leaf,
 }
 
 // merlict's intersection of one leaf with a world ray; leaf < 0 if none.
-// The first 200 bytes of a leaf record (T, tinv, params, r2, primitive) in
-// 16-byte loads: a warp whose lanes hold different leaves issues half as
-// many load requests as with 8-byte loads.
-static_assert(offsetof(LeafRec, tinv) == 96 && offsetof(LeafRec, params) == 120 &&
-              offsetof(LeafRec, r2) == 184 && offsetof(LeafRec, primitive) == 192,
+// The leaf record in 16-byte loads: the first line (transform, inverse
+// translation, primitive), the squared radius with the first parameter, and
+// only as many further parameter pairs as the primitive has parameters --
+// a warp whose lanes hold different leaves issues one request per lane and
+// load, so every load left out counts.
+static_assert(offsetof(LeafRec, tinv) == 96 && offsetof(LeafRec, primitive) == 120 &&
+              offsetof(LeafRec, r2) == 128 && offsetof(LeafRec, params) == 136,
               "load_leaf reads the leaf record in 16-byte pieces");
+__device__ __forceinline__ int primitive_params(int32_t prim) {
+    switch (prim) {
+    case MLGPU_PRIM_DISC: case MLGPU_PRIM_HEX_PLANE: case MLGPU_PRIM_SPHERE: return 1;
+    case MLGPU_PRIM_SPHERE_CAP_HEX: case MLGPU_PRIM_SPHERE_CAP_CYL: case MLGPU_PRIM_PLANE:
+    case MLGPU_PRIM_ANNULUS: case MLGPU_PRIM_CYLINDER: return 2;
+    case MLGPU_PRIM_SPHERE_CAP_RECT: return 3;
+    case MLGPU_PRIM_PLANE_DUAL_SPHERE: return 5;
+    case MLGPU_PRIM_TRIANGLE: return 6;
+    case MLGPU_PRIM_ELLIPTIC_CAP_HEX: return 7;
+    default: return 0;
+    }
+}
+
 __device__ __forceinline__ void load_leaf(const LeafRec* L, double* T, double* ti, double* pr,
                                           double* r2, int32_t* prim) {
     const double2* q = reinterpret_cast<const double2*>(L);
-    double v[24];
+    double v[14];
 #pragma unroll
-    for (int k = 0; k < 12; k++) {
+    for (int k = 0; k < 7; k++) {
         const double2 x = __ldg(q + k);
         v[2*k] = x.x;
         v[2*k + 1] = x.y;
     }
+    const double2 tail = __ldg(q + 7);                     // tinv[2], primitive | sensor
+    const double2 r2p0 = __ldg(q + 8);                     // r2, params[0]
 #pragma unroll
     for (int k = 0; k < 12; k++) T[k] = v[k];
-    ti[0] = v[12]; ti[1] = v[13]; ti[2] = v[14];
+    ti[0] = v[12]; ti[1] = v[13]; ti[2] = tail.x;
+    *prim = (int32_t)(uint32_t)(__double_as_longlong(tail.y) & 0xffffffffll);
+    *r2 = r2p0.x;
+    pr[0] = r2p0.y;
 #pragma unroll
-    for (int k = 0; k < MLGPU_LEAF_PARAMS; k++) pr[k] = v[15 + k];
-    *r2 = v[23];
-    *prim = __ldg(&L->primitive);
+    for (int k = 1; k < MLGPU_LEAF_PARAMS; k++) pr[k] = 0.0;
+    const int np = primitive_params(*prim);
+    if (np > 1) { const double2 x = __ldg(q + 9); pr[1] = x.x; pr[2] = x.y; }
+    if (np > 3) { const double2 x = __ldg(q + 10); pr[3] = x.x; pr[4] = x.y; }
+    if (np > 5) { const double2 x = __ldg(q + 11); pr[5] = x.x; pr[6] = x.y; }
 }
 
 __device__ __forceinline__ Isec leaf_hit(const DevScene& sc, int32_t leaf, v3 s, v3 d) {

@@ -12,22 +12,27 @@
 
 namespace mlgpu {
 
-// One leaf surface in 256 bytes (two 128-byte lines): the 3x4 frame-to-world
-// transform, the translation part of its inverse, primitive parameters, the
-// squared bounding radius and the surface's property-table ids.
+// One leaf surface in 256 bytes (two 128-byte lines).  The first line holds
+// what every candidate test needs -- the 3x4 frame-to-world transform, the
+// translation part of its inverse, the primitive and sensor -- the second
+// the squared bounding radius beside the primitive parameters (so that a
+// one-parameter primitive, the lixels and pixels, adds one 16-byte load),
+// then the surface's flags and property-table ids.
 struct __align__(256) LeafRec {
     double T[12];          // rows of the 3x4 homogeneous transform
     double tinv[3];        // T00*T03 + T10*T13 + T20*T23, ... (HomTra3.cpp:200-216)
-    double params[MLGPU_LEAF_PARAMS];
-    double r2;             // bounding sphere radius squared
     int32_t primitive;
     int32_t sensor;
+    double r2;             // bounding sphere radius squared
+    double params[MLGPU_LEAF_PARAMS];
     int32_t allowed_node;
     int32_t flags;
     int32_t fn[6];         // outer/inner reflection, refraction, absorption
-    int32_t pad[2];
+    int32_t pad[6];
 };
 static_assert(sizeof(LeafRec) == 256, "LeafRec must be 256 bytes");
+static_assert(offsetof(LeafRec, primitive) == 120 && offsetof(LeafRec, r2) == 128 &&
+              offsetof(LeafRec, params) == 136, "LeafRec's first line ends with the primitive");
 
 // FP32 image of a leaf for the batched tracer: transform relative to the
 // leaf's own origin, parameters in float, 128 bytes.

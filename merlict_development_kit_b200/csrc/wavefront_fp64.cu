@@ -174,14 +174,31 @@ wave_intake_kernel(const TraceArgs a, const WaveBuffers w, const RayPool cur) {
     }
 }
 
+// The child references of a BVH node, four per int4 (kept in registers).
+struct ChildRefs {
+    int4 g0, g1;
+};
+static_assert(kBvhWidth == 8, "ChildRefs holds eight children");
+
+__device__ __forceinline__ int32_t child_ref(const ChildRefs& c, int k) {
+    const int4 q = k < 4 ? c.g0 : c.g1;
+    switch (k & 3) {
+    case 0: return q.x;
+    case 1: return q.y;
+    case 2: return q.z;
+    default: return q.w;
+    }
+}
+
 // Four child boxes of a BVH node: slab tests in single precision on boxes
 // widened by the ray's rounding (o.w).  Bit k of the result: child k is hit.
 __device__ __forceinline__ uint32_t node_box_hits(float4 lx, float4 ly, float4 lz, float4 hx,
-                                                  float4 hy, float4 hz, const int32_t* child,
+                                                  float4 hy, float4 hz, int4 child,
                                                   float4 o, float4 iv) {
     const float lox[4] = {lx.x, lx.y, lx.z, lx.w}, loy[4] = {ly.x, ly.y, ly.z, ly.w};
     const float loz[4] = {lz.x, lz.y, lz.z, lz.w}, hix[4] = {hx.x, hx.y, hx.z, hx.w};
     const float hiy[4] = {hy.x, hy.y, hy.z, hy.w}, hiz[4] = {hz.x, hz.y, hz.z, hz.w};
+    const int32_t ch[4] = {child.x, child.y, child.z, child.w};
     uint32_t hit = 0;
 #pragma unroll
     for (int k = 0; k < 4; k++) {
@@ -190,7 +207,7 @@ __device__ __forceinline__ uint32_t node_box_hits(float4 lx, float4 ly, float4 l
         const float az = (loz[k] - o.w - o.z)*iv.z, bz = (hiz[k] + o.w - o.z)*iv.z;
         const float tmin = fmaxf(fmaxf(fminf(ax, bx), fminf(ay, by)), fmaxf(fminf(az, bz), 0.0f));
         const float tmax = fminf(fminf(fmaxf(ax, bx), fmaxf(ay, by)), fmaxf(az, bz));
-        if (tmin <= tmax && child[k] != kBvhEmpty) hit |= 1u << k;
+        if (tmin <= tmax && ch[k] != kBvhEmpty) hit |= 1u << k;
     }
     return hit;
 }
@@ -199,20 +216,17 @@ __device__ __forceinline__ uint32_t node_box_hits(float4 lx, float4 ly, float4 l
 // path, or shared memory), four at a time; their references into `child`.
 template <bool kShared>
 __device__ __forceinline__ uint32_t node_hits(const float4* nq, float4 o, float4 iv,
-                                              int32_t* child) {
+                                              ChildRefs* child) {
     auto ld = [nq](int k) { return kShared ? nq[k] : __ldg(nq + k); };
-    uint32_t hit = 0;
-#pragma unroll
-    for (int g = 0; g < kBvhGroups; g++) {
-        const float4 c = ld(6*kBvhGroups + g);
-        int32_t* cg = child + 4*g;
-        cg[0] = __float_as_int(c.x); cg[1] = __float_as_int(c.y);
-        cg[2] = __float_as_int(c.z); cg[3] = __float_as_int(c.w);
-        hit |= node_box_hits(ld(g), ld(kBvhGroups + g), ld(2*kBvhGroups + g),
-                             ld(3*kBvhGroups + g), ld(4*kBvhGroups + g), ld(5*kBvhGroups + g),
-                             cg, o, iv) << (4*g);
-    }
-    return hit;
+    const float4 c0 = ld(6*kBvhGroups), c1 = ld(6*kBvhGroups + 1);
+    child->g0 = make_int4(__float_as_int(c0.x), __float_as_int(c0.y), __float_as_int(c0.z),
+                          __float_as_int(c0.w));
+    child->g1 = make_int4(__float_as_int(c1.x), __float_as_int(c1.y), __float_as_int(c1.z),
+                          __float_as_int(c1.w));
+    return node_box_hits(ld(0), ld(kBvhGroups), ld(2*kBvhGroups), ld(3*kBvhGroups),
+                         ld(4*kBvhGroups), ld(5*kBvhGroups), child->g0, o, iv) |
+        (node_box_hits(ld(1), ld(kBvhGroups + 1), ld(2*kBvhGroups + 1), ld(3*kBvhGroups + 1),
+                       ld(4*kBvhGroups + 1), ld(5*kBvhGroups + 1), child->g1, o, iv) << 4);
 }
 
 // merlict's bounding-sphere test of a leaf (RayAndFrame.cpp:16-107) in
@@ -258,7 +272,8 @@ wave_level_kernel(const TraceArgs a, const WaveBuffers w, int level, int staged)
     for (uint32_t first = warp_first(); first < n; first += gridDim.x*blockDim.x) {
         const uint32_t e = first + (uint32_t)lane;
         uint32_t slot = 0, node = 0;
-        int32_t child[kBvhWidth];
+        ChildRefs child;
+        child.g0 = child.g1 = make_int4(kBvhEmpty, kBvhEmpty, kBvhEmpty, kBvhEmpty);
         uint32_t hit = 0;   // bit k: child k hit
         WalkRay r;
         r.o = make_float4(0.f, 0.f, 0.f, 0.f);
@@ -267,20 +282,20 @@ wave_level_kernel(const TraceArgs a, const WaveBuffers w, int level, int staged)
             get_entry(sc, in, e, &slot, &node, &r);
             if ((uint32_t)((int32_t)node - base) < (uint32_t)staged)
                 hit = node_hits<true>(stage + (sizeof(BvhNode)/16)*((int32_t)node - base), r.o,
-                                      r.iv, child);
+                                      r.iv, &child);
             else
                 hit = node_hits<false>(reinterpret_cast<const float4*>(sc.bvh + node), r.o, r.iv,
-                                       child);
+                                       &child);
         }
         uint32_t nn = 0, ranges = 0;   // bit k of ranges: child k is a hit leaf range
 #pragma unroll
         for (int k = 0; k < kBvhWidth; k++)
-            if (hit & (1u << k)) { if (child[k] < 0) ranges |= 1u << k; else nn++; }
+            if (hit & (1u << k)) { if (child_ref(child, k) < 0) ranges |= 1u << k; else nn++; }
         uint32_t nb = warp_reserve(&w.counters->level_len[last ? level : level + 1], last ? 0u : nn);
 #pragma unroll
         for (int k = 0; k < kBvhWidth; k++) {
-            if (!(hit & (1u << k)) || child[k] < 0) continue;
-            if (!last && nb < w.level_cap) put_entry(out, nb, slot, (uint32_t)child[k], r);
+            if (!(hit & (1u << k)) || child_ref(child, k) < 0) continue;
+            if (!last && nb < w.level_cap) put_entry(out, nb, slot, (uint32_t)child_ref(child, k), r);
             else mark_overflow(w, slot);
             nb++;
         }
@@ -294,8 +309,9 @@ wave_level_kernel(const TraceArgs a, const WaveBuffers w, int level, int staged)
             uint32_t pass = 0;   // bit j: leaf j of the range
             int32_t start = 0;
             if (is_range) {
-                start = (child[k] & 0x7fffffff) >> 3;
-                const int32_t count = (child[k] & 7) + 1;
+                const int32_t ref = child_ref(child, k);
+                start = (ref & 0x7fffffff) >> 3;
+                const int32_t count = (ref & 7) + 1;
                 for (int32_t j = 0; j < count; j++)
                     if (sphere_cull32(__ldg(sc.bvh_sphere_f + start + j), r.o, dv))
                         pass |= 1u << j;
@@ -349,17 +365,17 @@ wave_walk_kernel(const TraceArgs a, const WaveBuffers w, const RayPool cur) {
             int sp = 0;
             stack[sp++] = (int32_t)root;
             while (sp > 0 && !over) {
-                int32_t child[kBvhWidth];
+                ChildRefs child;
                 const uint32_t hit = node_hits<false>(
-                    reinterpret_cast<const float4*>(sc.bvh + stack[--sp]), o, iv, child);
+                    reinterpret_cast<const float4*>(sc.bvh + stack[--sp]), o, iv, &child);
                 for (int k = kBvhWidth - 1; k >= 0; k--) {
                     if (!(hit & (1u << k))) continue;
-                    if (child[k] >= 0) {
-                        if (sp < kWalkStack) stack[sp++] = child[k];
+                    const int32_t ref = child_ref(child, k);
+                    if (ref >= 0) {
+                        if (sp < kWalkStack) stack[sp++] = ref;
                         else over = true;
                         continue;
                     }
-                    const int32_t ref = child[k];
                     const int32_t start = (ref & 0x7fffffff) >> 3;
                     const int32_t count = (ref & 7) + 1;
                     if (!kF32 && !have_ray) {
