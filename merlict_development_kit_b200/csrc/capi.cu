@@ -454,7 +454,7 @@ int wave_buffers(mlgpu_scene* scene, uint32_t pool, int grid, int staged, uint32
     const size_t level_cap = queue_cap ? queue_cap : 8*P;
     const size_t isect_cap = queue_cap ? queue_cap : 16*P;
     const size_t per_pool = 8*up(P*8) + 5*up(P*4);
-    const size_t rest = up(P*4) + up(P*48) + 2*up(level_cap*32) +
+    const size_t rest = up(P*4) + 2*up(P*16) + up(P*48) + 2*up(level_cap*8) +
         up(isect_cap*8) + up(isect_cap*8) + up(P*8) + 3*up(P*4);
     MLGPU_CUDA(scene->wave.reserve(256 + 2*per_pool + rest));
     if (!scene->wave_host) MLGPU_CUDA(cudaMallocHost(&scene->wave_host, sizeof(WaveCounters)));
@@ -478,8 +478,10 @@ int wave_buffers(mlgpu_scene* scene, uint32_t pool, int grid, int staged, uint32
     w->staged_levels = staged;
     w->step = reinterpret_cast<int32_t*>(take(P*4));
     w->ray_sd = reinterpret_cast<double2*>(take(P*48));
-    w->level_q[0] = reinterpret_cast<uint4*>(take(level_cap*32));
-    w->level_q[1] = reinterpret_cast<uint4*>(take(level_cap*32));
+    w->ray_o = reinterpret_cast<float4*>(take(P*16));
+    w->ray_i = reinterpret_cast<float4*>(take(P*16));
+    w->level_q[0] = reinterpret_cast<uint2*>(take(level_cap*8));
+    w->level_q[1] = reinterpret_cast<uint2*>(take(level_cap*8));
     w->level_cap = (uint32_t)level_cap;
     w->isect_q = reinterpret_cast<uint2*>(take(isect_cap*8));
     w->isect_dist = reinterpret_cast<double*>(take(isect_cap*8));

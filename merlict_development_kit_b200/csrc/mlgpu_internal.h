@@ -199,9 +199,9 @@ struct WaveBuffers {
     int32_t* step;           // [pool] 0, or kNoStep: the photon takes no step
     double2* ray_sd;         // [pool][3] the FP64 support and direction, one 48-byte
                              // record per slot for the kernels that read rays by queue
-    uint4* level_q[2];       // (ray, node) entries of two uint4 each, ping-pong between
-                             // BVH levels: {slot, node, origin x, y}, {origin z, 1/dir x,
-                             // y, z} (floats as bits): each entry carries its ray
+    float4* ray_o;           // [pool] single-precision origin, box inflation
+    float4* ray_i;           // [pool] reciprocal direction
+    uint2* level_q[2];       // (slot, node) pairs, ping-pong between BVH levels
     uint32_t level_cap;
     uint2* isect_q;          // (slot, leaf) candidates
     double* isect_dist;      // distance to each candidate's hit, -1: none

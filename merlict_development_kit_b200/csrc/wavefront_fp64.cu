@@ -27,32 +27,9 @@ namespace {
 constexpr int kTreeCands = 16;   // candidates of a frame-tree walk before it overflows
 constexpr int kMaxStagedNodes = 32768/(int)sizeof(BvhNode);   // 32 KB of shared memory per block
 
-// A (ray, BVH node) work item with the ray's FP32 origin and reciprocal
-// direction, so that the level kernels read their rays with the queue.
-struct WalkRay {
-    float4 o;    // origin, box inflation
-    float4 iv;   // reciprocal direction
-};
-
+// The box inflation of a ray's FP32 slab tests: its rounding to FP32.
 __device__ __forceinline__ float box_inflation(const DevScene& sc, float ox, float oy, float oz) {
     return sc.bvh_eps + 4e-7f*(fabsf(ox) + fabsf(oy) + fabsf(oz));
-}
-
-__device__ __forceinline__ void put_entry(uint4* q, uint32_t e, uint32_t slot, uint32_t node,
-                                          const WalkRay& r) {
-    q[2*e] = make_uint4(slot, node, __float_as_uint(r.o.x), __float_as_uint(r.o.y));
-    q[2*e + 1] = make_uint4(__float_as_uint(r.o.z), __float_as_uint(r.iv.x),
-                            __float_as_uint(r.iv.y), __float_as_uint(r.iv.z));
-}
-
-__device__ __forceinline__ void get_entry(const DevScene& sc, const uint4* q, uint32_t e,
-                                          uint32_t* slot, uint32_t* node, WalkRay* r) {
-    const uint4 a = q[2*e], b = q[2*e + 1];
-    *slot = a.x;
-    *node = a.y;
-    const float ox = __uint_as_float(a.z), oy = __uint_as_float(a.w), oz = __uint_as_float(b.x);
-    r->o = make_float4(ox, oy, oz, box_inflation(sc, ox, oy, oz));
-    r->iv = make_float4(__uint_as_float(b.y), __uint_as_float(b.z), __uint_as_float(b.w), 0.0f);
 }
 
 template <typename In>
@@ -69,7 +46,6 @@ wave_intake_kernel(const TraceArgs a, const WaveBuffers w, const RayPool cur) {
     const uint32_t max_int = a.max_interactions;
     const uint32_t hist_len = max_int + 1;
     bool bvh = false;          // queue the BVH root for this ray
-    WalkRay wr;                // its FP32 walk ray
     int nc = 0;                // candidates of a frame-tree walk
     int32_t cand[kTreeCands];
     if (slot < total) {
@@ -155,8 +131,8 @@ wave_intake_kernel(const TraceArgs a, const WaveBuffers w, const RayPool cur) {
                     if (fabsf(fdx) < 1e-30f) fdx = copysignf(1e-30f, fdx);
                     if (fabsf(fdy) < 1e-30f) fdy = copysignf(1e-30f, fdy);
                     if (fabsf(fdz) < 1e-30f) fdz = copysignf(1e-30f, fdz);
-                    wr.o = make_float4(ox, oy, oz, box_inflation(sc, ox, oy, oz));
-                    wr.iv = make_float4(1.0f/fdx, 1.0f/fdy, 1.0f/fdz, 0.0f);
+                    w.ray_o[slot] = make_float4(ox, oy, oz, box_inflation(sc, ox, oy, oz));
+                    w.ray_i[slot] = make_float4(1.0f/fdx, 1.0f/fdy, 1.0f/fdz, 0.0f);
                 }
             }
         }
@@ -164,7 +140,7 @@ wave_intake_kernel(const TraceArgs a, const WaveBuffers w, const RayPool cur) {
     // queue the BVH root and the frame-tree candidates (all lanes take part)
     const uint32_t qb = warp_reserve(&w.counters->level_len[0], bvh ? 1u : 0u);
     if (bvh) {
-        if (qb < w.level_cap) put_entry(w.level_q[0], qb, slot, 0u, wr);
+        if (qb < w.level_cap) w.level_q[0][qb] = make_uint2(slot, 0u);
         else mark_overflow(w, slot);
     }
     const uint32_t cb = warp_reserve(&w.counters->isect_len, (uint32_t)nc);
@@ -252,16 +228,33 @@ __device__ __forceinline__ bool sphere_cull32(float4 c, float4 o, float3 dv) {
 // `staged` > 0 the block first copies the level's `staged` nodes (a
 // contiguous range, the tree being numbered breadth first) into shared
 // memory and reads them from there.
-__global__ void __launch_bounds__(256)
+//
+// Hit leaf ranges: their leaves pass a conservative FP32 version of
+// merlict's bounding-sphere test (sphere_cull32) or not; those that pass are
+// the ray's candidates.  A warp's hit ranges are spread over its lanes
+// through shared memory -- one range per lane, as many rounds as the warp
+// has ranges / 32 -- so that the up to eight tests of a range run beside
+// the other lanes' instead of one lane at a time.
+constexpr int kLevelThreads = 256;
+constexpr int kLevelWarps = kLevelThreads/32;
+
+struct WalkRay {        // a lane's ray, published to its warp
+    float4 o;           // origin, box inflation
+    float4 dv;          // direction (from the reciprocal); w: the slot, as bits
+};
+
+__global__ void __launch_bounds__(kLevelThreads)
 wave_level_kernel(const TraceArgs a, const WaveBuffers w, int level, int staged) {
     extern __shared__ float4 stage[];
+    __shared__ WalkRay s_ray[kLevelWarps][32];
+    __shared__ int2 s_range[kLevelWarps][32*kBvhWidth];   // (leaf-range reference, lane)
     const DevScene& sc = a.scene;
-    const uint4* in = w.level_q[level & 1];
-    uint4* out = w.level_q[(level + 1) & 1];
+    const uint2* in = w.level_q[level & 1];
+    uint2* out = w.level_q[(level + 1) & 1];
     const uint32_t len = w.counters->level_len[level];
     const uint32_t n = len < w.level_cap ? len : w.level_cap;
     const bool last = level + 1 >= kMaxBvhLevels;
-    const int lane = threadIdx.x & 31;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int32_t base = sc.bvh_level_start[level];
     if (staged > 0) {
         const float4* src = reinterpret_cast<const float4*>(sc.bvh + base);
@@ -271,20 +264,21 @@ wave_level_kernel(const TraceArgs a, const WaveBuffers w, int level, int staged)
     }
     for (uint32_t first = warp_first(); first < n; first += gridDim.x*blockDim.x) {
         const uint32_t e = first + (uint32_t)lane;
-        uint32_t slot = 0, node = 0;
+        uint32_t slot = 0;
         ChildRefs child;
         child.g0 = child.g1 = make_int4(kBvhEmpty, kBvhEmpty, kBvhEmpty, kBvhEmpty);
         uint32_t hit = 0;   // bit k: child k hit
-        WalkRay r;
-        r.o = make_float4(0.f, 0.f, 0.f, 0.f);
-        r.iv = make_float4(1.f, 1.f, 1.f, 0.f);
+        float4 o = make_float4(0.f, 0.f, 0.f, 0.f), iv = make_float4(1.f, 1.f, 1.f, 0.f);
         if (e < n) {
-            get_entry(sc, in, e, &slot, &node, &r);
-            if ((uint32_t)((int32_t)node - base) < (uint32_t)staged)
-                hit = node_hits<true>(stage + (sizeof(BvhNode)/16)*((int32_t)node - base), r.o,
-                                      r.iv, &child);
+            const uint2 q = in[e];
+            slot = q.x;
+            o = w.ray_o[slot];
+            iv = w.ray_i[slot];
+            if ((uint32_t)((int32_t)q.y - base) < (uint32_t)staged)
+                hit = node_hits<true>(stage + (sizeof(BvhNode)/16)*((int32_t)q.y - base), o, iv,
+                                      &child);
             else
-                hit = node_hits<false>(reinterpret_cast<const float4*>(sc.bvh + node), r.o, r.iv,
+                hit = node_hits<false>(reinterpret_cast<const float4*>(sc.bvh + q.y), o, iv,
                                        &child);
         }
         uint32_t nn = 0, ranges = 0;   // bit k of ranges: child k is a hit leaf range
@@ -295,25 +289,40 @@ wave_level_kernel(const TraceArgs a, const WaveBuffers w, int level, int staged)
 #pragma unroll
         for (int k = 0; k < kBvhWidth; k++) {
             if (!(hit & (1u << k)) || child_ref(child, k) < 0) continue;
-            if (!last && nb < w.level_cap) put_entry(out, nb, slot, (uint32_t)child_ref(child, k), r);
+            if (!last && nb < w.level_cap) out[nb] = make_uint2(slot, (uint32_t)child_ref(child, k));
             else mark_overflow(w, slot);
             nb++;
         }
-        // the leaves of the hit leaf ranges whose bounding spheres the ray
-        // may pass become candidates, one leaf range of the warp at a time
-        const float3 dv = make_float3(1.0f/r.iv.x, 1.0f/r.iv.y, 1.0f/r.iv.z);
+        // the warp's hit leaf ranges, listed in shared memory
+        const uint32_t nr = (uint32_t)__popc(ranges);
+        uint32_t incl = nr;
 #pragma unroll
-        for (int k = 0; k < kBvhWidth; k++) {
-            const bool is_range = (ranges >> k) & 1u;
-            if (!__any_sync(kFull, is_range)) continue;
-            uint32_t pass = 0;   // bit j: leaf j of the range
+        for (int d = 1; d < 32; d <<= 1) {
+            const uint32_t y = __shfl_up_sync(kFull, incl, d);
+            if (lane >= d) incl += y;
+        }
+        const uint32_t total = __shfl_sync(kFull, incl, 31);
+        if (total == 0) continue;   // warp-uniform
+        s_ray[warp][lane].o = o;
+        s_ray[warp][lane].dv = make_float4(1.0f/iv.x, 1.0f/iv.y, 1.0f/iv.z, __uint_as_float(slot));
+        uint32_t at = incl - nr;
+#pragma unroll
+        for (int k = 0; k < kBvhWidth; k++)
+            if ((ranges >> k) & 1u) s_range[warp][at++] = make_int2(child_ref(child, k), lane);
+        __syncwarp();
+        for (uint32_t r0 = 0; r0 < total; r0 += 32) {
+            const uint32_t t = r0 + (uint32_t)lane;
+            uint32_t pass = 0, src_slot = 0;   // bit j: leaf j of the range
             int32_t start = 0;
-            if (is_range) {
-                const int32_t ref = child_ref(child, k);
-                start = (ref & 0x7fffffff) >> 3;
-                const int32_t count = (ref & 7) + 1;
+            if (t < total) {
+                const int2 item = s_range[warp][t];
+                const WalkRay rr = s_ray[warp][item.y];
+                src_slot = __float_as_uint(rr.dv.w);
+                start = (item.x & 0x7fffffff) >> 3;
+                const int32_t count = (item.x & 7) + 1;
+                const float3 dv = make_float3(rr.dv.x, rr.dv.y, rr.dv.z);
                 for (int32_t j = 0; j < count; j++)
-                    if (sphere_cull32(__ldg(sc.bvh_sphere_f + start + j), r.o, dv))
+                    if (sphere_cull32(__ldg(sc.bvh_sphere_f + start + j), rr.o, dv))
                         pass |= 1u << j;
             }
             uint32_t cb = warp_reserve(&w.counters->isect_len, (uint32_t)__popc(pass));
@@ -321,11 +330,12 @@ wave_level_kernel(const TraceArgs a, const WaveBuffers w, int level, int staged)
                 const int j = __ffs(pass) - 1;
                 pass &= pass - 1u;
                 if (cb < w.isect_cap)
-                    w.isect_q[cb] = make_uint2(slot, (uint32_t)__ldg(sc.bvh_leaf + start + j));
-                else mark_overflow(w, slot);
+                    w.isect_q[cb] = make_uint2(src_slot, (uint32_t)__ldg(sc.bvh_leaf + start + j));
+                else mark_overflow(w, src_slot);
                 cb++;
             }
         }
+        __syncwarp();   // the lists are rewritten by the next round of entries
     }
 }
 
@@ -353,10 +363,10 @@ wave_walk_kernel(const TraceArgs a, const WaveBuffers w, const RayPool cur) {
         uint32_t nc = 0;
         bool over = false;
         if (e < n) {
-            uint32_t root = 0;
-            WalkRay r;
-            get_entry(sc, w.level_q[0], e, &slot, &root, &r);
-            const float4 o = r.o, iv = r.iv;
+            const uint2 q = w.level_q[0][e];
+            slot = q.x;
+            const uint32_t root = q.y;
+            const float4 o = w.ray_o[slot], iv = w.ray_i[slot];
             const float3 dv = make_float3(1.0f/iv.x, 1.0f/iv.y, 1.0f/iv.z);
             v3 s = mk(0, 0, 0), d = mk(0, 0, 0);
             double sd = 0.0;
