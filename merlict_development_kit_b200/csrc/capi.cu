@@ -5,6 +5,7 @@
 #include <algorithm>
 #include <cstring>
 #include <string>
+#include <mutex>
 #include <vector>
 
 #include "mlgpu_internal.h"
@@ -128,10 +129,19 @@ struct Profiler {
 constexpr int kHostChunks = 4;
 constexpr int kHostPieces = kHostChunks + 1;
 
+struct PendingUpload {
+    std::vector<char> bytes;
+    const void** out;
+};
+
 struct mlgpu_scene {
     int device = 0;
     DevScene dev;
     std::vector<void*> owned;        // device allocations of the scene
+    std::vector<PendingUpload> pending;   // arrays staged while the scene is built
+    void* arena = nullptr;           // the scene's read-only arrays, one allocation
+    size_t arena_bytes = 0;
+    bool l2_raised = false;          // this scene holds a raise of the persisting-L2 set-aside
     unsigned int* error_word = nullptr;
     // staging for mlgpu_propagate_host and scratch for binning
     DeviceBuffer staging_in, staging_out, staging_hist, staging_rng, bin_scratch, tune_out;
@@ -162,14 +172,39 @@ struct mlgpu_scene {
 
 namespace {
 
+// The scene's arrays are staged on the host while the scene is built and
+// then copied into one device allocation (the scene arena), so that a single
+// L2 access-policy window covers all of them.
 template <typename T>
 int upload(mlgpu_scene* s, const T* host, size_t count, const T** out) {
     if (count == 0) count = 1;
-    void* p = nullptr;
-    MLGPU_CUDA(cudaMalloc(&p, count*sizeof(T)));
-    s->owned.push_back(p);
-    if (host) MLGPU_CUDA(cudaMemcpy(p, host, count*sizeof(T), cudaMemcpyHostToDevice));
-    *out = static_cast<const T*>(p);
+    PendingUpload u;
+    u.bytes.assign(count*sizeof(T), 0);
+    if (host) std::memcpy(u.bytes.data(), host, count*sizeof(T));
+    u.out = reinterpret_cast<const void**>(out);
+    s->pending.push_back(std::move(u));
+    return MLGPU_OK;
+}
+
+// Allocates the arena, copies the staged arrays in (each on a 256-byte
+// boundary) and sets the device pointers.
+int finish_uploads(mlgpu_scene* s) {
+    size_t total = 0;
+    for (const PendingUpload& u : s->pending) total += (u.bytes.size() + 255) & ~size_t(255);
+    void* arena = nullptr;
+    MLGPU_CUDA(cudaMalloc(&arena, total));
+    s->owned.push_back(arena);
+    s->arena = arena;
+    s->arena_bytes = total;
+    std::vector<char> image(total, 0);
+    size_t at = 0;
+    for (const PendingUpload& u : s->pending) {
+        std::memcpy(image.data() + at, u.bytes.data(), u.bytes.size());
+        *u.out = static_cast<char*>(arena) + at;
+        at += (u.bytes.size() + 255) & ~size_t(255);
+    }
+    s->pending.clear();
+    MLGPU_CUDA(cudaMemcpy(arena, image.data(), total, cudaMemcpyHostToDevice));
     return MLGPU_OK;
 }
 
@@ -355,8 +390,8 @@ int build_device_scene(mlgpu_scene* s, const mlgpu_flat_scene* f) {
     }
     const unsigned int* ew = nullptr;
     if ((st = upload<unsigned int>(s, nullptr, 1, &ew))) return st;
+    if ((st = finish_uploads(s))) return st;
     s->error_word = const_cast<unsigned int*>(ew);
-    MLGPU_CUDA(cudaMemset(s->error_word, 0, sizeof(unsigned int)));
     s->dev.error_word = s->error_word;
     s->dev.num_nodes = nn;
     s->dev.num_leaves = nl;
@@ -414,6 +449,8 @@ int check_propagate_args(const mlgpu_scene* scene, const mlgpu_photons* ph,
         return fail(MLGPU_ERR_INVALID_ARGUMENT, "unknown walk %d", st->walk);
     if (st->queue_capacity != 0 && (st->queue_capacity < 32 || st->queue_capacity > (1u << 28)))
         return fail(MLGPU_ERR_INVALID_ARGUMENT, "queue_capacity must be 0 or in [32, 2^28]");
+    if (st->scene_l2 < MLGPU_L2_DEFAULT || st->scene_l2 > MLGPU_L2_OFF)
+        return fail(MLGPU_ERR_INVALID_ARGUMENT, "unknown scene_l2 %d", st->scene_l2);
     return MLGPU_OK;
 }
 
@@ -496,14 +533,85 @@ int wave_buffers(mlgpu_scene* scene, uint32_t pool, int grid, int staged, uint32
     return MLGPU_OK;
 }
 
+// The persisting-L2 set-aside of the context, shared by the scenes that
+// keep their arrays in L2: raised to the largest scene's need, restored to
+// the value found before the first raise when the last of them is destroyed.
+std::mutex g_l2_mutex;
+int g_l2_holders = 0;
+size_t g_l2_before = 0;
+
+// The access-policy window that marks the scene arena as persisting in L2
+// (num_bytes 0: none), raising the set-aside on first use.
+int scene_l2_window(mlgpu_scene* scene, bool on, cudaAccessPolicyWindow* out) {
+    std::memset(out, 0, sizeof(*out));
+    int max_window = 0, max_persist = 0;
+    cudaDeviceGetAttribute(&max_window, cudaDevAttrMaxAccessPolicyWindowSize, scene->device);
+    cudaDeviceGetAttribute(&max_persist, cudaDevAttrMaxPersistingL2CacheSize, scene->device);
+    if (on && max_window > 0 && max_persist > 0) {
+        const size_t window = std::min(scene->arena_bytes, (size_t)max_window);
+        const size_t aside = std::min(window, (size_t)max_persist);
+        {
+            std::lock_guard<std::mutex> lock(g_l2_mutex);
+            size_t current = 0;
+            MLGPU_CUDA(cudaDeviceGetLimit(&current, cudaLimitPersistingL2CacheSize));
+            if (!scene->l2_raised) {
+                if (g_l2_holders == 0) g_l2_before = current;
+                g_l2_holders++;
+                scene->l2_raised = true;
+            }
+            if (current < aside) MLGPU_CUDA(cudaDeviceSetLimit(cudaLimitPersistingL2CacheSize, aside));
+        }
+        out->base_ptr = scene->arena;
+        out->num_bytes = window;
+        out->hitRatio = (float)std::min(1.0, (double)aside/(double)window);
+        out->hitProp = cudaAccessPropertyPersisting;
+        out->missProp = cudaAccessPropertyStreaming;
+    }
+    return MLGPU_OK;
+}
+
+// Sets the window on every kernel node of a recorded graph.
+int apply_l2_window(cudaGraph_t graph, const cudaAccessPolicyWindow& window) {
+    size_t count = 0;
+    MLGPU_CUDA(cudaGraphGetNodes(graph, nullptr, &count));
+    std::vector<cudaGraphNode_t> nodes(count);
+    MLGPU_CUDA(cudaGraphGetNodes(graph, nodes.data(), &count));
+    cudaKernelNodeAttrValue v;
+    std::memset(&v, 0, sizeof(v));
+    v.accessPolicyWindow = window;
+    for (cudaGraphNode_t node : nodes) {
+        cudaGraphNodeType type;
+        MLGPU_CUDA(cudaGraphNodeGetType(node, &type));
+        if (type == cudaGraphNodeTypeKernel)
+            MLGPU_CUDA(cudaGraphKernelNodeSetAttribute(
+                node, cudaKernelNodeAttributeAccessPolicyWindow, &v));
+    }
+    return MLGPU_OK;
+}
+
+// Gives back a scene's raise of the set-aside (scene destruction).
+void release_scene_l2(mlgpu_scene* scene) {
+    if (!scene->l2_raised) return;
+    std::lock_guard<std::mutex> lock(g_l2_mutex);
+    scene->l2_raised = false;
+    if (--g_l2_holders == 0) {
+        cudaCtxResetPersistingL2Cache();
+        cudaDeviceSetLimit(cudaLimitPersistingL2CacheSize, g_l2_before);
+        cudaGetLastError();
+    }
+}
+
 // Records `period` wavefront iterations (starting from ray pool 0) and the
 // copy of the counters to the host as one CUDA graph, on the scene's private
 // stream, and makes it the scene's executable graph (updated in place when
 // the previous one has the same shape).
 int record_wave_graph(mlgpu_scene* scene, const TraceArgs& a, const WaveBuffers& w,
-                      const RayPool* pools, int form, int period) {
+                      const RayPool* pools, int form, int period, bool scene_l2_on) {
     if (!scene->capture_stream)
         MLGPU_CUDA(cudaStreamCreateWithFlags(&scene->capture_stream, cudaStreamNonBlocking));
+    cudaAccessPolicyWindow window;
+    const int l2 = scene_l2_window(scene, scene_l2_on, &window);
+    if (l2) return l2;
     cudaStream_t cs = scene->capture_stream;
     MLGPU_CUDA(cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal));
     cudaError_t e = cudaSuccess;
@@ -515,6 +623,13 @@ int record_wave_graph(mlgpu_scene* scene, const TraceArgs& a, const WaveBuffers&
     if (e != cudaSuccess || e2 != cudaSuccess) {
         if (graph) cudaGraphDestroy(graph);
         return cuda_fail(e != cudaSuccess ? e : e2, "recording the wavefront graph");
+    }
+    if (window.num_bytes > 0) {
+        const int r = apply_l2_window(graph, window);
+        if (r) {
+            cudaGraphDestroy(graph);
+            return r;
+        }
     }
     bool updated = false;
     if (scene->wave_graph) {
@@ -579,7 +694,8 @@ int run_wavefront(mlgpu_scene* scene, TraceArgs a, const mlgpu_settings* st,
     int period = st->check_period > 0 ? st->check_period : 4;
     if (graph && (period & 1)) period++;   // a graph starts and ends on ray pool 0
     if (graph) {
-        const int r = record_wave_graph(scene, a, w, pools, form, period);
+        const int r = record_wave_graph(scene, a, w, pools, form, period,
+                                        st->scene_l2 != MLGPU_L2_OFF);
         if (r) return r;
     }
     MLGPU_CUDA(cudaMemsetAsync(w.counters, 0, sizeof(WaveCounters), stream));
@@ -773,6 +889,7 @@ int mlgpu_scene_destroy(mlgpu_scene* scene) {
     if (scene->wave_host) cudaFreeHost(scene->wave_host);
     if (scene->wave_graph) cudaGraphExecDestroy(scene->wave_graph);
     if (scene->capture_stream) cudaStreamDestroy(scene->capture_stream);
+    release_scene_l2(scene);
     for (cudaStream_t hs : scene->host_stream)
         if (hs) cudaStreamDestroy(hs);
     for (cudaEvent_t he : scene->host_event)
@@ -839,6 +956,7 @@ int mlgpu_scene_autotune(mlgpu_scene* scene, const mlgpu_photons* sample, uint64
     cur.staged_levels = 0;
     cur.photon_order = MLGPU_ORDER_DEFAULT;
     cur.walk = MLGPU_WALK_DEFAULT;
+    cur.scene_l2 = MLGPU_L2_DEFAULT;
     double cur_ms = 0.0;
     st = time_of(cur, &cur_ms);
     // candidate values of each knob, tried one knob at a time
@@ -849,9 +967,10 @@ int mlgpu_scene_autotune(mlgpu_scene* scene, const mlgpu_photons* sample, uint64
     const int graphs[] = {0, 1};
     const int orders[] = {MLGPU_ORDER_INPUT, MLGPU_ORDER_COHERENT};
     const int walks[] = {MLGPU_WALK_LEVELS, MLGPU_WALK_STACK};
+    const int l2s[] = {MLGPU_L2_ON, MLGPU_L2_OFF};
     for (int pass = 0; pass < 2 && st == MLGPU_OK; pass++) {
         const double start_ms = cur_ms;
-        for (int knob = 0; knob < 7 && st == MLGPU_OK; knob++) {
+        for (int knob = 0; knob < 8 && st == MLGPU_OK; knob++) {
             const int count = knob <= 1 ? 4 : knob <= 3 ? 3 : 2;
             for (int c = 0; c < count && st == MLGPU_OK; c++) {
                 mlgpu_settings cand = cur;
@@ -865,7 +984,8 @@ int mlgpu_scene_autotune(mlgpu_scene* scene, const mlgpu_photons* sample, uint64
                 case 3: cand.staged_levels = stages[c]; break;
                 case 4: cand.use_graph = graphs[c]; break;
                 case 5: cand.photon_order = orders[c]; break;
-                default: cand.walk = walks[c]; break;
+                case 6: cand.walk = walks[c]; break;
+                default: cand.scene_l2 = l2s[c]; break;
                 }
                 if (std::memcmp(&cand, &cur, sizeof(cand)) == 0) continue;
                 double ms = 0.0;
