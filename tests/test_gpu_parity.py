@@ -335,3 +335,34 @@ def test_stack_walk_finds_the_same_hits(eng, oracle, name, n):
         if tracer == "fp64":
             assert mismatches(ref, got[2]) == {}
     scene.close()
+
+
+@pytest.mark.parametrize("n", [1_000_000, 40_000_000])
+def test_bin_arrivals_counters_wide_and_narrow(eng, n):
+    """The binning keeps 16-bit per-warp counters when no warp can count
+    past 65,535 photons in one slice and 32-bit ones otherwise; 4e7 arrivals
+    on a scene of few sensors take the 32-bit path, 1e6 the 16-bit one.
+    Both against numpy's bincount, with time histograms, one sensor taking
+    a tenth of all arrivals (more than 65,535 per warp and slice)."""
+    import torch
+    flat, _, _, _ = load_golden("light_field_small")
+    scene = eng.Scene(flat)
+    g = torch.Generator(device="cuda").manual_seed(5)
+    ns = flat.num_sensors
+    sensor = torch.randint(-1, ns, (n,), device="cuda", dtype=torch.int32, generator=g)
+    sensor[::10] = 3
+    time = torch.rand(n, device="cuda", dtype=torch.float64, generator=g) * 1e-8
+    counts, hist = scene.bin_arrivals(sensor, time, 5, 0.0, 1e-8)
+    s = sensor.cpu().numpy()
+    t = time.cpu().numpy()
+    ok = s >= 0
+    ref_counts = np.bincount(s[ok], minlength=ns)
+    f = (t[ok] - 0.0) / (1e-8 - 0.0) * 5.0
+    inside = (f >= 0.0) & (f < 5.0)
+    ref_hist = np.zeros((ns, 5), np.int64)
+    np.add.at(ref_hist, (s[ok][inside], f[inside].astype(np.int64)), 1)
+    assert np.array_equal(counts.cpu().numpy(), ref_counts)
+    assert np.array_equal(hist.cpu().numpy(), ref_hist)
+    counts2, _ = scene.bin_arrivals(sensor)
+    assert np.array_equal(counts2.cpu().numpy(), ref_counts)
+    scene.close()
