@@ -265,9 +265,6 @@ def run_ours(args, world, rank, local):
         sample = {k: v[:min(n, 2_000_000)].contiguous() for k, v in dev.items()}
         tuning, _ = scene.autotune(sample, cfg, engine.Philox(3), tracer=tracer)
         del sample
-    if args.scene_l2 != "auto":
-        tuning = dict(tuning or {})
-        tuning["scene_l2"] = 1 if args.scene_l2 == "on" else 2
 
     def step(ev=None):
         if ev is not None:
@@ -944,9 +941,6 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-forms", action="store_true",
                     help="skip the FP32 form's line items in the default workload")
-    ap.add_argument("--scene-l2", choices=["auto", "on", "off"], default="auto",
-                    help="keep the scene's arrays resident in L2 (mlgpu_settings.scene_l2); "
-                         "auto: the autotuner's choice (or the default, on)")
     ap.add_argument("--no-autotune", dest="autotune", action="store_false",
                     help="default wavefront knobs instead of mlgpu_scene_autotune's")
     ap.add_argument("--workload", choices=["telescope", "bunches", "precision", "surrogate",

@@ -32,7 +32,7 @@
 extern "C" {
 #endif
 
-#define MLGPU_ABI_VERSION 7
+#define MLGPU_ABI_VERSION 8
 
 /* ---- status codes ------------------------------------------------------ */
 enum {
@@ -246,19 +246,7 @@ typedef struct mlgpu_settings {
                                walk instead (same results); a small capacity
                                only makes that fallback common.  0 or at
                                least 32.                                     */
-    int32_t scene_l2;       /* MLGPU_L2_*: keep the scene's arrays resident in L2
-                               during wavefront propagation                   */
 } mlgpu_settings;
-
-/* scene_l2: ON marks the scene's arrays (one allocation) as persisting in
- * L2 for the wavefront graph launches, so that the rays, queues and results
- * streaming through the cache do not evict the leaf records and tree nodes
- * every ray gathers.  It raises the current context's persisting-L2
- * set-aside (cudaLimitPersistingL2CacheSize) to the scene's size, at most
- * the device's maximum, and restores the earlier value when the last scene
- * that raised it is destroyed.  A setting of the process's context only:
- * nothing of it outlasts the process.  DEFAULT is ON.                       */
-enum { MLGPU_L2_DEFAULT = 0, MLGPU_L2_ON = 1, MLGPU_L2_OFF = 2 };
 
 /* walk: LEVELS runs one kernel per BVH level over queued (ray, node) pairs
  * and one over the hit leaf ranges; STACK walks each ray's whole BVH in one

@@ -11,7 +11,7 @@ from dataclasses import dataclass, field
 
 import numpy as np
 
-ABI_VERSION = 7
+ABI_VERSION = 8
 
 # status codes
 OK = 0
@@ -228,9 +228,6 @@ WALK_DEFAULT = 0
 WALK_LEVELS = 1
 WALK_STACK = 2
 
-L2_DEFAULT = 0
-L2_ON = 1
-L2_OFF = 2
 
 
 class mlgpu_settings(C.Structure):
@@ -248,11 +245,10 @@ class mlgpu_settings(C.Structure):
         ("photon_order", C.c_int32),
         ("walk", C.c_int32),
         ("queue_capacity", C.c_uint32),
-        ("scene_l2", C.c_int32),
     ]
 
     TUNING = ("pool_size", "check_period", "use_graph", "grid_blocks", "staged_levels",
-              "photon_order", "walk", "queue_capacity", "scene_l2")
+              "photon_order", "walk", "queue_capacity")
 
     def tuning(self) -> dict:
         return {k: int(getattr(self, k)) for k in self.TUNING}

@@ -141,7 +141,6 @@ struct mlgpu_scene {
     std::vector<PendingUpload> pending;   // arrays staged while the scene is built
     void* arena = nullptr;           // the scene's read-only arrays, one allocation
     size_t arena_bytes = 0;
-    bool l2_raised = false;          // this scene holds a raise of the persisting-L2 set-aside
     unsigned int* error_word = nullptr;
     // staging for mlgpu_propagate_host and scratch for binning
     DeviceBuffer staging_in, staging_out, staging_hist, staging_rng, bin_scratch, tune_out;
@@ -381,6 +380,23 @@ int build_device_scene(mlgpu_scene* s, const mlgpu_flat_scene* f) {
             for (int k = 0; k <= kMaxBvhLevels; k++)
                 s->dev.bvh_level_start[k] = k <= bvh.levels ? bvh.level_start[k] : s->dev.bvh_nodes;
         }
+        // the candidate records in slot order (the BVH's leaf order; every
+        // leaf with geometry has a slot)
+        {
+            const size_t slots = bvh.leaf_ids.size();
+            const size_t blocks = (slots + 7)/8;
+            std::vector<double2> rec(blocks*96 > 0 ? blocks*96 : 1, make_double2(0.0, 0.0));
+            std::vector<int32_t> leaf_slot(nl > 0 ? nl : 1, -1);
+            for (size_t j = 0; j < slots; j++) {
+                const double2* r = reinterpret_cast<const double2*>(&leaf[bvh.leaf_ids[j]]);
+                for (int pr = 0; pr < 12; pr++) rec[(j >> 3)*96 + pr*8 + (j & 7)] = r[pr];
+                leaf_slot[bvh.leaf_ids[j]] = (int32_t)j;
+            }
+            if ((st = upload(s, rec.data(), rec.size(), &s->dev.slot_rec))) return st;
+            if ((st = upload(s, bvh.leaf_ids.data(), bvh.leaf_ids.size(), &s->dev.slot_leaf))) return st;
+            if ((st = upload(s, leaf_slot.data(), leaf_slot.size(), &s->dev.leaf_slot))) return st;
+            s->dev.num_slots = (int32_t)slots;
+        }
         // a tree deeper than the walk's level queues: merlict's frame walk
         if (s->dev.bvh_levels >= kMaxBvhLevels) {
             s->dev.bvh_nodes = 0;
@@ -449,8 +465,6 @@ int check_propagate_args(const mlgpu_scene* scene, const mlgpu_photons* ph,
         return fail(MLGPU_ERR_INVALID_ARGUMENT, "unknown walk %d", st->walk);
     if (st->queue_capacity != 0 && (st->queue_capacity < 32 || st->queue_capacity > (1u << 28)))
         return fail(MLGPU_ERR_INVALID_ARGUMENT, "queue_capacity must be 0 or in [32, 2^28]");
-    if (st->scene_l2 < MLGPU_L2_DEFAULT || st->scene_l2 > MLGPU_L2_OFF)
-        return fail(MLGPU_ERR_INVALID_ARGUMENT, "unknown scene_l2 %d", st->scene_l2);
     return MLGPU_OK;
 }
 
@@ -521,6 +535,7 @@ int wave_buffers(mlgpu_scene* scene, uint32_t pool, int grid, int staged, uint32
     w->level_q[1] = reinterpret_cast<uint2*>(take(level_cap*8));
     w->level_cap = (uint32_t)level_cap;
     w->isect_q = reinterpret_cast<uint2*>(take(isect_cap*8));
+    w->slot_leaf_of = scene->dev.slot_leaf;
     w->isect_dist = reinterpret_cast<double*>(take(isect_cap*8));
     w->isect_cap = (uint32_t)isect_cap;
     w->best_key = reinterpret_cast<unsigned long long*>(take(P*8));
@@ -533,85 +548,14 @@ int wave_buffers(mlgpu_scene* scene, uint32_t pool, int grid, int staged, uint32
     return MLGPU_OK;
 }
 
-// The persisting-L2 set-aside of the context, shared by the scenes that
-// keep their arrays in L2: raised to the largest scene's need, restored to
-// the value found before the first raise when the last of them is destroyed.
-std::mutex g_l2_mutex;
-int g_l2_holders = 0;
-size_t g_l2_before = 0;
-
-// The access-policy window that marks the scene arena as persisting in L2
-// (num_bytes 0: none), raising the set-aside on first use.
-int scene_l2_window(mlgpu_scene* scene, bool on, cudaAccessPolicyWindow* out) {
-    std::memset(out, 0, sizeof(*out));
-    int max_window = 0, max_persist = 0;
-    cudaDeviceGetAttribute(&max_window, cudaDevAttrMaxAccessPolicyWindowSize, scene->device);
-    cudaDeviceGetAttribute(&max_persist, cudaDevAttrMaxPersistingL2CacheSize, scene->device);
-    if (on && max_window > 0 && max_persist > 0) {
-        const size_t window = std::min(scene->arena_bytes, (size_t)max_window);
-        const size_t aside = std::min(window, (size_t)max_persist);
-        {
-            std::lock_guard<std::mutex> lock(g_l2_mutex);
-            size_t current = 0;
-            MLGPU_CUDA(cudaDeviceGetLimit(&current, cudaLimitPersistingL2CacheSize));
-            if (!scene->l2_raised) {
-                if (g_l2_holders == 0) g_l2_before = current;
-                g_l2_holders++;
-                scene->l2_raised = true;
-            }
-            if (current < aside) MLGPU_CUDA(cudaDeviceSetLimit(cudaLimitPersistingL2CacheSize, aside));
-        }
-        out->base_ptr = scene->arena;
-        out->num_bytes = window;
-        out->hitRatio = (float)std::min(1.0, (double)aside/(double)window);
-        out->hitProp = cudaAccessPropertyPersisting;
-        out->missProp = cudaAccessPropertyStreaming;
-    }
-    return MLGPU_OK;
-}
-
-// Sets the window on every kernel node of a recorded graph.
-int apply_l2_window(cudaGraph_t graph, const cudaAccessPolicyWindow& window) {
-    size_t count = 0;
-    MLGPU_CUDA(cudaGraphGetNodes(graph, nullptr, &count));
-    std::vector<cudaGraphNode_t> nodes(count);
-    MLGPU_CUDA(cudaGraphGetNodes(graph, nodes.data(), &count));
-    cudaKernelNodeAttrValue v;
-    std::memset(&v, 0, sizeof(v));
-    v.accessPolicyWindow = window;
-    for (cudaGraphNode_t node : nodes) {
-        cudaGraphNodeType type;
-        MLGPU_CUDA(cudaGraphNodeGetType(node, &type));
-        if (type == cudaGraphNodeTypeKernel)
-            MLGPU_CUDA(cudaGraphKernelNodeSetAttribute(
-                node, cudaKernelNodeAttributeAccessPolicyWindow, &v));
-    }
-    return MLGPU_OK;
-}
-
-// Gives back a scene's raise of the set-aside (scene destruction).
-void release_scene_l2(mlgpu_scene* scene) {
-    if (!scene->l2_raised) return;
-    std::lock_guard<std::mutex> lock(g_l2_mutex);
-    scene->l2_raised = false;
-    if (--g_l2_holders == 0) {
-        cudaCtxResetPersistingL2Cache();
-        cudaDeviceSetLimit(cudaLimitPersistingL2CacheSize, g_l2_before);
-        cudaGetLastError();
-    }
-}
-
 // Records `period` wavefront iterations (starting from ray pool 0) and the
 // copy of the counters to the host as one CUDA graph, on the scene's private
 // stream, and makes it the scene's executable graph (updated in place when
 // the previous one has the same shape).
 int record_wave_graph(mlgpu_scene* scene, const TraceArgs& a, const WaveBuffers& w,
-                      const RayPool* pools, int form, int period, bool scene_l2_on) {
+                      const RayPool* pools, int form, int period) {
     if (!scene->capture_stream)
         MLGPU_CUDA(cudaStreamCreateWithFlags(&scene->capture_stream, cudaStreamNonBlocking));
-    cudaAccessPolicyWindow window;
-    const int l2 = scene_l2_window(scene, scene_l2_on, &window);
-    if (l2) return l2;
     cudaStream_t cs = scene->capture_stream;
     MLGPU_CUDA(cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal));
     cudaError_t e = cudaSuccess;
@@ -623,13 +567,6 @@ int record_wave_graph(mlgpu_scene* scene, const TraceArgs& a, const WaveBuffers&
     if (e != cudaSuccess || e2 != cudaSuccess) {
         if (graph) cudaGraphDestroy(graph);
         return cuda_fail(e != cudaSuccess ? e : e2, "recording the wavefront graph");
-    }
-    if (window.num_bytes > 0) {
-        const int r = apply_l2_window(graph, window);
-        if (r) {
-            cudaGraphDestroy(graph);
-            return r;
-        }
     }
     bool updated = false;
     if (scene->wave_graph) {
@@ -694,8 +631,7 @@ int run_wavefront(mlgpu_scene* scene, TraceArgs a, const mlgpu_settings* st,
     int period = st->check_period > 0 ? st->check_period : 4;
     if (graph && (period & 1)) period++;   // a graph starts and ends on ray pool 0
     if (graph) {
-        const int r = record_wave_graph(scene, a, w, pools, form, period,
-                                        st->scene_l2 != MLGPU_L2_OFF);
+        const int r = record_wave_graph(scene, a, w, pools, form, period);
         if (r) return r;
     }
     MLGPU_CUDA(cudaMemsetAsync(w.counters, 0, sizeof(WaveCounters), stream));
@@ -889,7 +825,6 @@ int mlgpu_scene_destroy(mlgpu_scene* scene) {
     if (scene->wave_host) cudaFreeHost(scene->wave_host);
     if (scene->wave_graph) cudaGraphExecDestroy(scene->wave_graph);
     if (scene->capture_stream) cudaStreamDestroy(scene->capture_stream);
-    release_scene_l2(scene);
     for (cudaStream_t hs : scene->host_stream)
         if (hs) cudaStreamDestroy(hs);
     for (cudaEvent_t he : scene->host_event)
@@ -956,7 +891,6 @@ int mlgpu_scene_autotune(mlgpu_scene* scene, const mlgpu_photons* sample, uint64
     cur.staged_levels = 0;
     cur.photon_order = MLGPU_ORDER_DEFAULT;
     cur.walk = MLGPU_WALK_DEFAULT;
-    cur.scene_l2 = MLGPU_L2_DEFAULT;
     double cur_ms = 0.0;
     st = time_of(cur, &cur_ms);
     // candidate values of each knob, tried one knob at a time
@@ -967,10 +901,9 @@ int mlgpu_scene_autotune(mlgpu_scene* scene, const mlgpu_photons* sample, uint64
     const int graphs[] = {0, 1};
     const int orders[] = {MLGPU_ORDER_INPUT, MLGPU_ORDER_COHERENT};
     const int walks[] = {MLGPU_WALK_LEVELS, MLGPU_WALK_STACK};
-    const int l2s[] = {MLGPU_L2_ON, MLGPU_L2_OFF};
     for (int pass = 0; pass < 2 && st == MLGPU_OK; pass++) {
         const double start_ms = cur_ms;
-        for (int knob = 0; knob < 8 && st == MLGPU_OK; knob++) {
+        for (int knob = 0; knob < 7 && st == MLGPU_OK; knob++) {
             const int count = knob <= 1 ? 4 : knob <= 3 ? 3 : 2;
             for (int c = 0; c < count && st == MLGPU_OK; c++) {
                 mlgpu_settings cand = cur;
@@ -984,8 +917,7 @@ int mlgpu_scene_autotune(mlgpu_scene* scene, const mlgpu_photons* sample, uint64
                 case 3: cand.staged_levels = stages[c]; break;
                 case 4: cand.use_graph = graphs[c]; break;
                 case 5: cand.photon_order = orders[c]; break;
-                case 6: cand.walk = walks[c]; break;
-                default: cand.scene_l2 = l2s[c]; break;
+                default: cand.walk = walks[c]; break;
                 }
                 if (std::memcmp(&cand, &cur, sizeof(cand)) == 0) continue;
                 double ms = 0.0;

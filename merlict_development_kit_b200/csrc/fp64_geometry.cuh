@@ -428,6 +428,35 @@ __device__ __forceinline__ void load_leaf(const LeafRec* L, double* T, double* t
     if (np > 5) { const double2 x = __ldg(q + 11); pr[5] = x.x; pr[6] = x.y; }
 }
 
+// load_leaf on the slot-ordered candidate records (DevScene::slot_rec):
+// the same twelve pairs, the same selection by parameter count.
+__device__ __forceinline__ void load_leaf_slot(const DevScene& sc, uint32_t j, double* T,
+                                               double* ti, double* pr, double* r2,
+                                               int32_t* prim) {
+    const double2* q = sc.slot_rec + (size_t)(j >> 3)*96 + (j & 7);
+    double v[14];
+#pragma unroll
+    for (int k = 0; k < 7; k++) {
+        const double2 x = __ldg(q + 8*k);
+        v[2*k] = x.x;
+        v[2*k + 1] = x.y;
+    }
+    const double2 tail = __ldg(q + 8*7);                   // tinv[2], primitive | sensor
+    const double2 r2p0 = __ldg(q + 8*8);                   // r2, params[0]
+#pragma unroll
+    for (int k = 0; k < 12; k++) T[k] = v[k];
+    ti[0] = v[12]; ti[1] = v[13]; ti[2] = tail.x;
+    *prim = (int32_t)(uint32_t)(__double_as_longlong(tail.y) & 0xffffffffll);
+    *r2 = r2p0.x;
+    pr[0] = r2p0.y;
+#pragma unroll
+    for (int k = 1; k < MLGPU_LEAF_PARAMS; k++) pr[k] = 0.0;
+    const int np = primitive_params(*prim);
+    if (np > 1) { const double2 x = __ldg(q + 8*9); pr[1] = x.x; pr[2] = x.y; }
+    if (np > 3) { const double2 x = __ldg(q + 8*10); pr[3] = x.x; pr[4] = x.y; }
+    if (np > 5) { const double2 x = __ldg(q + 8*11); pr[5] = x.x; pr[6] = x.y; }
+}
+
 __device__ __forceinline__ Isec leaf_hit(const DevScene& sc, int32_t leaf, v3 s, v3 d) {
     double T[12], ti[3], pr[MLGPU_LEAF_PARAMS], r2;
     int32_t prim;

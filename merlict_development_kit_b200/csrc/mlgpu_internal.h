@@ -108,6 +108,15 @@ struct DevScene {
     // BVH over the leaves with geometry (empty: walk the frame tree)
     const BvhNode* bvh;
     const int32_t* bvh_leaf;
+    // The candidate records: the first 192 bytes of the leaf record of
+    // every leaf with geometry, in slot order (the BVH's leaf order), eight
+    // slots to a block of 96 double2 holding pair p of slot 8b + i at
+    // 96 b + 8 p + i -- the up to eight leaves of a leaf range, tested by
+    // neighbouring lanes, share one 128-byte line per pair.
+    const double2* slot_rec;
+    const int32_t* slot_leaf;   // [slots] leaf of each slot
+    const int32_t* leaf_slot;   // [num_leaves] slot of each leaf, -1: no geometry
+    int32_t num_slots;
     const double4* bvh_sphere;  // per BVH leaf slot: world centre and radius^2 of that leaf
     const float4* bvh_sphere_f; // the same in FP32: centre (rounded) and radius (rounded up)
     int32_t bvh_nodes;
@@ -203,7 +212,8 @@ struct WaveBuffers {
     float4* ray_i;           // [pool] reciprocal direction
     uint2* level_q[2];       // (slot, node) pairs, ping-pong between BVH levels
     uint32_t level_cap;
-    uint2* isect_q;          // (slot, leaf) candidates
+    uint2* isect_q;          // (ray slot, leaf slot) candidates
+    const int32_t* slot_leaf_of;   // the scene's slot -> leaf map (DevScene::slot_leaf)
     double* isect_dist;      // distance to each candidate's hit, -1: none
     uint32_t isect_cap;
     unsigned long long* best_key;   // [pool] smallest hit distance (bits of a positive double)

@@ -104,25 +104,25 @@ wave_isect_kernel(const TraceArgs a, const WaveBuffers w, const RayPool cur) {
     for (uint32_t e = blockIdx.x*blockDim.x + threadIdx.x; e < n; e += gridDim.x*blockDim.x) {
         const uint2 q = w.isect_q[e];
         const uint32_t slot = q.x;
-        const int32_t leaf = (int32_t)q.y;
         v3 s, d;
         load_ray(w, slot, &s, &d);
         double dist = -1.0;
         if (kIsect == kIsectFp64) {
             double T[12], ti[3], pr[MLGPU_LEAF_PARAMS], r2;
             int32_t prim;
-            load_leaf(sc.leaf + leaf, T, ti, pr, &r2, &prim);
+            load_leaf_slot(sc, q.y, T, ti, pr, &r2, &prim);
             // merlict's bounding-sphere test of the leaf (RayAndFrame.cpp:
             // 16-107; the sphere is centred on the frame's position,
             // Frame::position_in_world): the walk proposed the leaf with a
             // conservative single-precision version of it
             if (sphere_cull(make_double4(T[3], T[7], T[11], r2), s, d, dot(s, d))) {
                 Isec h;
-                intersect_leaf(sc, leaf, prim, pr, r2, position_inverse(T, ti, s),
+                intersect_leaf(sc, (int32_t)q.y, prim, pr, r2, position_inverse(T, ti, s),
                                orientation_inverse(T, d), &h);
                 if (h.leaf >= 0) dist = h.dist;
             }
         } else {
+            const int32_t leaf = __ldg(sc.slot_leaf + q.y);
             const fp32::Hit32 h = fp32::intersect32<false>(sc, leaf, fp32::dmk(s.x, s.y, s.z),
                                                     fp32::dmk(d.x, d.y, d.z),
                                                     kIsect == kIsectFp32Pure);
@@ -141,7 +141,7 @@ wave_tie_kernel(const WaveBuffers w) {
         if (!(dist >= 0.0)) continue;
         const uint2 q = w.isect_q[e];
         if ((unsigned long long)__double_as_longlong(dist) == w.best_key[q.x])
-            atomicMin(&w.best_leaf[q.x], (int32_t)q.y);
+            atomicMin(&w.best_leaf[q.x], __ldg(w.slot_leaf_of + q.y));
     }
 }
 

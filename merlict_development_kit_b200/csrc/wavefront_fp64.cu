@@ -111,8 +111,13 @@ wave_intake_kernel(const TraceArgs a, const WaveBuffers w, const RayPool cur) {
                         continue;
                     }
                     if (meta.y >= 0) {
-                        if (nc < kTreeCands) cand[nc++] = meta.y;
-                        else over = true;
+                        // candidates by slot; a leaf without geometry has none
+                        // (and no intersection in merlict either)
+                        const int32_t sl = __ldg(sc.leaf_slot + meta.y);
+                        if (sl >= 0) {
+                            if (nc < kTreeCands) cand[nc++] = sl;
+                            else over = true;
+                        }
                     }
                     i++;
                 }
@@ -319,7 +324,7 @@ wave_level_kernel(const TraceArgs a, const WaveBuffers w, int level, int staged)
                 const int32_t count = (rref & 7) + 1;
                 if (k < count && sphere_cull32(__ldg(sc.bvh_sphere_f + start + k), o, dv)) {
                     pass = true;
-                    leaf = __ldg(sc.bvh_leaf + start + k);
+                    leaf = start + k;   // the leaf's slot
                 }
             }
             const uint32_t cb = warp_reserve(&w.counters->isect_len, pass ? 1u : 0u);
@@ -395,7 +400,7 @@ wave_walk_kernel(const TraceArgs a, const WaveBuffers w, const RayPool cur) {
                             pass = sphere_cull(make_double4(c01.x, c01.y, c23.x, c23.y), s, d, sd);
                         }
                         if (pass) {
-                            if (nc < (uint32_t)kWalkCands) cand[nc++] = __ldg(sc.bvh_leaf + j);
+                            if (nc < (uint32_t)kWalkCands) cand[nc++] = j;   // the leaf's slot
                             else over = true;
                         }
                     }

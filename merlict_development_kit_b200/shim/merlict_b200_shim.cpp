@@ -8,6 +8,7 @@
 #include <map>
 #include <mutex>
 #include <stdexcept>
+#include <string>
 
 namespace merlict_b200 {
 namespace ml = merlict;
@@ -35,6 +36,12 @@ std::map<std::pair<const ml::Frame*, const ml::sensor::Sensors*>, DeviceScene*> 
 
 DeviceScene* scene_for(const ml::Frame* world, const ml::sensor::Sensors* sensors) {
     std::lock_guard<std::mutex> lock(cache_mutex);
+    // the engine's structs must be the ones this file was compiled against
+    if (mlgpu_abi_version() != MLGPU_ABI_VERSION)
+        throw std::runtime_error(
+            "merlict_b200: libmerlict_b200.so has ABI version " +
+            std::to_string(mlgpu_abi_version()) + ", this drop-in was built for " +
+            std::to_string(MLGPU_ABI_VERSION) + "; rebuild the drop-in");
     const auto key = std::make_pair(world->root(), sensors);
     auto it = cache.find(key);
     if (it != cache.end()) return it->second;
