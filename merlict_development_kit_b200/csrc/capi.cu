@@ -506,7 +506,7 @@ int wave_buffers(mlgpu_scene* scene, uint32_t pool, int grid, int staged, uint32
     const size_t isect_cap = queue_cap ? queue_cap : 16*P;
     const size_t per_pool = 8*up(P*8) + 5*up(P*4);
     const size_t rest = up(P*4) + 2*up(P*16) + up(P*48) + 2*up(level_cap*8) +
-        up(isect_cap*8) + up(P*16) + 2*up(P*4);
+        up(isect_cap*8) + up(isect_cap*8) + up(P*8) + 3*up(P*4);
     MLGPU_CUDA(scene->wave.reserve(256 + 2*per_pool + rest));
     if (!scene->wave_host) MLGPU_CUDA(cudaMallocHost(&scene->wave_host, sizeof(WaveCounters)));
     if (!scene->wave_host_dev)
@@ -536,8 +536,10 @@ int wave_buffers(mlgpu_scene* scene, uint32_t pool, int grid, int staged, uint32
     w->level_cap = (uint32_t)level_cap;
     w->isect_q = reinterpret_cast<uint2*>(take(isect_cap*8));
     w->slot_leaf_of = scene->dev.slot_leaf;
+    w->isect_dist = reinterpret_cast<double*>(take(isect_cap*8));
     w->isect_cap = (uint32_t)isect_cap;
-    w->best = reinterpret_cast<ulonglong2*>(take(P*16));
+    w->best_key = reinterpret_cast<unsigned long long*>(take(P*8));
+    w->best_leaf = reinterpret_cast<int32_t*>(take(P*4));
     w->overflow = reinterpret_cast<uint32_t*>(take(P*4));
     w->overflow_flag = reinterpret_cast<uint32_t*>(take(P*4));
     const size_t fn_bytes = (size_t)scene->dev.num_fn_points*3*sizeof(double) +
@@ -636,15 +638,15 @@ int run_wavefront(mlgpu_scene* scene, TraceArgs a, const mlgpu_settings* st,
     // every iteration advances each live photon by one step
     const uint64_t bound = (a.num_photons*(uint64_t)(a.max_interactions + 1))/pool +
         a.max_interactions + 16 + (uint64_t)period;
-    // launches per iteration: intake and its counters, the walk, intersections,
-    // the overflow walk, resolve and its counters
+    // launches per iteration: intake and its counters, the walk, intersections
+    // and ties, the overflow walk, resolve and its counters
     const int walk_launches = w.walk == MLGPU_WALK_STACK ? 1 : scene->dev.bvh_levels;
     uint64_t iteration = 0;
     while (true) {
         if (graph) {
             MLGPU_CUDA(cudaGraphLaunch(scene->wave_graph, stream));
             iteration += (uint64_t)period;
-            scene->launches += (uint64_t)period*((uint64_t)walk_launches + 6) + 1;
+            scene->launches += (uint64_t)period*((uint64_t)walk_launches + 7) + 1;
         } else {
             for (int g = 0; g < period; g++, iteration++) {
                 const RayPool& cur = pools[iteration & 1];
@@ -654,12 +656,12 @@ int run_wavefront(mlgpu_scene* scene, TraceArgs a, const mlgpu_settings* st,
                 const cudaError_t e = launch_wave_iteration(a, w, cur, nxt, form, stream,
                                                             timed ? ch.ev : nullptr);
                 if (e != cudaSuccess) return cuda_fail(e, "wavefront kernels");
-                scene->launches += (uint64_t)walk_launches + 6;
+                scene->launches += (uint64_t)walk_launches + 7;
                 if (timed) {
                     ch.n = 5;
                     const int cls[4] = {MLGPU_KERNEL_INTAKE, MLGPU_KERNEL_WALK,
                                         MLGPU_KERNEL_INTERSECT, MLGPU_KERNEL_RESOLVE};
-                    const int launches[4] = {2, walk_launches, 1, 3};
+                    const int launches[4] = {2, walk_launches, 2, 3};
                     for (int k = 0; k < 4; k++) { ch.cls[k] = cls[k]; ch.launches[k] = launches[k]; }
                     scene->prof.add(ch);
                 }

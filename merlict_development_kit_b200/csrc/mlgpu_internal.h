@@ -214,8 +214,10 @@ struct WaveBuffers {
     uint32_t level_cap;
     uint2* isect_q;          // (ray slot, leaf slot) candidates
     const int32_t* slot_leaf_of;   // the scene's slot -> leaf map (DevScene::slot_leaf)
+    double* isect_dist;      // distance to each candidate's hit, -1: none
     uint32_t isect_cap;
-    ulonglong2* best;        // [pool] closest hit: (distance bits, leaf), the smallest pair
+    unsigned long long* best_key;   // [pool] smallest hit distance (bits of a positive double)
+    int32_t* best_leaf;      // [pool] leaf of the closest hit, lowest index on ties
     uint32_t* overflow;      // [pool] slots for merlict's own walk
     uint32_t* overflow_flag; // [pool]
 };

@@ -1,11 +1,12 @@
 // wave_resolve.cuh -- the per-candidate and per-slot steps of the wavefront
 // tracers, shared by the FP64 and FP32 forms:
 //   intersect  one thread per (ray, candidate leaf): the distance to the
-//              leaf's hit; each ray keeps the smallest (distance, leaf) pair
-//              of its hits with a 128-bit compare-and-swap (positive doubles
-//              order like their bit patterns; at equal distances the lowest
-//              leaf index wins, which is the leaf merlict visits first,
-//              RayAndFrame.cpp:160-173);
+//              leaf's hit; the smallest distance of each ray is kept with a
+//              64-bit atomic minimum on its bits (positive doubles order like
+//              their bit patterns);
+//   ties       one thread per candidate: among the candidates at exactly that
+//              distance the lowest leaf index wins, which is the leaf merlict
+//              visits first (RayAndFrame.cpp:160-173);
 //   overflow   rays whose walk overflowed a queue get merlict's own walk of
 //              the frame tree;
 //   resolve    one thread per ray: the winner's full intersection, recomputed
@@ -36,7 +37,7 @@ using namespace fp64;
 
 constexpr unsigned kFull = 0xffffffffu;
 constexpr int kNoStep = -2;             // step state: the photon takes no step
-constexpr int32_t kNoLeaf = INT32_MAX;  // best leaf of a ray without a hit
+constexpr int32_t kNoLeaf = INT32_MAX;  // best_leaf of a ray without a hit
 constexpr unsigned long long kNoKey = ~0ull;
 
 constexpr int kIsectFp64 = 0;
@@ -95,37 +96,6 @@ __device__ __forceinline__ void load_ray(const WaveBuffers& w, uint32_t slot, v3
     *d = mk(b.y, c.x, c.y);
 }
 
-// One 128-bit compare-and-swap on global memory: returns whether *addr
-// held `cmp` (then it holds `val`); `seen` receives what it held.
-__device__ __forceinline__ bool cas128(ulonglong2* addr, ulonglong2 cmp, ulonglong2 val,
-                                       ulonglong2* seen) {
-    unsigned long long lo, hi;
-    asm volatile("{\n\t.reg .b128 d, c, n;\n\t"
-                 "mov.b128 c, {%2, %3};\n\t"
-                 "mov.b128 n, {%4, %5};\n\t"
-                 "atom.global.cas.b128 d, [%6], c, n;\n\t"
-                 "mov.b128 {%0, %1}, d;\n\t}"
-                 : "=l"(lo), "=l"(hi)
-                 : "l"(cmp.x), "l"(cmp.y), "l"(val.x), "l"(val.y), "l"(addr)
-                 : "memory");
-    *seen = make_ulonglong2(lo, hi);
-    return lo == cmp.x && hi == cmp.y;
-}
-
-// Lowers a ray's closest hit to (distance bits, leaf) if that pair is
-// smaller (distance first, then leaf).  Each failed exchange returns a
-// smaller pair than the one tried, so the loop ends after at most as many
-// rounds as other candidates of the ray lowered the pair meanwhile.
-__device__ __forceinline__ void lower_best(ulonglong2* best, unsigned long long key,
-                                           unsigned long long leaf) {
-    ulonglong2 cur = __ldcg(best);   // from L2: another candidate may have lowered it
-    while (key < cur.x || (key == cur.x && leaf < cur.y)) {
-        ulonglong2 seen;
-        if (cas128(best, cur, make_ulonglong2(key, leaf), &seen)) break;
-        cur = seen;
-    }
-}
-
 template <int kIsect>
 __global__ void __launch_bounds__(256)
 wave_isect_kernel(const TraceArgs a, const WaveBuffers w, const RayPool cur) {
@@ -158,9 +128,20 @@ wave_isect_kernel(const TraceArgs a, const WaveBuffers w, const RayPool cur) {
                                                     kIsect == kIsectFp32Pure);
             if (h.leaf >= 0) dist = h.v;
         }
-        if (dist >= 0.0)
-            lower_best(w.best + slot, (unsigned long long)__double_as_longlong(dist),
-                       (unsigned long long)(uint32_t)__ldg(w.slot_leaf_of + q.y));
+        w.isect_dist[e] = dist;
+        if (dist >= 0.0) atomicMin(&w.best_key[slot], (unsigned long long)__double_as_longlong(dist));
+    }
+}
+
+__global__ void __launch_bounds__(256)
+wave_tie_kernel(const WaveBuffers w) {
+    const uint32_t n = w.counters->isect_len < w.isect_cap ? w.counters->isect_len : w.isect_cap;
+    for (uint32_t e = blockIdx.x*blockDim.x + threadIdx.x; e < n; e += gridDim.x*blockDim.x) {
+        const double dist = w.isect_dist[e];
+        if (!(dist >= 0.0)) continue;
+        const uint2 q = w.isect_q[e];
+        if ((unsigned long long)__double_as_longlong(dist) == w.best_key[q.x])
+            atomicMin(&w.best_leaf[q.x], __ldg(w.slot_leaf_of + q.y));
     }
 }
 
@@ -174,7 +155,7 @@ wave_overflow_kernel(const TraceArgs a, const WaveBuffers w, const RayPool cur) 
         const v3 s = mk(cur.sx[slot], cur.sy[slot], cur.sz[slot]);
         const v3 d = mk(cur.dx[slot], cur.dy[slot], cur.dz[slot]);
         const Isec is = first_intersection_tree(a.scene, cur.root[slot], s, d);
-        w.best[slot].y = (unsigned long long)(is.leaf >= 0 ? is.leaf : kNoLeaf);
+        w.best_leaf[slot] = is.leaf >= 0 ? is.leaf : kNoLeaf;
     }
 }
 
@@ -246,7 +227,7 @@ wave_resolve_kernel(const TraceArgs a, const WaveBuffers w, const RayPool cur, c
             {
                 // the winner of the intersection and tie kernels (or of
                 // merlict's own walk), recomputed by the same code
-                const int32_t best = (int32_t)w.best[slot].y;
+                const int32_t best = w.best_leaf[slot];
                 if (best == kNoLeaf) {
                     set_void(&is, s, d);
                 } else if (kIsect == kIsectFp64) {

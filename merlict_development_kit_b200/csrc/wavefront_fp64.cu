@@ -88,7 +88,8 @@ wave_intake_kernel(const TraceArgs a, const WaveBuffers w, const RayPool cur) {
         w.ray_sd[3*slot] = make_double2(s.x, s.y);
         w.ray_sd[3*slot + 1] = make_double2(s.z, d.x);
         w.ray_sd[3*slot + 2] = make_double2(d.y, d.z);
-        w.best[slot] = make_ulonglong2(kNoKey, (unsigned long long)kNoLeaf);
+        w.best_key[slot] = kNoKey;
+        w.best_leaf[slot] = kNoLeaf;
         w.overflow_flag[slot] = 0u;
         if (n_int > max_int) {
             w.step[slot] = kNoStep;
@@ -479,6 +480,7 @@ cudaError_t launch_wave_iteration(const TraceArgs& a, const WaveBuffers& w, cons
     if (ev) cudaEventRecord(ev[2], s);
     if (form == MLGPU_TRACER_FP64) {
         wave_isect_kernel<kIsectFp64><<<w.grid, 256, 0, s>>>(a, w, cur);
+        wave_tie_kernel<<<w.grid, 256, 0, s>>>(w);
         if (ev) cudaEventRecord(ev[3], s);
         wave_overflow_kernel<<<148, 128, 0, s>>>(a, w, cur);
         if (a.out_dtype == MLGPU_F64)
