@@ -229,35 +229,42 @@ __device__ __forceinline__ bool sphere_cull32(float4 c, float4 o, float3 dv) {
     return true;
 }
 
-// One BVH level: the child boxes of each queued (ray, node) pair, eight
-// lanes per pair and one child per lane.  A warp holds four pairs, so each
-// of a lane's seven 4-byte loads of its child (low and high bounds on the
-// three axes, the reference) touches at most four nodes per warp-wide load,
-// where a lane per pair gathering whole nodes touches up to 32; the ray
-// and the entry are read once per group and broadcast.  With `staged` > 0
-// the block first copies the level's `staged` nodes (a contiguous range,
-// the tree being numbered breadth first) into shared memory and reads them
-// from there.
+// One BVH level: the child boxes of each queued (ray, node) pair, a lane
+// per pair.  With `staged` > 0 the block first copies the level's `staged`
+// nodes (a contiguous range, the tree being numbered breadth first) into
+// shared memory and reads them from there.  (Eight lanes per pair, one child
+// each, loads fewer sectors per request but repeats the ray's setup and the
+// queue bookkeeping on every lane: measured 1.3x slower in total.)
 //
-// A hit child node is queued for the next level by its lane.  A hit leaf
-// range is tested by the whole group, one leaf per lane (one coalesced
-// load of the range's eight spheres): a leaf that passes a conservative
-// FP32 version of merlict's bounding-sphere test (sphere_cull32) becomes a
-// candidate of the ray; merlict's exact FP64 test follows in the
-// intersection kernel.
+// Hit leaf ranges: their leaves pass a conservative FP32 version of
+// merlict's bounding-sphere test (sphere_cull32) or not; those that pass are
+// the ray's candidates, queued as (ray slot, leaf slot).  A warp's hit
+// ranges are spread over its lanes through shared memory -- one range per
+// lane, as many rounds as the warp has ranges / 32 -- so that the up to
+// eight tests of a range run beside the other lanes' instead of one lane at
+// a time; a range's candidates stay adjacent in the queue, so that the
+// intersection kernel reads neighbouring slot records with neighbouring
+// threads.
 constexpr int kLevelThreads = 256;
+constexpr int kLevelWarps = kLevelThreads/32;
 
-__global__ void __launch_bounds__(kLevelThreads)
+struct WalkRay {        // a lane's ray, published to its warp
+    float4 o;           // origin, box inflation
+    float4 dv;          // direction (from the reciprocal); w: the slot, as bits
+};
+
+__global__ void __launch_bounds__(kLevelThreads, 4)
 wave_level_kernel(const TraceArgs a, const WaveBuffers w, int level, int staged) {
     extern __shared__ float4 stage[];
+    __shared__ WalkRay s_ray[kLevelWarps][32];
+    __shared__ int2 s_range[kLevelWarps][32*kBvhWidth];   // (leaf-range reference, lane)
     const DevScene& sc = a.scene;
     const uint2* in = w.level_q[level & 1];
     uint2* out = w.level_q[(level + 1) & 1];
     const uint32_t len = w.counters->level_len[level];
     const uint32_t n = len < w.level_cap ? len : w.level_cap;
     const bool last = level + 1 >= kMaxBvhLevels;
-    const int lane = threadIdx.x & 31;
-    const int group = lane >> 3, k = lane & 7;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int32_t base = sc.bvh_level_start[level];
     if (staged > 0) {
         const float4* src = reinterpret_cast<const float4*>(sc.bvh + base);
@@ -265,74 +272,80 @@ wave_level_kernel(const TraceArgs a, const WaveBuffers w, int level, int staged)
         for (int t = threadIdx.x; t < words; t += blockDim.x) stage[t] = __ldg(src + t);
         __syncthreads();
     }
-    // four pairs per warp, the warps of the grid in turn
-    const uint32_t warps = gridDim.x*(blockDim.x >> 5);
-    for (uint32_t p0 = 4u*(blockIdx.x*(blockDim.x >> 5) + (threadIdx.x >> 5)); p0 < n;
-         p0 += 4u*warps) {
-        const uint32_t e = p0 + (uint32_t)group;
-        const bool valid = e < n;
+    for (uint32_t first = warp_first(); first < n; first += gridDim.x*blockDim.x) {
+        const uint32_t e = first + (uint32_t)lane;
         uint32_t slot = 0;
-        int32_t ref = kBvhEmpty;
-        bool hit = false;
+        ChildRefs child;
+        child.g0 = child.g1 = make_int4(kBvhEmpty, kBvhEmpty, kBvhEmpty, kBvhEmpty);
+        uint32_t hit = 0;   // bit k: child k hit
         float4 o = make_float4(0.f, 0.f, 0.f, 0.f), iv = make_float4(1.f, 1.f, 1.f, 0.f);
-        if (valid) {
+        if (e < n) {
             const uint2 q = in[e];
             slot = q.x;
             o = w.ray_o[slot];
             iv = w.ray_i[slot];
-            const int32_t local = (int32_t)q.y - base;
-            const float* nf = (uint32_t)local < (uint32_t)staged
-                ? reinterpret_cast<const float*>(stage + (sizeof(BvhNode)/16)*local)
-                : reinterpret_cast<const float*>(sc.bvh + q.y);
-            const bool shared_node = (uint32_t)local < (uint32_t)staged;
-            auto ld = [nf, shared_node](int word) { return shared_node ? nf[word] : __ldg(nf + word); };
-            // BvhNode: lo[3][8], hi[3][8], child[8] as 32-bit words
-            const float lx = ld(k), ly = ld(8 + k), lz = ld(16 + k);
-            const float hx = ld(24 + k), hy = ld(32 + k), hz = ld(40 + k);
-            ref = __float_as_int(ld(48 + k));
-            const float ax = (lx - o.w - o.x)*iv.x, bx = (hx + o.w - o.x)*iv.x;
-            const float ay = (ly - o.w - o.y)*iv.y, by = (hy + o.w - o.y)*iv.y;
-            const float az = (lz - o.w - o.z)*iv.z, bz = (hz + o.w - o.z)*iv.z;
-            const float tmin = fmaxf(fmaxf(fminf(ax, bx), fminf(ay, by)), fmaxf(fminf(az, bz), 0.0f));
-            const float tmax = fminf(fminf(fmaxf(ax, bx), fmaxf(ay, by)), fmaxf(az, bz));
-            hit = tmin <= tmax && ref != kBvhEmpty;
+            if ((uint32_t)((int32_t)q.y - base) < (uint32_t)staged)
+                hit = node_hits<true>(stage + (sizeof(BvhNode)/16)*((int32_t)q.y - base), o, iv,
+                                      &child);
+            else
+                hit = node_hits<false>(reinterpret_cast<const float4*>(sc.bvh + q.y), o, iv,
+                                       &child);
         }
-        // a hit child node: queued for the next level by its lane
-        const bool is_node = hit && ref >= 0;
-        const uint32_t nb = warp_reserve(&w.counters->level_len[last ? level : level + 1],
-                                         (is_node && !last) ? 1u : 0u);
-        if (is_node) {
-            if (!last && nb < w.level_cap) out[nb] = make_uint2(slot, (uint32_t)ref);
+        uint32_t nn = 0, ranges = 0;   // bit k of ranges: child k is a hit leaf range
+#pragma unroll
+        for (int k = 0; k < kBvhWidth; k++)
+            if (hit & (1u << k)) { if (child_ref(child, k) < 0) ranges |= 1u << k; else nn++; }
+        uint32_t nb = warp_reserve(&w.counters->level_len[last ? level : level + 1], last ? 0u : nn);
+#pragma unroll
+        for (int k = 0; k < kBvhWidth; k++) {
+            if (!(hit & (1u << k)) || child_ref(child, k) < 0) continue;
+            if (!last && nb < w.level_cap) out[nb] = make_uint2(slot, (uint32_t)child_ref(child, k));
             else mark_overflow(w, slot);
+            nb++;
         }
-        // hit leaf ranges: the group tests one range at a time, a leaf per lane
-        const uint32_t ranges = __ballot_sync(kFull, hit && ref < 0);
-        const uint32_t mine = (ranges >> (8*group)) & 0xffu;   // this group's ranges
-        const int todo = __popc(mine);
-        const int rounds = (int)__reduce_max_sync(kFull, (unsigned)todo);
-        if (rounds == 0) continue;   // warp-uniform
-        const float3 dv = make_float3(1.0f/iv.x, 1.0f/iv.y, 1.0f/iv.z);
-        uint32_t left = mine;
-        for (int r = 0; r < rounds; r++) {
-            const int src = left ? __ffs(left) - 1 : 0;   // the child holding the range
-            left &= left - 1u;
-            const int32_t rref = __shfl_sync(kFull, ref, 8*group + src);
-            bool pass = false;
-            int32_t leaf = 0;
-            if (r < todo) {
-                const int32_t start = (rref & 0x7fffffff) >> 3;
-                const int32_t count = (rref & 7) + 1;
-                if (k < count && sphere_cull32(__ldg(sc.bvh_sphere_f + start + k), o, dv)) {
-                    pass = true;
-                    leaf = start + k;   // the leaf's slot
-                }
+        // the warp's hit leaf ranges, listed in shared memory
+        const uint32_t nr = (uint32_t)__popc(ranges);
+        uint32_t incl = nr;
+#pragma unroll
+        for (int d = 1; d < 32; d <<= 1) {
+            const uint32_t y = __shfl_up_sync(kFull, incl, d);
+            if (lane >= d) incl += y;
+        }
+        const uint32_t total = __shfl_sync(kFull, incl, 31);
+        if (total == 0) continue;   // warp-uniform
+        s_ray[warp][lane].o = o;
+        s_ray[warp][lane].dv = make_float4(1.0f/iv.x, 1.0f/iv.y, 1.0f/iv.z, __uint_as_float(slot));
+        uint32_t at = incl - nr;
+#pragma unroll
+        for (int k = 0; k < kBvhWidth; k++)
+            if ((ranges >> k) & 1u) s_range[warp][at++] = make_int2(child_ref(child, k), lane);
+        __syncwarp();
+        for (uint32_t r0 = 0; r0 < total; r0 += 32) {
+            const uint32_t t = r0 + (uint32_t)lane;
+            uint32_t pass = 0, src_slot = 0;   // bit j: leaf j of the range
+            int32_t start = 0;
+            if (t < total) {
+                const int2 item = s_range[warp][t];
+                const WalkRay rr = s_ray[warp][item.y];
+                src_slot = __float_as_uint(rr.dv.w);
+                start = (item.x & 0x7fffffff) >> 3;
+                const int32_t count = (item.x & 7) + 1;
+                const float3 dv = make_float3(rr.dv.x, rr.dv.y, rr.dv.z);
+                for (int32_t j = 0; j < count; j++)
+                    if (sphere_cull32(__ldg(sc.bvh_sphere_f + start + j), rr.o, dv))
+                        pass |= 1u << j;
             }
-            const uint32_t cb = warp_reserve(&w.counters->isect_len, pass ? 1u : 0u);
-            if (pass) {
-                if (cb < w.isect_cap) w.isect_q[cb] = make_uint2(slot, (uint32_t)leaf);
-                else mark_overflow(w, slot);
+            uint32_t cb = warp_reserve(&w.counters->isect_len, (uint32_t)__popc(pass));
+            while (pass) {
+                const int j = __ffs(pass) - 1;
+                pass &= pass - 1u;
+                // the candidate by its slot (leaf slots follow the BVH's ranges)
+                if (cb < w.isect_cap) w.isect_q[cb] = make_uint2(src_slot, (uint32_t)(start + j));
+                else mark_overflow(w, src_slot);
+                cb++;
             }
         }
+        __syncwarp();   // the lists are rewritten by the next round of entries
     }
 }
 
