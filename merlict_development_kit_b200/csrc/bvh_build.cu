@@ -231,4 +231,47 @@ void build_bvh(const mlgpu_flat_scene* f, double inflate, BvhHost* out) {
     out->level_start[0] = 0;
 }
 
+// Quantises a node's float boxes (already rounded outwards) to QNode: per
+// axis the origin is the smallest low bound and the step the smallest power
+// of two with 255 steps reaching the largest high bound; each bound is
+// rounded outwards to whole steps.  origin + q * 2^e is evaluated in double,
+// where it is exact for the magnitudes a scenery has, and each bound is
+// checked against the float box it stands for.
+void quantise_bvh_node(const BvhNode& n, QNode* q) {
+    std::memset(q, 0, sizeof(*q));
+    uint32_t exps = 0;
+    for (int a = 0; a < 3; a++) {
+        float lo = FLT_MAX, hi = -FLT_MAX;
+        for (int k = 0; k < kBvhWidth; k++) {
+            if (n.child[k] == kBvhEmpty) continue;
+            lo = std::min(lo, n.lo[a][k]);
+            hi = std::max(hi, n.hi[a][k]);
+        }
+        if (lo > hi) { lo = 0.0f; hi = 0.0f; }   // no children (not built)
+        const double ext = (double)hi - (double)lo;
+        int e = -126;                            // the smallest normal step
+        while (e < 127 && std::ldexp(255.0, e) < ext) e++;
+        const double step = std::ldexp(1.0, e);
+        q->origin[a] = lo;
+        exps |= (uint32_t)(e + 127) << (8*a);
+        for (int k = 0; k < kBvhWidth; k++) {
+            uint32_t ql = 0, qh = 0;
+            if (n.child[k] != kBvhEmpty) {
+                double l = std::floor(((double)n.lo[a][k] - (double)lo)/step);
+                double h = std::ceil(((double)n.hi[a][k] - (double)lo)/step);
+                l = std::min(std::max(l, 0.0), 255.0);
+                h = std::min(std::max(h, 0.0), 255.0);
+                while (l > 0.0 && (double)lo + l*step > (double)n.lo[a][k]) l -= 1.0;
+                while (h < 255.0 && (double)lo + h*step < (double)n.hi[a][k]) h += 1.0;
+                ql = (uint32_t)l;
+                qh = (uint32_t)h;
+            }
+            q->qlo[a][k >> 2] |= ql << (8*(k & 3));
+            q->qhi[a][k >> 2] |= qh << (8*(k & 3));
+        }
+    }
+    q->exps = exps;
+    for (int k = 0; k < kBvhWidth; k++) q->child[k] = n.child[k];
+}
+
 }  // namespace mlgpu

@@ -363,6 +363,9 @@ int build_device_scene(mlgpu_scene* s, const mlgpu_flat_scene* f) {
         build_bvh(f, 0.0, &bvh);
         if (!bvh.nodes.empty()) {
             if ((st = upload(s, bvh.nodes.data(), bvh.nodes.size(), &s->dev.bvh))) return st;
+            std::vector<QNode> qn(bvh.nodes.size());
+            for (size_t j = 0; j < qn.size(); j++) quantise_bvh_node(bvh.nodes[j], &qn[j]);
+            if ((st = upload(s, qn.data(), qn.size(), &s->dev.bvh_q))) return st;
             if ((st = upload(s, bvh.leaf_ids.data(), bvh.leaf_ids.size(), &s->dev.bvh_leaf))) return st;
             // merlict's own bounding sphere of each leaf, in BVH order
             std::vector<double4> sph(bvh.leaf_ids.size());

@@ -83,6 +83,24 @@ struct __align__(128) BvhNode {
 static_assert(sizeof(BvhNode) == 32*kBvhWidth, "BvhNode must be 32 bytes per child");
 static_assert(offsetof(BvhNode, child) == 6*kBvhGroups*16,
               "BvhNode references must follow the boxes");
+// The same node quantised to 96 bytes (the level kernels' copy): per axis
+// a float origin (the children's smallest low bound) and a power-of-two
+// step 2^e, and per child and axis 8-bit low and high bounds in steps,
+// rounded outwards, so that origin + q * 2^e bounds the float box of the
+// BvhNode.  Read as six 16-byte words: (origin, the three biased exponents
+// in bytes 0-2 of w), the references of children 0-3 and 4-7, then the
+// bounds, each axis and side as two words of four children's bytes:
+// lo x, lo y | lo z, hi x | hi y, hi z.
+struct __align__(16) QNode {
+    float origin[3];
+    uint32_t exps;
+    int32_t child[kBvhWidth];
+    uint32_t qlo[3][2];
+    uint32_t qhi[3][2];
+};
+static_assert(sizeof(QNode) == 96 && kBvhWidth == 8, "QNode: six 16-byte words, eight children");
+void quantise_bvh_node(const BvhNode& n, QNode* q);
+
 constexpr int32_t kBvhLeafFlag = (int32_t)0x80000000u;
 constexpr int32_t kBvhEmpty = 0x7fffffff;
 constexpr int kBvhStack = 64;
@@ -107,6 +125,7 @@ struct DevScene {
     unsigned int* error_word;   // first device-side error code
     // BVH over the leaves with geometry (empty: walk the frame tree)
     const BvhNode* bvh;
+    const QNode* bvh_q;         // the same nodes quantised (the level kernels read these)
     const int32_t* bvh_leaf;
     // The candidate records: the first 192 bytes of the leaf record of
     // every leaf with geometry, in slot order (the BVH's leaf order), eight

@@ -25,7 +25,9 @@ namespace mlgpu {
 namespace {
 
 constexpr int kTreeCands = 16;   // candidates of a frame-tree walk before it overflows
-constexpr int kMaxStagedNodes = 32768/(int)sizeof(BvhNode);   // 32 KB of shared memory per block
+// staged nodes of a level: 20 KB of shared memory per block, which with the
+// level kernel's own 24 KB stays under the 48 KB a block gets by default
+constexpr int kMaxStagedNodes = 20480/(int)sizeof(QNode);
 
 // The box inflation of a ray's FP32 slab tests: its rounding to FP32.
 __device__ __forceinline__ float box_inflation(const DevScene& sc, float ox, float oy, float oz) {
@@ -171,43 +173,55 @@ __device__ __forceinline__ int32_t child_ref(const ChildRefs& c, int k) {
     }
 }
 
-// Four child boxes of a BVH node: slab tests in single precision on boxes
-// widened by the ray's rounding (o.w).  Bit k of the result: child k is hit.
-__device__ __forceinline__ uint32_t node_box_hits(float4 lx, float4 ly, float4 lz, float4 hx,
-                                                  float4 hy, float4 hz, int4 child,
-                                                  float4 o, float4 iv) {
-    const float lox[4] = {lx.x, lx.y, lx.z, lx.w}, loy[4] = {ly.x, ly.y, ly.z, ly.w};
-    const float loz[4] = {lz.x, lz.y, lz.z, lz.w}, hix[4] = {hx.x, hx.y, hx.z, hx.w};
-    const float hiy[4] = {hy.x, hy.y, hy.z, hy.w}, hiz[4] = {hz.x, hz.y, hz.z, hz.w};
-    const int32_t ch[4] = {child.x, child.y, child.z, child.w};
-    uint32_t hit = 0;
-#pragma unroll
-    for (int k = 0; k < 4; k++) {
-        const float ax = (lox[k] - o.w - o.x)*iv.x, bx = (hix[k] + o.w - o.x)*iv.x;
-        const float ay = (loy[k] - o.w - o.y)*iv.y, by = (hiy[k] + o.w - o.y)*iv.y;
-        const float az = (loz[k] - o.w - o.z)*iv.z, bz = (hiz[k] + o.w - o.z)*iv.z;
-        const float tmin = fmaxf(fmaxf(fminf(ax, bx), fminf(ay, by)), fmaxf(fminf(az, bz), 0.0f));
-        const float tmax = fminf(fminf(fmaxf(ax, bx), fmaxf(ay, by)), fmaxf(az, bz));
-        if (tmin <= tmax && ch[k] != kBvhEmpty) hit |= 1u << k;
-    }
-    return hit;
-}
-
-// All children of the node at `nq` (global memory through the read-only
-// path, or shared memory), four at a time; their references into `child`.
+// The eight children of a quantised node (QNode, global memory through the
+// read-only path or shared memory); their references into `child`.  A bound
+// decodes as origin + q * 2^e; the slab distance (bound -+ o.w - o) * iv is
+// evaluated as q * (2^e iv) + (origin -+ o.w - o) iv, one fused
+// multiply-add per bound (the byte becomes a float by the exponent trick:
+// 0x4b0000qq is 2^23 + q).  The rounding of that form stays inside the box
+// inflation o.w, which covers several units in the last place of the
+// scenery's extent and of the ray's origin.
 template <bool kShared>
-__device__ __forceinline__ uint32_t node_hits(const float4* nq, float4 o, float4 iv,
-                                              ChildRefs* child) {
+__device__ __forceinline__ uint32_t qnode_hits(const float4* nq, float4 o, float4 iv,
+                                               ChildRefs* child) {
     auto ld = [nq](int k) { return kShared ? nq[k] : __ldg(nq + k); };
-    const float4 c0 = ld(6*kBvhGroups), c1 = ld(6*kBvhGroups + 1);
+    const float4 w0 = ld(0), c0 = ld(1), c1 = ld(2), b0 = ld(3), b1 = ld(4), b2 = ld(5);
     child->g0 = make_int4(__float_as_int(c0.x), __float_as_int(c0.y), __float_as_int(c0.z),
                           __float_as_int(c0.w));
     child->g1 = make_int4(__float_as_int(c1.x), __float_as_int(c1.y), __float_as_int(c1.z),
                           __float_as_int(c1.w));
-    return node_box_hits(ld(0), ld(kBvhGroups), ld(2*kBvhGroups), ld(3*kBvhGroups),
-                         ld(4*kBvhGroups), ld(5*kBvhGroups), child->g0, o, iv) |
-        (node_box_hits(ld(1), ld(kBvhGroups + 1), ld(2*kBvhGroups + 1), ld(3*kBvhGroups + 1),
-                       ld(4*kBvhGroups + 1), ld(5*kBvhGroups + 1), child->g1, o, iv) << 4);
+    const uint32_t ex = __float_as_uint(w0.w);
+    const float sx = __uint_as_float((ex & 0xffu) << 23);
+    const float sy = __uint_as_float(((ex >> 8) & 0xffu) << 23);
+    const float sz = __uint_as_float(((ex >> 16) & 0xffu) << 23);
+    const float Sx = sx*iv.x, Sy = sy*iv.y, Sz = sz*iv.z;
+    const float Lx = (w0.x - o.w - o.x)*iv.x, Hx = (w0.x + o.w - o.x)*iv.x;
+    const float Ly = (w0.y - o.w - o.y)*iv.y, Hy = (w0.y + o.w - o.y)*iv.y;
+    const float Lz = (w0.z - o.w - o.z)*iv.z, Hz = (w0.z + o.w - o.z)*iv.z;
+    // bound words: lo x = (b0.x, b0.y), lo y = (b0.z, b0.w), lo z = (b1.x, b1.y),
+    // hi x = (b1.z, b1.w), hi y = (b2.x, b2.y), hi z = (b2.z, b2.w)
+    const uint32_t lox[2] = {__float_as_uint(b0.x), __float_as_uint(b0.y)};
+    const uint32_t loy[2] = {__float_as_uint(b0.z), __float_as_uint(b0.w)};
+    const uint32_t loz[2] = {__float_as_uint(b1.x), __float_as_uint(b1.y)};
+    const uint32_t hix[2] = {__float_as_uint(b1.z), __float_as_uint(b1.w)};
+    const uint32_t hiy[2] = {__float_as_uint(b2.x), __float_as_uint(b2.y)};
+    const uint32_t hiz[2] = {__float_as_uint(b2.z), __float_as_uint(b2.w)};
+    uint32_t hit = 0;
+#pragma unroll
+    for (int k = 0; k < kBvhWidth; k++) {
+        const int g = k >> 2;
+        const uint32_t sel = 0x7540u | (uint32_t)(k & 3);
+        auto dq = [sel](uint32_t word) {
+            return __uint_as_float(__byte_perm(word, 0x4b000000u, sel)) - 8388608.0f;
+        };
+        const float ax = __fmaf_rn(dq(lox[g]), Sx, Lx), bx = __fmaf_rn(dq(hix[g]), Sx, Hx);
+        const float ay = __fmaf_rn(dq(loy[g]), Sy, Ly), by = __fmaf_rn(dq(hiy[g]), Sy, Hy);
+        const float az = __fmaf_rn(dq(loz[g]), Sz, Lz), bz = __fmaf_rn(dq(hiz[g]), Sz, Hz);
+        const float tmin = fmaxf(fmaxf(fminf(ax, bx), fminf(ay, by)), fmaxf(fminf(az, bz), 0.0f));
+        const float tmax = fminf(fminf(fmaxf(ax, bx), fmaxf(ay, by)), fmaxf(az, bz));
+        if (tmin <= tmax && child_ref(*child, k) != kBvhEmpty) hit |= 1u << k;
+    }
+    return hit;
 }
 
 // merlict's bounding-sphere test of a leaf (RayAndFrame.cpp:16-107) in
@@ -267,8 +281,8 @@ wave_level_kernel(const TraceArgs a, const WaveBuffers w, int level, int staged)
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int32_t base = sc.bvh_level_start[level];
     if (staged > 0) {
-        const float4* src = reinterpret_cast<const float4*>(sc.bvh + base);
-        const int words = staged*(int)(sizeof(BvhNode)/16);
+        const float4* src = reinterpret_cast<const float4*>(sc.bvh_q + base);
+        const int words = staged*(int)(sizeof(QNode)/16);
         for (int t = threadIdx.x; t < words; t += blockDim.x) stage[t] = __ldg(src + t);
         __syncthreads();
     }
@@ -285,11 +299,11 @@ wave_level_kernel(const TraceArgs a, const WaveBuffers w, int level, int staged)
             o = w.ray_o[slot];
             iv = w.ray_i[slot];
             if ((uint32_t)((int32_t)q.y - base) < (uint32_t)staged)
-                hit = node_hits<true>(stage + (sizeof(BvhNode)/16)*((int32_t)q.y - base), o, iv,
-                                      &child);
-            else
-                hit = node_hits<false>(reinterpret_cast<const float4*>(sc.bvh + q.y), o, iv,
+                hit = qnode_hits<true>(stage + (sizeof(QNode)/16)*((int32_t)q.y - base), o, iv,
                                        &child);
+            else
+                hit = qnode_hits<false>(reinterpret_cast<const float4*>(sc.bvh_q + q.y), o, iv,
+                                        &child);
         }
         uint32_t nn = 0, ranges = 0;   // bit k of ranges: child k is a hit leaf range
 #pragma unroll
@@ -386,8 +400,8 @@ wave_walk_kernel(const TraceArgs a, const WaveBuffers w, const RayPool cur) {
             stack[sp++] = (int32_t)root;
             while (sp > 0 && !over) {
                 ChildRefs child;
-                const uint32_t hit = node_hits<false>(
-                    reinterpret_cast<const float4*>(sc.bvh + stack[--sp]), o, iv, &child);
+                const uint32_t hit = qnode_hits<false>(
+                    reinterpret_cast<const float4*>(sc.bvh_q + stack[--sp]), o, iv, &child);
                 for (int k = kBvhWidth - 1; k >= 0; k--) {
                     if (!(hit & (1u << k))) continue;
                     const int32_t ref = child_ref(child, k);
@@ -486,7 +500,7 @@ cudaError_t launch_wave_iteration(const TraceArgs& a, const WaveBuffers& w, cons
         for (int k = 0; k < a.scene.bvh_levels; k++) {
             const int count = a.scene.bvh_level_start[k + 1] - a.scene.bvh_level_start[k];
             const int staged = k < w.staged_levels && count <= kMaxStagedNodes ? count : 0;
-            wave_level_kernel<<<w.grid, 256, (size_t)staged*sizeof(BvhNode), s>>>(a, w, k,
+            wave_level_kernel<<<w.grid, 256, (size_t)staged*sizeof(QNode), s>>>(a, w, k,
                                                                                    staged);
         }
     }
