@@ -544,7 +544,10 @@ int mlgpu_scene_autotune(
  * callers that want per-sensor statistics rather than arrival lists:
  * counts[s] = photons whose final surface is sensor s; time_hist[s][b] =
  * those arrivals with time in bin b of [t_min, t_max) (num_time_bins, may
- * be 0).  Device pointers.  `counts` and `time_hist` are overwritten.     */
+ * be 0).  Device pointers.  `counts` and `time_hist` are overwritten.
+ * Sensor ids outside [0, num_sensors) (no arrival: -1) are not counted.
+ * Two kernel launches (zero the outputs, one pass of atomic additions);
+ * allocates no device memory.                                            */
 int mlgpu_bin_arrivals(
     mlgpu_scene* scene,
     const int32_t* sensor,
@@ -566,28 +569,14 @@ int mlgpu_bin_arrivals(
  * allocator (a cudaMalloc behind its back can exceed its fixed budget or
  * fragment the pool), or an event loop with real-time deadlines, where
  * cudaMalloc and cudaFree may synchronise the device and stall the other
- * streams.  mlgpu_bin_arrivals grows a scratch buffer with cudaMalloc on
- * demand; this entry point instead uses one fixed scratch array compiled
- * into the library: MLGPU_NOALLOC_BIN_SCRATCH_WORDS 32-bit words (16 MiB)
- * on every GPU that loads the library, held until the process exits.
- *
- * Limit: num_sensors x (num_time_bins + 1) must not exceed
- * MLGPU_NOALLOC_BIN_SCRATCH_WORDS; larger requests return
- * MLGPU_ERR_INVALID_ARGUMENT and do nothing.  The inputs and outputs are
- * the caller's device buffers, as for mlgpu_bin_arrivals.  The scene's
- * device must be the current device (else MLGPU_ERR_INVALID_ARGUMENT).
- * Its two kernel launches count in mlgpu_scene_kernel_launches and, while
- * profiling is on, in the MLGPU_KERNEL_BIN times.
- *
- * The first call on a device looks up the array's device address (this
- * may load the library's device code into the context); make that first
- * call before any stream capture.  Every call overwrites all the scratch
- * words it reads, so nothing carries over from one call to the next; but
- * all calls on a device share the one array, so calls that overlap on the
- * GPU (issued to different streams, or from threads without ordering
- * between them) race and give wrong results.  Calls allocate nothing.   */
-#define MLGPU_NOALLOC_BIN_SCRATCH_WORDS (4u * 1024u * 1024u)
-
+ * streams.  The binning kernels accumulate in the caller's output buffers
+ * and use no scratch, so neither entry point allocates; this one also
+ * checks that the scene's device is the current device (else
+ * MLGPU_ERR_INVALID_ARGUMENT) before it launches anything.  The inputs and
+ * outputs are the caller's device buffers, as for mlgpu_bin_arrivals.  Its
+ * two kernel launches count in mlgpu_scene_kernel_launches and, while
+ * profiling is on, in the MLGPU_KERNEL_BIN times.  Calls share no state,
+ * so calls on different streams may overlap.                             */
 int mlgpu_bin_arrivals_noalloc(
     mlgpu_scene* scene,
     const int32_t* sensor,

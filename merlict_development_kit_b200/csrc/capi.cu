@@ -143,7 +143,7 @@ struct mlgpu_scene {
     size_t arena_bytes = 0;
     unsigned int* error_word = nullptr;
     // staging for mlgpu_propagate_host and scratch for binning
-    DeviceBuffer staging_in, staging_out, staging_hist, staging_rng, bin_scratch, tune_out;
+    DeviceBuffer staging_in, staging_out, staging_hist, staging_rng, tune_out;
     DeviceBuffer staging_bins;           // counts and time histograms of a host call
     DeviceBuffer order;                  // tracing order of a batch and its sort scratch
     DeviceBuffer queue;                  // the work-queue tracer's counter
@@ -817,7 +817,6 @@ int mlgpu_scene_destroy(mlgpu_scene* scene) {
     scene->staging_out.release();
     scene->staging_hist.release();
     scene->staging_rng.release();
-    scene->bin_scratch.release();
     scene->staging_bins.release();
     scene->tune_out.release();
     scene->order.release();
@@ -1344,17 +1343,14 @@ int propagate_host(mlgpu_scene* scene, const mlgpu_photons* photons, uint64_t n,
         // last piece is traced: bin them there, copy the bins back
         const size_t ns = (size_t)scene->dev.num_sensors;
         const size_t keys = ns*(bin->num_bins + 1ull);
-        const size_t slices = 32;
-        if (scene->bin_scratch.reserve(slices*keys*sizeof(uint32_t) + 256) != cudaSuccess ||
-            scene->staging_bins.reserve(keys*sizeof(uint32_t)) != cudaSuccess)
+        if (scene->staging_bins.reserve(keys*sizeof(uint32_t)) != cudaSuccess)
             return drain(cuda_fail(cudaGetLastError(), "binning buffers"));
         uint32_t* dcounts = static_cast<uint32_t*>(scene->staging_bins.ptr);
         uint32_t* dhist = bin->num_bins ? dcounts + ns : nullptr;
         cudaError_t e = launch_bin_arrivals(
             scene->dev, static_cast<const int32_t*>(dev_plane[0]),
             static_cast<const double*>(dev_plane[3]), n, dcounts, dhist, bin->num_bins,
-            bin->t_min, bin->t_max, static_cast<uint32_t*>(scene->bin_scratch.ptr),
-            scene->bin_scratch.bytes/sizeof(uint32_t), trace);
+            bin->t_min, bin->t_max, trace);
         if (e != cudaSuccess) return drain(cuda_fail(e, "binning kernels"));
         scene->launches += 2;
         e = cudaMemcpyAsync(bin->counts, dcounts, ns*sizeof(uint32_t), cudaMemcpyDeviceToHost,
@@ -1398,17 +1394,13 @@ int mlgpu_bin_arrivals(mlgpu_scene* scene, const int32_t* sensor, const double* 
     const uint64_t keys = (uint64_t)scene->dev.num_sensors * (num_time_bins + 1ull);
     if (keys >= (1ull << 31))
         return fail(MLGPU_ERR_INVALID_ARGUMENT, "too many sensor x time bins");
-    // partial histograms: one slice of `keys` words per photon slice
-    const size_t slices = 32;
-    MLGPU_CUDA(scene->bin_scratch.reserve(slices*keys*sizeof(uint32_t) + 256));
     const cudaStream_t stream = static_cast<cudaStream_t>(cuda_stream);
     Profiler::Chain ch;
     const bool timed = scene->prof.on && scene->prof.take(2, ch.ev);
     if (timed) cudaEventRecord(ch.ev[0], stream);
     const cudaError_t e = launch_bin_arrivals(
         scene->dev, sensor, time, n, counts, num_time_bins ? time_hist : nullptr,
-        num_time_bins, t_min, t_max, static_cast<uint32_t*>(scene->bin_scratch.ptr),
-        scene->bin_scratch.bytes / sizeof(uint32_t), stream);
+        num_time_bins, t_min, t_max, stream);
     if (timed) {
         cudaEventRecord(ch.ev[1], stream);
         ch.n = 2; ch.cls[0] = MLGPU_KERNEL_BIN; ch.launches[0] = 2;

@@ -324,11 +324,12 @@ size_t photon_order_scratch_bytes(uint64_t n);
 cudaError_t launch_photon_order(const DevPhotons& p, int in_dtype, uint64_t n, uint32_t* order,
                                 void* scratch, int grid, cudaStream_t s);
 int wave_persistent_blocks();
+// Zeroes counts (and time_hist) and bins n arrivals into them: two kernel
+// launches, no scratch memory (bin.cu).
 cudaError_t launch_bin_arrivals(const DevScene& sc, const int32_t* sensor,
                                 const double* time, uint64_t n, uint32_t* counts,
                                 uint32_t* time_hist, uint32_t num_bins,
-                                double t_min, double t_max, uint32_t* scratch,
-                                size_t scratch_words, cudaStream_t s);
+                                double t_min, double t_max, cudaStream_t s);
 
 // Records a message for mlgpu_last_error and returns `code` (capi.cu).
 int report_error(int code, const char* message);
