@@ -507,9 +507,8 @@ int wave_buffers(mlgpu_scene* scene, uint32_t pool, int grid, int staged, uint32
     const size_t P = pool;
     const size_t level_cap = queue_cap ? queue_cap : 8*P;
     const size_t isect_cap = queue_cap ? queue_cap : 16*P;
-    const size_t per_pool = 8*up(P*8) + 5*up(P*4);
-    const size_t rest = up(P*4) + 2*up(P*16) + up(P*48) + 2*up(level_cap*8) +
-        up(isect_cap*8) + up(isect_cap*8) + up(P*8) + 3*up(P*4);
+    const size_t per_pool = up(P*48) + 3*up(P*8) + 8*up(P*4) + 2*up(P*16);
+    const size_t rest = 2*up(level_cap*8) + up(isect_cap*8) + up(isect_cap*8) + up(P*4);
     MLGPU_CUDA(scene->wave.reserve(256 + 2*per_pool + rest));
     if (!scene->wave_host) MLGPU_CUDA(cudaMallocHost(&scene->wave_host, sizeof(WaveCounters)));
     if (!scene->wave_host_dev)
@@ -522,18 +521,20 @@ int wave_buffers(mlgpu_scene* scene, uint32_t pool, int grid, int staged, uint32
     auto take = [&](size_t bytes) { char* p = b; b += up(bytes); return p; };
     RayPool* pools[2] = {p0, p1};
     for (RayPool* p : pools) {
-        double** d[8] = {&p->sx, &p->sy, &p->sz, &p->dx, &p->dy, &p->dz, &p->lambda, &p->tof};
-        for (double** q : d) *q = reinterpret_cast<double*>(take(P*8));
-        int32_t** i[5] = {&p->photon, &p->root, &p->n_int, &p->k_draw, &p->err};
+        p->sd = reinterpret_cast<double2*>(take(P*48));
+        p->lambda = reinterpret_cast<double*>(take(P*8));
+        p->tof = reinterpret_cast<double*>(take(P*8));
+        p->best_key = reinterpret_cast<unsigned long long*>(take(P*8));
+        int32_t** i[7] = {&p->photon, &p->root, &p->n_int, &p->k_draw, &p->err, &p->step,
+                          &p->best_leaf};
         for (int32_t** q : i) *q = reinterpret_cast<int32_t*>(take(P*4));
+        p->overflow_flag = reinterpret_cast<uint32_t*>(take(P*4));
+        p->ray_o = reinterpret_cast<float4*>(take(P*16));
+        p->ray_i = reinterpret_cast<float4*>(take(P*16));
     }
     w->pool = pool;
     w->grid = grid > 0 ? grid : scene->wave_grid;
     w->staged_levels = staged;
-    w->step = reinterpret_cast<int32_t*>(take(P*4));
-    w->ray_sd = reinterpret_cast<double2*>(take(P*48));
-    w->ray_o = reinterpret_cast<float4*>(take(P*16));
-    w->ray_i = reinterpret_cast<float4*>(take(P*16));
     w->level_q[0] = reinterpret_cast<uint2*>(take(level_cap*8));
     w->level_q[1] = reinterpret_cast<uint2*>(take(level_cap*8));
     w->level_cap = (uint32_t)level_cap;
@@ -541,10 +542,7 @@ int wave_buffers(mlgpu_scene* scene, uint32_t pool, int grid, int staged, uint32
     w->slot_leaf_of = scene->dev.slot_leaf;
     w->isect_dist = reinterpret_cast<double*>(take(isect_cap*8));
     w->isect_cap = (uint32_t)isect_cap;
-    w->best_key = reinterpret_cast<unsigned long long*>(take(P*8));
-    w->best_leaf = reinterpret_cast<int32_t*>(take(P*4));
     w->overflow = reinterpret_cast<uint32_t*>(take(P*4));
-    w->overflow_flag = reinterpret_cast<uint32_t*>(take(P*4));
     const size_t fn_bytes = (size_t)scene->dev.num_fn_points*3*sizeof(double) +
         ((size_t)scene->dev.num_functions + 1)*sizeof(int32_t);
     w->fn_smem_bytes = fn_bytes <= 16384 ? (int)fn_bytes : 0;

@@ -205,16 +205,26 @@ struct WaveCounters {
 };
 static_assert(sizeof(WaveCounters) <= 256, "the counters sit in the first 256 bytes of the pool");
 
+// One pool of ray slots; two pools alternate between iterations.  The
+// resolve step of an iteration writes each surviving ray into the next
+// pool ready to walk -- its FP64 record, its FP32 walk record, its cleared
+// closest hit and what the intake has to queue for it -- so that the next
+// intake only queues survivors and fills the free slots with new photons.
 struct RayPool {
     int32_t* photon;
-    double* sx; double* sy; double* sz;
-    double* dx; double* dy; double* dz;
+    double2* sd;             // [pool][3] support and direction, one 48-byte record per slot
     double* lambda;
     double* tof;
     int32_t* root;
     int32_t* n_int;
     int32_t* k_draw;
     int32_t* err;            // error | time-of-flight error << 8
+    int32_t* step;           // kNoStep, or what to queue: kStepNone, kStepBvh, kStepTree
+    float4* ray_o;           // single-precision origin, box inflation (kStepBvh rays)
+    float4* ray_i;           // reciprocal direction (kStepBvh rays)
+    unsigned long long* best_key;   // smallest hit distance (bits of a positive double)
+    int32_t* best_leaf;      // leaf of the closest hit, lowest index on ties
+    uint32_t* overflow_flag; // the slot is queued for merlict's own walk
 };
 
 struct WaveBuffers {
@@ -224,21 +234,13 @@ struct WaveBuffers {
     int staged_levels;       // BVH levels whose nodes each block stages in shared memory
     int walk;                // MLGPU_WALK_LEVELS or MLGPU_WALK_STACK
     int fn_smem_bytes;       // property tables staged in shared memory (0: read from global)
-    int32_t* step;           // [pool] 0, or kNoStep: the photon takes no step
-    double2* ray_sd;         // [pool][3] the FP64 support and direction, one 48-byte
-                             // record per slot for the kernels that read rays by queue
-    float4* ray_o;           // [pool] single-precision origin, box inflation
-    float4* ray_i;           // [pool] reciprocal direction
     uint2* level_q[2];       // (slot, node) pairs, ping-pong between BVH levels
     uint32_t level_cap;
     uint2* isect_q;          // (ray slot, leaf slot) candidates
     const int32_t* slot_leaf_of;   // the scene's slot -> leaf map (DevScene::slot_leaf)
     double* isect_dist;      // distance to each candidate's hit, -1: none
     uint32_t isect_cap;
-    unsigned long long* best_key;   // [pool] smallest hit distance (bits of a positive double)
-    int32_t* best_leaf;      // [pool] leaf of the closest hit, lowest index on ties
     uint32_t* overflow;      // [pool] slots for merlict's own walk
-    uint32_t* overflow_flag; // [pool]
 };
 
 // One iteration of a wavefront tracer: walk, queue and intersect the

@@ -37,6 +37,9 @@ using namespace fp64;
 
 constexpr unsigned kFull = 0xffffffffu;
 constexpr int kNoStep = -2;             // step state: the photon takes no step
+constexpr int kStepNone = 0;            // it takes a step; nothing to queue (no candidates)
+constexpr int kStepBvh = 1;             // it takes a step; the intake queues the BVH root
+constexpr int kStepTree = 2;            // it takes a step; the intake walks its frame subtree
 constexpr int32_t kNoLeaf = INT32_MAX;  // best_leaf of a ray without a hit
 constexpr unsigned long long kNoKey = ~0ull;
 
@@ -78,8 +81,10 @@ __device__ __forceinline__ uint32_t warp_reserve(unsigned int* counter, uint32_t
 }
 
 // Sends a slot to merlict's own walk (once per iteration).
-__device__ __forceinline__ void mark_overflow(const WaveBuffers& w, uint32_t slot) {
-    if (atomicExch(&w.overflow_flag[slot], 1u) == 0u)
+__device__ __forceinline__ void mark_overflow(const WaveBuffers& w, const RayPool& cur,
+                                              uint32_t slot) {
+    uint32_t* flag = cur.overflow_flag;
+    if (atomicExch(flag + slot, 1u) == 0u)
         w.overflow[atomicAdd(&w.counters->overflow_len, 1u)] = slot;
 }
 
@@ -89,11 +94,45 @@ __device__ __forceinline__ uint32_t warp_first() {
     return blockIdx.x*blockDim.x + (threadIdx.x & ~31u);
 }
 
-// The FP64 ray of a slot from its 48-byte record (written by the intake).
-__device__ __forceinline__ void load_ray(const WaveBuffers& w, uint32_t slot, v3* s, v3* d) {
-    const double2 a = w.ray_sd[3*slot], b = w.ray_sd[3*slot + 1], c = w.ray_sd[3*slot + 2];
+// The FP64 ray of a slot from its 48-byte record.
+__device__ __forceinline__ void load_ray(const RayPool& p, uint32_t slot, v3* s, v3* d) {
+    const double2 a = p.sd[3*slot], b = p.sd[3*slot + 1], c = p.sd[3*slot + 2];
     *s = mk(a.x, a.y, b.x);
     *d = mk(b.y, c.x, c.y);
+}
+
+__device__ __forceinline__ void store_ray(const RayPool& p, uint32_t slot, v3 s, v3 d) {
+    p.sd[3*slot] = make_double2(s.x, s.y);
+    p.sd[3*slot + 1] = make_double2(s.z, d.x);
+    p.sd[3*slot + 2] = make_double2(d.y, d.z);
+}
+
+// The box inflation of a ray's FP32 slab tests: its rounding to FP32.
+__device__ __forceinline__ float box_inflation(const DevScene& sc, float ox, float oy, float oz) {
+    return sc.bvh_eps + 4e-7f*(fabsf(ox) + fabsf(oy) + fabsf(oz));
+}
+
+// What the next intake queues for a ray about to take a step from s along d
+// in the frame subtree `root`, and its FP32 walk record when that is the
+// BVH: inside a lens (root != 0), or without a BVH, merlict's own walk of
+// the subtree (kStepTree); else merlict tests the root frame's sphere first
+// (RayAndFrame.cpp:137-149) and the BVH walk follows if the ray passes it.
+__device__ __forceinline__ int prepare_walk(const TraceArgs& a, const RayPool& p, uint32_t slot,
+                                            v3 s, v3 d, int32_t root) {
+    const DevScene& sc = a.scene;
+    if (root != 0 || sc.bvh_nodes == 0 || a.traversal == MLGPU_TRAVERSAL_FRAME_TREE)
+        return kStepTree;
+    const double2* np = reinterpret_cast<const double2*>(sc.node);
+    const double2 n01 = __ldg(np), n23 = __ldg(np + 1);
+    if (!sphere_cull(make_double4(n01.x, n01.y, n23.x, n23.y), s, d, dot(s, d))) return kStepNone;
+    const float ox = (float)s.x, oy = (float)s.y, oz = (float)s.z;
+    float fdx = (float)d.x, fdy = (float)d.y, fdz = (float)d.z;
+    if (fabsf(fdx) < 1e-30f) fdx = copysignf(1e-30f, fdx);
+    if (fabsf(fdy) < 1e-30f) fdy = copysignf(1e-30f, fdy);
+    if (fabsf(fdz) < 1e-30f) fdz = copysignf(1e-30f, fdz);
+    p.ray_o[slot] = make_float4(ox, oy, oz, box_inflation(sc, ox, oy, oz));
+    p.ray_i[slot] = make_float4(1.0f/fdx, 1.0f/fdy, 1.0f/fdz, 0.0f);
+    return kStepBvh;
 }
 
 template <int kIsect>
@@ -105,7 +144,7 @@ wave_isect_kernel(const TraceArgs a, const WaveBuffers w, const RayPool cur) {
         const uint2 q = w.isect_q[e];
         const uint32_t slot = q.x;
         v3 s, d;
-        load_ray(w, slot, &s, &d);
+        load_ray(cur, slot, &s, &d);
         double dist = -1.0;
         if (kIsect == kIsectFp64) {
             double T[12], ti[3], pr[MLGPU_LEAF_PARAMS], r2;
@@ -129,19 +168,19 @@ wave_isect_kernel(const TraceArgs a, const WaveBuffers w, const RayPool cur) {
             if (h.leaf >= 0) dist = h.v;
         }
         w.isect_dist[e] = dist;
-        if (dist >= 0.0) atomicMin(&w.best_key[slot], (unsigned long long)__double_as_longlong(dist));
+        if (dist >= 0.0) atomicMin(&cur.best_key[slot], (unsigned long long)__double_as_longlong(dist));
     }
 }
 
 __global__ void __launch_bounds__(256)
-wave_tie_kernel(const WaveBuffers w) {
+wave_tie_kernel(const WaveBuffers w, const RayPool cur) {
     const uint32_t n = w.counters->isect_len < w.isect_cap ? w.counters->isect_len : w.isect_cap;
     for (uint32_t e = blockIdx.x*blockDim.x + threadIdx.x; e < n; e += gridDim.x*blockDim.x) {
         const double dist = w.isect_dist[e];
         if (!(dist >= 0.0)) continue;
         const uint2 q = w.isect_q[e];
-        if ((unsigned long long)__double_as_longlong(dist) == w.best_key[q.x])
-            atomicMin(&w.best_leaf[q.x], __ldg(w.slot_leaf_of + q.y));
+        if ((unsigned long long)__double_as_longlong(dist) == cur.best_key[q.x])
+            atomicMin(&cur.best_leaf[q.x], __ldg(w.slot_leaf_of + q.y));
     }
 }
 
@@ -152,10 +191,10 @@ wave_overflow_kernel(const TraceArgs a, const WaveBuffers w, const RayPool cur) 
     const uint32_t n = w.counters->overflow_len;
     for (uint32_t e = blockIdx.x*blockDim.x + threadIdx.x; e < n; e += gridDim.x*blockDim.x) {
         const uint32_t slot = w.overflow[e];
-        const v3 s = mk(cur.sx[slot], cur.sy[slot], cur.sz[slot]);
-        const v3 d = mk(cur.dx[slot], cur.dy[slot], cur.dz[slot]);
+        v3 s, d;
+        load_ray(cur, slot, &s, &d);
         const Isec is = first_intersection_tree(a.scene, cur.root[slot], s, d);
-        w.best_leaf[slot] = is.leaf >= 0 ? is.leaf : kNoLeaf;
+        cur.best_leaf[slot] = is.leaf >= 0 ? is.leaf : kNoLeaf;
     }
 }
 
@@ -192,9 +231,8 @@ wave_resolve_kernel(const TraceArgs a, const WaveBuffers w, const RayPool cur, c
     double lambda = 0.0, tof = 0.0;
     int32_t count = 0;
     if (valid) {
-        s = mk(cur.sx[slot], cur.sy[slot], cur.sz[slot]);
-        d = mk(cur.dx[slot], cur.dy[slot], cur.dz[slot]);
-        count = w.step[slot];
+        load_ray(cur, slot, &s, &d);
+        count = cur.step[slot];
     }
 
     if (valid) {
@@ -227,7 +265,7 @@ wave_resolve_kernel(const TraceArgs a, const WaveBuffers w, const RayPool cur, c
             {
                 // the winner of the intersection and tie kernels (or of
                 // merlict's own walk), recomputed by the same code
-                const int32_t best = w.best_leaf[slot];
+                const int32_t best = cur.best_leaf[slot];
                 if (best == kNoLeaf) {
                     set_void(&is, s, d);
                 } else if (kIsect == kIsectFp64) {
@@ -406,15 +444,20 @@ wave_resolve_kernel(const TraceArgs a, const WaveBuffers w, const RayPool cur, c
         base = __shfl_sync(kFull, base, __ffs(m) - 1);
         if (survive) {
             const uint32_t o = base + __popc(m & ((1u << lane) - 1u));
+            // the ray as the next iteration takes it: merlict's state, the
+            // cleared closest hit, and what the intake has to queue
             nxt.photon[o] = photon;
-            nxt.sx[o] = s.x; nxt.sy[o] = s.y; nxt.sz[o] = s.z;
-            nxt.dx[o] = d.x; nxt.dy[o] = d.y; nxt.dz[o] = d.z;
+            store_ray(nxt, o, s, d);
             nxt.lambda[o] = lambda;
             nxt.tof[o] = tof;
             nxt.root[o] = root;
             nxt.n_int[o] = n_next;
             nxt.k_draw[o] = k_draw;
             nxt.err[o] = err;
+            nxt.best_key[o] = kNoKey;
+            nxt.best_leaf[o] = kNoLeaf;
+            nxt.overflow_flag[o] = 0u;
+            nxt.step[o] = prepare_walk(a, nxt, o, s, d, root);
         }
     }
 }

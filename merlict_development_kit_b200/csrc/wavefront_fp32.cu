@@ -22,7 +22,7 @@ cudaError_t launch_wave32_isect_resolve(const TraceArgs& a, const WaveBuffers& w
     const int blocks = (int)((w.pool + 255)/256);
     if (pure) wave_isect_kernel<kIsectFp32Pure><<<w.grid, 256, 0, s>>>(a, w, cur);
     else wave_isect_kernel<kIsectFp32><<<w.grid, 256, 0, s>>>(a, w, cur);
-    wave_tie_kernel<<<w.grid, 256, 0, s>>>(w);
+    wave_tie_kernel<<<w.grid, 256, 0, s>>>(w, cur);
     if (mid) cudaEventRecord(mid, s);
     wave_overflow_kernel<<<148, 128, 0, s>>>(a, w, cur);
     if (pure) {

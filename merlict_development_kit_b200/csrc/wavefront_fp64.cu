@@ -29,11 +29,11 @@ constexpr int kTreeCands = 16;   // candidates of a frame-tree walk before it ov
 // level kernel's own 24 KB stays under the 48 KB a block gets by default
 constexpr int kMaxStagedNodes = 20480/(int)sizeof(QNode);
 
-// The box inflation of a ray's FP32 slab tests: its rounding to FP32.
-__device__ __forceinline__ float box_inflation(const DevScene& sc, float ox, float oy, float oz) {
-    return sc.bvh_eps + 4e-7f*(fabsf(ox) + fabsf(oy) + fabsf(oz));
-}
-
+// The intake: new photons enter the free slots (merlict::Photon's
+// constructor, Ray.cpp:16-20, RayForPropagation.cpp:52-64) and are prepared
+// like the survivors the previous resolve step prepared; then every ray of
+// the pool is queued -- the BVH root, or the candidates of merlict's own
+// walk of its frame subtree (a ray inside a lens, RayAndFrame.cpp:137-149).
 template <typename In>
 __global__ void __launch_bounds__(256)
 wave_intake_kernel(const TraceArgs a, const WaveBuffers w, const RayPool cur) {
@@ -51,23 +51,17 @@ wave_intake_kernel(const TraceArgs a, const WaveBuffers w, const RayPool cur) {
     int nc = 0;                // candidates of a frame-tree walk
     int32_t cand[kTreeCands];
     if (slot < total) {
-        v3 s, d;
-        int32_t root;
-        uint32_t n_int;
+        int step;
         if (slot >= active) {
-            // a new photon: merlict::Photon's constructor (Ray.cpp:16-20,
-            // RayForPropagation.cpp:52-64)
             const uint64_t q = next_input + (slot - active);
             const uint64_t p = a.order ? (uint64_t)__ldg(a.order + q) : q;
-            s = mk(load_in<In>(a.photons.sx, p), load_in<In>(a.photons.sy, p),
-                   load_in<In>(a.photons.sz, p));
-            d = normalized(mk(load_in<In>(a.photons.dx, p), load_in<In>(a.photons.dy, p),
-                              load_in<In>(a.photons.dz, p)));
-            root = a.start_node;
-            n_int = 1;
+            const v3 s = mk(load_in<In>(a.photons.sx, p), load_in<In>(a.photons.sy, p),
+                            load_in<In>(a.photons.sz, p));
+            const v3 d = normalized(mk(load_in<In>(a.photons.dx, p), load_in<In>(a.photons.dy, p),
+                                       load_in<In>(a.photons.dz, p)));
+            const int32_t root = a.start_node;
             cur.photon[slot] = (int32_t)p;
-            cur.sx[slot] = s.x; cur.sy[slot] = s.y; cur.sz[slot] = s.z;
-            cur.dx[slot] = d.x; cur.dy[slot] = d.y; cur.dz[slot] = d.z;
+            store_ray(cur, slot, s, d);
             const double lambda = load_in<In>(a.photons.wavelength, p);
             // Photon::assert_wavelength_is_positive (Photon.cpp:20-28):
             // merlict throws std::invalid_argument before propagating
@@ -78,69 +72,50 @@ wave_intake_kernel(const TraceArgs a, const WaveBuffers w, const RayPool cur) {
             cur.n_int[slot] = 1;
             cur.k_draw[slot] = 0;
             cur.err[slot] = 0;
+            cur.best_key[slot] = kNoKey;
+            cur.best_leaf[slot] = kNoLeaf;
+            cur.overflow_flag[slot] = 0u;
             if (a.results.history)
                 store_hist(a.results.history + p*hist_len, s, d, 0.0,
                            MLGPU_LEAF_PHOTON_SOURCE, MLGPU_PRODUCTION, dot(d, d) < 0.0);
+            step = 1u > max_int ? kNoStep : prepare_walk(a, cur, slot, s, d, root);
+            cur.step[slot] = step;
         } else {
-            s = mk(cur.sx[slot], cur.sy[slot], cur.sz[slot]);
-            d = mk(cur.dx[slot], cur.dy[slot], cur.dz[slot]);
-            root = cur.root[slot];
-            n_int = (uint32_t)cur.n_int[slot];
+            step = cur.step[slot];   // prepared by the previous resolve step
         }
-        w.ray_sd[3*slot] = make_double2(s.x, s.y);
-        w.ray_sd[3*slot + 1] = make_double2(s.z, d.x);
-        w.ray_sd[3*slot + 2] = make_double2(d.y, d.z);
-        w.best_key[slot] = kNoKey;
-        w.best_leaf[slot] = kNoLeaf;
-        w.overflow_flag[slot] = 0u;
-        if (n_int > max_int) {
-            w.step[slot] = kNoStep;
-        } else {
-            w.step[slot] = 0;
+        bvh = step == kStepBvh;
+        if (step == kStepTree) {
+            // traversal restricted to a frame's subtree (inside a lens):
+            // merlict's own walk of that subtree
+            v3 s, d;
+            load_ray(cur, slot, &s, &d);
             const double sd = dot(s, d);
-            if (root != 0 || sc.bvh_nodes == 0 || a.traversal == MLGPU_TRAVERSAL_FRAME_TREE) {
-                // traversal restricted to a frame's subtree (inside a lens):
-                // merlict's own walk of that subtree
-                bool over = false;
-                int32_t i = root;
-                const int32_t end = __ldg(&sc.node_meta[root].x);
-                while (i < end) {
-                    const double2* np = reinterpret_cast<const double2*>(sc.node + i);
-                    const double2 n01 = __ldg(np), n23 = __ldg(np + 1);
-                    const int2 meta = __ldg(&sc.node_meta[i]);
-                    if (!sphere_cull(make_double4(n01.x, n01.y, n23.x, n23.y), s, d, sd)) {
-                        i = meta.x;
-                        continue;
-                    }
-                    if (meta.y >= 0) {
-                        // candidates by slot; a leaf without geometry has none
-                        // (and no intersection in merlict either)
-                        const int32_t sl = __ldg(sc.leaf_slot + meta.y);
-                        if (sl >= 0) {
-                            if (nc < kTreeCands) cand[nc++] = sl;
-                            else over = true;
-                        }
-                    }
-                    i++;
-                }
-                if (over) {
-                    mark_overflow(w, slot);
-                    nc = 0;
-                }
-            } else {
-                // merlict tests the root frame's own sphere first
-                const double2* np = reinterpret_cast<const double2*>(sc.node);
+            const int32_t root = cur.root[slot];
+            bool over = false;
+            int32_t i = root;
+            const int32_t end = __ldg(&sc.node_meta[root].x);
+            while (i < end) {
+                const double2* np = reinterpret_cast<const double2*>(sc.node + i);
                 const double2 n01 = __ldg(np), n23 = __ldg(np + 1);
-                if (sphere_cull(make_double4(n01.x, n01.y, n23.x, n23.y), s, d, sd)) {
-                    bvh = true;
-                    const float ox = (float)s.x, oy = (float)s.y, oz = (float)s.z;
-                    float fdx = (float)d.x, fdy = (float)d.y, fdz = (float)d.z;
-                    if (fabsf(fdx) < 1e-30f) fdx = copysignf(1e-30f, fdx);
-                    if (fabsf(fdy) < 1e-30f) fdy = copysignf(1e-30f, fdy);
-                    if (fabsf(fdz) < 1e-30f) fdz = copysignf(1e-30f, fdz);
-                    w.ray_o[slot] = make_float4(ox, oy, oz, box_inflation(sc, ox, oy, oz));
-                    w.ray_i[slot] = make_float4(1.0f/fdx, 1.0f/fdy, 1.0f/fdz, 0.0f);
+                const int2 meta = __ldg(&sc.node_meta[i]);
+                if (!sphere_cull(make_double4(n01.x, n01.y, n23.x, n23.y), s, d, sd)) {
+                    i = meta.x;
+                    continue;
                 }
+                if (meta.y >= 0) {
+                    // candidates by slot; a leaf without geometry has none
+                    // (and no intersection in merlict either)
+                    const int32_t sl = __ldg(sc.leaf_slot + meta.y);
+                    if (sl >= 0) {
+                        if (nc < kTreeCands) cand[nc++] = sl;
+                        else over = true;
+                    }
+                }
+                i++;
+            }
+            if (over) {
+                mark_overflow(w, cur, slot);
+                nc = 0;
             }
         }
     }
@@ -148,12 +123,12 @@ wave_intake_kernel(const TraceArgs a, const WaveBuffers w, const RayPool cur) {
     const uint32_t qb = warp_reserve(&w.counters->level_len[0], bvh ? 1u : 0u);
     if (bvh) {
         if (qb < w.level_cap) w.level_q[0][qb] = make_uint2(slot, 0u);
-        else mark_overflow(w, slot);
+        else mark_overflow(w, cur, slot);
     }
     const uint32_t cb = warp_reserve(&w.counters->isect_len, (uint32_t)nc);
     for (int k = 0; k < nc; k++) {
         if (cb + k < w.isect_cap) w.isect_q[cb + k] = make_uint2(slot, (uint32_t)cand[k]);
-        else mark_overflow(w, slot);
+        else mark_overflow(w, cur, slot);
     }
 }
 
@@ -268,13 +243,17 @@ struct WalkRay {        // a lane's ray, published to its warp
 };
 
 __global__ void __launch_bounds__(kLevelThreads, 4)
-wave_level_kernel(const TraceArgs a, const WaveBuffers w, int level, int staged) {
+wave_level_kernel(const TraceArgs a, const WaveBuffers w, const RayPool cur, int level,
+                  int staged) {
     extern __shared__ float4 stage[];
     __shared__ WalkRay s_ray[kLevelWarps][32];
     __shared__ int2 s_range[kLevelWarps][32*kBvhWidth];   // (leaf-range reference, lane)
     const DevScene& sc = a.scene;
-    const uint2* in = w.level_q[level & 1];
-    uint2* out = w.level_q[(level + 1) & 1];
+    // the ping-pong queues chosen by a select: an index into the parameter
+    // array would make the compiler copy the whole parameter block to local
+    // memory
+    const uint2* in = (level & 1) ? w.level_q[1] : w.level_q[0];
+    uint2* out = (level & 1) ? w.level_q[0] : w.level_q[1];
     const uint32_t len = w.counters->level_len[level];
     const uint32_t n = len < w.level_cap ? len : w.level_cap;
     const bool last = level + 1 >= kMaxBvhLevels;
@@ -296,8 +275,8 @@ wave_level_kernel(const TraceArgs a, const WaveBuffers w, int level, int staged)
         if (e < n) {
             const uint2 q = in[e];
             slot = q.x;
-            o = w.ray_o[slot];
-            iv = w.ray_i[slot];
+            o = cur.ray_o[slot];
+            iv = cur.ray_i[slot];
             if ((uint32_t)((int32_t)q.y - base) < (uint32_t)staged)
                 hit = qnode_hits<true>(stage + (sizeof(QNode)/16)*((int32_t)q.y - base), o, iv,
                                        &child);
@@ -314,7 +293,7 @@ wave_level_kernel(const TraceArgs a, const WaveBuffers w, int level, int staged)
         for (int k = 0; k < kBvhWidth; k++) {
             if (!(hit & (1u << k)) || child_ref(child, k) < 0) continue;
             if (!last && nb < w.level_cap) out[nb] = make_uint2(slot, (uint32_t)child_ref(child, k));
-            else mark_overflow(w, slot);
+            else mark_overflow(w, cur, slot);
             nb++;
         }
         // the warp's hit leaf ranges, listed in shared memory
@@ -355,7 +334,7 @@ wave_level_kernel(const TraceArgs a, const WaveBuffers w, int level, int staged)
                 pass &= pass - 1u;
                 // the candidate by its slot (leaf slots follow the BVH's ranges)
                 if (cb < w.isect_cap) w.isect_q[cb] = make_uint2(src_slot, (uint32_t)(start + j));
-                else mark_overflow(w, src_slot);
+                else mark_overflow(w, cur, src_slot);
                 cb++;
             }
         }
@@ -390,7 +369,7 @@ wave_walk_kernel(const TraceArgs a, const WaveBuffers w, const RayPool cur) {
             const uint2 q = w.level_q[0][e];
             slot = q.x;
             const uint32_t root = q.y;
-            const float4 o = w.ray_o[slot], iv = w.ray_i[slot];
+            const float4 o = cur.ray_o[slot], iv = cur.ray_i[slot];
             const float3 dv = make_float3(1.0f/iv.x, 1.0f/iv.y, 1.0f/iv.z);
             v3 s = mk(0, 0, 0), d = mk(0, 0, 0);
             double sd = 0.0;
@@ -413,7 +392,7 @@ wave_walk_kernel(const TraceArgs a, const WaveBuffers w, const RayPool cur) {
                     const int32_t start = (ref & 0x7fffffff) >> 3;
                     const int32_t count = (ref & 7) + 1;
                     if (!kF32 && !have_ray) {
-                        load_ray(w, slot, &s, &d);
+                        load_ray(cur, slot, &s, &d);
                         sd = dot(s, d);
                         have_ray = true;
                     }
@@ -435,13 +414,13 @@ wave_walk_kernel(const TraceArgs a, const WaveBuffers w, const RayPool cur) {
             }
         }
         if (over) {
-            mark_overflow(w, slot);
+            mark_overflow(w, cur, slot);
             nc = 0;
         }
         const uint32_t cb = warp_reserve(&w.counters->isect_len, nc);
         for (uint32_t k = 0; k < nc; k++) {
             if (cb + k < w.isect_cap) w.isect_q[cb + k] = make_uint2(slot, (uint32_t)cand[k]);
-            else mark_overflow(w, slot);
+            else mark_overflow(w, cur, slot);
         }
     }
 }
@@ -500,14 +479,14 @@ cudaError_t launch_wave_iteration(const TraceArgs& a, const WaveBuffers& w, cons
         for (int k = 0; k < a.scene.bvh_levels; k++) {
             const int count = a.scene.bvh_level_start[k + 1] - a.scene.bvh_level_start[k];
             const int staged = k < w.staged_levels && count <= kMaxStagedNodes ? count : 0;
-            wave_level_kernel<<<w.grid, 256, (size_t)staged*sizeof(QNode), s>>>(a, w, k,
+            wave_level_kernel<<<w.grid, 256, (size_t)staged*sizeof(QNode), s>>>(a, w, cur, k,
                                                                                    staged);
         }
     }
     if (ev) cudaEventRecord(ev[2], s);
     if (form == MLGPU_TRACER_FP64) {
         wave_isect_kernel<kIsectFp64><<<w.grid, 256, 0, s>>>(a, w, cur);
-        wave_tie_kernel<<<w.grid, 256, 0, s>>>(w);
+        wave_tie_kernel<<<w.grid, 256, 0, s>>>(w, cur);
         if (ev) cudaEventRecord(ev[3], s);
         wave_overflow_kernel<<<148, 128, 0, s>>>(a, w, cur);
         if (a.out_dtype == MLGPU_F64)
