@@ -594,30 +594,36 @@ int record_wave_graph(mlgpu_scene* scene, const TraceArgs& a, const WaveBuffers&
 // intersection arithmetic (FP64 or one of the FP32 forms).
 // The order in which a batch's photons enter the tracers: coherent (a sort
 // by support and direction, photon_order.cu) or the input order (a.order
-// stays null).
+// and a.sorted stay null).  With `records` the coherent order comes as the
+// photons themselves, sorted into 64-byte records (a.sorted) that the
+// wavefront intake reads in sequence, up to 2^28 photons (16 GiB of
+// records); otherwise, and beyond that, as photon indices (a.order).
 int tracing_order(mlgpu_scene* scene, TraceArgs* a, const mlgpu_settings* st,
-                  cudaStream_t stream) {
+                  cudaStream_t stream, bool records) {
     const bool coherent = a->num_photons < (1ull << 32) &&
         (st->photon_order == MLGPU_ORDER_COHERENT ||
          (st->photon_order == MLGPU_ORDER_DEFAULT && a->num_photons >= 65536));
     if (!coherent) return MLGPU_OK;
-    const size_t obytes = (size_t)a->num_photons*sizeof(uint32_t);
+    const bool rec = records && a->num_photons <= (1ull << 28);
+    const size_t obytes = (size_t)a->num_photons*(rec ? 4*sizeof(double2) : sizeof(uint32_t));
     MLGPU_CUDA(scene->order.reserve(obytes + 256 + photon_order_scratch_bytes(a->num_photons)));
-    uint32_t* order = static_cast<uint32_t*>(scene->order.ptr);
     char* scratch = static_cast<char*>(scene->order.ptr) + ((obytes + 255) & ~size_t(255));
     if (!scene->wave_grid) scene->wave_grid = wave_persistent_blocks();
+    uint32_t* order = rec ? nullptr : static_cast<uint32_t*>(scene->order.ptr);
+    double2* sorted = rec ? static_cast<double2*>(scene->order.ptr) : nullptr;
     const cudaError_t e = launch_photon_order(a->photons, a->in_dtype, a->num_photons, order,
-                                              scratch, scene->wave_grid, stream);
+                                              sorted, scratch, scene->wave_grid, stream);
     if (e != cudaSuccess) return cuda_fail(e, "photon order kernels");
     scene->launches += 7;
     a->order = order;
+    a->sorted = sorted;
     return MLGPU_OK;
 }
 
 int run_wavefront(mlgpu_scene* scene, TraceArgs a, const mlgpu_settings* st,
                   cudaStream_t stream) {
     const int form = st->tracer;
-    const int ro = tracing_order(scene, &a, st, stream);
+    const int ro = tracing_order(scene, &a, st, stream, true);
     if (ro) return ro;
     const uint32_t want = st->pool_size ? st->pool_size : kWavePool;
     const uint32_t pool = (uint32_t)std::min<uint64_t>(a.num_photons, want);
@@ -692,7 +698,7 @@ int launch(mlgpu_scene* scene, const TraceArgs& a, const mlgpu_settings* st,
     case MLGPU_TRACER_FP32_PURE: return run_wavefront(scene, a, st, stream);
     case MLGPU_TRACER_FP64_QUEUE: {
         TraceArgs q = a;
-        const int ro = tracing_order(scene, &q, st, stream);
+        const int ro = tracing_order(scene, &q, st, stream, false);
         if (ro) return ro;
         MLGPU_CUDA(scene->queue.reserve(256));
         int sms = 0, dev = 0;

@@ -181,7 +181,10 @@ struct TraceArgs {
     uint32_t max_interactions;
     int32_t start_node;
     int32_t traversal;          // MLGPU_TRAVERSAL_*
-    const uint32_t* order;      // wavefront intake order of the photons, or null (input order)
+    const uint32_t* order;      // tracing order of the photons, or null (input order)
+    // or the photons themselves in tracing order, 64 bytes each (then
+    // `order` is null): (sx, sy), (sz, dx), (dy, dz), (wavelength, index bits)
+    const double2* sorted;
 };
 
 struct BvhHost {
@@ -321,10 +324,13 @@ cudaError_t launch_signal_chain_scatter(const SignalChainArgs& a, void* pulse_sc
                                         size_t pulse_bytes, uint64_t num_pulses, int grid,
                                         cudaStream_t s);
 // A coherent tracing order of a photon batch (photon_order.cu): `order`
-// receives n photon indices; `scratch` holds photon_order_scratch_bytes(n).
+// receives n photon indices or, when `sorted` is not null, `sorted` receives
+// the photons themselves in that order (TraceArgs::sorted's 64-byte
+// records; `order` is then unused); `scratch` holds
+// photon_order_scratch_bytes(n).
 size_t photon_order_scratch_bytes(uint64_t n);
 cudaError_t launch_photon_order(const DevPhotons& p, int in_dtype, uint64_t n, uint32_t* order,
-                                void* scratch, int grid, cudaStream_t s);
+                                double2* sorted, void* scratch, int grid, cudaStream_t s);
 int wave_persistent_blocks();
 // Zeroes counts (and time_hist) and bins n arrivals into them: two kernel
 // launches, no scratch memory (bin.cu).

@@ -174,6 +174,29 @@ order_scatter_kernel(uint64_t n, const uint32_t* key, uint32_t* next, uint32_t* 
         order[atomicAdd(&next[key[i]], 1u)] = (uint32_t)i;
 }
 
+// The photons themselves into their place in the order: one 64-byte record
+// each, (sx, sy), (sz, dx), (dy, dz), (wavelength, index), the values as
+// the tracers read them (a float input widened to double, which is exact).
+// The input planes are read in order and the record stored whole, so that
+// the intake reads the records sequentially instead of gathering seven
+// planes through a permutation.
+template <typename In>
+__global__ void __launch_bounds__(256)
+order_scatter_records_kernel(const DevPhotons p, uint64_t n, const uint32_t* key, uint32_t* next,
+                             double2* sorted) {
+    for (uint64_t i = blockIdx.x*(uint64_t)blockDim.x + threadIdx.x; i < n;
+         i += (uint64_t)gridDim.x*blockDim.x) {
+        auto ld = [i](const void* plane) { return (double)__ldg(static_cast<const In*>(plane) + i); };
+        const double sx = ld(p.sx), sy = ld(p.sy), sz = ld(p.sz);
+        const double dx = ld(p.dx), dy = ld(p.dy), dz = ld(p.dz), wl = ld(p.wavelength);
+        double2* r = sorted + 4*(uint64_t)atomicAdd(&next[key[i]], 1u);
+        r[0] = make_double2(sx, sy);
+        r[1] = make_double2(sz, dx);
+        r[2] = make_double2(dy, dz);
+        r[3] = make_double2(wl, __longlong_as_double((long long)i));
+    }
+}
+
 }  // namespace
 
 size_t photon_order_scratch_bytes(uint64_t n) {
@@ -181,7 +204,7 @@ size_t photon_order_scratch_bytes(uint64_t n) {
 }
 
 cudaError_t launch_photon_order(const DevPhotons& p, int in_dtype, uint64_t n, uint32_t* order,
-                                void* scratch, int grid, cudaStream_t s) {
+                                double2* sorted, void* scratch, int grid, cudaStream_t s) {
     uint32_t* key = static_cast<uint32_t*>(scratch);
     uint32_t* hist = key + n;
     uint32_t* block_sum = hist + kCells;
@@ -204,7 +227,12 @@ cudaError_t launch_photon_order(const DevPhotons& p, int in_dtype, uint64_t n, u
     order_scan_blocks_kernel<<<kCells/kScanBlock, kScanBlock, 0, s>>>(hist, block_sum);
     order_scan_sums_kernel<<<1, kScanBlock, 0, s>>>(block_sum, (int)(kCells/kScanBlock));
     order_scan_add_kernel<<<kCells/kScanBlock, kScanBlock, 0, s>>>(hist, block_sum);
-    order_scatter_kernel<<<grid, 256, 0, s>>>(n, key, hist, order);
+    if (!sorted)
+        order_scatter_kernel<<<grid, 256, 0, s>>>(n, key, hist, order);
+    else if (in_dtype == MLGPU_F64)
+        order_scatter_records_kernel<double><<<grid, 256, 0, s>>>(p, n, key, hist, sorted);
+    else
+        order_scatter_records_kernel<float><<<grid, 256, 0, s>>>(p, n, key, hist, sorted);
     return cudaGetLastError();
 }
 

@@ -54,15 +54,29 @@ wave_intake_kernel(const TraceArgs a, const WaveBuffers w, const RayPool cur) {
         int step;
         if (slot >= active) {
             const uint64_t q = next_input + (slot - active);
-            const uint64_t p = a.order ? (uint64_t)__ldg(a.order + q) : q;
-            const v3 s = mk(load_in<In>(a.photons.sx, p), load_in<In>(a.photons.sy, p),
-                            load_in<In>(a.photons.sz, p));
-            const v3 d = normalized(mk(load_in<In>(a.photons.dx, p), load_in<In>(a.photons.dy, p),
-                                       load_in<In>(a.photons.dz, p)));
+            uint64_t p;
+            v3 s, d;
+            double lambda;
+            if (a.sorted) {
+                // the photon's record in tracing order
+                const double2* r = a.sorted + 4*q;
+                const double2 r0 = __ldcs(r), r1 = __ldcs(r + 1), r2 = __ldcs(r + 2),
+                              r3 = __ldcs(r + 3);
+                s = mk(r0.x, r0.y, r1.x);
+                d = normalized(mk(r1.y, r2.x, r2.y));
+                lambda = r3.x;
+                p = (uint64_t)__double_as_longlong(r3.y);
+            } else {
+                p = a.order ? (uint64_t)__ldg(a.order + q) : q;
+                s = mk(load_in<In>(a.photons.sx, p), load_in<In>(a.photons.sy, p),
+                       load_in<In>(a.photons.sz, p));
+                d = normalized(mk(load_in<In>(a.photons.dx, p), load_in<In>(a.photons.dy, p),
+                                  load_in<In>(a.photons.dz, p)));
+                lambda = load_in<In>(a.photons.wavelength, p);
+            }
             const int32_t root = a.start_node;
             cur.photon[slot] = (int32_t)p;
             store_ray(cur, slot, s, d);
-            const double lambda = load_in<In>(a.photons.wavelength, p);
             // Photon::assert_wavelength_is_positive (Photon.cpp:20-28):
             // merlict throws std::invalid_argument before propagating
             if (lambda <= 0.0) raise_error(sc.error_word, MLGPU_ERR_INVALID_ARGUMENT);
