@@ -49,10 +49,18 @@ FLOP_STAGE = {"nodes": "walk", "leaves": "intersect", "caps": "intersect",
               "funcs": "resolve"}
 FP64_PEAK_TFLOPS_NOMINAL = 37.0   # B200 vector FP64 with FMAs, nominal
 # DRAM bytes per photon of each kernel class on the light-field telescope,
-# from an ncu capture of the timed step (dram__bytes_read.sum +
-# dram__bytes_write.sum summed over the class's launches, divided by the
-# photons of the step; profiles/wavefront_fp64_light_field_telescope.md)
-STAGE_DRAM_BYTES_PER_PHOTON = {}
+# from an ncu capture of the timed step of 4e6 photons (dram__bytes_read.sum
+# + dram__bytes_write.sum summed over the class's launches, divided by the
+# photons of the step; profiles/wavefront_fp64_light_field_telescope.md):
+# walk = the BVH level kernels; intake = intake + counter kernel;
+# intersect = intersection + tie kernels; resolve = overflow walk +
+# resolve + counter kernel; bin = zeroing + binning kernels.  The tracing
+# order's kernels (run once per call, before the first iteration) are in
+# no class: 188 B per photon.  The traffic of a step grows with its photons
+# (the same scene and pool), so the bench scales these figures by its own
+# photon count.
+STAGE_DRAM_BYTES_PER_PHOTON = {"walk": 807.0, "intake": 247.5, "intersect": 1079.9,
+                               "resolve": 897.4, "bin": 4.0}
 FP32_PEAK_TFLOPS_NOMINAL = 75.0   # B200 vector FP32 (non-tensor), nominal
 WORKLOAD = "light-field telescope, 1039 lenses x 61 lixels (config 1)"
 # the signal chain after binning (workload "signal"): quantum efficiency,
