@@ -4,6 +4,7 @@
 #include <cstdio>
 #include <algorithm>
 #include <cstring>
+#include <functional>
 #include <string>
 #include <mutex>
 #include <vector>
@@ -162,10 +163,11 @@ struct mlgpu_scene {
     cudaStream_t capture_stream = nullptr;
     uint64_t launches = 0;               // kernels launched for this scene
     mlgpu_wavefront_stats wave_stats = {0, 0, 0};
-    // mlgpu_propagate_host's pipeline: trace, upload and download streams;
-    // events: the caller's default stream, inputs of each piece, results of each piece
-    cudaStream_t host_stream[3] = {nullptr, nullptr, nullptr};
-    cudaEvent_t host_event[1 + 2*kHostPieces] = {};
+    // mlgpu_propagate_host's pipeline: trace, upload, download and ordering
+    // streams; events: the caller's default stream, then per piece its
+    // inputs, its sorted records and its results, then the cleared counters
+    cudaStream_t host_stream[4] = {nullptr, nullptr, nullptr, nullptr};
+    cudaEvent_t host_event[2 + 3*kMaxFeedChunks] = {};
     Profiler prof;
 };
 
@@ -509,7 +511,7 @@ int wave_buffers(mlgpu_scene* scene, uint32_t pool, int grid, int staged, uint32
     const size_t isect_cap = queue_cap ? queue_cap : 16*P;
     const size_t per_pool = up(P*48) + 3*up(P*8) + 8*up(P*4) + 2*up(P*16);
     const size_t rest = 2*up(level_cap*8) + up(isect_cap*8) + up(isect_cap*8) + up(P*4);
-    MLGPU_CUDA(scene->wave.reserve(256 + 2*per_pool + rest));
+    MLGPU_CUDA(scene->wave.reserve(kWaveCounterBytes + 2*per_pool + rest));
     if (!scene->wave_host) MLGPU_CUDA(cudaMallocHost(&scene->wave_host, sizeof(WaveCounters)));
     if (!scene->wave_host_dev)
         MLGPU_CUDA(cudaHostGetDevicePointer(reinterpret_cast<void**>(&scene->wave_host_dev),
@@ -517,7 +519,7 @@ int wave_buffers(mlgpu_scene* scene, uint32_t pool, int grid, int staged, uint32
     if (!scene->wave_grid) scene->wave_grid = wave_persistent_blocks();
     char* b = static_cast<char*>(scene->wave.ptr);
     w->counters = reinterpret_cast<WaveCounters*>(b);
-    b += 256;
+    b += kWaveCounterBytes;
     auto take = [&](size_t bytes) { char* p = b; b += up(bytes); return p; };
     RayPool* pools[2] = {p0, p1};
     for (RayPool* p : pools) {
@@ -612,7 +614,7 @@ int tracing_order(mlgpu_scene* scene, TraceArgs* a, const mlgpu_settings* st,
     uint32_t* order = rec ? nullptr : static_cast<uint32_t*>(scene->order.ptr);
     double2* sorted = rec ? static_cast<double2*>(scene->order.ptr) : nullptr;
     const cudaError_t e = launch_photon_order(a->photons, a->in_dtype, a->num_photons, order,
-                                              sorted, scratch, scene->wave_grid, stream);
+                                              sorted, 0, scratch, scene->wave_grid, stream);
     if (e != cudaSuccess) return cuda_fail(e, "photon order kernels");
     scene->launches += 7;
     a->order = order;
@@ -620,11 +622,37 @@ int tracing_order(mlgpu_scene* scene, TraceArgs* a, const mlgpu_settings* st,
     return MLGPU_OK;
 }
 
+// A fed propagation (mlgpu_propagate_host's pipeline): the batch's photon
+// planes arrive on the device piece by piece (in_ready[c] fires when piece
+// c's planes are there); each piece is sorted into its records on the
+// ordering stream and published to the tracer, and `download(c)` is called
+// once every photon of piece c has finished.
+struct FeedPlan {
+    int pieces;
+    uint64_t start[kMaxFeedChunks + 1];   // piece c: photons [start[c], start[c + 1])
+    const void* planes[7];                // the whole batch's device planes
+    cudaStream_t order;
+    const cudaEvent_t* in_ready;
+    const cudaEvent_t* ord_ready;
+    cudaEvent_t ctr_ready;
+    double2* records;
+    void* scratch;                        // photon_order_scratch_bytes of the largest piece
+    std::function<int(int)> download;
+};
+
 int run_wavefront(mlgpu_scene* scene, TraceArgs a, const mlgpu_settings* st,
-                  cudaStream_t stream) {
+                  cudaStream_t stream, const FeedPlan* feed = nullptr) {
     const int form = st->tracer;
-    const int ro = tracing_order(scene, &a, st, stream, true);
-    if (ro) return ro;
+    if (feed) {
+        a.sorted = feed->records;
+        a.order = nullptr;
+        a.fed = 1;
+        a.feed_chunks = feed->pieces;
+        for (int c = 0; c <= feed->pieces; c++) a.feed_start[c] = feed->start[c];
+    } else {
+        const int ro = tracing_order(scene, &a, st, stream, true);
+        if (ro) return ro;
+    }
     const uint32_t want = st->pool_size ? st->pool_size : kWavePool;
     const uint32_t pool = (uint32_t)std::min<uint64_t>(a.num_photons, want);
     WaveBuffers w;
@@ -642,9 +670,34 @@ int run_wavefront(mlgpu_scene* scene, TraceArgs a, const mlgpu_settings* st,
         if (r) return r;
     }
     MLGPU_CUDA(cudaMemsetAsync(w.counters, 0, sizeof(WaveCounters), stream));
+    bool downloaded[kMaxFeedChunks] = {};
+    if (feed) {
+        // each piece: sorted into its records once its planes are on the
+        // device, then published; the tracer starts with the first piece
+        MLGPU_CUDA(cudaEventRecord(feed->ctr_ready, stream));
+        MLGPU_CUDA(cudaStreamWaitEvent(feed->order, feed->ctr_ready, 0));
+        const size_t ein = a.in_dtype == MLGPU_F64 ? 8 : 4;
+        for (int c = 0; c < feed->pieces; c++) {
+            const uint64_t a0 = feed->start[c], len = feed->start[c + 1] - a0;
+            MLGPU_CUDA(cudaStreamWaitEvent(feed->order, feed->in_ready[c], 0));
+            DevPhotons p;
+            const void** dp[7] = {&p.sx, &p.sy, &p.sz, &p.dx, &p.dy, &p.dz, &p.wavelength};
+            for (int k = 0; k < 7; k++)
+                *dp[k] = static_cast<const char*>(feed->planes[k]) + a0*ein;
+            cudaError_t e = launch_photon_order(p, a.in_dtype, len, nullptr, feed->records + 4*a0,
+                                                a0, feed->scratch, scene->wave_grid, feed->order);
+            if (e == cudaSuccess) e = launch_feed_publish(w.counters, a0 + len, feed->order);
+            if (e == cudaSuccess) e = cudaEventRecord(feed->ord_ready[c], feed->order);
+            if (e != cudaSuccess) return cuda_fail(e, "ordering a piece");
+            scene->launches += 8;
+        }
+        MLGPU_CUDA(cudaStreamWaitEvent(stream, feed->ord_ready[0], 0));
+        MLGPU_CUDA(launch_feed_snapshot(w.counters, stream));
+        scene->launches++;
+    }
     // every iteration advances each live photon by one step
     const uint64_t bound = (a.num_photons*(uint64_t)(a.max_interactions + 1))/pool +
-        a.max_interactions + 16 + (uint64_t)period;
+        a.max_interactions + 16 + (uint64_t)period*(feed ? feed->pieces + 1 : 1);
     // launches per iteration: intake and its counters, the walk, intersections
     // and ties, the overflow walk, resolve and its counters
     const int walk_launches = w.walk == MLGPU_WALK_STACK ? 1 : scene->dev.bvh_levels;
@@ -679,7 +732,26 @@ int run_wavefront(mlgpu_scene* scene, TraceArgs a, const mlgpu_settings* st,
             scene->launches++;
         }
         MLGPU_CUDA(cudaStreamSynchronize(stream));
-        if (scene->wave_host->active == 0 && scene->wave_host->next_input >= a.num_photons) break;
+        const WaveCounters& h = *scene->wave_host;
+        if (feed) {
+            // pieces whose photons have all finished go back to the host
+            for (int c = 0; c < feed->pieces; c++) {
+                if (downloaded[c] || h.done[c] < feed->start[c + 1] - feed->start[c]) continue;
+                downloaded[c] = true;
+                const int r = feed->download(c);
+                if (r) return r;
+            }
+            // an empty pool with the next piece still on its way: the trace
+            // stream waits for that piece (no kernel spins on it)
+            if (h.active == 0 && h.next_input == h.avail_snap && h.next_input < a.num_photons) {
+                int c = 0;
+                while (c + 1 < feed->pieces && feed->start[c + 1] <= h.next_input) c++;
+                MLGPU_CUDA(cudaStreamWaitEvent(stream, feed->ord_ready[c], 0));
+                MLGPU_CUDA(launch_feed_snapshot(w.counters, stream));
+                scene->launches++;
+            }
+        }
+        if (h.active == 0 && h.next_input >= a.num_photons) break;
         if (iteration > bound)
             return fail(MLGPU_ERR_RUNTIME, "wavefront tracer did not drain its pool");
     }
@@ -1251,8 +1323,19 @@ int propagate_host(mlgpu_scene* scene, const mlgpu_photons* photons, uint64_t n,
     for (const Plane& b : back) all_pinned = all_pinned && pinned(b.host);
     const uint64_t pool = settings->tracer == MLGPU_TRACER_FP64_PLAIN || !settings->pool_size
         ? kWavePool : settings->pool_size;
-    const int chunks = all_pinned
-        ? (int)std::max<uint64_t>(1, std::min<uint64_t>(kHostChunks, n/pool)) : 1;
+    // A wavefront form in the coherent order is fed: one propagation over
+    // the batch that admits each piece's photons as their sorted records
+    // land, pieces of a quarter pool or more, each piece's results going
+    // back as soon as its photons have all finished.  Otherwise each piece
+    // is a propagation of its own, traced while the next one uploads.
+    const bool wavefront = settings->tracer == MLGPU_TRACER_FP64 ||
+        settings->tracer == MLGPU_TRACER_FP32 || settings->tracer == MLGPU_TRACER_FP32_PURE;
+    const bool coherent = settings->photon_order == MLGPU_ORDER_COHERENT ||
+        (settings->photon_order == MLGPU_ORDER_DEFAULT && n >= 65536);
+    const bool fed = all_pinned && wavefront && coherent && n >= pool && n <= (1ull << 28);
+    const int chunks = !all_pinned ? 1
+        : fed ? (int)std::max<uint64_t>(1, std::min<uint64_t>(kMaxFeedChunks - 1, n/(pool/4)))
+              : (int)std::max<uint64_t>(1, std::min<uint64_t>(kHostChunks, n/pool));
     // With two or more whole pieces the first and the last are halves: only
     // the first piece's inputs and the last piece's results wait uncovered.
     const int pieces = chunks > 1 ? chunks + 1 : 1;
@@ -1264,9 +1347,10 @@ int propagate_host(mlgpu_scene* scene, const mlgpu_photons* photons, uint64_t n,
             MLGPU_CUDA(cudaEventCreateWithFlags(&he, cudaEventDisableTiming));
     }
     cudaStream_t trace = scene->host_stream[0], upload = scene->host_stream[1],
-                 download = scene->host_stream[2];
+                 download = scene->host_stream[2], ordering = scene->host_stream[3];
     cudaEvent_t* in_ready = scene->host_event + 1;
-    cudaEvent_t* out_ready = scene->host_event + 1 + kHostPieces;
+    cudaEvent_t* ord_ready = scene->host_event + 1 + kMaxFeedChunks;
+    cudaEvent_t* out_ready = scene->host_event + 1 + 2*kMaxFeedChunks;
     // after the caller's work on the legacy default stream, as a call on it would be
     MLGPU_CUDA(cudaEventRecord(scene->host_event[0], 0));
     MLGPU_CUDA(cudaStreamWaitEvent(upload, scene->host_event[0], 0));
@@ -1293,11 +1377,71 @@ int propagate_host(mlgpu_scene* scene, const mlgpu_photons* photons, uint64_t n,
     // a failed piece leaves no copy in flight behind it
     auto drain = [&](int code) {
         cudaStreamSynchronize(upload);
+        cudaStreamSynchronize(ordering);
         cudaStreamSynchronize(trace);
         cudaStreamSynchronize(download);
         return code;
     };
-    for (int c = 0; c < pieces; c++) {
+    // results of photons [a0, a0 + len) back to the host once the trace
+    // stream's work so far is done
+    auto results_back = [&](uint64_t a0, uint64_t len) -> int {
+        if (cudaEventRecord(out_ready[0], trace) != cudaSuccess ||
+            cudaStreamWaitEvent(download, out_ready[0], 0) != cudaSuccess)
+            return cuda_fail(cudaGetLastError(), "pipeline event");
+        for (int k = 0; k < kPlanes; k++) {
+            if (!back[k].host) continue;
+            const cudaError_t e = cudaMemcpyAsync(
+                static_cast<char*>(back[k].host) + a0*back[k].bytes,
+                static_cast<char*>(dev_plane[k]) + a0*back[k].bytes, len*back[k].bytes,
+                cudaMemcpyDeviceToHost, download);
+            if (e != cudaSuccess) return cuda_fail(e, "copying results to the host");
+        }
+        return MLGPU_OK;
+    };
+    if (fed) {
+        uint64_t max_len = 0;
+        for (int c = 0; c < pieces; c++) max_len = std::max(max_len, first(c + 1) - first(c));
+        const size_t rbytes = (size_t)n*4*sizeof(double2);
+        if (scene->order.reserve(rbytes + 256 + photon_order_scratch_bytes(max_len)) != cudaSuccess)
+            return drain(cuda_fail(cudaGetLastError(), "photon records"));
+        if (!scene->wave_grid) scene->wave_grid = wave_persistent_blocks();
+        FeedPlan plan;
+        plan.pieces = pieces;
+        for (int c = 0; c <= pieces; c++) plan.start[c] = first(c);
+        for (int k = 0; k < 7; k++) plan.planes[k] = din + k*n*ein;
+        plan.order = ordering;
+        plan.in_ready = in_ready;
+        plan.ord_ready = ord_ready;
+        plan.ctr_ready = scene->host_event[1 + 3*kMaxFeedChunks];
+        plan.records = static_cast<double2*>(scene->order.ptr);
+        plan.scratch = static_cast<char*>(scene->order.ptr) + ((rbytes + 255) & ~size_t(255));
+        plan.download = [&](int c) { return results_back(first(c), first(c + 1) - first(c)); };
+        mlgpu_photons dph = *photons;
+        const void** dp[7] = {&dph.support_x, &dph.support_y, &dph.support_z, &dph.direction_x,
+                              &dph.direction_y, &dph.direction_z, &dph.wavelength};
+        for (int k = 0; k < 7; k++) *dp[k] = din + k*n*ein;
+        dph.simulation_truth_id = nullptr;
+        mlgpu_rng drng = *rng;
+        if (stride) drng.uniforms = static_cast<const double*>(scene->staging_rng.ptr);
+        mlgpu_results dres;
+        std::memset(&dres, 0, sizeof(dres));
+        dres.dtype = results->dtype;
+        dres.sensor = static_cast<int32_t*>(dev_plane[0]);
+        dres.x = dev_plane[1];
+        dres.y = dev_plane[2];
+        dres.time = static_cast<double*>(dev_plane[3]);
+        dres.theta_x = dev_plane[4];
+        dres.theta_y = dev_plane[5];
+        dres.final_leaf = static_cast<int32_t*>(dev_plane[6]);
+        dres.info = static_cast<uint32_t*>(dev_plane[7]);
+        dres.final_position = static_cast<double*>(dev_plane[8]);
+        dres.final_direction = static_cast<double*>(dev_plane[9]);
+        dres.history = static_cast<mlgpu_history_entry*>(dev_plane[10]);
+        const TraceArgs a = make_args(scene, &dph, n, settings, &drng, &dres);
+        st = run_wavefront(scene, a, settings, trace, &plan);
+        if (st) return drain(st);
+    }
+    for (int c = 0; !fed && c < pieces; c++) {
         const uint64_t a0 = first(c), len = first(c + 1) - a0;
         if (cudaStreamWaitEvent(trace, in_ready[c], 0) != cudaSuccess)
             return drain(cuda_fail(cudaGetLastError(), "pipeline event"));

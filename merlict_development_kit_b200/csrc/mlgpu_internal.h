@@ -144,6 +144,8 @@ struct DevScene {
     int32_t bvh_level_start[kMaxBvhLevels + 1];   // nodes of level k: [start[k], start[k+1])
 };
 
+constexpr int kMaxFeedChunks = 16;   // chunks of a fed propagation
+
 struct DevPhotons {
     const void* sx; const void* sy; const void* sz;
     const void* dx; const void* dy; const void* dz;
@@ -185,6 +187,13 @@ struct TraceArgs {
     // or the photons themselves in tracing order, 64 bytes each (then
     // `order` is null): (sx, sy), (sz, dx), (dy, dz), (wavelength, index bits)
     const double2* sorted;
+    // Fed propagation (the host call's pipeline): the records arrive chunk
+    // by chunk; the intake admits photons up to WaveCounters::avail_snap
+    // instead of num_photons, and finished photons are counted per chunk
+    // (chunk c holds the photon indices [feed_start[c], feed_start[c + 1])).
+    int32_t fed;
+    int32_t feed_chunks;
+    uint64_t feed_start[kMaxFeedChunks + 1];
 };
 
 struct BvhHost {
@@ -205,8 +214,16 @@ struct WaveCounters {
     unsigned int overflow_len;       // slots sent to merlict's own walk
     unsigned int level_len[kMaxBvhLevels];   // (slot, node) pairs of each BVH level
     unsigned long long overflow_total;       // overflow_len summed over the iterations
+    // fed propagation: photons whose records have arrived (raised by the
+    // chunks' publish kernels on another stream), its value as the current
+    // iteration uses it, and the finished photons of each chunk
+    unsigned long long avail;
+    unsigned long long avail_snap;
+    unsigned int done[kMaxFeedChunks];
 };
-static_assert(sizeof(WaveCounters) <= 256, "the counters sit in the first 256 bytes of the pool");
+constexpr size_t kWaveCounterBytes = 512;
+static_assert(sizeof(WaveCounters) <= kWaveCounterBytes,
+              "the counters sit in the first 512 bytes of the pool");
 
 // One pool of ray slots; two pools alternate between iterations.  The
 // resolve step of an iteration writes each surviving ray into the next
@@ -330,7 +347,12 @@ cudaError_t launch_signal_chain_scatter(const SignalChainArgs& a, void* pulse_sc
 // photon_order_scratch_bytes(n).
 size_t photon_order_scratch_bytes(uint64_t n);
 cudaError_t launch_photon_order(const DevPhotons& p, int in_dtype, uint64_t n, uint32_t* order,
-                                double2* sorted, void* scratch, int grid, cudaStream_t s);
+                                double2* sorted, uint64_t index_base, void* scratch, int grid,
+                                cudaStream_t s);
+// Fed propagation: raises WaveCounters::avail to `avail` once the work
+// before it on `s` is done; copies avail into avail_snap.
+cudaError_t launch_feed_publish(WaveCounters* c, uint64_t avail, cudaStream_t s);
+cudaError_t launch_feed_snapshot(WaveCounters* c, cudaStream_t s);
 int wave_persistent_blocks();
 // Zeroes counts (and time_hist) and bins n arrivals into them: two kernel
 // launches, no scratch memory (bin.cu).

@@ -175,7 +175,7 @@ order_scatter_kernel(uint64_t n, const uint32_t* key, uint32_t* next, uint32_t* 
 }
 
 // The photons themselves into their place in the order: one 64-byte record
-// each, (sx, sy), (sz, dx), (dy, dz), (wavelength, index), the values as
+// each, (sx, sy), (sz, dx), (dy, dz), (wavelength, index_base + i), the values as
 // the tracers read them (a float input widened to double, which is exact).
 // The input planes are read in order and the record stored whole, so that
 // the intake reads the records sequentially instead of gathering seven
@@ -183,7 +183,7 @@ order_scatter_kernel(uint64_t n, const uint32_t* key, uint32_t* next, uint32_t* 
 template <typename In>
 __global__ void __launch_bounds__(256)
 order_scatter_records_kernel(const DevPhotons p, uint64_t n, const uint32_t* key, uint32_t* next,
-                             double2* sorted) {
+                             double2* sorted, uint64_t index_base) {
     for (uint64_t i = blockIdx.x*(uint64_t)blockDim.x + threadIdx.x; i < n;
          i += (uint64_t)gridDim.x*blockDim.x) {
         auto ld = [i](const void* plane) { return (double)__ldg(static_cast<const In*>(plane) + i); };
@@ -193,7 +193,7 @@ order_scatter_records_kernel(const DevPhotons p, uint64_t n, const uint32_t* key
         r[0] = make_double2(sx, sy);
         r[1] = make_double2(sz, dx);
         r[2] = make_double2(dy, dz);
-        r[3] = make_double2(wl, __longlong_as_double((long long)i));
+        r[3] = make_double2(wl, __longlong_as_double((long long)(index_base + i)));
     }
 }
 
@@ -204,7 +204,8 @@ size_t photon_order_scratch_bytes(uint64_t n) {
 }
 
 cudaError_t launch_photon_order(const DevPhotons& p, int in_dtype, uint64_t n, uint32_t* order,
-                                double2* sorted, void* scratch, int grid, cudaStream_t s) {
+                                double2* sorted, uint64_t index_base, void* scratch, int grid,
+                                cudaStream_t s) {
     uint32_t* key = static_cast<uint32_t*>(scratch);
     uint32_t* hist = key + n;
     uint32_t* block_sum = hist + kCells;
@@ -230,9 +231,11 @@ cudaError_t launch_photon_order(const DevPhotons& p, int in_dtype, uint64_t n, u
     if (!sorted)
         order_scatter_kernel<<<grid, 256, 0, s>>>(n, key, hist, order);
     else if (in_dtype == MLGPU_F64)
-        order_scatter_records_kernel<double><<<grid, 256, 0, s>>>(p, n, key, hist, sorted);
+        order_scatter_records_kernel<double><<<grid, 256, 0, s>>>(p, n, key, hist, sorted,
+                                                                  index_base);
     else
-        order_scatter_records_kernel<float><<<grid, 256, 0, s>>>(p, n, key, hist, sorted);
+        order_scatter_records_kernel<float><<<grid, 256, 0, s>>>(p, n, key, hist, sorted,
+                                                                 index_base);
     return cudaGetLastError();
 }
 

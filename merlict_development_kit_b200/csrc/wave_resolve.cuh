@@ -225,6 +225,7 @@ wave_resolve_kernel(const TraceArgs a, const WaveBuffers w, const RayPool cur, c
     const uint32_t hist_len = max_int + 1;
 
     bool survive = false;
+    int32_t finished_chunk = -1;   // fed propagation: the chunk of a photon that ends here
     // state of this slot after the step (written to the next pool if it survives)
     int32_t photon = 0, root = 0, n_next = 0, k_draw = 0, err = 0;
     v3 s = mk(0, 0, 0), d = mk(0, 0, 0);
@@ -434,6 +435,21 @@ wave_resolve_kernel(const TraceArgs a, const WaveBuffers w, const RayPool cur, c
                 for (uint32_t k = (uint32_t)n_next; k < hist_len; k++)
                     store_hist(&hist[k], mk(0, 0, 0), mk(0, 0, 0), 0.0, MLGPU_LEAF_PHOTON_SOURCE, 0, false);
             if (err) raise_error(sc.error_word, (unsigned int)err);
+            if (a.fed) {
+                int32_t c = 0;
+                while (c + 1 < a.feed_chunks && p >= a.feed_start[c + 1]) c++;
+                finished_chunk = c;
+            }
+        }
+    }
+    // fed propagation: finished photons per chunk, one addition per chunk
+    // and warp (a warp's photons mostly come from one chunk)
+    if (a.fed) {
+        const unsigned fin = __ballot_sync(kFull, finished_chunk >= 0);
+        if (finished_chunk >= 0) {
+            const unsigned same = __match_any_sync(fin, finished_chunk);
+            if (lane == __ffs(same) - 1)
+                atomicAdd(&w.counters->done[finished_chunk], (unsigned)__popc(same));
         }
     }
     // warp-ballot compaction of the surviving rays into the next pool

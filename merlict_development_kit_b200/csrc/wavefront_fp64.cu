@@ -40,7 +40,9 @@ wave_intake_kernel(const TraceArgs a, const WaveBuffers w, const RayPool cur) {
     const DevScene& sc = a.scene;
     const uint32_t active = w.counters->active;
     const unsigned long long next_input = w.counters->next_input;
-    const unsigned long long remaining = a.num_photons - next_input;
+    // a fed propagation admits only the photons whose records have arrived
+    const unsigned long long limit = a.fed ? w.counters->avail_snap : a.num_photons;
+    const unsigned long long remaining = limit - next_input;
     const uint32_t room = w.pool - active;
     const uint32_t fresh = (uint32_t)(remaining < room ? remaining : room);
     const uint32_t total = active + fresh;
@@ -60,8 +62,8 @@ wave_intake_kernel(const TraceArgs a, const WaveBuffers w, const RayPool cur) {
             if (a.sorted) {
                 // the photon's record in tracing order
                 const double2* r = a.sorted + 4*q;
-                const double2 r0 = __ldcs(r), r1 = __ldcs(r + 1), r2 = __ldcs(r + 2),
-                              r3 = __ldcs(r + 3);
+                const double2 r0 = __ldcg(r), r1 = __ldcg(r + 1), r2 = __ldcg(r + 2),
+                              r3 = __ldcg(r + 3);
                 s = mk(r0.x, r0.y, r1.x);
                 d = normalized(mk(r1.y, r2.x, r2.y));
                 lambda = r3.x;
@@ -440,8 +442,10 @@ wave_walk_kernel(const TraceArgs a, const WaveBuffers w, const RayPool cur) {
 }
 
 // counters between the kernels of an iteration
-__global__ void wave_after_intake_kernel(WaveCounters* c, uint32_t pool, uint64_t num_photons) {
-    const unsigned long long remaining = num_photons - c->next_input;
+__global__ void wave_after_intake_kernel(WaveCounters* c, uint32_t pool, uint64_t num_photons,
+                                         int fed) {
+    const unsigned long long limit = fed ? c->avail_snap : num_photons;
+    const unsigned long long remaining = limit - c->next_input;
     const uint32_t room = pool - c->active;
     const uint32_t fresh = (uint32_t)(remaining < room ? remaining : room);
     c->total = c->active + fresh;
@@ -449,8 +453,18 @@ __global__ void wave_after_intake_kernel(WaveCounters* c, uint32_t pool, uint64_
     c->next = 0;
 }
 
-__global__ void wave_after_resolve_kernel(WaveCounters* c) {
+// The value of avail the next iteration admits photons up to: read once
+// here, so that the intake and its counter kernel agree on it.  avail is
+// raised by kernels of another stream after the records they publish are
+// written, so a fence orders the read before the intake's record reads.
+__device__ __forceinline__ void snapshot_avail(WaveCounters* c) {
+    c->avail_snap = atomicAdd(&c->avail, 0ull);
+    __threadfence();
+}
+
+__global__ void wave_after_resolve_kernel(WaveCounters* c, int fed) {
     if (threadIdx.x == 0) {
+        if (fed) snapshot_avail(c);
         c->overflow_total += c->overflow_len;
         c->active = c->next;
         c->isect_len = 0;
@@ -458,6 +472,15 @@ __global__ void wave_after_resolve_kernel(WaveCounters* c) {
     }
     for (int k = threadIdx.x; k < kMaxBvhLevels; k += blockDim.x) c->level_len[k] = 0;
 }
+
+// Fed propagation: the records below `avail` are written (by the kernels
+// before this one on its stream); raise the counter for the trace stream.
+__global__ void feed_publish_kernel(WaveCounters* c, unsigned long long avail) {
+    __threadfence();
+    atomicMax(&c->avail, avail);
+}
+
+__global__ void feed_snapshot_kernel(WaveCounters* c) { snapshot_avail(c); }
 
 // The counters into pinned host memory, stored by the SM rather than moved
 // by a copy engine, so that the host's check after a period never queues
@@ -469,6 +492,16 @@ __global__ void wave_counters_to_host_kernel(const WaveCounters* c, WaveCounters
 }
 
 }  // namespace
+
+cudaError_t launch_feed_publish(WaveCounters* c, uint64_t avail, cudaStream_t s) {
+    feed_publish_kernel<<<1, 1, 0, s>>>(c, (unsigned long long)avail);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_feed_snapshot(WaveCounters* c, cudaStream_t s) {
+    feed_snapshot_kernel<<<1, 1, 0, s>>>(c);
+    return cudaGetLastError();
+}
 
 cudaError_t launch_wave_counters_to_host(const WaveCounters* c, WaveCounters* host,
                                          cudaStream_t s) {
@@ -484,7 +517,7 @@ cudaError_t launch_wave_iteration(const TraceArgs& a, const WaveBuffers& w, cons
         wave_intake_kernel<double><<<slot_blocks, 256, 0, s>>>(a, w, cur);
     else
         wave_intake_kernel<float><<<slot_blocks, 256, 0, s>>>(a, w, cur);
-    wave_after_intake_kernel<<<1, 1, 0, s>>>(w.counters, w.pool, a.num_photons);
+    wave_after_intake_kernel<<<1, 1, 0, s>>>(w.counters, w.pool, a.num_photons, a.fed);
     if (ev) cudaEventRecord(ev[1], s);
     if (w.walk == MLGPU_WALK_STACK) {
         if (form == MLGPU_TRACER_FP64) wave_walk_kernel<false><<<w.grid, 256, 0, s>>>(a, w, cur);
@@ -513,7 +546,7 @@ cudaError_t launch_wave_iteration(const TraceArgs& a, const WaveBuffers& w, cons
                                                           ev ? ev[3] : nullptr);
         if (e != cudaSuccess) return e;
     }
-    wave_after_resolve_kernel<<<1, 64, 0, s>>>(w.counters);
+    wave_after_resolve_kernel<<<1, 64, 0, s>>>(w.counters, a.fed);
     if (ev) cudaEventRecord(ev[4], s);
     return cudaGetLastError();
 }

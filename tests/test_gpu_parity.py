@@ -143,9 +143,11 @@ def test_propagate_and_bin_host_entry_point(eng, oracle):
     scene.close()
 
 
-def host_call_pinned(scene, photons, max_int, tracer, pool, seed=0, uniforms=None):
+def host_call_pinned(scene, photons, max_int, tracer, pool, seed=0, uniforms=None,
+                     order=None):
     """mlgpu_propagate_host on page-locked buffers (so that it pipelines the
-    batch in pieces of at least `pool` photons)."""
+    batch in pieces of at least `pool` photons, or a quarter pool when it
+    feeds one propagation)."""
     import torch
     from merlict_development_kit_b200 import _native, abi
     n = len(photons["wavelength"])
@@ -178,6 +180,8 @@ def host_call_pinned(scene, photons, max_int, tracer, pool, seed=0, uniforms=Non
     tracers = {"fp64": abi.TRACER_FP64, "fp32": abi.TRACER_FP32, "fp64_plain": abi.TRACER_FP64_PLAIN}
     st = abi.mlgpu_settings(max_int, 0, tracers[tracer], 0, abi.TRAVERSAL_BVH)
     st.pool_size = pool
+    if order is not None:
+        st.photon_order = order
     rng = abi.mlgpu_rng()
     if uniforms is None:
         rng.mode = abi.RNG_PHILOX
@@ -195,21 +199,30 @@ def host_call_pinned(scene, photons, max_int, tracer, pool, seed=0, uniforms=Non
 
 @pytest.mark.parametrize("tracer", ["fp64", "fp32"])
 @pytest.mark.parametrize("rng_mode", ["philox", "replay"])
-def test_propagate_host_in_pieces(eng, tracer, rng_mode):
-    """Pinned host buffers and a 1024-slot pool: mlgpu_propagate_host traces
-    the 4000 photons in four pieces (666, 1334, 1333 and 667 photons: three
-    whole pieces, the first and the last cut in half) whose copies overlap
-    the tracing.
-    Photon i of a piece keeps its own random stream, so every result and
-    history entry equals one call on device buffers (and, for the FP64
-    tracer with Philox draws, merlict's own)."""
+@pytest.mark.parametrize("fed", [False, True])
+def test_propagate_host_in_pieces(eng, tracer, rng_mode, fed):
+    """Pinned host buffers and a 1024-slot pool.  In the input order
+    mlgpu_propagate_host traces the 4000 photons in four pieces (666, 1334,
+    1333 and 667 photons: three whole pieces, the first and the last cut in
+    half), one propagation each, whose copies overlap the tracing.  In the
+    coherent order it feeds one propagation: sixteen pieces (133 photons
+    first and last, 266 or 267 between) sorted on their own stream as they
+    land, admitted as they are published, their results copied back as
+    their photons finish -- one wavefront call instead of four.
+    Photon i keeps its own random stream, so every result and history entry
+    equals one call on device buffers (and, for the FP64 tracer with Philox
+    draws, merlict's own)."""
+    from merlict_development_kit_b200 import abi
     flat, photons, ref, meta = load_golden("light_field_small")
     uniforms = None
     if rng_mode == "replay":
         uniforms = np.random.default_rng(5).random((len(photons["wavelength"]), 64))
     scene = eng.Scene(flat)
+    calls0 = scene.wavefront_stats()["calls"]
     got = host_call_pinned(scene, photons, meta["max_interactions"], tracer, 1024,
-                           seed=meta["seed"], uniforms=uniforms)
+                           seed=meta["seed"], uniforms=uniforms,
+                           order=abi.ORDER_COHERENT if fed else abi.ORDER_INPUT)
+    assert scene.wavefront_stats()["calls"] - calls0 == (1 if fed else 4)
     scene.close()
     want = run_gpu(eng, flat, photons, meta["max_interactions"], seed=meta["seed"],
                    uniforms=uniforms, history=True, tracer=tracer)
