@@ -11,7 +11,6 @@
 // LixelStatistic fields as merlict computes them.
 #include <cmath>
 #include <cstdint>
-#include <cub/cub.cuh>
 
 #include "mlgpu_internal.h"
 
@@ -86,10 +85,7 @@ stats_reduce_kernel(const uint32_t* __restrict__ key, const uint32_t* __restrict
 }  // namespace
 
 size_t lixel_stats_scratch_bytes(uint64_t n) {
-    size_t cub_bytes = 0;
-    cub::DeviceRadixSort::SortPairs(nullptr, cub_bytes, (const uint32_t*)nullptr, (uint32_t*)nullptr,
-                                    (const uint32_t*)nullptr, (uint32_t*)nullptr, (int)n);
-    return 4*((n*4 + 255) & ~uint64_t(255)) + cub_bytes + 256;
+    return 6*((n*4 + 255) & ~uint64_t(255)) + radix_sort_temp_bytes(n) + 256;
 }
 
 cudaError_t launch_lixel_stats(const int32_t* sensor, const float* const* values, uint64_t n,
@@ -101,14 +97,14 @@ cudaError_t launch_lixel_stats(const int32_t* sensor, const float* const* values
     uint32_t* idx_in = reinterpret_cast<uint32_t*>(p + a);
     uint32_t* key_out = reinterpret_cast<uint32_t*>(p + 2*a);
     uint32_t* idx_out = reinterpret_cast<uint32_t*>(p + 3*a);
-    void* temp = p + 4*a;
-    size_t temp_bytes = scratch_bytes - 4*a;
+    uint32_t* key_tmp = reinterpret_cast<uint32_t*>(p + 4*a);
+    uint32_t* idx_tmp = reinterpret_cast<uint32_t*>(p + 5*a);
+    void* temp = p + 6*a;
     stats_keys_kernel<<<grid, 256, 0, s>>>(sensor, n, key_in, idx_in);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
-    // stable: photons of one sensor keep their order
-    e = cub::DeviceRadixSort::SortPairs(temp, temp_bytes, key_in, key_out, idx_in, idx_out, (int)n,
-                                        0, 32, s);
+    // stable: photons of one sensor keep their order (device_sort.cu)
+    e = radix_sort_pairs(key_in, idx_in, key_out, idx_out, key_tmp, idx_tmp, n, 32, temp, s);
     if (e != cudaSuccess) return e;
     stats_reduce_kernel<<<(num_sensors + 127)/128, 128, 0, s>>>(
         key_out, idx_out, n, num_sensors, values[0], values[1], values[2], values[3], values[4],

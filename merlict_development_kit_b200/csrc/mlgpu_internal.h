@@ -354,6 +354,33 @@ cudaError_t launch_photon_order(const DevPhotons& p, int in_dtype, uint64_t n, u
 cudaError_t launch_feed_publish(WaveCounters* c, uint64_t avail, cudaStream_t s);
 cudaError_t launch_feed_snapshot(WaveCounters* c, cudaStream_t s);
 int wave_persistent_blocks();
+// device_sort.cu: a stable LSD radix sort of (key, value) pairs on the low
+// key_bits bits of the keys (ping-pong through key_tmp/val_tmp; `temp`
+// holds radix_sort_temp_bytes(n)), exclusive sums into 64-bit offsets
+// (`temp`: exclusive_sum_temp_bytes(n); in and out may be the same array
+// for the 64-bit form), and a sort of each listed run [begin[t], end[t])
+// of a segmented array by (64-bit key, value) into key_out/val_out (key_in
+// and val_in are overwritten; empty runs are skipped).
+size_t radix_sort_temp_bytes(uint64_t n);
+cudaError_t radix_sort_pairs(const uint32_t* key_in, const uint32_t* val_in, uint32_t* key_out,
+                             uint32_t* val_out, uint32_t* key_tmp, uint32_t* val_tmp, uint64_t n,
+                             int key_bits, void* temp, cudaStream_t s);
+size_t exclusive_sum_temp_bytes(uint64_t n);
+cudaError_t exclusive_sum_u64(const uint64_t* in, uint64_t* out, uint64_t n, void* temp,
+                              cudaStream_t s);
+cudaError_t exclusive_sum_u32(const uint32_t* in, uint64_t* out, uint64_t n, void* temp,
+                              cudaStream_t s);
+cudaError_t sort_long_runs(uint64_t* key_in, uint32_t* val_in, uint64_t* key_out,
+                           uint32_t* val_out, const uint64_t* begin, const uint64_t* end,
+                           uint32_t runs, cudaStream_t s);
+// A counting sort by keys in [0, keys): index_out receives the input
+// indices grouped by key (ascending keys; the order within a key is not
+// defined), offset[k] where key k starts (keys + 1 entries, the last the
+// total).  `temp`: counting_sort_temp_bytes(n, keys).  n < 2^32.
+size_t counting_sort_temp_bytes(uint64_t n, uint32_t keys);
+cudaError_t counting_sort(const uint32_t* key, uint64_t n, uint32_t keys, uint32_t* index_out,
+                          uint64_t* offset, void* temp, cudaStream_t s);
+
 // Zeroes counts (and time_hist) and bins n arrivals into them: two kernel
 // launches, no scratch memory (bin.cu).
 cudaError_t launch_bin_arrivals(const DevScene& sc, const int32_t* sensor,

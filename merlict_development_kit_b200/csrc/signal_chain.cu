@@ -7,10 +7,11 @@
 // 9-35).
 //
 // Layout of the work:
-//   1. pipelines: a radix sort by sensor (only the bits the sensor count
-//      needs; photons without a sensor last), then every sensor's run by
-//      (arrival time, input index) -- ranks in shared memory for runs of up
-//      to 4096 photons, a segmented radix sort beyond -- then the photons'
+//   1. pipelines: a counting sort by sensor (device_sort.cu; photons
+//      without a sensor last; it also gives every pipeline's offset), then
+//      every sensor's run by (arrival time, input index) -- ranks in shared
+//      memory for runs of up to 4096 photons, a stable radix sort of each
+//      longer run by one block (device_sort.cu) -- then the photons'
 //      time, wavelength and truth id gathered into pipeline order,
 //      contiguous per lixel;
 //   2. the exposure window: min/max of the Cherenkov arrival times (one
@@ -34,7 +35,6 @@
 // the last bit.
 #include <cmath>
 #include <cstdint>
-#include <cub/cub.cuh>
 
 #include "merlict_b200_philox.h"
 #include "mlgpu_internal.h"
@@ -73,15 +73,6 @@ __device__ __forceinline__ void raise_error(unsigned int* err, int code) {
     atomicCAS(err, 0u, (unsigned)code);
 }
 
-__device__ __forceinline__ uint64_t lower_bound_u32(const uint32_t* a, uint64_t n, uint32_t v) {
-    uint64_t lo = 0, hi = n;
-    while (lo < hi) {
-        const uint64_t mid = (lo + hi) >> 1;
-        if (__ldg(a + mid) < v) lo = mid + 1; else hi = mid;
-    }
-    return lo;
-}
-
 // ---- 1. pipelines ------------------------------------------------------------
 
 __global__ void __launch_bounds__(256)
@@ -97,14 +88,6 @@ sc_sensor_keys_kernel(const int32_t* __restrict__ sensor, uint64_t n, uint32_t n
     }
 }
 
-// pipeline offsets: the first photon of every sensor in the sorted keys
-__global__ void __launch_bounds__(128)
-sc_offsets_kernel(const uint32_t* __restrict__ skey, uint64_t n, uint32_t num_sensors,
-                  uint64_t* __restrict__ pipe_off) {
-    const uint32_t s = blockIdx.x*blockDim.x + threadIdx.x;
-    if (s <= num_sensors) pipe_off[s] = lower_bound_u32(skey, n, s);
-}
-
 __global__ void __launch_bounds__(256)
 sc_time_keys_kernel(const uint32_t* __restrict__ idx, const double* __restrict__ time,
                     const uint64_t* __restrict__ pipe_off, uint32_t num_sensors,
@@ -118,7 +101,9 @@ sc_time_keys_kernel(const uint32_t* __restrict__ idx, const double* __restrict__
 // Every sensor's run by (time key, input index), i.e. stable by time: runs
 // of up to kWarpSegment photons by one warp in shared memory, up to
 // kBlockSegment by one block (sc_segsort_block_kernel), longer ones by a
-// segmented radix sort.  Each element's place is its rank in the run.
+// radix sort of the run by (time key, index) by one block (sort_long_runs).
+// Each element's place is its rank in the run, so the order the counting
+// sort left within a sensor does not matter.
 constexpr uint32_t kWarpSegment = 256;
 constexpr uint32_t kBlockSegment = 4096;
 constexpr int kSegWarps = 8;
@@ -520,24 +505,15 @@ struct PhotonScratch {
 uint64_t large_slots_for(uint64_t n) { return n/(kBlockSegment + 1) + 1; }
 
 size_t photon_temp_bytes(uint64_t n, uint32_t ns) {
-    size_t a = 0, b = 0, c = 0;
-    cub::DeviceRadixSort::SortPairs(nullptr, a, (const uint32_t*)nullptr, (uint32_t*)nullptr,
-                                    (const uint32_t*)nullptr, (uint32_t*)nullptr, (int)n, 0,
-                                    sensor_key_bits(ns));
-    cub::DeviceSegmentedRadixSort::SortPairs(nullptr, b, (const uint64_t*)nullptr,
-                                             (uint64_t*)nullptr, (const uint32_t*)nullptr,
-                                             (uint32_t*)nullptr, (int)n, (int)large_slots_for(n),
-                                             (const uint64_t*)nullptr, (const uint64_t*)nullptr);
-    cub::DeviceScan::ExclusiveSum(nullptr, c, (const uint64_t*)nullptr, (uint64_t*)nullptr,
-                                  (int)ns + 1);
-    size_t t = a > b ? a : b;
-    return t > c ? t : c;
+    const size_t a = counting_sort_temp_bytes(n, ns + 1);
+    const size_t c = exclusive_sum_temp_bytes((uint64_t)ns + 1);
+    return a > c ? a : c;
 }
 
 PhotonScratch photon_layout(uint64_t n, uint32_t ns, void* scratch, size_t bytes) {
     PhotonScratch c;
     char* p = static_cast<char*>(scratch);
-    const uint64_t a4 = align256(n*4), a8 = align256(n*8), as = align256((uint64_t)(ns + 1)*8);
+    const uint64_t a4 = align256(n*4), a8 = align256(n*8), as = align256((uint64_t)(ns + 2)*8);
     c.skey_in = reinterpret_cast<uint32_t*>(p); p += a4;
     c.skey_out = reinterpret_cast<uint32_t*>(p); p += a4;
     c.idx_in = reinterpret_cast<uint32_t*>(p); p += a4;
@@ -575,12 +551,7 @@ struct PulseScratch {
     size_t temp_bytes;
 };
 
-size_t pulse_temp_bytes(uint64_t np) {
-    size_t a = 0;
-    cub::DeviceScan::ExclusiveSum(nullptr, a, (const uint32_t*)nullptr, (uint64_t*)nullptr,
-                                  (int)np + 1);
-    return a;
-}
+size_t pulse_temp_bytes(uint64_t np) { return exclusive_sum_temp_bytes(np + 1); }
 
 PulseScratch pulse_layout(uint64_t np, void* scratch, size_t bytes) {
     PulseScratch c;
@@ -599,7 +570,7 @@ PulseScratch pulse_layout(uint64_t np, void* scratch, size_t bytes) {
 }  // namespace
 
 size_t signal_chain_photon_scratch_bytes(uint64_t n, uint32_t ns) {
-    const uint64_t a4 = align256(n*4), a8 = align256(n*8), as = align256((uint64_t)(ns + 1)*8);
+    const uint64_t a4 = align256(n*4), a8 = align256(n*8), as = align256((uint64_t)(ns + 2)*8);
     const uint64_t nbins = (uint64_t)(2.0 + sqrt((double)n)) + 1;
     return 5*a4 + 4*a8 + 3*as + align256((uint64_t)(ns + 1)*4) +
            2*align256(large_slots_for(n)*8) + align256(nbins*4) + 256 +
@@ -626,14 +597,14 @@ cudaError_t launch_signal_chain_count(const SignalChainArgs& a, void* scratch, s
     *start_dev = c.start;
     cudaError_t e = cudaMemsetAsync(c.pipe_off, 0, (uint64_t)(ns + 1)*8, s);
     if (e != cudaSuccess) return e;
-    // 1. by sensor (stable), then every sensor's run by time (stable)
+    // 1. by sensor, then every sensor's run by (time, input index)
     if (n > 0) {
-        size_t tb = c.temp_bytes;
         sc_sensor_keys_kernel<<<grid, 256, 0, s>>>(a.sensor, n, ns, c.skey_in, c.idx_in, a.err);
-        e = cub::DeviceRadixSort::SortPairs(c.temp, tb, c.skey_in, c.skey_out, c.idx_in,
-                                            c.idx_out, (int)n, 0, sensor_key_bits(ns), s);
+        // grouped by sensor (device_sort.cu: a counting sort, which also
+        // gives each pipeline's offset; the order within a sensor is set by
+        // the sort by (time, index) below)
+        e = counting_sort(c.skey_in, n, ns + 1, c.idx_out, c.pipe_off, c.temp, s);
         if (e != cudaSuccess) return e;
-        sc_offsets_kernel<<<(ns + 1 + 127)/128, 128, 0, s>>>(c.skey_out, n, ns, c.pipe_off);
         sc_time_keys_kernel<<<grid, 256, 0, s>>>(c.idx_out, a.time, c.pipe_off, ns, c.tkey_in);
         if (ns > 0) {
             e = cudaMemsetAsync(c.seg_counts, 0, 8, s);
@@ -652,10 +623,8 @@ cudaError_t launch_signal_chain_count(const SignalChainArgs& a, void* scratch, s
                     c.tkey_in, c.idx_out, c.pipe_off, c.medium, c.seg_counts, c.tkey_out, c.idx_in);
             }
             if (n > kBlockSegment) {
-                tb = c.temp_bytes;
-                e = cub::DeviceSegmentedRadixSort::SortPairs(
-                    c.temp, tb, c.tkey_in, c.tkey_out, c.idx_out, c.idx_in, (int)n,
-                    (int)c.large_slots, c.large_begin, c.large_end, 0, 64, s);
+                e = sort_long_runs(c.tkey_in, c.idx_out, c.tkey_out, c.idx_in, c.large_begin,
+                                   c.large_end, (uint32_t)c.large_slots, s);
                 if (e != cudaSuccess) return e;
             }
         }
@@ -684,8 +653,7 @@ cudaError_t launch_signal_chain_count(const SignalChainArgs& a, void* scratch, s
         sc_lixel_kernel<false><<<(ns + 127)/128, 128, 0, s>>>(
             a.params, a.seed, a.offset, c.pipe_off, c.t, c.w, c.r, a.efficiency, ns, c.start,
             c.counts, a.nsb_count, nullptr, nullptr, nullptr, nullptr, a.err);
-    size_t tb = c.temp_bytes;
-    e = cub::DeviceScan::ExclusiveSum(c.temp, tb, c.counts, c.e_off, (int)ns + 1, s);
+    e = exclusive_sum_u64(c.counts, c.e_off, (uint64_t)ns + 1, c.temp, s);
     if (e != cudaSuccess) return e;
     return cudaGetLastError();
 }
@@ -711,9 +679,7 @@ cudaError_t launch_signal_chain_extract(const SignalChainArgs& a, void* scratch,
             nullptr, nullptr, c.e_off, q.time, q.truth, q.lixel, a.err);
     sc_extract_kernel<<<grid, 256, 0, s>>>(a.params, a.seed, a.offset, c.e_off, q.time, q.lixel,
                                            num_pulses, ns, q.slice, q.keep);
-    size_t tb = q.temp_bytes;
-    cudaError_t e = cub::DeviceScan::ExclusiveSum(q.temp, tb, q.keep, q.pos, (int)num_pulses + 1,
-                                                  s);
+    cudaError_t e = exclusive_sum_u32(q.keep, q.pos, num_pulses + 1, q.temp, s);
     if (e != cudaSuccess) return e;
     sc_channel_offsets_kernel<<<(ns + 1 + 127)/128, 128, 0, s>>>(c.e_off, q.pos, ns,
                                                                  a.channel_offset);

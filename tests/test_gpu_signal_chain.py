@@ -51,7 +51,7 @@ def gpu_chain(eng, scene, cfg, sensor, t, w, tr, eff, seed, offset, capacity=Non
 
 
 @pytest.mark.parametrize("case", ["default", "no_dark", "crosstalk", "empty", "one_lixel",
-                                  "wide_spread"])
+                                  "wide_spread", "bright_lixel"])
 def test_gpu_matches_oracle_and_merlict(eng, scene, case):
     g = geometry()
     nl = g.num_lixels
@@ -65,6 +65,10 @@ def test_gpu_matches_oracle_and_merlict(eng, scene, case):
         n = 0
     elif case == "one_lixel":
         n, one = 400, 17
+    elif case == "bright_lixel":
+        # a run longer than one block's shared-memory sort (4,096 photons):
+        # the stable radix sort of long runs
+        n, one = 12_000, 17
     elif case == "wide_spread":
         spread = 400e-9
     sensor, t, w, tr, eff = event(3, n, nl, spread, one)
