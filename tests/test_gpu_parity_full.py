@@ -157,3 +157,43 @@ def test_queue_capacity_is_validated(eng):
     flat, photons, _, meta = load_golden("reflector_camera")
     with pytest.raises(ValueError):
         gpu_trace(eng, flat, photons, meta["max_interactions"], 1, tuning={"queue_capacity": 8})
+
+
+def test_production_mode_on_the_light_field_telescope(eng):
+    """Production random streams on the benchmarked telescope: merlict's own
+    multi-threaded path (an Mt19937 per photon, seeded from one generator,
+    merlict_multi_thread.cpp:12-55) against the GPU's Philox streams on
+    the same 2e6 photons.  Per-lixel counts: chi-squared within five sigma
+    of its degrees of freedom, and a Jensen-Shannon divergence no larger
+    than the noise floor between two GPU runs with independent seeds (plus
+    a tenth of it); arrival times: a two-sample KS test."""
+    from scipy import stats
+    from merlict_development_kit_b200.precision import js_divergence
+    c = CONFIGS["config1_light_field_telescope"]
+    flat = c["build"]().flatten()
+    ref_scene = O.RefScene(c["kind"], c["params"])
+    ph = P.downward_disc_source(2_000_000, 23, *c["source"])
+    status, ref, _ = ref_scene.propagate(ph, c["max_int"], O.REFERENCE_MULTI_THREAD, seed=5,
+                                         threads=THREADS)
+    assert status == 0, ref_scene.last_error()
+    a = gpu_trace(eng, flat, ph, c["max_int"], 101)
+    b = gpu_trace(eng, flat, ph, c["max_int"], 202)
+    ns = flat.num_sensors
+
+    def hist(r):
+        s = r["sensor"]
+        return np.bincount(s[s >= 0], minlength=ns).astype(np.float64)
+    h_ref, h_a, h_b = hist(ref), hist(a), hist(b)
+    assert h_ref.sum() > 0.2 * len(ph["wavelength"])
+    m = (h_ref + h_a) > 0
+    chi2 = (((h_ref - h_a) ** 2)[m] / (h_ref + h_a)[m]).sum()
+    dof = int(m.sum())
+    assert chi2 < dof + 5 * np.sqrt(2 * dof), (chi2, dof)
+    floor = js_divergence(h_a, h_b)
+    assert js_divergence(h_ref, h_a) <= 1.1 * floor, (js_divergence(h_ref, h_a), floor)
+    t_ref = ref["time"][ref["sensor"] >= 0]
+    t_gpu = a["time"][a["sensor"] >= 0]
+    rng = np.random.default_rng(0)
+    ks = stats.ks_2samp(rng.choice(t_ref, 200_000, replace=False),
+                        rng.choice(t_gpu, 200_000, replace=False))
+    assert ks.pvalue > 1e-3, ks
