@@ -349,9 +349,15 @@ int mlgpu_scene_sync_errors(mlgpu_scene* scene, void* cuda_stream);
  * traces, copies the results out and synchronises.  This is the call the
  * reference-side C++ shim makes.  When every buffer is page-locked
  * (cudaHostAlloc, cudaHostRegister, torch pin_memory) the batch moves in
- * pieces (up to four of at least one ray pool each, the first and the last
- * cut in half) whose copies overlap the tracing of their neighbours; the
- * results are those of one call.
+ * pieces whose copies overlap the tracing.  With a wavefront form in the
+ * coherent photon order one propagation is fed piece by piece (up to
+ * sixteen pieces of at least a quarter ray pool, the first and the last
+ * half as large): each piece is sorted on the device as soon as it has
+ * landed and its photons are admitted from then on, and each piece's
+ * results are copied back as soon as all its photons have finished.
+ * Otherwise each piece (up to four of at least one ray pool) is a
+ * propagation of its own, traced while the next one uploads.  Either way
+ * the results are those of one call.
  * Ordered after earlier work on the legacy default stream.               */
 int mlgpu_propagate_host(
     mlgpu_scene* scene,
