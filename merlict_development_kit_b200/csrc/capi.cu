@@ -398,6 +398,14 @@ int build_device_scene(mlgpu_scene* s, const mlgpu_flat_scene* f) {
                 leaf_slot[bvh.leaf_ids[j]] = (int32_t)j;
             }
             if ((st = upload(s, rec.data(), rec.size(), &s->dev.slot_rec))) return st;
+            std::vector<uint4> rec_f(blocks*72 > 0 ? blocks*72 : 1, make_uint4(0u, 0u, 0u, 0u));
+            for (size_t j = 0; j < slots; j++) {
+                const uint4* f = reinterpret_cast<const uint4*>(&leaf_f[bvh.leaf_ids[j]]);
+                const uint4* an = reinterpret_cast<const uint4*>(&anchor[bvh.leaf_ids[j]]);
+                for (int u = 0; u < 5; u++) rec_f[(j >> 3)*72 + u*8 + (j & 7)] = f[u];
+                for (int u = 0; u < 4; u++) rec_f[(j >> 3)*72 + (5 + u)*8 + (j & 7)] = an[u];
+            }
+            if ((st = upload(s, rec_f.data(), rec_f.size(), &s->dev.slot_rec_f))) return st;
             if ((st = upload(s, bvh.leaf_ids.data(), bvh.leaf_ids.size(), &s->dev.slot_leaf))) return st;
             if ((st = upload(s, leaf_slot.data(), leaf_slot.size(), &s->dev.leaf_slot))) return st;
             s->dev.num_slots = (int32_t)slots;

@@ -105,25 +105,73 @@ __device__ __forceinline__ double newton64(double a, double b, double c, double 
 // none of the FP64 transform; with kNeedHit (the closest candidate's full
 // hit) it is taken in the leaf frame of the FP64 transform, and the hit
 // point and normal follow in FP64.
-template <bool kNeedHit>
+// The FP64 transform entry T[k] and parameter params[k] of a leaf: by leaf
+// id from its record, or (kSlot) by candidate slot from the slot-ordered
+// records (pairs 0-5 the transform, pair 8 onwards (r2, params[0]),
+// (params[1], params[2]), ...).
+template <bool kSlot>
+__device__ __forceinline__ double leaf_T64(const DevScene& sc, int32_t id, int k) {
+    if (kSlot) {
+        const double2 x = __ldg(sc.slot_rec + (size_t)(id >> 3)*96 + (k >> 1)*8 + (id & 7));
+        return (k & 1) ? x.y : x.x;
+    }
+    return __ldg(&sc.leaf[id].T[k]);
+}
+template <bool kSlot>
+__device__ __forceinline__ double leaf_param64(const DevScene& sc, int32_t id, int k) {
+    if (kSlot) {
+        const int m = k + 1;
+        const double2 x = __ldg(sc.slot_rec + (size_t)(id >> 3)*96 + (8 + (m >> 1))*8 + (id & 7));
+        return (m & 1) ? x.y : x.x;
+    }
+    return __ldg(&sc.leaf[id].params[k]);
+}
+
+// 16-byte piece p of a leaf's LeafAnchor, by leaf id or (kSlot) by slot.
+template <bool kSlot>
+__device__ __forceinline__ double2 anchor_pair(const DevScene& sc, int32_t id, int p) {
+    if (kSlot) {
+        const uint4 x = __ldg(sc.slot_rec_f + (size_t)(id >> 3)*72 + (5 + p)*8 + (id & 7));
+        return make_double2(__hiloint2double((int)x.y, (int)x.x),
+                            __hiloint2double((int)x.w, (int)x.z));
+    }
+    return __ldg(reinterpret_cast<const double2*>(sc.leaf_anchor + id) + p);
+}
+
+// `leaf` is a leaf id, or with kSlot a candidate slot (the records then come
+// from the slot-ordered copies, where the eight slots of a leaf range sit
+// side by side, and Hit32::leaf holds the slot).
+template <bool kNeedHit, bool kSlot = false>
 __device__ Hit32 intersect32(const DevScene& sc, int32_t leaf, d3 s, d3 d, bool pure) {
     Hit32 h;
     h.leaf = -1;
     // R, params, r2 and primitive: the record's first 80 bytes in 16-byte loads
     static_assert(offsetof(LeafRecF, params) == 36 && offsetof(LeafRecF, r2) == 68 &&
                   offsetof(LeafRecF, primitive) == 72, "intersect32 reads LeafRecF in pieces");
-    const float4* Lq = reinterpret_cast<const float4*>(sc.leaf_f + leaf);
     float v[20];
+    double2 o01, o2R;   // the anchor: origin x, y; origin z, R
+    if (kSlot) {
+        const uint4* q = sc.slot_rec_f + (size_t)(leaf >> 3)*72 + (leaf & 7);
 #pragma unroll
-    for (int k = 0; k < 5; k++) {
-        const float4 x = __ldg(Lq + k);
-        v[4*k] = x.x; v[4*k + 1] = x.y; v[4*k + 2] = x.z; v[4*k + 3] = x.w;
+        for (int k = 0; k < 5; k++) {
+            const uint4 x = __ldg(q + 8*k);
+            v[4*k] = __uint_as_float(x.x); v[4*k + 1] = __uint_as_float(x.y);
+            v[4*k + 2] = __uint_as_float(x.z); v[4*k + 3] = __uint_as_float(x.w);
+        }
+        o01 = anchor_pair<true>(sc, leaf, 0);
+        o2R = anchor_pair<true>(sc, leaf, 1);
+    } else {
+        const float4* Lq = reinterpret_cast<const float4*>(sc.leaf_f + leaf);
+#pragma unroll
+        for (int k = 0; k < 5; k++) {
+            const float4 x = __ldg(Lq + k);
+            v[4*k] = x.x; v[4*k + 1] = x.y; v[4*k + 2] = x.z; v[4*k + 3] = x.w;
+        }
+        o01 = anchor_pair<false>(sc, leaf, 0);
+        o2R = anchor_pair<false>(sc, leaf, 1);
     }
     const int32_t prim = __float_as_int(v[18]);
     if (prim == MLGPU_PRIM_NONE) return h;
-    const LeafAnchor* A = sc.leaf_anchor + leaf;
-    const double2 o01 = __ldg(reinterpret_cast<const double2*>(A) + 0);   // origin x, y
-    const double2 o2R = __ldg(reinterpret_cast<const double2*>(A) + 1);   // origin z, R
     const d3 c = dmk(o01.x, o01.y, o2R.x);
     float R[9];
 #pragma unroll
@@ -211,8 +259,8 @@ __device__ Hit32 intersect32(const DevScene& sc, int32_t leaf, d3 s, d3 d, bool 
         if (!pure && !kNeedHit && !ell) {
             // one Newton step each on |m + t d|^2 - R^2, m = rebased support
             // - sphere centre, in FP64 world coordinates
-            const double2 c01 = __ldg(reinterpret_cast<const double2*>(A) + 2);   // centre x, y
-            const double2 c2p = __ldg(reinterpret_cast<const double2*>(A) + 3);   // centre z, pad
+            const double2 c01 = anchor_pair<kSlot>(sc, leaf, 2);   // centre x, y
+            const double2 c2p = anchor_pair<kSlot>(sc, leaf, 3);   // centre z, pad
             const d3 m = dmk(s.x + d.x*t0 - c01.x, s.y + d.y*t0 - c01.y, s.z + d.z*t0 - c2p.x);
             const double R = o2R.y;
 #pragma unroll
@@ -227,11 +275,12 @@ __device__ Hit32 intersect32(const DevScene& sc, int32_t leaf, d3 s, d3 d, bool 
         } else if (!pure) {
             // one Newton step each on the quadratic in FP64, in the leaf frame
             // of the FP64 transform
-            const double* T = sc.leaf[leaf].T;
             double Tr[9];
 #pragma unroll
             for (int k = 0; k < 3; k++) {
-                Tr[3*k] = __ldg(&T[4*k]); Tr[3*k + 1] = __ldg(&T[4*k + 1]); Tr[3*k + 2] = __ldg(&T[4*k + 2]);
+                Tr[3*k] = leaf_T64<kSlot>(sc, leaf, 4*k);
+                Tr[3*k + 1] = leaf_T64<kSlot>(sc, leaf, 4*k + 1);
+                Tr[3*k + 2] = leaf_T64<kSlot>(sc, leaf, 4*k + 2);
             }
             s64 = dmk(Tr[0]*rel.x + Tr[3]*rel.y + Tr[6]*rel.z,
                       Tr[1]*rel.x + Tr[4]*rel.y + Tr[7]*rel.z,
@@ -246,7 +295,7 @@ __device__ Hit32 intersect32(const DevScene& sc, int32_t leaf, d3 s, d3 d, bool 
                 b64 = 2.0*(s64.x*d64.x*iA + s64.y*d64.y*iB + d64.z*(s64.z - C)*iC);
                 c64 = s64.x*s64.x*iA + s64.y*s64.y*iB + (s64.z*s64.z - 2.0*s64.z*C)*iC;
             } else {
-                const double Rc = __ldg(&sc.leaf[leaf].params[0]);
+                const double Rc = leaf_param64<kSlot>(sc, leaf, 0);
                 a64 = d64.x*d64.x + d64.y*d64.y + d64.z*d64.z;
                 b64 = 2.0*(s64.x*d64.x + s64.y*d64.y + s64.z*d64.z - Rc*d64.z);
                 c64 = s64.x*s64.x + s64.y*s64.y + s64.z*s64.z - 2.0*Rc*s64.z;
@@ -299,12 +348,13 @@ __device__ Hit32 intersect32(const DevScene& sc, int32_t leaf, d3 s, d3 d, bool 
             const d3 p = dmk(s64.x + d64.x*best, s64.y + d64.y*best, s64.z + d64.z*best);
             d3 n;
             if (ell) {
-                const double iA = __ldg(&sc.leaf[leaf].params[3]), iB = __ldg(&sc.leaf[leaf].params[4]);
-                const double C = __ldg(&sc.leaf[leaf].params[2]);
+                const double iA = leaf_param64<kSlot>(sc, leaf, 3);
+                const double iB = leaf_param64<kSlot>(sc, leaf, 4);
+                const double C = leaf_param64<kSlot>(sc, leaf, 2);
                 const double f = C*0.5*sqrt(fmax(1.0 - p.x*p.x*iA - p.y*p.y*iB, 0.0));
                 n = dmk(f*(-2.0*p.x*iA), f*(-2.0*p.y*iA), 1.0);
             } else {
-                n = dmk(-p.x, -p.y, __ldg(&sc.leaf[leaf].params[0]) - p.z);
+                n = dmk(-p.x, -p.y, leaf_param64<kSlot>(sc, leaf, 0) - p.z);
             }
             const double inv = 1.0/sqrt(n.x*n.x + n.y*n.y + n.z*n.z);
             n = dmk(n.x*inv, n.y*inv, n.z*inv);

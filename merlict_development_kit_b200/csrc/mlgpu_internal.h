@@ -133,6 +133,11 @@ struct DevScene {
     // 96 b + 8 p + i -- the up to eight leaves of a leaf range, tested by
     // neighbouring lanes, share one 128-byte line per pair.
     const double2* slot_rec;
+    // The FP32 forms' candidate records in the same slot order: the first
+    // 80 bytes of LeafRecF and the 64 of LeafAnchor (origin, R, cap centre)
+    // as nine 16-byte units, eight slots to a block of 72, unit u of slot
+    // 8 b + i at 72 b + 8 u + i.
+    const uint4* slot_rec_f;
     const int32_t* slot_leaf;   // [slots] leaf of each slot
     const int32_t* leaf_slot;   // [num_leaves] slot of each leaf, -1: no geometry
     int32_t num_slots;

@@ -161,10 +161,10 @@ wave_isect_kernel(const TraceArgs a, const WaveBuffers w, const RayPool cur) {
                 if (h.leaf >= 0) dist = h.dist;
             }
         } else {
-            const int32_t leaf = __ldg(sc.slot_leaf + q.y);
-            const fp32::Hit32 h = fp32::intersect32<false>(sc, leaf, fp32::dmk(s.x, s.y, s.z),
-                                                    fp32::dmk(d.x, d.y, d.z),
-                                                    kIsect == kIsectFp32Pure);
+            // by slot: the FP32 records in slot order, like the FP64 ones
+            const fp32::Hit32 h = fp32::intersect32<false, true>(
+                sc, (int32_t)q.y, fp32::dmk(s.x, s.y, s.z), fp32::dmk(d.x, d.y, d.z),
+                kIsect == kIsectFp32Pure);
             if (h.leaf >= 0) dist = h.v;
         }
         w.isect_dist[e] = dist;
