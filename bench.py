@@ -56,11 +56,12 @@ FP64_PEAK_TFLOPS_NOMINAL = 37.0   # B200 vector FP64 with FMAs, nominal
 # intersect = intersection + tie kernels; resolve = overflow walk +
 # resolve + counter kernel; bin = zeroing + binning kernels.  The tracing
 # order's kernels (run once per call, before the first iteration) are in
-# no class: 188 B per photon.  The traffic of a step grows with its photons
+# no class (ORDER_DRAM_BYTES_PER_PHOTON).  The traffic of a step grows with its photons
 # (the same scene and pool), so the bench scales these figures by its own
 # photon count.
 STAGE_DRAM_BYTES_PER_PHOTON = {"walk": 807.0, "intake": 247.5, "intersect": 1079.9,
                                "resolve": 897.4, "bin": 4.0}
+ORDER_DRAM_BYTES_PER_PHOTON = 188.0
 FP32_PEAK_TFLOPS_NOMINAL = 75.0   # B200 vector FP32 (non-tensor), nominal
 WORKLOAD = "light-field telescope, 1039 lenses x 61 lixels (config 1)"
 # the signal chain after binning (workload "signal"): quantum efficiency,
@@ -475,6 +476,12 @@ def run_ours(args, world, rank, local):
                            else "fallback: 6,650 GB/s of the profiling recipe (no "
                                 "MEASURED_PEAKS.json)"),
            "bytes_per_photon": bpp, "scope": "whole propagate call"}
+    if STAGE_DRAM_BYTES_PER_PHOTON and not fp32:
+        # the FP64 tracer's measured DRAM traffic (ncu, all kernel classes and
+        # the tracing order) against the algorithmic bytes
+        measured = sum(STAGE_DRAM_BYTES_PER_PHOTON.values()) + ORDER_DRAM_BYTES_PER_PHOTON
+        hbm["dram_bytes_per_photon_measured"] = measured
+        hbm["dram_over_algorithmic"] = measured / bpp
     cpu = None
     if world == 1 and not args.no_cpu_baseline:
         v, secs, cores, kind, sample = cpu_reference_run(args.ref_photons, 2, 1)
