@@ -81,9 +81,18 @@ int mlgpu_sg_pack_weights(const float* params, void* images, void* cuda_stream);
 uint64_t mlgpu_sg_workspace_bytes(uint32_t batch, int training);
 
 /* Forward pass: inputs [batch][8] FP32 (the 5 normalised inputs, 3 unused)
- * -> outputs [batch][80] FP32 (the 73 outputs, 7 unused).                */
+ * -> outputs [batch][80] FP32 (the 73 outputs, 7 unused).  One launch:
+ * all five layers of each 128-row tile run with the activations in shared
+ * and tensor memory.  `workspace` is not used (may be NULL).             */
 int mlgpu_sg_forward(const float* params, const void* images, const float* inputs,
                      uint32_t batch, float* outputs, void* workspace, void* cuda_stream);
+
+/* The same forward pass one tensor-core launch per layer, the activations
+ * in `workspace` (mlgpu_sg_workspace_bytes(batch, 0) bytes): the form the
+ * training step runs.  Its outputs equal mlgpu_sg_forward's bit for bit.  */
+int mlgpu_sg_forward_layered(const float* params, const void* images, const float* inputs,
+                             uint32_t batch, float* outputs, void* workspace,
+                             void* cuda_stream);
 
 /* One training step: forward, the loss (binary cross-entropy of the reach
  * logit plus, for photons that reached a sensor, the negative log-

@@ -125,11 +125,13 @@ def _declare_surrogate(L) -> None:
     L.mlgpu_sg_gemm_f32.argtypes = [vp, u32, vp, u32, u32, u32, u32, vp, vp, vp]
     L.mlgpu_sg_pack_weights.argtypes = [vp, vp, vp]
     L.mlgpu_sg_forward.argtypes = [vp, vp, vp, u32, vp, vp, vp]
+    L.mlgpu_sg_forward_layered.argtypes = [vp, vp, vp, u32, vp, vp, vp]
     L.mlgpu_sg_train_step.argtypes = [vp, vp, vp, vp, vp, vp, vp, u32, u32, f32, vp, vp, vp, vp]
     L.mlgpu_sg_sample.argtypes = [vp, vp, u32, vp, vp, f32, f32, u64, u64,
                                   C.POINTER(mlgpu_sg_sensor_grid), vp, vp, vp, vp, vp, vp, vp]
     L.mlgpu_sg_sync_errors.argtypes = [vp]
     for name in ("mlgpu_sg_gemm_f32", "mlgpu_sg_pack_weights", "mlgpu_sg_forward",
+                 "mlgpu_sg_forward_layered",
                  "mlgpu_sg_train_step", "mlgpu_sg_sample", "mlgpu_sg_sync_errors"):
         getattr(L, name).restype = C.c_int
 
@@ -157,5 +159,6 @@ EXPORTED = (
     # include/merlict_b200_surrogate.h
     "mlgpu_sg_image_offset", "mlgpu_sg_gemm_f32", "mlgpu_sg_param_count", "mlgpu_sg_image_bytes",
     "mlgpu_sg_pack_weights", "mlgpu_sg_workspace_bytes", "mlgpu_sg_forward",
+    "mlgpu_sg_forward_layered",
     "mlgpu_sg_train_step", "mlgpu_sg_sample", "mlgpu_sg_sync_errors",
 )

@@ -156,7 +156,65 @@ __device__ __forceinline__ void tmem_ld32(uint32_t taddr, float* v) {
     for (int j = 0; j < 32; j++) v[j] = __uint_as_float(r[j]);
 }
 
-__device__ __forceinline__ float silu(float z) { return __fdividef(z, 1.0f + __expf(-z)); }
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, float* v) {
+    uint32_t r[16];
+    asm volatile("tcgen05.ld.sync.aligned.32x32b.x16.b32 "
+                 "{%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15}, [%16];"
+                 : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]),
+                   "=r"(r[6]), "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]),
+                   "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+                 : "r"(taddr));
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+    for (int j = 0; j < 16; j++) v[j] = __uint_as_float(r[j]);
+}
+
+// Paired FP32 arithmetic (Blackwell's f32x2 instructions: two IEEE
+// operations in one issue slot, each rounded like its scalar form).
+__device__ __forceinline__ uint64_t f2(float lo, float hi) {
+    uint64_t v;
+    asm("mov.b64 %0, {%1, %2};" : "=l"(v) : "f"(lo), "f"(hi));
+    return v;
+}
+__device__ __forceinline__ void f2_split(uint64_t v, float* lo, float* hi) {
+    asm("mov.b64 {%0, %1}, %2;" : "=f"(*lo), "=f"(*hi) : "l"(v));
+}
+__device__ __forceinline__ uint64_t mul2(uint64_t a, uint64_t b) {
+    uint64_t d;
+    asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+    return d;
+}
+__device__ __forceinline__ uint64_t add2(uint64_t a, uint64_t b) {
+    uint64_t d;
+    asm("add.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+    return d;
+}
+__device__ __forceinline__ float ex2_ftz(float a) {
+    float r;
+    asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(a));
+    return r;
+}
+__device__ __forceinline__ float rcp_ftz(float a) {
+    float r;
+    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(a));
+    return r;
+}
+
+constexpr float kLog2e = 1.4426950408889634f;
+// SiLU z / (1 + 2^(-z log2 e)) with the hardware's approximate base-2
+// exponential and reciprocal (relative error about 2^-22 each; for
+// z -> -inf the exponential overflows to inf and the result is -0).
+// silu_pair does the same on two values with paired instructions, to the
+// same bits.
+__device__ __forceinline__ float silu(float z) {
+    return __fmul_rn(z, rcp_ftz(__fadd_rn(1.0f, ex2_ftz(__fmul_rn(z, -kLog2e)))));
+}
+__device__ __forceinline__ uint64_t silu_pair(uint64_t z) {
+    float u0, u1, d0, d1;
+    f2_split(mul2(z, f2(-kLog2e, -kLog2e)), &u0, &u1);
+    f2_split(add2(f2(ex2_ftz(u0), ex2_ftz(u1)), f2(1.0f, 1.0f)), &d0, &d1);
+    return mul2(z, f2(rcp_ftz(d0), rcp_ftz(d1)));
+}
 __device__ __forceinline__ float dsilu(float z) {
     const float s = __fdividef(1.0f, 1.0f + __expf(-z));
     return s*(1.0f + z*(1.0f - s));
@@ -679,14 +737,15 @@ __global__ void pack_weights_kernel(const float* __restrict__ p, uint8_t* __rest
 // The fixed encoding of the 5 normalised inputs into kEnc features: the
 // inputs themselves, then sin(pi 2^l x_j) and cos(pi 2^l x_j) for j = 0..4
 // and l = 0..kFreq-1 (feature 5 + 2 (kFreq j + l) + c), then zeros.  The
-// argument 2^l x_j is exact in FP32 and sincospif reduces it exactly.
+// argument 2^l x_j (a product by a power of two) is exact in FP32 and
+// sincospif reduces it exactly.
 __device__ __forceinline__ float encoded(const float* xi, int f) {
     if (f < kIn) return xi[f];
     const int g = f - kIn;
     if (g >= 2*kFreq*kIn) return 0.0f;
     const int j = g/(2*kFreq), l = (g % (2*kFreq)) >> 1;
     float sn, cs;
-    sincospif(ldexpf(xi[j], l), &sn, &cs);
+    sincospif(__fmul_rn(xi[j], (float)(1 << l)), &sn, &cs);
     return (g & 1) ? cs : sn;
 }
 
@@ -709,6 +768,296 @@ encode_kernel(const float* __restrict__ x, uint32_t batch, uint8_t* __restrict__
     if (img_t) {
 #pragma unroll
         for (int k = 0; k < 8; k++) img_store1(img_t, kEnc, (uint32_t)(f0 + k), row, v[k]);
+    }
+}
+
+// ---- the fused inference forward ----------------------------------------------------
+//
+// All five layers of a 128-row tile in one persistent kernel, the
+// activations never leaving the SM: the tile's activation lives in shared
+// memory as a 128-row image (4 chunks of 64 columns, 16 KB each), the
+// layers' weights stream through a ring of 32 KB stages (one 64-wide K chunk
+// of one layer per stage; they stay in L2), and two accumulators in tensor
+// memory alternate between consecutive layers.  The epilogue of layer l
+// drains its accumulator 64 columns at a time into the activation chunk it
+// replaces (that chunk's readers, the MMAs of layer l, have completed) and
+// releases each chunk on its own barrier, so the MMAs of layer l+1 start on
+// chunk 0 while the epilogue is still on chunk 1: the tensor cores and the
+// epilogue overlap within a tile.  At the last layer the epilogue warps
+// first encode the next tile's inputs into chunks 0 and 1 (so its layer 0
+// runs while they drain the outputs) and then write the 80 FP32 outputs.
+//
+// The arithmetic is that of the layer-by-layer path (same encoding, K
+// order, bias addition, SiLU and BF16 rounding), so both give the same bits.
+//
+// Roles: warp 0 lane 0 copies weight chunks, warp 1 lane 0 issues the MMAs,
+// warps 2..17 encode and drain: warp w reads tensor-memory lane quarter
+// w % 4 (rows 32 (w % 4) ..) and takes 16 of each 64-column chunk's
+// columns (16 ((w - 2) / 4) ..), so that every scheduler has four such
+// warps to hide the latency of the epilogue's dependent arithmetic.  Every
+// wait is bounded; after a timeout every role leaves its loop, the kernel
+// records the error and waits (bounded) for its own copies and MMAs before
+// freeing tensor memory.
+
+constexpr int kFusedThreads = 576;
+constexpr int kEpiWarps = 16;
+constexpr int kWRing = 4;                       // weight stages
+constexpr uint32_t kWStage = 32768u;            // 256 rows x 64 K x 2 bytes
+constexpr uint32_t kActChunk = 16384u;          // 128 rows x 64 K x 2 bytes
+constexpr int kChunksPerTile = kEnc/64 + 3*(kH/64) + kH/64;   // 18
+constexpr int kBiasFloats = 4*kH + kOutPad;     // 1104
+constexpr uint32_t kFusedBarOff = 4u*kActChunk + kWRing*kWStage + (uint32_t)kBiasFloats*4u;
+
+__host__ __device__ constexpr uint32_t fused_smem_bytes() {
+    return kFusedBarOff + 16u*8u + 1024u;
+}
+
+// Weight chunk c (0..17) of a tile's sequence (layer 0: 2 chunks, layers
+// 1..4: 4 each): its offset in the images and its bytes.
+__device__ __forceinline__ void weight_chunk(uint32_t c, uint64_t* off, uint32_t* bytes) {
+    if (c < 2u) {
+        *off = kImgW0Off + (uint64_t)c*kWStage; *bytes = kWStage;
+    } else if (c < 14u) {
+        const uint32_t l = 1u + (c - 2u)/4u, kc = (c - 2u) % 4u;
+        *off = img_w((int)l) + (uint64_t)kc*kWStage; *bytes = kWStage;
+    } else {
+        *off = kImgW4Off + (uint64_t)(c - 14u)*(kOutPad*128u); *bytes = kOutPad*128u;
+    }
+}
+
+// Encodes features [64 p + 16 h, + 16) of row r of a tile (inputs xi) into
+// chunk p of the activation image: the values of encoded(), one sincospif
+// per (input, octave) for its sine and cosine features.  f0 is the same
+// for the whole warp, so the branches do not diverge.
+__device__ __forceinline__ void encode_part(uint8_t* act, uint32_t r, uint32_t p, uint32_t h,
+                                            const float* xi) {
+    const int f0 = (int)(p*64u + h*16u);
+    float v[16];
+    int pair = -1;
+    float sn = 0.0f, cs = 0.0f;
+#pragma unroll
+    for (int k = 0; k < 16; k++) {
+        const int f = f0 + k;
+        if (f < kIn) {
+            v[k] = xi[f];
+        } else if (f - kIn >= 2*kFreq*kIn) {
+            v[k] = 0.0f;
+        } else {
+            const int g = f - kIn;
+            if ((g >> 1) != pair) {
+                pair = g >> 1;
+                const int j = g/(2*kFreq), l = (g % (2*kFreq)) >> 1;
+                sincospif(__fmul_rn(xi[j], (float)(1 << l)), &sn, &cs);
+            }
+            v[k] = (g & 1) ? cs : sn;
+        }
+    }
+    uint8_t* rowp = act + p*kActChunk + r*128u;
+#pragma unroll
+    for (uint32_t u = 0; u < 2; u++) {
+        uint4 q;
+        q.x = pack_bf16x2(v[8*u], v[8*u + 1]); q.y = pack_bf16x2(v[8*u + 2], v[8*u + 3]);
+        q.z = pack_bf16x2(v[8*u + 4], v[8*u + 5]); q.w = pack_bf16x2(v[8*u + 6], v[8*u + 7]);
+        *reinterpret_cast<uint4*>(rowp + (((h*2u + u) ^ (r & 7u)) << 4)) = q;
+    }
+}
+
+// Makes this warp's shared-memory writes visible to the tensor cores and
+// arrives (once per warp) on `bar`.
+__device__ __forceinline__ void release_chunk(uint64_t* bar, int lane) {
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    tc_fence_before();
+    __syncwarp();
+    if (lane == 0) mbar_arrive(bar);
+}
+
+__global__ void __launch_bounds__(kFusedThreads, 1)
+fused_forward_kernel(const float* __restrict__ p, const uint8_t* __restrict__ img,
+                     const float* __restrict__ x, uint32_t num_tiles, float* __restrict__ y) {
+    extern __shared__ uint8_t smem_raw[];
+    uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) &
+                                               ~(uintptr_t)1023);
+    uint8_t* act = smem;                                        // 4 x 16 KB
+    uint8_t* ring = smem + 4u*kActChunk;                        // kWRing x 32 KB
+    float* s_bias = reinterpret_cast<float*>(ring + kWRing*kWStage);
+    uint64_t* w_full = reinterpret_cast<uint64_t*>(smem + kFusedBarOff);
+    uint64_t* w_empty = w_full + kWRing;
+    uint64_t* act_ready = w_empty + kWRing;                     // [4], one arrival per epilogue warp
+    uint64_t* acc_full = act_ready + 4;                         // [2]
+    uint64_t* drained = acc_full + 2;
+    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(drained + 1);
+    __shared__ int s_failed;
+    __shared__ uint32_t s_issued, s_consumed;   // weight chunks copied in / taken by the MMAs
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+
+    for (int i = threadIdx.x; i < kBiasFloats; i += kFusedThreads) {
+        const int l = i/kH, n = i % kH;
+        s_bias[i] = l < 4 ? __ldg(p + b_off(l) + n) : (n < kOut ? __ldg(p + kB4 + n) : 0.0f);
+    }
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < kWRing; s++) { mbar_init(&w_full[s], 1); mbar_init(&w_empty[s], 1); }
+        for (int c = 0; c < 4; c++) mbar_init(&act_ready[c], kEpiWarps);
+        for (int a = 0; a < 2; a++) mbar_init(&acc_full[a], 1);
+        mbar_init(drained, 1);
+        s_failed = 0;
+        s_issued = 0;
+        s_consumed = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (warp == 1) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;"
+                     :: "r"(smem_u32(tmem_slot)), "r"(512u));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = *tmem_slot;
+
+    if (warp == 0) {
+        if (lane == 0) {
+            uint32_t it = 0;
+            bool ok = true;
+            for (uint32_t tile = blockIdx.x; ok && tile < num_tiles; tile += gridDim.x) {
+                for (uint32_t c = 0; c < (uint32_t)kChunksPerTile; c++, it++) {
+                    const uint32_t s = it % kWRing;
+                    if (it >= (uint32_t)kWRing && !mbar_wait(&w_empty[s], ((it/kWRing) - 1) & 1)) {
+                        ok = false;
+                        break;
+                    }
+                    uint32_t bytes;
+                    uint64_t off;
+                    weight_chunk(c, &off, &bytes);
+                    mbar_expect_tx(&w_full[s], bytes);
+                    bulk_g2s(ring + s*kWStage, img + off, bytes, &w_full[s]);
+                    s_issued = it + 1;
+                }
+            }
+            if (!ok) s_failed = 1;
+        }
+    } else if (warp == 1) {
+        if (lane == 0) {
+            uint32_t it = 0, gl = 0;
+            uint32_t ready = 0;   // bit kc: parity of the next act_ready[kc] phase
+            bool ok = true;
+            for (uint32_t tile = blockIdx.x; ok && tile < num_tiles; tile += gridDim.x) {
+                for (uint32_t l = 0; ok && l < 5; l++, gl++) {
+                    const uint32_t idesc = l == 4 ? idesc_bf16(128, kOutPad) : idesc_bf16(128, kH);
+                    const uint32_t d = tmem + (gl & 1u)*256u;
+                    const uint32_t chunks = l == 0 ? (uint32_t)(kEnc/64) : (uint32_t)(kH/64);
+                    for (uint32_t kc = 0; kc < chunks; kc++, it++) {
+                        if (!mbar_wait(&act_ready[kc], (ready >> kc) & 1u)) { ok = false; break; }
+                        ready ^= 1u << kc;
+                        const uint32_t s = it % kWRing;
+                        if (!mbar_wait(&w_full[s], (it/kWRing) & 1)) { ok = false; break; }
+                        s_consumed = it + 1;
+                        tc_fence_after();
+                        const uint32_t a_addr = smem_u32(act + kc*kActChunk);
+                        const uint32_t b_addr = smem_u32(ring + s*kWStage);
+#pragma unroll
+                        for (uint32_t ks = 0; ks < 4; ks++)
+                            umma_bf16(d, sw128_desc(a_addr + ks*32u), sw128_desc(b_addr + ks*32u),
+                                      idesc, (kc | ks) != 0u ? 1u : 0u);
+                        umma_commit(&w_empty[s]);
+                    }
+                    if (ok) umma_commit(&acc_full[gl & 1u]);
+                }
+            }
+            if (!ok) s_failed = 1;
+            // arrives when every MMA issued above has completed
+            umma_commit(drained);
+        }
+    } else {
+        const uint32_t q = (uint32_t)warp & 3u;
+        const uint32_t h = (uint32_t)(warp - 2) >> 2;          // 16-column slice 0..3
+        const uint32_t r = q*32u + (uint32_t)lane;             // row within the tile
+        const uint32_t lane_base = (q*32u) << 16;
+        float xi[kIn];
+        uint32_t tile = blockIdx.x, gl = 0;
+        if (tile < num_tiles) {
+#pragma unroll
+            for (int j = 0; j < kIn; j++) xi[j] = __ldg(x + ((uint64_t)tile*128u + r)*kInLd + j);
+            encode_part(act, r, 0, h, xi);
+            release_chunk(&act_ready[0], lane);
+            encode_part(act, r, 1, h, xi);
+            release_chunk(&act_ready[1], lane);
+        }
+        bool ok = true;
+        for (; ok && tile < num_tiles; tile += gridDim.x) {
+            for (uint32_t l = 0; l < 5; l++, gl++) {
+                ok = __all_sync(0xffffffffu, mbar_wait(&acc_full[gl & 1u], (gl >> 1) & 1u));
+                tc_fence_after();
+                if (!ok) break;
+                const uint32_t taddr = tmem + (gl & 1u)*256u + lane_base;
+                if (l < 4) {
+                    const float* bl = s_bias + l*kH;
+                    for (uint32_t kc = 0; kc < 4; kc++) {
+                        const uint32_t c = kc*64u + h*16u;
+                        float v[16];
+                        tmem_ld16(taddr + c, v);
+                        uint32_t pk[8];
+#pragma unroll
+                        for (int j = 0; j < 16; j += 4) {
+                            const float4 b = *reinterpret_cast<const float4*>(bl + c + j);
+                            float a0, a1, a2, a3;
+                            f2_split(silu_pair(add2(f2(v[j], v[j + 1]), f2(b.x, b.y))), &a0, &a1);
+                            f2_split(silu_pair(add2(f2(v[j + 2], v[j + 3]), f2(b.z, b.w))), &a2, &a3);
+                            pk[j/2] = pack_bf16x2(a0, a1);
+                            pk[j/2 + 1] = pack_bf16x2(a2, a3);
+                        }
+                        uint8_t* rowp = act + kc*kActChunk + r*128u;
+#pragma unroll
+                        for (uint32_t u = 0; u < 2; u++)
+                            *reinterpret_cast<uint4*>(rowp + (((h*2u + u) ^ (r & 7u)) << 4)) =
+                                make_uint4(pk[4*u], pk[4*u + 1], pk[4*u + 2], pk[4*u + 3]);
+                        release_chunk(&act_ready[kc], lane);
+                    }
+                } else {
+                    // the next tile's inputs first: its layer 0 overlaps the outputs below
+                    const uint32_t next = tile + gridDim.x;
+                    if (next < num_tiles) {
+#pragma unroll
+                        for (int j = 0; j < kIn; j++)
+                            xi[j] = __ldg(x + ((uint64_t)next*128u + r)*kInLd + j);
+                        encode_part(act, r, 0, h, xi);
+                        release_chunk(&act_ready[0], lane);
+                        encode_part(act, r, 1, h, xi);
+                        release_chunk(&act_ready[1], lane);
+                    }
+                    const float* bl = s_bias + 4*kH;
+                    float* orow = y + ((uint64_t)tile*128u + r)*kOutPad;
+                    for (uint32_t c = h*16u; c < (uint32_t)kOutPad; c += 64u) {
+                        float v[16];
+                        tmem_ld16(taddr + c, v);
+#pragma unroll
+                        for (int j = 0; j < 16; j += 4)
+                            *reinterpret_cast<float4*>(orow + c + j) =
+                                make_float4(v[j] + bl[c + j], v[j + 1] + bl[c + j + 1],
+                                            v[j + 2] + bl[c + j + 2], v[j + 3] + bl[c + j + 3]);
+                    }
+                    tc_fence_before();
+                }
+            }
+        }
+        if (!ok) s_failed = 1;
+    }
+    tc_fence_before();
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        if (s_failed) {
+            atomicCAS(&g_error, 0u, (unsigned)MLGPU_ERR_RUNTIME);
+            // the weight chunks no MMA consumed
+            for (uint32_t it = s_consumed; it < s_issued; it++)
+                mbar_wait(&w_full[it % kWRing], (it/kWRing) & 1);
+        }
+        // the MMAs' final commit (also on success: no arrive left pending)
+        mbar_wait(drained, 0);
+    }
+    __syncthreads();
+    if (warp == 1) {
+        tc_fence_after();
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;"
+                     :: "r"(tmem), "r"(512u));
     }
 }
 
@@ -1005,6 +1354,24 @@ cudaError_t forward(const float* p, const uint8_t* img, const float* x, uint32_t
     return e;
 }
 
+// The inference forward pass in one launch (fused_forward_kernel).
+cudaError_t forward_fused(const float* p, const uint8_t* img, const float* x, uint32_t batch,
+                          float* y, cudaStream_t s) {
+    constexpr uint32_t smem = fused_smem_bytes();
+    static bool attr = false;
+    if (!attr) {
+        const cudaError_t e = cudaFuncSetAttribute(fused_forward_kernel,
+                                                   cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                   (int)smem);
+        if (e != cudaSuccess) return e;
+        attr = true;
+    }
+    const uint32_t tiles = batch/128u;
+    const uint32_t grid = tiles < (uint32_t)sm_count() ? tiles : (uint32_t)sm_count();
+    fused_forward_kernel<<<grid, kFusedThreads, smem, s>>>(p, img, x, tiles, y);
+    return cudaGetLastError();
+}
+
 cudaError_t train_step(float* p, uint8_t* img, float* m, float* v, const float* x,
                        const float* targets, const uint8_t* reached, uint32_t batch,
                        uint32_t step, float lr, float* loss_out, float* grads_out, const Work& w,
@@ -1134,6 +1501,19 @@ int mlgpu_sg_pack_weights(const float* params, void* images, void* cuda_stream) 
 
 int mlgpu_sg_forward(const float* params, const void* images, const float* inputs,
                      uint32_t batch, float* outputs, void* workspace, void* cuda_stream) {
+    (void)workspace;   // the fused pass keeps its activations on chip
+    if (!params || !images || !inputs || !outputs)
+        return report_error(MLGPU_ERR_INVALID_ARGUMENT, "NULL argument");
+    if (batch == 0 || batch % 128)
+        return report_error(MLGPU_ERR_INVALID_ARGUMENT, "batch must be a positive multiple of 128");
+    const cudaError_t e = forward_fused(params, static_cast<const uint8_t*>(images), inputs, batch,
+                                        outputs, static_cast<cudaStream_t>(cuda_stream));
+    if (e != cudaSuccess) return report_error(MLGPU_ERR_CUDA, cudaGetErrorString(e));
+    return MLGPU_OK;
+}
+
+int mlgpu_sg_forward_layered(const float* params, const void* images, const float* inputs,
+                             uint32_t batch, float* outputs, void* workspace, void* cuda_stream) {
     if (!params || !images || !inputs || !outputs || !workspace)
         return report_error(MLGPU_ERR_INVALID_ARGUMENT, "NULL argument");
     if (batch == 0 || batch % 128)

@@ -341,15 +341,23 @@ class Surrogate:
                 log(f"epoch {ep}: loss {history[-1]:.4f}")
         return history
 
-    def forward(self, x: torch.Tensor) -> torch.Tensor:
+    def forward(self, x: torch.Tensor, layered: bool = False) -> torch.Tensor:
+        """The network's outputs [n][80] for inputs [n][8]: one fused launch
+        (mlgpu_sg_forward), or with `layered` one launch per layer with the
+        activations in device memory (mlgpu_sg_forward_layered, the training
+        step's form; the same bits)."""
         n = x.shape[0]
         pad = (-n) % TILE
         if pad:
             x = torch.cat([x, torch.zeros((pad, IN_LD), dtype=x.dtype, device=x.device)])
         y = torch.empty((n + pad, OUT_LD), dtype=torch.float32, device=self.device)
-        check(lib().mlgpu_sg_forward(self.params.data_ptr(), self.images.data_ptr(),
-                                     x.data_ptr(), n + pad, y.data_ptr(),
-                                     self._workspace(n + pad, False).data_ptr(), None))
+        if layered:
+            check(lib().mlgpu_sg_forward_layered(self.params.data_ptr(), self.images.data_ptr(),
+                                                 x.data_ptr(), n + pad, y.data_ptr(),
+                                                 self._workspace(n + pad, False).data_ptr(), None))
+        else:
+            check(lib().mlgpu_sg_forward(self.params.data_ptr(), self.images.data_ptr(),
+                                         x.data_ptr(), n + pad, y.data_ptr(), None, None))
         return y[:n]
 
     def sample(self, y: torch.Tensor, x: torch.Tensor, seed: int, photon_offset: int = 0,
@@ -440,23 +448,31 @@ class Surrogate:
 
 def _forward_probe(n: int, repeats: int = 3) -> None:
     """Times the forward pass of an untrained network on the light-field
-    telescope on n random inputs (the tensor-core layers' throughput)."""
+    telescope on n random inputs (the tensor-core layers' throughput), fused
+    and layer by layer, and checks that both give the same bits."""
     from . import factories
     model = Surrogate(factories.light_field_telescope().flatten(), seed=1)
     x = torch.rand((n, IN_LD), device=model.device) * 2.0 - 1.0
-    model.forward(x)
-    torch.cuda.synchronize()
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    e0.record()
-    for _ in range(repeats):
-        model.forward(x)
-    e1.record()
-    torch.cuda.synchronize()
-    sync_errors()
-    ms = e0.elapsed_time(e1) / repeats
     flops = 2.0 * sum(fin * (80 if fout == 73 else fout) for fin, fout in LAYERS) * n
-    print(f"forward of {n} photons: {ms:.3f} ms, {flops / ms / 1e9:.1f} TFLOP/s on the "
-          f"tensor-core layers, {n / ms / 1e3:.1f} M photons/s")
+    out = {}
+    for layered in (False, True):
+        out[layered] = model.forward(x, layered=layered).clone()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(repeats):
+            model.forward(x, layered=layered)
+        e1.record()
+        torch.cuda.synchronize()
+        sync_errors()
+        ms = e0.elapsed_time(e1) / repeats
+        print(f"{'layered' if layered else 'fused'} forward of {n} photons: {ms:.3f} ms, "
+              f"{flops / ms / 1e9:.1f} TFLOP/s on the tensor-core layers, "
+              f"{n / ms / 1e3:.1f} M photons/s")
+    same = torch.equal(out[False][:, :73], out[True][:, :73])
+    print(f"fused == layered bit for bit: {same}")
+    if not same:
+        raise SystemExit(1)
 
 
 if __name__ == "__main__":

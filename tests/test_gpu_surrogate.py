@@ -136,6 +136,27 @@ def test_forward_pass_matches_oracle(sg):
     assert fro < 1e-3 and worst < 1e-2, (fro, worst)
 
 
+@pytest.mark.parametrize("tiles", [1, 5, 148, 149, 445])
+def test_fused_forward_equals_the_layered_one(sg, tiles):
+    """The one-launch forward (activations on chip, several tiles per CTA
+    beyond 148 tiles, the last CTAs with one tile fewer) gives the layered
+    form's bits: same encoding, K order, bias, SiLU and BF16 rounding."""
+    import torch
+    flat = load_golden("light_field_small")[0]
+    model = sg.Surrogate(flat, seed=11)
+    w4, _, b4 = sg.param_slices()[4]
+    model.params[w4] *= 30.0
+    model.pack()
+    g = torch.Generator(device="cuda").manual_seed(tiles)
+    x = torch.rand((tiles * 128, 8), generator=g, device="cuda") * 2.0 - 1.0
+    fused = model.forward(x)
+    layered = model.forward(x, layered=True)
+    sg.sync_errors()
+    assert torch.isfinite(fused[:, :73]).all()
+    assert torch.equal(fused[:, :73], layered[:, :73])
+    assert torch.count_nonzero(fused[:, 73:]) == 0
+
+
 def test_training_reduces_the_loss(sg):
     import torch
     from merlict_development_kit_b200 import engine
