@@ -773,19 +773,21 @@ encode_kernel(const float* __restrict__ x, uint32_t batch, uint8_t* __restrict__
 
 // ---- the fused inference forward ----------------------------------------------------
 //
-// All five layers of a 128-row tile in one persistent kernel, the
-// activations never leaving the SM: the tile's activation lives in shared
-// memory as a 128-row image (4 chunks of 64 columns, 16 KB each), the
-// layers' weights stream through a ring of 32 KB stages (one 64-wide K chunk
-// of one layer per stage; they stay in L2), and two accumulators in tensor
-// memory alternate between consecutive layers.  The epilogue of layer l
-// drains its accumulator 64 columns at a time into the activation chunk it
-// replaces (that chunk's readers, the MMAs of layer l, have completed) and
-// releases each chunk on its own barrier, so the MMAs of layer l+1 start on
-// chunk 0 while the epilogue is still on chunk 1: the tensor cores and the
-// epilogue overlap within a tile.  At the last layer the epilogue warps
-// first encode the next tile's inputs into chunks 0 and 1 (so its layer 0
-// runs while they drain the outputs) and then write the 80 FP32 outputs.
+// All five layers of 128-row tiles in one persistent kernel, the
+// activations never leaving the SM.  Each CTA keeps two tiles in flight, in
+// slots 0 and 1: a slot holds its tile's activation in shared memory as a
+// 128-row image (4 chunks of 64 columns, 16 KB each) and its accumulator in
+// tensor memory (256 columns).  The layers' weights stream through a ring
+// of 32 KB stages (one 64-wide K chunk of one layer per stage; they stay in
+// L2).  The two slots take turns: while the tensor cores run layer l of one
+// slot, the epilogue warps drain layer l - 1 of the other into its
+// activation image (bias, SiLU, BF16), so the MMAs and the epilogue overlap
+// across tiles.  Steps run in the order (pair, layer, slot); the epilogue
+// of a step releases the slot's four activation chunks on four barriers
+// (after the last of them the accumulator is free as well), and the MMAs of
+// the slot's next step wait for all four.  At the last layer the epilogue
+// warps first encode the slot's next tile into chunks 0 and 1, then write
+// the 80 FP32 outputs, then release chunks 2 and 3.
 //
 // The arithmetic is that of the layer-by-layer path (same encoding, K
 // order, bias addition, SiLU and BF16 rounding), so both give the same bits.
@@ -801,29 +803,46 @@ encode_kernel(const float* __restrict__ x, uint32_t batch, uint8_t* __restrict__
 
 constexpr int kFusedThreads = 576;
 constexpr int kEpiWarps = 16;
-constexpr int kWRing = 4;                       // weight stages
+constexpr int kWRing = 3;                       // weight stages
 constexpr uint32_t kWStage = 32768u;            // 256 rows x 64 K x 2 bytes
 constexpr uint32_t kActChunk = 16384u;          // 128 rows x 64 K x 2 bytes
-constexpr int kChunksPerTile = kEnc/64 + 3*(kH/64) + kH/64;   // 18
-constexpr int kBiasFloats = 4*kH + kOutPad;     // 1104
-constexpr uint32_t kFusedBarOff = 4u*kActChunk + kWRing*kWStage + (uint32_t)kBiasFloats*4u;
+constexpr uint32_t kSlotBytes = 4u*kActChunk;   // one tile's activation image
+constexpr uint32_t kFusedBarOff = 2u*kSlotBytes + kWRing*kWStage;
 
 __host__ __device__ constexpr uint32_t fused_smem_bytes() {
-    return kFusedBarOff + 16u*8u + 1024u;
+    return kFusedBarOff + 24u*8u + 1024u;
 }
 
-// Weight chunk c (0..17) of a tile's sequence (layer 0: 2 chunks, layers
-// 1..4: 4 each): its offset in the images and its bytes.
-__device__ __forceinline__ void weight_chunk(uint32_t c, uint64_t* off, uint32_t* bytes) {
-    if (c < 2u) {
-        *off = kImgW0Off + (uint64_t)c*kWStage; *bytes = kWStage;
-    } else if (c < 14u) {
-        const uint32_t l = 1u + (c - 2u)/4u, kc = (c - 2u) % 4u;
+// K chunk kc of layer l's weight image: its offset in the images and its
+// bytes (layer 0: 256 x 128, 2 chunks; 1..3: 256 x 256; 4: 80 x 256).
+__device__ __forceinline__ void weight_chunk(uint32_t l, uint32_t kc, uint64_t* off,
+                                             uint32_t* bytes) {
+    if (l == 0) {
+        *off = kImgW0Off + (uint64_t)kc*kWStage; *bytes = kWStage;
+    } else if (l < 4) {
         *off = img_w((int)l) + (uint64_t)kc*kWStage; *bytes = kWStage;
     } else {
-        *off = kImgW4Off + (uint64_t)(c - 14u)*(kOutPad*128u); *bytes = kOutPad*128u;
+        *off = kImgW4Off + (uint64_t)kc*(kOutPad*128u); *bytes = kOutPad*128u;
     }
 }
+
+// The steps of a CTA that owns `n` tiles, in order: step i is (pair, layer,
+// slot) = (i / 10, (i / 2) % 5, i % 2), skipped when its tile (local index
+// 2 pair + slot) does not exist.
+struct StepIter {
+    uint32_t n, i;
+    __device__ __forceinline__ bool next(uint32_t* k, uint32_t* l, uint32_t* s) {
+        for (;; i++) {
+            const uint32_t kk = 2u*(i/10u) + (i & 1u);
+            if (2u*(i/10u) >= n) return false;
+            if (kk < n) {
+                *k = kk; *l = (i >> 1) % 5u; *s = i & 1u;
+                i++;
+                return true;
+            }
+        }
+    }
+};
 
 // Encodes features [64 p + 16 h, + 16) of row r of a tile (inputs xi) into
 // chunk p of the activation image: the values of encoded(), one sincospif
@@ -877,26 +896,22 @@ fused_forward_kernel(const float* __restrict__ p, const uint8_t* __restrict__ im
     extern __shared__ uint8_t smem_raw[];
     uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) &
                                                ~(uintptr_t)1023);
-    uint8_t* act = smem;                                        // 4 x 16 KB
-    uint8_t* ring = smem + 4u*kActChunk;                        // kWRing x 32 KB
-    float* s_bias = reinterpret_cast<float*>(ring + kWRing*kWStage);
+    uint8_t* ring = smem + 2u*kSlotBytes;                       // kWRing x 32 KB
     uint64_t* w_full = reinterpret_cast<uint64_t*>(smem + kFusedBarOff);
     uint64_t* w_empty = w_full + kWRing;
-    uint64_t* act_ready = w_empty + kWRing;                     // [4], one arrival per epilogue warp
-    uint64_t* acc_full = act_ready + 4;                         // [2]
+    uint64_t* act_ready = w_empty + kWRing;                     // [slot][chunk], one arrival per epilogue warp
+    uint64_t* acc_full = act_ready + 8;                         // [slot]
     uint64_t* drained = acc_full + 2;
     uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(drained + 1);
     __shared__ int s_failed;
     __shared__ uint32_t s_issued, s_consumed;   // weight chunks copied in / taken by the MMAs
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    // this CTA's tiles: blockIdx.x + k gridDim.x, k < n
+    const uint32_t n = blockIdx.x < num_tiles ? (num_tiles - blockIdx.x + gridDim.x - 1)/gridDim.x : 0u;
 
-    for (int i = threadIdx.x; i < kBiasFloats; i += kFusedThreads) {
-        const int l = i/kH, n = i % kH;
-        s_bias[i] = l < 4 ? __ldg(p + b_off(l) + n) : (n < kOut ? __ldg(p + kB4 + n) : 0.0f);
-    }
     if (threadIdx.x == 0) {
         for (int s = 0; s < kWRing; s++) { mbar_init(&w_full[s], 1); mbar_init(&w_empty[s], 1); }
-        for (int c = 0; c < 4; c++) mbar_init(&act_ready[c], kEpiWarps);
+        for (int c = 0; c < 8; c++) mbar_init(&act_ready[c], kEpiWarps);
         for (int a = 0; a < 2; a++) mbar_init(&acc_full[a], 1);
         mbar_init(drained, 1);
         s_failed = 0;
@@ -916,10 +931,12 @@ fused_forward_kernel(const float* __restrict__ p, const uint8_t* __restrict__ im
 
     if (warp == 0) {
         if (lane == 0) {
-            uint32_t it = 0;
+            uint32_t it = 0, k, l, sl;
             bool ok = true;
-            for (uint32_t tile = blockIdx.x; ok && tile < num_tiles; tile += gridDim.x) {
-                for (uint32_t c = 0; c < (uint32_t)kChunksPerTile; c++, it++) {
+            StepIter st{n, 0};
+            while (ok && st.next(&k, &l, &sl)) {
+                const uint32_t chunks = l == 0 ? (uint32_t)(kEnc/64) : (uint32_t)(kH/64);
+                for (uint32_t kc = 0; kc < chunks; kc++, it++) {
                     const uint32_t s = it % kWRing;
                     if (it >= (uint32_t)kWRing && !mbar_wait(&w_empty[s], ((it/kWRing) - 1) & 1)) {
                         ok = false;
@@ -927,7 +944,7 @@ fused_forward_kernel(const float* __restrict__ p, const uint8_t* __restrict__ im
                     }
                     uint32_t bytes;
                     uint64_t off;
-                    weight_chunk(c, &off, &bytes);
+                    weight_chunk(l, kc, &off, &bytes);
                     mbar_expect_tx(&w_full[s], bytes);
                     bulk_g2s(ring + s*kWStage, img + off, bytes, &w_full[s]);
                     s_issued = it + 1;
@@ -937,31 +954,36 @@ fused_forward_kernel(const float* __restrict__ p, const uint8_t* __restrict__ im
         }
     } else if (warp == 1) {
         if (lane == 0) {
-            uint32_t it = 0, gl = 0;
-            uint32_t ready = 0;   // bit kc: parity of the next act_ready[kc] phase
+            uint32_t it = 0, k, l, sl;
+            uint32_t ready = 0;   // bit 4 slot + chunk: parity of the next act_ready phase
             bool ok = true;
-            for (uint32_t tile = blockIdx.x; ok && tile < num_tiles; tile += gridDim.x) {
-                for (uint32_t l = 0; ok && l < 5; l++, gl++) {
-                    const uint32_t idesc = l == 4 ? idesc_bf16(128, kOutPad) : idesc_bf16(128, kH);
-                    const uint32_t d = tmem + (gl & 1u)*256u;
-                    const uint32_t chunks = l == 0 ? (uint32_t)(kEnc/64) : (uint32_t)(kH/64);
-                    for (uint32_t kc = 0; kc < chunks; kc++, it++) {
-                        if (!mbar_wait(&act_ready[kc], (ready >> kc) & 1u)) { ok = false; break; }
-                        ready ^= 1u << kc;
-                        const uint32_t s = it % kWRing;
-                        if (!mbar_wait(&w_full[s], (it/kWRing) & 1)) { ok = false; break; }
-                        s_consumed = it + 1;
-                        tc_fence_after();
-                        const uint32_t a_addr = smem_u32(act + kc*kActChunk);
-                        const uint32_t b_addr = smem_u32(ring + s*kWStage);
-#pragma unroll
-                        for (uint32_t ks = 0; ks < 4; ks++)
-                            umma_bf16(d, sw128_desc(a_addr + ks*32u), sw128_desc(b_addr + ks*32u),
-                                      idesc, (kc | ks) != 0u ? 1u : 0u);
-                        umma_commit(&w_empty[s]);
-                    }
-                    if (ok) umma_commit(&acc_full[gl & 1u]);
+            StepIter st{n, 0};
+            while (ok && st.next(&k, &l, &sl)) {
+                // the slot's activation chunks written and its accumulator drained
+                for (uint32_t c = 0; ok && c < 4; c++) {
+                    const uint32_t b = sl*4u + c;
+                    ok = mbar_wait(&act_ready[b], (ready >> b) & 1u);
+                    ready ^= 1u << b;
                 }
+                if (!ok) break;
+                tc_fence_after();
+                const uint32_t idesc = l == 4 ? idesc_bf16(128, kOutPad) : idesc_bf16(128, kH);
+                const uint32_t d = tmem + sl*256u;
+                const uint32_t chunks = l == 0 ? (uint32_t)(kEnc/64) : (uint32_t)(kH/64);
+                for (uint32_t kc = 0; kc < chunks; kc++, it++) {
+                    const uint32_t s = it % kWRing;
+                    if (!mbar_wait(&w_full[s], (it/kWRing) & 1)) { ok = false; break; }
+                    s_consumed = it + 1;
+                    tc_fence_after();
+                    const uint32_t a_addr = smem_u32(smem + sl*kSlotBytes + kc*kActChunk);
+                    const uint32_t b_addr = smem_u32(ring + s*kWStage);
+#pragma unroll
+                    for (uint32_t ks = 0; ks < 4; ks++)
+                        umma_bf16(d, sw128_desc(a_addr + ks*32u), sw128_desc(b_addr + ks*32u),
+                                  idesc, (kc | ks) != 0u ? 1u : 0u);
+                    umma_commit(&w_empty[s]);
+                }
+                if (ok) umma_commit(&acc_full[sl]);
             }
             if (!ok) s_failed = 1;
             // arrives when every MMA issued above has completed
@@ -973,69 +995,84 @@ fused_forward_kernel(const float* __restrict__ p, const uint8_t* __restrict__ im
         const uint32_t r = q*32u + (uint32_t)lane;             // row within the tile
         const uint32_t lane_base = (q*32u) << 16;
         float xi[kIn];
-        uint32_t tile = blockIdx.x, gl = 0;
-        if (tile < num_tiles) {
+        // the first tile of each slot: its inputs encoded, its accumulator free
+        for (uint32_t sl = 0; sl < 2u && sl < n; sl++) {
+            const uint64_t row = (uint64_t)(blockIdx.x + sl*gridDim.x)*128u + r;
 #pragma unroll
-            for (int j = 0; j < kIn; j++) xi[j] = __ldg(x + ((uint64_t)tile*128u + r)*kInLd + j);
+            for (int j = 0; j < kIn; j++) xi[j] = __ldg(x + row*kInLd + j);
+            uint8_t* act = smem + sl*kSlotBytes;
             encode_part(act, r, 0, h, xi);
-            release_chunk(&act_ready[0], lane);
+            release_chunk(&act_ready[sl*4u + 0u], lane);
             encode_part(act, r, 1, h, xi);
-            release_chunk(&act_ready[1], lane);
+            release_chunk(&act_ready[sl*4u + 1u], lane);
+            release_chunk(&act_ready[sl*4u + 2u], lane);
+            release_chunk(&act_ready[sl*4u + 3u], lane);
         }
+        uint32_t accp = 0, k, l, sl;   // accp bit s: parity of acc_full[s]'s next phase
         bool ok = true;
-        for (; ok && tile < num_tiles; tile += gridDim.x) {
-            for (uint32_t l = 0; l < 5; l++, gl++) {
-                ok = __all_sync(0xffffffffu, mbar_wait(&acc_full[gl & 1u], (gl >> 1) & 1u));
-                tc_fence_after();
-                if (!ok) break;
-                const uint32_t taddr = tmem + (gl & 1u)*256u + lane_base;
-                if (l < 4) {
-                    const float* bl = s_bias + l*kH;
-                    for (uint32_t kc = 0; kc < 4; kc++) {
-                        const uint32_t c = kc*64u + h*16u;
-                        float v[16];
-                        tmem_ld16(taddr + c, v);
-                        uint32_t pk[8];
+        StepIter st{n, 0};
+        while (st.next(&k, &l, &sl)) {
+            ok = __all_sync(0xffffffffu, mbar_wait(&acc_full[sl], (accp >> sl) & 1u));
+            accp ^= 1u << sl;
+            tc_fence_after();
+            if (!ok) break;
+            uint8_t* act = smem + sl*kSlotBytes;
+            uint64_t* ready = act_ready + sl*4u;
+            const uint32_t taddr = tmem + sl*256u + lane_base;
+            if (l < 4) {
+                const float* bl = p + b_off((int)l);
+                for (uint32_t kc = 0; kc < 4; kc++) {
+                    const uint32_t c = kc*64u + h*16u;
+                    float v[16];
+                    tmem_ld16(taddr + c, v);
+                    uint32_t pk[8];
 #pragma unroll
-                        for (int j = 0; j < 16; j += 4) {
-                            const float4 b = *reinterpret_cast<const float4*>(bl + c + j);
-                            float a0, a1, a2, a3;
-                            f2_split(silu_pair(add2(f2(v[j], v[j + 1]), f2(b.x, b.y))), &a0, &a1);
-                            f2_split(silu_pair(add2(f2(v[j + 2], v[j + 3]), f2(b.z, b.w))), &a2, &a3);
-                            pk[j/2] = pack_bf16x2(a0, a1);
-                            pk[j/2 + 1] = pack_bf16x2(a2, a3);
+                    for (int j = 0; j < 16; j += 4) {
+                        const float4 b = __ldg(reinterpret_cast<const float4*>(bl + c + j));
+                        float a0, a1, a2, a3;
+                        f2_split(silu_pair(add2(f2(v[j], v[j + 1]), f2(b.x, b.y))), &a0, &a1);
+                        f2_split(silu_pair(add2(f2(v[j + 2], v[j + 3]), f2(b.z, b.w))), &a2, &a3);
+                        pk[j/2] = pack_bf16x2(a0, a1);
+                        pk[j/2 + 1] = pack_bf16x2(a2, a3);
+                    }
+                    uint8_t* rowp = act + kc*kActChunk + r*128u;
+#pragma unroll
+                    for (uint32_t u = 0; u < 2; u++)
+                        *reinterpret_cast<uint4*>(rowp + (((h*2u + u) ^ (r & 7u)) << 4)) =
+                            make_uint4(pk[4*u], pk[4*u + 1], pk[4*u + 2], pk[4*u + 3]);
+                    release_chunk(&ready[kc], lane);
+                }
+            } else {
+                // the slot's next tile first: its layer 0 can start once the
+                // outputs below are out of tensor memory
+                const uint32_t next = k + 2u;
+                if (next < n) {
+                    const uint64_t row = (uint64_t)(blockIdx.x + next*gridDim.x)*128u + r;
+#pragma unroll
+                    for (int j = 0; j < kIn; j++) xi[j] = __ldg(x + row*kInLd + j);
+                    encode_part(act, r, 0, h, xi);
+                    release_chunk(&ready[0], lane);
+                    encode_part(act, r, 1, h, xi);
+                    release_chunk(&ready[1], lane);
+                }
+                float* orow = y + ((uint64_t)(blockIdx.x + k*gridDim.x)*128u + r)*kOutPad;
+                for (uint32_t c = h*16u; c < (uint32_t)kOutPad; c += 64u) {
+                    float v[16];
+                    tmem_ld16(taddr + c, v);
+#pragma unroll
+                    for (int j = 0; j < 16; j += 4) {
+                        float o[4];
+#pragma unroll
+                        for (int u = 0; u < 4; u++) {
+                            const uint32_t col = c + (uint32_t)(j + u);
+                            o[u] = v[j + u] + (col < (uint32_t)kOut ? __ldg(p + kB4 + col) : 0.0f);
                         }
-                        uint8_t* rowp = act + kc*kActChunk + r*128u;
-#pragma unroll
-                        for (uint32_t u = 0; u < 2; u++)
-                            *reinterpret_cast<uint4*>(rowp + (((h*2u + u) ^ (r & 7u)) << 4)) =
-                                make_uint4(pk[4*u], pk[4*u + 1], pk[4*u + 2], pk[4*u + 3]);
-                        release_chunk(&act_ready[kc], lane);
+                        *reinterpret_cast<float4*>(orow + c + j) = make_float4(o[0], o[1], o[2], o[3]);
                     }
-                } else {
-                    // the next tile's inputs first: its layer 0 overlaps the outputs below
-                    const uint32_t next = tile + gridDim.x;
-                    if (next < num_tiles) {
-#pragma unroll
-                        for (int j = 0; j < kIn; j++)
-                            xi[j] = __ldg(x + ((uint64_t)next*128u + r)*kInLd + j);
-                        encode_part(act, r, 0, h, xi);
-                        release_chunk(&act_ready[0], lane);
-                        encode_part(act, r, 1, h, xi);
-                        release_chunk(&act_ready[1], lane);
-                    }
-                    const float* bl = s_bias + 4*kH;
-                    float* orow = y + ((uint64_t)tile*128u + r)*kOutPad;
-                    for (uint32_t c = h*16u; c < (uint32_t)kOutPad; c += 64u) {
-                        float v[16];
-                        tmem_ld16(taddr + c, v);
-#pragma unroll
-                        for (int j = 0; j < 16; j += 4)
-                            *reinterpret_cast<float4*>(orow + c + j) =
-                                make_float4(v[j] + bl[c + j], v[j + 1] + bl[c + j + 1],
-                                            v[j + 2] + bl[c + j + 2], v[j + 3] + bl[c + j + 3]);
-                    }
-                    tc_fence_before();
+                }
+                if (next < n) {
+                    release_chunk(&ready[2], lane);
+                    release_chunk(&ready[3], lane);
                 }
             }
         }
