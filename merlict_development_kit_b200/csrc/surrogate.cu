@@ -25,6 +25,7 @@
 #include "merlict_b200_philox.h"
 #include "merlict_b200_surrogate.h"
 #include "mlgpu_internal.h"
+#include "paired_f32.cuh"
 
 namespace mlgpu {
 namespace sg {
@@ -169,26 +170,6 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float* v) {
     for (int j = 0; j < 16; j++) v[j] = __uint_as_float(r[j]);
 }
 
-// Paired FP32 arithmetic (Blackwell's f32x2 instructions: two IEEE
-// operations in one issue slot, each rounded like its scalar form).
-__device__ __forceinline__ uint64_t f2(float lo, float hi) {
-    uint64_t v;
-    asm("mov.b64 %0, {%1, %2};" : "=l"(v) : "f"(lo), "f"(hi));
-    return v;
-}
-__device__ __forceinline__ void f2_split(uint64_t v, float* lo, float* hi) {
-    asm("mov.b64 {%0, %1}, %2;" : "=f"(*lo), "=f"(*hi) : "l"(v));
-}
-__device__ __forceinline__ uint64_t mul2(uint64_t a, uint64_t b) {
-    uint64_t d;
-    asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
-    return d;
-}
-__device__ __forceinline__ uint64_t add2(uint64_t a, uint64_t b) {
-    uint64_t d;
-    asm("add.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
-    return d;
-}
 __device__ __forceinline__ float ex2_ftz(float a) {
     float r;
     asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(a));
