@@ -809,6 +809,170 @@ def run_precision(args, world, rank, local):
         }), flush=True)
 
 
+def run_calibration(args, world, rank, local):
+    """merlict's plenoscope calibration (Calibrator::run_calibration,
+    Calibrator.cpp:145-168) of the config-1 light-field telescope: one step =
+    `--calibration-photons` calibration photons (8e6, calibration/Config.cpp:
+    8-9) generated, propagated (5 interactions) and reduced to every lixel's
+    statistics, through calibration.calibrate (the statistics come back to the
+    host).  Beside it: the statistics kernel alone (mlgpu_lixel_statistics) on
+    per-photon results of the same size, and merlict's own
+    LixelStatisticsFiller on the same arrays on one host core."""
+    import numpy as np
+    import torch
+    from merlict_development_kit_b200 import calibration as CAL, engine, factories as F
+
+    torch.cuda.set_device(local)
+    flat = F.light_field_telescope(**SCENE).flatten()
+    scene = engine.Scene(flat)
+    n = args.calibration_photons
+    fov_radius = np.deg2rad(SCENE["fov_deg"]) / 2.0
+    clocks = ClockSampler(local)
+
+    def step(seed):
+        return CAL.calibrate(scene, SCENE["aperture_radius"], fov_radius, num_photons=n,
+                             seed=seed)
+    for w in range(args.warmup):
+        step(100 + w)
+    torch.cuda.synchronize()
+    clocks.start()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for s in range(args.steps):
+        st = step(1 + s)
+    e1.record()
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    ms = e0.elapsed_time(e1) / args.steps
+    eff = st["efficiency"]
+    # the statistics kernel alone, on per-photon results of the same size
+    rng = np.random.default_rng(5)
+    sensor = rng.integers(-1, flat.num_sensors, size=n).astype(np.int32)
+    sensor[rng.random(n) < 0.4] = -1
+    vals = [rng.normal(size=n).astype(np.float32) * s_ for s_ in (0.02, 0.02, 2.0, 2.0, 3e-9)]
+    dev = [torch.as_tensor(v, device="cuda") for v in [sensor] + vals]
+    per_lixel = n / flat.num_sensors
+    CAL.lixel_statistics(scene, *dev, per_lixel)
+    torch.cuda.synchronize()
+    e0.record()
+    for _ in range(args.steps):
+        got = CAL.lixel_statistics(scene, *dev, per_lixel)
+    e1.record()
+    torch.cuda.synchronize()
+    stats_ms = e0.elapsed_time(e1) / args.steps
+    ref = None
+    if not args.no_cpu_baseline:
+        from oracle import oracle as O
+        if O.harness_available():
+            t0 = time.perf_counter()
+            r = O.lixel_statistics_reference(sensor, *vals, flat.num_sensors, 1, n)
+            ref_s = time.perf_counter() - t0
+            g = np.stack([got[f] for f in CAL.FIELDS], axis=1)
+            ref = {"value": n / ref_s, "unit": "photons/s", "cores": 1, "kind": "reference",
+                   "sample": f"merlict's LixelStatisticsFiller on the same {n} per-photon results",
+                   "identical_to_device": bool(np.array_equal(g, r, equal_nan=True))}
+    scene.close()
+    if rank == 0:
+        print(json.dumps({
+            "metric": "photons/s", "value": n / (ms * 1e-3), "unit": "photons/s",
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic",
+            "config": {"workload": "plenoscope calibration of the light-field telescope "
+                                   "(63,379 lixels): photons, propagation, lixel statistics",
+                       "photons_per_step": n, "max_interactions": 5,
+                       "lixels_seen": int(np.sum(eff > 0))},
+            "lixel_statistics_kernel": {"ms": stats_ms, "photons_per_s": n / (stats_ms * 1e-3)},
+            "cpu_baseline": ref, "clocks": clk,
+        }), flush=True)
+
+
+def run_corsika(args, world, rank, local):
+    """merlict's EventIoPhotonFactory (merlict_corsika/PhotonFactory.cpp:
+    8-136) on the device: one step = `--bunches` CORSIKA photon bunches
+    (resident in HBM; weights uniform in [0, 16], a seventh of them whole)
+    expanded into photons by mlgpu_corsika_photons, which returns the
+    photon count to the host.  The bound is HBM: 32 bytes in per bunch, 60
+    bytes out per photon (seven FP64 planes and the bunch id).  Beside it:
+    merlict's own factory on a sample of the bunches on one host core."""
+    import numpy as np
+    import torch
+    from merlict_development_kit_b200 import engine, factories as F
+
+    torch.cuda.set_device(local)
+    flat = F.light_field_telescope(**SCENE).flatten()
+    scene = engine.Scene(flat)
+    n = args.bunches
+    rng = np.random.default_rng(3)
+    b = np.zeros((n, 8), np.float32)
+    b[:, 0] = rng.uniform(-15000, 15000, n)
+    b[:, 1] = rng.uniform(-15000, 15000, n)
+    th = np.deg2rad(rng.uniform(0, 4, n))
+    ph = rng.uniform(0, 2 * np.pi, n)
+    b[:, 2] = np.sin(th) * np.cos(ph)
+    b[:, 3] = np.sin(th) * np.sin(ph)
+    b[:, 4] = rng.normal(0, 5, n)
+    b[:, 5] = rng.uniform(5e5, 2e6, n)
+    w = rng.uniform(0, 16, n)
+    w[::7] = np.floor(w[::7])
+    b[:, 6] = w
+    b[:, 7] = rng.uniform(-700, -250, n)
+    bunches = torch.as_tensor(b, device="cuda")
+    clocks = ClockSampler(local)
+    for wu in range(args.warmup):
+        out = scene.corsika_photons(bunches, engine.Philox(wu))
+    del out
+    torch.cuda.synchronize()
+    clocks.start()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    total = 0
+    for s in range(args.steps):
+        out = scene.corsika_photons(bunches, engine.Philox(10 + s))
+        total += int(out["id"].numel())
+        del out
+    e1.record()
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    ms = e0.elapsed_time(e1) / args.steps
+    photons = total / args.steps
+    moved = 32.0 * n + 60.0 * photons
+    peaks = {}
+    p = os.path.join(REPO, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            peaks = json.load(f)
+    peak = peaks.get("hbm_gbs", 6650.0)
+    ref = None
+    if not args.no_cpu_baseline:
+        from oracle import oracle as O
+        if O.harness_available():
+            m = min(n, 500_000)
+            u = rng.random(m)
+            t0 = time.perf_counter()
+            r = O.corsika_photons_reference(b[:m], u)
+            ref_s = time.perf_counter() - t0
+            ref = {"value": r["id"].size / ref_s, "unit": "photons/s", "cores": 1,
+                   "kind": "reference",
+                   "sample": f"merlict's EventIoPhotonFactory on the first {m} bunches"}
+    scene.close()
+    if rank == 0:
+        print(json.dumps({
+            "metric": "photons/s", "value": photons / (ms * 1e-3), "unit": "photons/s",
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic",
+            "config": {"workload": "CORSIKA photon bunches expanded on the device",
+                       "bunches_per_step": n, "photons_per_step": photons},
+            "roofline": {"bound": "hbm", "achieved": moved / (ms * 1e-3) / 1e9,
+                         "peak": peak, "unit": "GB/s",
+                         "frac": moved / (ms * 1e-3) / 1e9 / peak,
+                         "algorithmic_bytes": "32 per bunch + 60 per photon",
+                         "peak_source": "MEASURED_PEAKS.json hbm_gbs"},
+            "cpu_baseline": ref, "clocks": clk,
+        }), flush=True)
+
+
 def run_surrogate(args, world, rank, local):
     """The learned surrogate (config 4) on the light-field telescope: trained
     on `--train-photons` photons traced exactly (FP64), evaluated on
@@ -959,12 +1123,16 @@ def main():
     ap.add_argument("--no-autotune", dest="autotune", action="store_false",
                     help="default wavefront knobs instead of mlgpu_scene_autotune's")
     ap.add_argument("--workload", choices=["telescope", "bunches", "precision", "surrogate",
-                                           "signal"],
+                                           "signal", "calibration", "corsika"],
                     default="telescope",
                     help="telescope: the light-field telescope batch; bunches: 4096 "
                          "air-shower-like events of uneven sizes, batched vs one call per event; "
                          "precision: the FP32 forms against FP64 on the large reflector; "
-                         "signal: the signal chain after binning of one config-1 event")
+                         "signal: the signal chain after binning of one config-1 event; "
+                         "calibration: the plenoscope calibration (8e6 photons); "
+                         "corsika: CORSIKA bunches expanded into photons on the device")
+    ap.add_argument("--calibration-photons", type=int, default=8_000_000)
+    ap.add_argument("--bunches", type=int, default=8_000_000)
     ap.add_argument("--events", type=int, default=4096)
     ap.add_argument("--precision-photons", type=int, default=100_000_000,
                     help="photons of the precision study (config 3) in the default line's forms")
@@ -990,6 +1158,10 @@ def main():
             run_surrogate(args, world, rank, local)
         elif args.workload == "signal":
             run_signal(args, world, rank, local)
+        elif args.workload == "calibration":
+            run_calibration(args, world, rank, local)
+        elif args.workload == "corsika":
+            run_corsika(args, world, rank, local)
         else:
             run_ours(args, world, rank, local)
     finally:

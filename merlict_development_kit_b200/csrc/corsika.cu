@@ -12,7 +12,8 @@
 // order, compiled with --fmad=false, so the photons are bit-identical to
 // the reference's given the same draws.
 //
-// Three passes: counts per bunch, an exclusive scan, the expansion.
+// Three passes: counts per bunch, an exclusive scan, the expansion (a
+// warp per 32 bunches, writing their photons as one contiguous run).
 #include <cstdint>
 
 #include "merlict_b200_philox.h"
@@ -119,39 +120,74 @@ scan_add_kernel(uint64_t* __restrict__ out, uint64_t n, const uint64_t* __restri
         out[i] += sums[i/kScan];
 }
 
-__global__ void __launch_bounds__(256)
+// The expansion, a warp per 32 consecutive bunches: each lane computes its
+// bunch's photon (merlict's arithmetic) into shared memory, then the warp
+// writes the group's photons as one contiguous run -- lane p of a round
+// writes photon p, found in the bunch whose inclusive count first exceeds p
+// (a five-step binary search over the group's counts) -- so that every
+// store instruction covers consecutive addresses.
+constexpr int kExpandWarps = 8;
+
+__global__ void __launch_bounds__(32*kExpandWarps)
 corsika_expand_kernel(const float* __restrict__ b, uint64_t n, const uint32_t* __restrict__ count,
                       const uint64_t* __restrict__ offset, const int32_t* __restrict__ ids,
                       double* __restrict__ sx, double* __restrict__ sy, double* __restrict__ sz,
                       double* __restrict__ dx, double* __restrict__ dy, double* __restrict__ dz,
                       double* __restrict__ wl, int32_t* __restrict__ out_id) {
-    for (uint64_t i = blockIdx.x*(uint64_t)blockDim.x + threadIdx.x; i < n;
-         i += (uint64_t)gridDim.x*blockDim.x) {
-        const uint32_t c = count[i];
-        if (c == 0) continue;
-        const float* r = b + 8*i;
-        // direction_of_motion, PhotonFactory.cpp:113-118
-        const double u = (double)__ldg(r + 2), v = (double)__ldg(r + 3);
-        const double z = sqrt(1.0 - u*u - v*v);
-        const double cx = u, cy = v, cz = -z;
-        // Ray(ground point, -direction): direction normalised (Ray.cpp:16-20)
-        const double ux = cx*-1.0, uy = cy*-1.0, uz = cz*-1.0;
-        const double un = sqrt(ux*ux + uy*uy + uz*uz);
-        const double nx = ux/un, ny = uy/un, nz = uz/un;
-        // ray_parameter_for_production_point, PhotonFactory.cpp:58-62
-        const double t = (double)__ldg(r + 4)*1e-9;
-        const double par = t*299792458.0 + 1e3;
-        const double gx = (double)__ldg(r + 0)*1e-2, gy = (double)__ldg(r + 1)*1e-2, gz = 0.0;
-        const double px = gx + nx*par, py = gy + ny*par, pz = gz + nz*par;
-        const double lam = fabs((double)__ldg(r + 7)*1e-9);
-        const int32_t id = ids ? __ldg(ids + i) : (int32_t)i;
-        const uint64_t o = offset[i];
-        for (uint32_t k = 0; k < c; k++) {
-            sx[o + k] = px; sy[o + k] = py; sz[o + k] = pz;
-            dx[o + k] = cx; dy[o + k] = cy; dz[o + k] = cz;
-            wl[o + k] = lam;
-            if (out_id) out_id[o + k] = id;
+    __shared__ double s_val[kExpandWarps][32][7];
+    __shared__ int32_t s_id[kExpandWarps][32];
+    __shared__ uint32_t s_incl[kExpandWarps][32];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const uint64_t groups = (n + 31)/32;
+    for (uint64_t grp = (uint64_t)blockIdx.x*kExpandWarps + warp; grp < groups;
+         grp += (uint64_t)gridDim.x*kExpandWarps) {
+        const uint64_t i = grp*32 + (uint64_t)lane;
+        const uint32_t c = i < n ? count[i] : 0u;
+        if (c != 0) {
+            const float* r = b + 8*i;
+            // direction_of_motion, PhotonFactory.cpp:113-118
+            const double u = (double)__ldg(r + 2), v = (double)__ldg(r + 3);
+            const double z = sqrt(1.0 - u*u - v*v);
+            const double cx = u, cy = v, cz = -z;
+            // Ray(ground point, -direction): direction normalised (Ray.cpp:16-20)
+            const double ux = cx*-1.0, uy = cy*-1.0, uz = cz*-1.0;
+            const double un = sqrt(ux*ux + uy*uy + uz*uz);
+            const double nx = ux/un, ny = uy/un, nz = uz/un;
+            // ray_parameter_for_production_point, PhotonFactory.cpp:58-62
+            const double t = (double)__ldg(r + 4)*1e-9;
+            const double par = t*299792458.0 + 1e3;
+            const double gx = (double)__ldg(r + 0)*1e-2, gy = (double)__ldg(r + 1)*1e-2, gz = 0.0;
+            double* sv = s_val[warp][lane];
+            sv[0] = gx + nx*par; sv[1] = gy + ny*par; sv[2] = gz + nz*par;
+            sv[3] = cx; sv[4] = cy; sv[5] = cz;
+            sv[6] = fabs((double)__ldg(r + 7)*1e-9);
+            s_id[warp][lane] = ids ? __ldg(ids + i) : (int32_t)i;
         }
+        uint32_t incl = c;
+#pragma unroll
+        for (int d = 1; d < 32; d <<= 1) {
+            const uint32_t y = __shfl_up_sync(0xffffffffu, incl, d);
+            if (lane >= d) incl += y;
+        }
+        s_incl[warp][lane] = incl;
+        const uint32_t total = __shfl_sync(0xffffffffu, incl, 31);
+        const uint64_t o0 = offset[grp*32];   // the group's first photon
+        __syncwarp();
+        for (uint32_t ph = (uint32_t)lane; ph < total; ph += 32) {
+            // the lanes whose inclusive count is <= ph are a prefix: its length
+            // is the bunch of photon ph
+            uint32_t at = 0;
+#pragma unroll
+            for (uint32_t step = 16; step > 0; step >>= 1)
+                if (s_incl[warp][at + step - 1] <= ph) at += step;
+            const double* sv = s_val[warp][at];
+            const uint64_t o = o0 + ph;
+            sx[o] = sv[0]; sy[o] = sv[1]; sz[o] = sv[2];
+            dx[o] = sv[3]; dy[o] = sv[4]; dz[o] = sv[5];
+            wl[o] = sv[6];
+            if (out_id) out_id[o] = s_id[warp][at];
+        }
+        __syncwarp();   // the group's values are rewritten by the next one
     }
 }
 
@@ -184,9 +220,10 @@ cudaError_t launch_corsika_expand(const float* bunches, uint64_t n, const int32_
     const uint32_t* count = static_cast<const uint32_t*>(scratch);
     const uint64_t* offset = reinterpret_cast<const uint64_t*>(
         static_cast<const char*>(scratch) + ((n*4 + 255) & ~uint64_t(255)));
-    corsika_expand_kernel<<<grid, 256, 0, s>>>(bunches, n, count, offset, ids, planes[0], planes[1],
-                                               planes[2], planes[3], planes[4], planes[5],
-                                               planes[6], out_id);
+    corsika_expand_kernel<<<grid, 32*kExpandWarps, 0, s>>>(bunches, n, count, offset, ids,
+                                                          planes[0], planes[1], planes[2],
+                                                          planes[3], planes[4], planes[5],
+                                                          planes[6], out_id);
     return cudaGetLastError();
 }
 
