@@ -136,10 +136,10 @@ def test_forward_pass_matches_oracle(sg):
     assert fro < 1e-3 and worst < 1e-2, (fro, worst)
 
 
-@pytest.mark.parametrize("tiles", [1, 5, 148, 149, 445])
+@pytest.mark.parametrize("tiles", [1, 5, 148, 149, 445, 4096])
 def test_fused_forward_equals_the_layered_one(sg, tiles):
-    """The one-launch forward (activations on chip, several tiles per CTA
-    beyond 148 tiles, the last CTAs with one tile fewer) gives the layered
+    """The one-launch forward (activations on chip, two tiles in flight per
+    CTA: a CTA with one tile, an odd number or 28 tiles) gives the layered
     form's bits: same encoding, K order, bias, SiLU and BF16 rounding."""
     import torch
     flat = load_golden("light_field_small")[0]
