@@ -367,6 +367,15 @@ int mlgpu_propagate_host(
     const mlgpu_rng* rng,
     mlgpu_results* results);
 
+/* Page-locked host memory for the buffers of the host-buffer calls
+ * (cudaMallocHost / cudaFreeHost), for callers that do not link the CUDA
+ * runtime themselves, such as the reference-side C++ shim: with every
+ * buffer of mlgpu_propagate_host in such memory the batch moves in pieces
+ * whose copies overlap the tracing.  *ptr is NULL after a failure and for
+ * 0 bytes; freeing NULL does nothing.                                    */
+int mlgpu_host_alloc(uint64_t bytes, void** ptr);
+int mlgpu_host_free(void* ptr);
+
 /* Propagation and arrival binning in one host-buffer call: the pair a
  * merlict application runs per event, propagate_photons_in_frame_with_config
  * then Sensors::assign_photons (merlict/Photons.cpp:9-22,

@@ -151,7 +151,7 @@ def check(status: int) -> None:
 EXPORTED = (
     "mlgpu_abi_version", "mlgpu_last_error", "mlgpu_scene_create", "mlgpu_scene_destroy",
     "mlgpu_propagate", "mlgpu_scene_sync_errors", "mlgpu_propagate_host",
-    "mlgpu_propagate_and_bin_host",
+    "mlgpu_propagate_and_bin_host", "mlgpu_host_alloc", "mlgpu_host_free",
     "mlgpu_bin_arrivals", "mlgpu_bin_arrivals_noalloc", "mlgpu_scene_kernel_launches",
     "mlgpu_scene_wavefront_stats", "mlgpu_probe_fp64_rate",
     "mlgpu_scene_set_profiling", "mlgpu_scene_kernel_times", "mlgpu_scene_autotune",

@@ -868,6 +868,25 @@ extern "C" {
 
 int mlgpu_abi_version(void) { return MLGPU_ABI_VERSION; }
 
+int mlgpu_host_alloc(uint64_t bytes, void** ptr) {
+    if (!ptr) return fail(MLGPU_ERR_INVALID_ARGUMENT, "NULL argument");
+    *ptr = nullptr;
+    if (bytes == 0) return MLGPU_OK;
+    const cudaError_t e = cudaMallocHost(ptr, bytes);
+    if (e != cudaSuccess) {
+        *ptr = nullptr;
+        return cuda_fail(e, "cudaMallocHost");
+    }
+    return MLGPU_OK;
+}
+
+int mlgpu_host_free(void* ptr) {
+    if (!ptr) return MLGPU_OK;
+    const cudaError_t e = cudaFreeHost(ptr);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaFreeHost");
+    return MLGPU_OK;
+}
+
 int mlgpu_last_error(char* buffer, size_t buffer_size) {
     if (!buffer || buffer_size == 0) return (int)g_last_error.size();
     std::snprintf(buffer, buffer_size, "%s", g_last_error.c_str());

@@ -29,7 +29,29 @@ namespace {
 struct DeviceScene {
     FlatScene flat;
     mlgpu_scene* scene = nullptr;
+    // page-locked staging of the host-buffer calls (grown as needed, kept
+    // for the scene's lifetime), and the lock that serialises calls on the
+    // scene (the engine's scene is not re-entrant)
+    void* pinned = nullptr;
+    size_t pinned_bytes = 0;
+    std::mutex call;
 };
+
+// `bytes` of the scene's page-locked staging (its contents are not kept).
+void* staging(DeviceScene* ds, size_t bytes) {
+    if (bytes > ds->pinned_bytes) {
+        void* old = ds->pinned;
+        ds->pinned = nullptr;
+        ds->pinned_bytes = 0;
+        throw_on_error(mlgpu_host_free(old));
+        const size_t grown = bytes + bytes/4;
+        void* p = nullptr;
+        throw_on_error(mlgpu_host_alloc(grown, &p));
+        ds->pinned = p;
+        ds->pinned_bytes = grown;
+    }
+    return ds->pinned;
+}
 
 std::mutex cache_mutex;
 std::map<std::pair<const ml::Frame*, const ml::sensor::Sensors*>, DeviceScene*> cache;
@@ -57,31 +79,41 @@ DeviceScene* scene_for(const ml::Frame* world, const ml::sensor::Sensors* sensor
     return ds;
 }
 
+// The photons' planes, written into `d` (7 n doubles: support x, y, z,
+// direction x, y, z, wavelength) and `id` (n ints).
+mlgpu_photons fill_planes(const std::vector<ml::Photon>& photons, double* d, int32_t* id) {
+    const size_t n = photons.size();
+    double* sx = d; double* sy = d + n; double* sz = d + 2*n;
+    double* dx = d + 3*n; double* dy = d + 4*n; double* dz = d + 5*n;
+    double* wavelength = d + 6*n;
+    for (size_t i = 0; i < n; i++) {
+        const ml::Photon& p = photons[i];
+        if (p.num_interactions() != 1)
+            throw std::invalid_argument(
+                "merlict_b200: photons must be fresh (only their production "
+                "interaction) when handed to the GPU engine.");
+        sx[i] = p.support().x; sy[i] = p.support().y; sz[i] = p.support().z;
+        dx[i] = p.direction().x; dy[i] = p.direction().y; dz[i] = p.direction().z;
+        wavelength[i] = p.wavelength;
+        id[i] = p.simulation_truth_id;
+    }
+    mlgpu_photons view;
+    std::memset(&view, 0, sizeof(view));
+    view.dtype = MLGPU_F64;
+    view.support_x = sx; view.support_y = sy; view.support_z = sz;
+    view.direction_x = dx; view.direction_y = dy; view.direction_z = dz;
+    view.wavelength = wavelength;
+    view.simulation_truth_id = id;
+    return view;
+}
+
 struct PhotonPlanes {
-    std::vector<double> sx, sy, sz, dx, dy, dz, wavelength;
+    std::vector<double> planes;
     std::vector<int32_t> id;
     mlgpu_photons view;
-    explicit PhotonPlanes(const std::vector<ml::Photon>& photons) {
-        const size_t n = photons.size();
-        sx.resize(n); sy.resize(n); sz.resize(n);
-        dx.resize(n); dy.resize(n); dz.resize(n);
-        wavelength.resize(n); id.resize(n);
-        for (size_t i = 0; i < n; i++) {
-            const ml::Photon& p = photons[i];
-            if (p.num_interactions() != 1)
-                throw std::invalid_argument(
-                    "merlict_b200: photons must be fresh (only their production "
-                    "interaction) when handed to the GPU engine.");
-            sx[i] = p.support().x; sy[i] = p.support().y; sz[i] = p.support().z;
-            dx[i] = p.direction().x; dy[i] = p.direction().y; dz[i] = p.direction().z;
-            wavelength[i] = p.wavelength;
-            id[i] = p.simulation_truth_id;
-        }
-        view.dtype = MLGPU_F64;
-        view.support_x = sx.data(); view.support_y = sy.data(); view.support_z = sz.data();
-        view.direction_x = dx.data(); view.direction_y = dy.data(); view.direction_z = dz.data();
-        view.wavelength = wavelength.data();
-        view.simulation_truth_id = id.data();
+    explicit PhotonPlanes(const std::vector<ml::Photon>& photons)
+        : planes(7*photons.size()), id(photons.size()) {
+        view = fill_planes(photons, planes.data(), id.data());
     }
 };
 
@@ -113,6 +145,7 @@ void propagate_photons_in_frame_with_config(
 ) {
     if (photons->empty()) return;
     DeviceScene* ds = scene_for(world, nullptr);
+    std::lock_guard<std::mutex> lock(ds->call);
     PhotonPlanes planes(*photons);
     const mlgpu_settings st = settings_for(ds, world, settings);
     const mlgpu_rng rng = rng_for(prng);
@@ -154,19 +187,31 @@ void propagate_and_assign_photons(
 ) {
     if (photons->empty()) return;
     DeviceScene* ds = scene_for(world, sensors);
-    PhotonPlanes planes(*photons);
+    std::lock_guard<std::mutex> lock(ds->call);
+    const size_t n = photons->size();
+    // inputs and results in page-locked staging, so that the engine moves
+    // the batch in pieces whose copies overlap the tracing: 7 n doubles of
+    // planes, 5 n doubles of results (x, y, t, theta x, theta y), n ids, n
+    // sensors
+    double* mem = static_cast<double*>(staging(ds, n*(12*sizeof(double) + 2*sizeof(int32_t))));
+    double* out = mem + 7*n;
+    int32_t* ids = reinterpret_cast<int32_t*>(out + 5*n);
+    int32_t* sensor = ids + n;
+    const mlgpu_photons view = fill_planes(*photons, mem, ids);
     const mlgpu_settings st = settings_for(ds, world, settings);
     const mlgpu_rng rng = rng_for(prng);
-    const size_t n = photons->size();
-    std::vector<int32_t> sensor(n);
-    std::vector<double> x(n), y(n), t(n), tx(n), ty(n);
+    const double* x = out;
+    const double* y = out + n;
+    const double* t = out + 2*n;
+    const double* tx = out + 3*n;
+    const double* ty = out + 4*n;
     mlgpu_results res;
     std::memset(&res, 0, sizeof(res));
     res.dtype = MLGPU_F64;
-    res.sensor = sensor.data();
-    res.x = x.data(); res.y = y.data(); res.time = t.data();
-    res.theta_x = tx.data(); res.theta_y = ty.data();
-    throw_on_error(mlgpu_propagate_host(ds->scene, &planes.view, n, &st, &rng, &res));
+    res.sensor = sensor;
+    res.x = out; res.y = out + n; res.time = out + 2*n;
+    res.theta_x = out + 3*n; res.theta_y = out + 4*n;
+    throw_on_error(mlgpu_propagate_host(ds->scene, &view, n, &st, &rng, &res));
     // Sensors::assign_photons order: photon by photon (Sensors.cpp:31-37).
     for (size_t i = 0; i < n; i++) {
         if (sensor[i] < 0) continue;

@@ -84,6 +84,25 @@ def test_drop_in_fast_path_writes_merlicts_arrivals(scenes, name):
         assert np.array_equal(got[k][hit], want[k][hit]), k
 
 
+def test_drop_in_fast_path_above_one_ray_pool(scenes):
+    """propagate_and_assign_photons stages its inputs and results in
+    page-locked memory, so a batch of more than one ray pool (2^21 photons)
+    is fed to one propagation piece by piece: the arrivals are still
+    merlict's, photon for photon."""
+    _, _, source, max_int = SCENES["light_field_telescope"]
+    sc = scenes["light_field_telescope"]
+    ph = P.downward_disc_source(2_200_000, 33, *source)
+    status, got, seed = sc.shim_propagate(ph, max_int, 2, mt_seed=11)
+    assert status == 0, sc.last_error()
+    status, want, _ = sc.propagate(ph, max_int, O.REPLAY_PHILOX, seed=seed, threads=THREADS)
+    assert status == 0
+    assert np.array_equal(got["sensor"], want["sensor"])
+    hit = want["sensor"] >= 0
+    assert hit.mean() > 0.2
+    for k in ARRIVAL[1:]:
+        assert np.array_equal(got[k][hit], want[k][hit]), k
+
+
 def test_drop_in_raises_merlicts_exception_type(scenes):
     """A wavelength outside a property table: merlict's Func1 throws
     std::out_of_range (function/Limits.cpp:37-46); the drop-in raises the
