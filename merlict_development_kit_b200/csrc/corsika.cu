@@ -121,12 +121,13 @@ scan_add_kernel(uint64_t* __restrict__ out, uint64_t n, const uint64_t* __restri
 }
 
 // The expansion, a warp per 32 consecutive bunches: each lane computes its
-// bunch's photon (merlict's arithmetic) into shared memory, then the warp
-// writes the group's photons as one contiguous run -- lane p of a round
-// writes photon p, found in the bunch whose inclusive count first exceeds p
-// (a five-step binary search over the group's counts) -- so that every
-// store instruction covers consecutive addresses.
+// bunch's photon (merlict's arithmetic) into shared memory as four 16-byte
+// words and marks the group's photons it owns in an owner list, then the
+// warp writes the group's photons as one contiguous run -- lane p of a
+// round writes photon p, reading its bunch from the owner list -- so that
+// every store instruction covers consecutive addresses.
 constexpr int kExpandWarps = 8;
+constexpr int kGroupPhotons = 32*17;   // at most 17 photons per bunch
 
 __global__ void __launch_bounds__(32*kExpandWarps)
 corsika_expand_kernel(const float* __restrict__ b, uint64_t n, const uint32_t* __restrict__ count,
@@ -134,15 +135,23 @@ corsika_expand_kernel(const float* __restrict__ b, uint64_t n, const uint32_t* _
                       double* __restrict__ sx, double* __restrict__ sy, double* __restrict__ sz,
                       double* __restrict__ dx, double* __restrict__ dy, double* __restrict__ dz,
                       double* __restrict__ wl, int32_t* __restrict__ out_id) {
-    __shared__ double s_val[kExpandWarps][32][7];
-    __shared__ int32_t s_id[kExpandWarps][32];
-    __shared__ uint32_t s_incl[kExpandWarps][32];
+    // per bunch: (support x, y), (support z, direction x), (direction y, z),
+    // (wavelength, id bits)
+    __shared__ double2 s_val[kExpandWarps][32][4];
+    __shared__ uint8_t s_owner[kExpandWarps][kGroupPhotons];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const uint64_t groups = (n + 31)/32;
     for (uint64_t grp = (uint64_t)blockIdx.x*kExpandWarps + warp; grp < groups;
          grp += (uint64_t)gridDim.x*kExpandWarps) {
         const uint64_t i = grp*32 + (uint64_t)lane;
         const uint32_t c = i < n ? count[i] : 0u;
+        uint32_t incl = c;
+#pragma unroll
+        for (int d = 1; d < 32; d <<= 1) {
+            const uint32_t y = __shfl_up_sync(0xffffffffu, incl, d);
+            if (lane >= d) incl += y;
+        }
+        const uint32_t total = __shfl_sync(0xffffffffu, incl, 31);
         if (c != 0) {
             const float* r = b + 8*i;
             // direction_of_motion, PhotonFactory.cpp:113-118
@@ -157,35 +166,25 @@ corsika_expand_kernel(const float* __restrict__ b, uint64_t n, const uint32_t* _
             const double t = (double)__ldg(r + 4)*1e-9;
             const double par = t*299792458.0 + 1e3;
             const double gx = (double)__ldg(r + 0)*1e-2, gy = (double)__ldg(r + 1)*1e-2, gz = 0.0;
-            double* sv = s_val[warp][lane];
-            sv[0] = gx + nx*par; sv[1] = gy + ny*par; sv[2] = gz + nz*par;
-            sv[3] = cx; sv[4] = cy; sv[5] = cz;
-            sv[6] = fabs((double)__ldg(r + 7)*1e-9);
-            s_id[warp][lane] = ids ? __ldg(ids + i) : (int32_t)i;
+            const int32_t id = ids ? __ldg(ids + i) : (int32_t)i;
+            double2* sv = s_val[warp][lane];
+            sv[0] = make_double2(gx + nx*par, gy + ny*par);
+            sv[1] = make_double2(gz + nz*par, cx);
+            sv[2] = make_double2(cy, cz);
+            sv[3] = make_double2(fabs((double)__ldg(r + 7)*1e-9),
+                                 __longlong_as_double((long long)(uint32_t)id));
+            for (uint32_t k = incl - c; k < incl; k++) s_owner[warp][k] = (uint8_t)lane;
         }
-        uint32_t incl = c;
-#pragma unroll
-        for (int d = 1; d < 32; d <<= 1) {
-            const uint32_t y = __shfl_up_sync(0xffffffffu, incl, d);
-            if (lane >= d) incl += y;
-        }
-        s_incl[warp][lane] = incl;
-        const uint32_t total = __shfl_sync(0xffffffffu, incl, 31);
         const uint64_t o0 = offset[grp*32];   // the group's first photon
         __syncwarp();
         for (uint32_t ph = (uint32_t)lane; ph < total; ph += 32) {
-            // the lanes whose inclusive count is <= ph are a prefix: its length
-            // is the bunch of photon ph
-            uint32_t at = 0;
-#pragma unroll
-            for (uint32_t step = 16; step > 0; step >>= 1)
-                if (s_incl[warp][at + step - 1] <= ph) at += step;
-            const double* sv = s_val[warp][at];
+            const double2* sv = s_val[warp][s_owner[warp][ph]];
+            const double2 v0 = sv[0], v1 = sv[1], v2 = sv[2], v3 = sv[3];
             const uint64_t o = o0 + ph;
-            sx[o] = sv[0]; sy[o] = sv[1]; sz[o] = sv[2];
-            dx[o] = sv[3]; dy[o] = sv[4]; dz[o] = sv[5];
-            wl[o] = sv[6];
-            if (out_id) out_id[o] = s_id[warp][at];
+            sx[o] = v0.x; sy[o] = v0.y; sz[o] = v1.x;
+            dx[o] = v1.y; dy[o] = v2.x; dz[o] = v2.y;
+            wl[o] = v3.x;
+            if (out_id) out_id[o] = (int32_t)(uint32_t)__double_as_longlong(v3.y);
         }
         __syncwarp();   // the group's values are rewritten by the next one
     }
